@@ -1,0 +1,118 @@
+/* C ABI of libspgrid_gpu_solver.so — the B200 narrow-band SPGrid elasticity
+ * solver.
+ *
+ * fem_solve() is the drop-in entry: same symbol, same arguments and same
+ * ownership rules as the reference CPU solver library (libSPGridCPUSolver.so),
+ * so a caller linked against that library can link against this one instead.
+ * The sgs_* functions are additive: a session API that keeps the problem on the
+ * GPU between calls, used by the Python layer, the tests and the benchmark.
+ */
+#ifndef SPGRID_FEM_H
+#define SPGRID_FEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SGS_API __attribute__((visibility("default")))
+
+/* Error codes (FEMOutputs.error_code and sgs_* return values). */
+#define SGS_OK 0
+#define SGS_ERR_INPUT 1      /* invalid arguments or parameters */
+#define SGS_ERR_UNSUPPORTED 2 /* mode the solver does not implement (use_density_only = false) */
+#define SGS_ERR_MG_LEVEL 3   /* mg_level = 2 */
+#define SGS_ERR_GRID 4       /* blocks outside the grid, unaligned blocks, non-finite values */
+#define SGS_ERR_ACTIVATION 5 /* a material cell lacks its +1 neighbour blocks */
+#define SGS_ERR_PADDING 6    /* blocks too close to the grid border for the hierarchy */
+#define SGS_ERR_BREAKDOWN 8  /* CG breakdown (s.q <= 0), non-finite residual, singular bottom */
+#define SGS_ERR_WIRE 9       /* malformed input blob */
+#define SGS_ERR_CUDA 10      /* CUDA runtime failure */
+#define SGS_ERR_INTERNAL 11
+
+/* Replaces: extern "C" void fem_solve(void *input, void *output)
+ *   (reference topo_opt/fem_interface.h:11, solver/SPGrid_CPU_Solver.cpp:26).
+ * input : serialized FEMInputs blob; its first 8 bytes hold the total length
+ *         (topo_opt/serialization.h:318-329).
+ * output: really a void**; receives a serialized FEMOutputs blob allocated with
+ *         new char[] that the caller releases with delete[] (or fem_solve_free)
+ *         (fem_interface.h:414-441, 477).
+ * Never aborts or throws: failures come back as success = 0 with error_code and
+ * info set.  Extra knobs (all optional) in FEMInputs.extra_ints:
+ *   "sgs_precision"  0 = reference arithmetic (float-rounded CG updates and
+ *                        V-cycle casts, the default), 1 = FP64, 2 = FP32 V-cycle
+ *                        with FP64 outer PCG;
+ *   "sgs_honor_max_iterations"  1 = stop at krylov.max_iterations instead of 500. */
+SGS_API void fem_solve(void* input, void* output);
+
+/* Release an output blob from fem_solve (callers that cannot call delete[]). */
+SGS_API void fem_solve_free(void* blob);
+
+/* ---- session API ---------------------------------------------------------- */
+typedef struct sgs_session sgs_session;
+
+typedef struct {
+  int32_t iterations;
+  int32_t levels;
+  double initial_residual; /* L-inf of the zero-guess residual */
+  double final_residual;   /* L-inf of the last CG residual */
+  double setup_seconds;
+  double solve_seconds;    /* PCG only, host wall clock */
+  int64_t launches_per_iteration;
+  int64_t dof;             /* 3 * nodes of the active level-0 blocks */
+  int64_t bottom_unknowns;
+} sgs_stats;
+
+/* Build a session from an FEMInputs blob.  precision: 0 reference, 1 fp64, 2 mixed,
+ * or SGS_HOST_SETUP_ONLY to build only the host-side hierarchy (no GPU needed;
+ * the inspection calls below work, the solve calls return SGS_ERR_INPUT).
+ * Returns 0 and *out, or an error code with a message in err. */
+#define SGS_HOST_SETUP_ONLY 3
+SGS_API int sgs_create(const void* input_blob, int precision, sgs_session** out, char* err, int errlen);
+SGS_API void sgs_destroy(sgs_session* s);
+SGS_API const char* sgs_last_error(sgs_session* s);
+
+/* Run the PCG.  tolerance <= 0 keeps the blob's krylov.tolerance; max_iterations
+ * <= 0 keeps 500.  Relative L-inf stopping rule (SPGrid_CPU_Solver.cpp:320-326). */
+SGS_API int sgs_solve(sgs_session* s, double tolerance, int max_iterations, sgs_stats* stats);
+SGS_API int sgs_residual_history(sgs_session* s, double* out, int cap);
+
+/* Displacements per input block: out[nblocks][64][4] = (u_x, u_y, u_z, |r|_inf),
+ * input block order and in-block index i*16 + j*4 + k (SPGrid_CPU_Solver.cpp:343-364). */
+SGS_API int sgs_displacements(sgs_session* s, double* out);
+
+/* SIMP compliance sensitivity after a solve (topo_opt/objective/minimal_compliance.cpp:86-146).
+ * density: [nblocks][64] cell densities of the input blocks.  Writes
+ * dc[nblocks][64] = p rho^(p-1) (1 - Emin) u_e^T K0 u_e and, when non-null,
+ * element_energy[nblocks][64] = u_e^T K0 u_e (K0 with the material mu, lambda; no dx).
+ * Returns the objective sum u_e^T K0 u_e (Emin + rho^p (1 - Emin)). */
+SGS_API double sgs_sensitivity(sgs_session* s, const double* density, double* dc, double* element_energy);
+
+/* ---- inspection and unit operators (tests) ------------------------------ */
+SGS_API int sgs_level_count(sgs_session* s);
+/* Active blocks of a level in SPGrid page order; coords may be null. */
+SGS_API int sgs_level_blocks(sgs_session* s, int level, int32_t* coords);
+SGS_API int sgs_level_flags(sgs_session* s, int level, uint32_t* flags);
+SGS_API int sgs_boundary_blocks(sgs_session* s, int level, int32_t* ordinals);
+
+/* Apply one operator to host arrays in the compact layout [3][nblocks*128]:
+ *  0 level-0 K*u            1 level-0 residual b - K u
+ *  2 one smoothing sweep    (arg bit0 forward, bit1 boundary band only)
+ *  3 restriction level -> level+1     4 prolongation level+1 -> level (accumulate)
+ *  5 stencil multiply       6 bottom solve (last level)   7 one V-cycle on level 0 */
+SGS_API int sgs_apply(sgs_session* s, int op, int level, int arg, const double* in, const double* in2, double* out);
+
+/* Galerkin stencils of a level as [nblocks*128][243] (row node, comp v; column
+ * neighbour (i,j,k)-1, comp w at ((i*3+j)*3+k)*9 + v*3 + w) and spoke masks. */
+SGS_API int sgs_level_stencils(sgs_session* s, int level, double* out, uint32_t* spokes);
+
+/* Decode a blob and encode it again with this library's codec (which = 0 for
+ * FEMInputs, 1 for FEMOutputs); *out receives a new[] blob for fem_solve_free.
+ * Lets callers check byte compatibility without a GPU. */
+SGS_API int sgs_codec_roundtrip(const void* blob, int which, void** out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

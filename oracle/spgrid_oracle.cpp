@@ -1369,8 +1369,9 @@ void oracle_get_material(void* h, double* mu, double* la) {
 //  1: level-0 residual       in=u, in2=b     out=b - dx*K u
 //  2: smoothing sweep        in=u, in2=b     out=u after one sweep; arg bit0 forward, bit1 boundary
 //  3: restriction            in=fine (level) out=coarse (level+1), then Dirichlet projection
-//  4: prolongation           in=coarse(level+1), in2=fine(level) out=fine + P coarse, then projection
-//  5: stencil multiply       in=u (level)    out=A u
+//  4: prolongation           in=coarse(level+1), in2=fine(level) out=fine + P coarse, then the
+//                            Dirichlet projection, the float cast (REF) and the null-space projection
+//  5: stencil multiply       in=u (level)    out=A u with Dirichlet components zeroed
 //  6: bottom solve           in=b (last level) out=u
 //  7: V-cycle                in=r (level 0)  out=z (projected), scratch restored
 int oracle_apply(void* h, int op, int level, int arg, const double* in, const double* in2, double* out) {
@@ -1388,9 +1389,12 @@ int oracle_apply(void* h, int op, int level, int arg, const double* in, const do
       return 0;
     case 4:
       if (level + 1 >= int(s.L.size())) return -1;
-      put3(s.L[level + 1], A, in); put3(l, C, in2); prolongate_level(l, s.L[level + 1], C, A); project(l, C); get3(l, C, out);
+      put3(s.L[level + 1], A, in); put3(l, C, in2); prolongate_level(l, s.L[level + 1], C, A); project(l, C);
+      if (s.P.mode == MODE_REF) cast3(l, C);
+      project_null(l, C);
+      get3(l, C, out);
       return 0;
-    case 5: put3(l, A, in); stencil_multiply(s, level, A, C); get3(l, C, out); return 0;
+    case 5: put3(l, A, in); stencil_multiply(s, level, A, C); project(l, C); get3(l, C, out); return 0;
     case 6: put3(l, B, in); bottom_solve(s, A, B); get3(l, A, out); return 0;
     case 7: put3(l, B, in); precondition(s, B, A); get3(l, A, out); return 0;
   }

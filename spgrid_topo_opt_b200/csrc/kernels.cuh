@@ -1,0 +1,353 @@
+// CUDA kernels of the narrow-band SPGrid elasticity MGPCG (sm_100a).
+//
+// Layout: a level holds nb active blocks of 4x4x8 nodes in SPGrid page order;
+// node slot e = x*32 + y*8 + z inside a block, global node index b*128 + e.
+// A 3-vector field is stored as three planes of N = nb*128 values ([3][N]).
+// Level 0 carries the per-cell stiffness scale E (cell = its min-corner node,
+// 0 = empty); the element matrix of a cell is E * (mu0*K_mu + lambda0*K_la).
+// Coarse levels carry 27-point Galerkin stencils in planes [243][N], entry
+// ((i*3+j)*3+k)*9 + v*3 + w = row (node, v), column (node + (i,j,k) - 1, w).
+#pragma once
+#include <cstdint>
+
+namespace sgs {
+
+constexpr uint32_t ACTIVE_NODE = 0x10, DIR_X = 0x20, DIR_Y = 0x40, DIR_Z = 0x80, BOUNDARY_NODE = 0x1000;
+
+// Combined element matrix Kc[I][J][v][w] = mu0*K_mu + lambda0*K_la (set per solve)
+__constant__ double c_Kc64[8 * 8 * 9];
+__constant__ float c_Kc32[8 * 8 * 9];
+
+template <typename T>
+__device__ __forceinline__ T kc(int idx);
+template <>
+__device__ __forceinline__ double kc<double>(int idx) { return c_Kc64[idx]; }
+template <>
+__device__ __forceinline__ float kc<float>(int idx) { return c_Kc32[idx]; }
+
+__device__ __forceinline__ double round_to_float(double v) { return double(float(v)); }
+
+// ---------------------------------------------------------------------------
+// Level-0 matrix-free operator on one block per CTA (128 threads, one node each)
+// OP_KU: out = dx*K*u, OP_RES: out = b - dx*K*u, OP_GS: colour-`color` Gauss-Seidel
+// update of u in place (solver/CPU_Kernels/SPGrid_Gauss_Seidel.h:876-1180).
+// ---------------------------------------------------------------------------
+enum { OP_KU = 0, OP_RES = 1, OP_GS = 2 };
+
+// halo geometry: nodes [-1,4]x[-1,4]x[-1,8] (6x6x10), cells [-1,3]x[-1,3]x[-1,7] (5x5x9)
+constexpr int HU = 360, HE = 225;
+
+template <typename T, int OP>
+__global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ block_list, int nblocks,
+                                                        const int* __restrict__ nbr, const T* __restrict__ E,
+                                                        const T* u, T* out_u, const T* __restrict__ b,
+                                                        T* __restrict__ out, const uint32_t* __restrict__ flags,
+                                                        long N, T dx, int color, int boundary_only) {
+  __shared__ T su[3][HU];
+  __shared__ T sE[HE];
+  __shared__ int snb[27];
+  const int bi = block_list ? block_list[blockIdx.x] : blockIdx.x;
+  if (bi >= 0 && threadIdx.x < 27) snb[threadIdx.x] = nbr[long(bi) * 27 + threadIdx.x];
+  __syncthreads();
+  // stage u halo
+  for (int h = threadIdx.x; h < HU; h += 128) {
+    const int sx = h / 60, sy = (h / 10) % 6, sz = h % 10;
+    const int lx = sx - 1, ly = sy - 1, lz = sz - 1;
+    const int dxb = lx < 0 ? 0 : (lx > 3 ? 2 : 1), dyb = ly < 0 ? 0 : (ly > 3 ? 2 : 1), dzb = lz < 0 ? 0 : (lz > 7 ? 2 : 1);
+    const int nb = snb[dxb * 9 + dyb * 3 + dzb];
+    T a = 0, bb = 0, c = 0;
+    if (nb >= 0) {
+      const long idx = long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7);
+      a = u[idx];
+      bb = u[idx + N];
+      c = u[idx + 2 * N];
+    }
+    su[0][h] = a;
+    su[1][h] = bb;
+    su[2][h] = c;
+  }
+  for (int h = threadIdx.x; h < HE; h += 128) {
+    const int sx = h / 45, sy = (h / 9) % 5, sz = h % 9;
+    const int lx = sx - 1, ly = sy - 1, lz = sz - 1;
+    const int dxb = lx < 0 ? 0 : 1, dyb = ly < 0 ? 0 : 1, dzb = lz < 0 ? 0 : 1;
+    const int nb = snb[dxb * 9 + dyb * 3 + dzb];
+    sE[h] = nb >= 0 ? E[long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7)] : T(0);
+  }
+  __syncthreads();
+  const int e = threadIdx.x;
+  const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
+  const long gidx = long(bi) * 128 + e;
+  uint32_t fl = 0;
+  if (OP == OP_GS) {
+    if (((x & 1) << 2 | (y & 1) << 1 | (z & 1)) != color) return;
+    fl = flags[gidx];
+    const bool act = (fl & ACTIVE_NODE) && (!boundary_only || (fl & BOUNDARY_NODE));
+    if (!act) {
+      // inactive nodes keep u; Dirichlet components are still cleared
+      if (fl & DIR_X) out_u[gidx] = T(0);
+      if (fl & DIR_Y) out_u[gidx + N] = T(0);
+      if (fl & DIR_Z) out_u[gidx + 2 * N] = T(0);
+      return;
+    }
+  }
+  T f0 = 0, f1 = 0, f2 = 0;
+  T d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0;
+#pragma unroll
+  for (int I = 0; I < 8; ++I) {
+    const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
+    const int cx = x - Ix, cy = y - Iy, cz = z - Iz;  // cell, in [-1,3]x[-1,3]x[-1,7]
+    const T Ec = sE[((cx + 1) * 5 + (cy + 1)) * 9 + (cz + 1)];
+    T g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+    for (int J = 0; J < 8; ++J) {
+      const int nx = cx + (J >> 2) + 1, ny = cy + ((J >> 1) & 1) + 1, nz = cz + (J & 1) + 1;
+      const int h = (nx * 6 + ny) * 10 + nz;
+      const T ux = su[0][h], uy = su[1][h], uz = su[2][h];
+      const int k = (I * 8 + J) * 9;
+      g0 += kc<T>(k + 0) * ux + kc<T>(k + 1) * uy + kc<T>(k + 2) * uz;
+      g1 += kc<T>(k + 3) * ux + kc<T>(k + 4) * uy + kc<T>(k + 5) * uz;
+      g2 += kc<T>(k + 6) * ux + kc<T>(k + 7) * uy + kc<T>(k + 8) * uz;
+      if (OP == OP_GS && J == I) {
+        d0 += Ec * kc<T>(k + 0);
+        d1 += Ec * kc<T>(k + 4);
+        d2 += Ec * kc<T>(k + 8);
+        d3 += Ec * kc<T>(k + 1);
+        d4 += Ec * kc<T>(k + 2);
+        d5 += Ec * kc<T>(k + 5);
+      }
+    }
+    f0 += Ec * g0;
+    f1 += Ec * g1;
+    f2 += Ec * g2;
+  }
+  f0 *= dx;
+  f1 *= dx;
+  f2 *= dx;
+  if (OP == OP_KU) {
+    out[gidx] = f0;
+    out[gidx + N] = f1;
+    out[gidx + 2 * N] = f2;
+    return;
+  }
+  if (OP == OP_RES) {
+    out[gidx] = b[gidx] - f0;
+    out[gidx + N] = b[gidx + N] - f1;
+    out[gidx + 2 * N] = b[gidx + 2 * N] - f2;
+    return;
+  }
+  // Gauss-Seidel update: u += D^{-1} (b - K u) with Dirichlet rows replaced by identity
+  const T r0 = b[gidx] - f0, r1 = b[gidx + N] - f1, r2 = b[gidx + 2 * N] - f2;
+  d0 *= dx; d1 *= dx; d2 *= dx; d3 *= dx; d4 *= dx; d5 *= dx;
+  const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
+  if (fx) { d0 = 1; d3 = 0; d4 = 0; }
+  if (fy) { d1 = 1; d3 = 0; d5 = 0; }
+  if (fz) { d2 = 1; d4 = 0; d5 = 0; }
+  const T m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
+  const T m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
+  const T inv = T(1) / (d0 * m11 + d3 * m12 + d4 * m13);
+  T a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
+  if (fx) { a0 = 0; a3 = 0; a4 = 0; }
+  if (fy) { a1 = 0; a3 = 0; a5 = 0; }
+  if (fz) { a2 = 0; a4 = 0; a5 = 0; }
+  const int hc = ((x + 1) * 6 + (y + 1)) * 10 + (z + 1);
+  T u0 = su[0][hc] + r0 * a0 + r1 * a3 + r2 * a4;
+  T u1 = su[1][hc] + r0 * a3 + r1 * a1 + r2 * a5;
+  T u2 = su[2][hc] + r0 * a4 + r1 * a5 + r2 * a2;
+  if (fx) u0 = 0;
+  if (fy) u1 = 0;
+  if (fz) u2 = 0;
+  out_u[gidx] = u0;
+  out_u[gidx + N] = u1;
+  out_u[gidx + 2 * N] = u2;
+}
+
+// ---------------------------------------------------------------------------
+// Coarse-level stencil operators (solver/MG/SPGrid_Stencil_Multiply.h:15-280)
+// ---------------------------------------------------------------------------
+struct GridView {
+  const int* bgrid;  // dense block grid -> active block index or -1
+  int gx, gy, gz;
+  __device__ __forceinline__ long node(int x, int y, int z) const {
+    if (x < 0 || y < 0 || z < 0) return -1;
+    const int bx = x >> 2, by = y >> 2, bz = z >> 3;
+    if (bx >= gx || by >= gy || bz >= gz) return -1;
+    const int b = bgrid[(long(bx) * gy + by) * gz + bz];
+    return b < 0 ? -1 : long(b) * 128 + ((x & 3) << 5) + ((y & 3) << 3) + (z & 7);
+  }
+};
+
+enum { SOP_MUL = 0, SOP_RES = 1, SOP_GS = 2 };
+
+// One thread per node; GS updates only colour-`color` nodes.  Reads neighbours
+// through the block grid.  Results with a Dirichlet flag are zeroed (Project).
+template <typename T, int OP>
+__global__ void stencil_op_kernel(const int* __restrict__ block_list, int nblocks, const int* __restrict__ coords,
+                                  GridView g, const T* __restrict__ A, const uint32_t* __restrict__ flags,
+                                  const T* u, T* out_u, const T* __restrict__ b, T* __restrict__ out, long N,
+                                  int color, int boundary_only, int round_out) {
+  const int per = (OP == SOP_GS) ? 16 : 128;
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long blk = t / per;
+  if (blk >= nblocks) return;
+  const int bi = block_list ? block_list[blk] : int(blk);
+  int e;
+  if (OP == SOP_GS) {
+    const int q = int(t % per);  // 16 nodes of the colour: (x/2, y/2, z/2) in 2x2x4
+    const int px = (color >> 2) & 1, py = (color >> 1) & 1, pz = color & 1;
+    e = (((q >> 3) * 2 + px) << 5) + ((((q >> 2) & 1) * 2 + py) << 3) + ((q & 3) * 2 + pz);
+  } else {
+    e = int(t % per);
+  }
+  const long gidx = long(bi) * 128 + e;
+  const uint32_t fl = flags[gidx];
+  if (OP == SOP_GS) {
+    if (!(fl & ACTIVE_NODE)) return;
+    if (boundary_only && !(fl & BOUNDARY_NODE)) return;
+  }
+  const int x = coords[3 * bi] + (e >> 5), y = coords[3 * bi + 1] + ((e >> 3) & 3), z = coords[3 * bi + 2] + (e & 7);
+  T f0 = 0, f1 = 0, f2 = 0;
+#pragma unroll 3
+  for (int q = 0; q < 27; ++q) {
+    const long n = g.node(x + q / 9 - 1, y + (q / 3) % 3 - 1, z + q % 3 - 1);
+    if (n < 0) continue;
+    const T ux = u[n], uy = u[n + N], uz = u[n + 2 * N];
+    const T* a = A + long(q) * 9 * N + gidx;
+    f0 += a[0] * ux + a[N] * uy + a[2 * N] * uz;
+    f1 += a[3 * N] * ux + a[4 * N] * uy + a[5 * N] * uz;
+    f2 += a[6 * N] * ux + a[7 * N] * uy + a[8 * N] * uz;
+  }
+  if (OP == SOP_MUL) {
+    out[gidx] = (fl & DIR_X) ? T(0) : f0;
+    out[gidx + N] = (fl & DIR_Y) ? T(0) : f1;
+    out[gidx + 2 * N] = (fl & DIR_Z) ? T(0) : f2;
+    return;
+  }
+  const T r0 = b[gidx] - f0, r1 = b[gidx + N] - f1, r2 = b[gidx + 2 * N] - f2;
+  if (OP == SOP_RES) {
+    T o0 = (fl & DIR_X) ? T(0) : r0, o1 = (fl & DIR_Y) ? T(0) : r1, o2 = (fl & DIR_Z) ? T(0) : r2;
+    if (round_out) { o0 = T(round_to_float(o0)); o1 = T(round_to_float(o1)); o2 = T(round_to_float(o2)); }
+    out[gidx] = o0;
+    out[gidx + N] = o1;
+    out[gidx + 2 * N] = o2;
+    return;
+  }
+  const T* c = A + long(13) * 9 * N + gidx;
+  T d0 = c[0], d1 = c[4 * N], d2 = c[8 * N], d3 = c[N], d4 = c[2 * N], d5 = c[5 * N];
+  const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
+  if (fx) { d0 = 1; d3 = 0; d4 = 0; }
+  if (fy) { d1 = 1; d3 = 0; d5 = 0; }
+  if (fz) { d2 = 1; d4 = 0; d5 = 0; }
+  const T m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
+  const T m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
+  const T inv = T(1) / (d0 * m11 + d3 * m12 + d4 * m13);
+  T a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
+  if (fx) { a0 = 0; a3 = 0; a4 = 0; }
+  if (fy) { a1 = 0; a3 = 0; a5 = 0; }
+  if (fz) { a2 = 0; a4 = 0; a5 = 0; }
+  T u0 = u[gidx] + (a0 * r0 + a3 * r1 + a4 * r2);
+  T u1 = u[gidx + N] + (a3 * r0 + a1 * r1 + a5 * r2);
+  T u2 = u[gidx + 2 * N] + (a4 * r0 + a5 * r1 + a2 * r2);
+  if (fx) u0 = 0;
+  if (fy) u1 = 0;
+  if (fz) u2 = 0;
+  out_u[gidx] = u0;
+  out_u[gidx + N] = u1;
+  out_u[gidx + 2 * N] = u2;
+}
+
+// ---------------------------------------------------------------------------
+// Transfers (solver/MG/Restriction.h:52-88, solver/MG/Prolongation.h:151-193)
+// ---------------------------------------------------------------------------
+// coarse(c) = sum_{d in {-1,0,1}^3} w(d) fine(2c - (4,4,8) + d), w = prod (1/2,1,1/2);
+// Dirichlet components zeroed afterwards.
+template <typename T>
+__global__ void restrict_kernel(int nb, const int* __restrict__ coords, const uint32_t* __restrict__ cflags,
+                                GridView fine, const T* __restrict__ fin, long Nf, T* __restrict__ cout, long Nc) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nb) * 128) return;
+  const int bi = int(t >> 7), e = int(t & 127);
+  const int x = coords[3 * bi] + (e >> 5), y = coords[3 * bi + 1] + ((e >> 3) & 3), z = coords[3 * bi + 2] + (e & 7);
+  const int fx = 2 * x - 4, fy = 2 * y - 4, fz = 2 * z - 8;
+  T v0 = 0, v1 = 0, v2 = 0;
+  for (int q = 0; q < 27; ++q) {
+    const int i = q / 9, j = (q / 3) % 3, k = q % 3;
+    const long n = fine.node(fx + i - 1, fy + j - 1, fz + k - 1);
+    if (n < 0) continue;
+    const T w = T((i == 1 ? 1.0 : 0.5) * (j == 1 ? 1.0 : 0.5) * (k == 1 ? 1.0 : 0.5));
+    v0 += w * fin[n];
+    v1 += w * fin[n + Nf];
+    v2 += w * fin[n + 2 * Nf];
+  }
+  const uint32_t fl = cflags[t];
+  cout[t] = (fl & DIR_X) ? T(0) : v0;
+  cout[t + Nc] = (fl & DIR_Y) ? T(0) : v1;
+  cout[t + 2 * Nc] = (fl & DIR_Z) ? T(0) : v2;
+}
+
+// fine(f) += sum of trilinear weights * coarse(((f + (4,4,8)) >> 1) + {0,1}^3); then
+// Project (Dirichlet), optional float rounding, Project_Null_Space (inactive nodes),
+// as Run_VCycle does after Prolongate (solver/MG/Multigrid_Hierarchy.h:600-603).
+template <typename T>
+__global__ void prolongate_kernel(int nb, const int* __restrict__ coords, const uint32_t* __restrict__ fflags,
+                                  GridView coarse, const T* __restrict__ cin, long Nc, T* __restrict__ fu, long Nf,
+                                  int round_out) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nb) * 128) return;
+  const int bi = int(t >> 7), e = int(t & 127);
+  const int lx = e >> 5, ly = (e >> 3) & 3, lz = e & 7;
+  const int x = coords[3 * bi] + lx, y = coords[3 * bi + 1] + ly, z = coords[3 * bi + 2] + lz;
+  const int cx = (x + 4) >> 1, cy = (y + 4) >> 1, cz = (z + 8) >> 1;
+  T v0 = fu[t], v1 = fu[t + Nf], v2 = fu[t + 2 * Nf];
+  for (int q = 0; q < 8; ++q) {
+    const int ii = q >> 2, jj = (q >> 1) & 1, kk = q & 1;
+    const double wx = (lx & 1) ? 0.5 : (ii ? 0.0 : 1.0);
+    const double wy = (ly & 1) ? 0.5 : (jj ? 0.0 : 1.0);
+    const double wz = (lz & 1) ? 0.5 : (kk ? 0.0 : 1.0);
+    const T w = T(wx * wy * wz);
+    if (!(w > T(0))) continue;
+    const long n = coarse.node(cx + ii, cy + jj, cz + kk);
+    if (n < 0) continue;
+    v0 += w * cin[n];
+    v1 += w * cin[n + Nc];
+    v2 += w * cin[n + 2 * Nc];
+  }
+  const uint32_t fl = fflags[t];
+  if (fl & DIR_X) v0 = 0;
+  if (fl & DIR_Y) v1 = 0;
+  if (fl & DIR_Z) v2 = 0;
+  if (round_out) { v0 = T(round_to_float(v0)); v1 = T(round_to_float(v1)); v2 = T(round_to_float(v2)); }
+  if (!(fl & ACTIVE_NODE)) v0 = v1 = v2 = 0;
+  fu[t] = v0;
+  fu[t + Nf] = v1;
+  fu[t + 2 * Nf] = v2;
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise helpers
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void round_float_kernel(T* p, long n) {
+  long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < n) p[t] = T(round_to_float(p[t]));
+}
+
+template <typename T>
+__global__ void zero_list_kernel(T* p, const int* __restrict__ idx, int n) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) p[idx[t]] = T(0);
+}
+
+// zero the three components of nodes without ACTIVE_NODE (Project_Null_Space.h:223-232)
+template <typename T>
+__global__ void project_null_kernel(T* p, const uint32_t* __restrict__ flags, long N) {
+  long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < N && !(flags[t] & ACTIVE_NODE)) p[t] = p[t + N] = p[t + 2 * N] = T(0);
+}
+
+template <typename TD, typename TS>
+__global__ void convert_kernel(TD* __restrict__ d, const TS* __restrict__ s, long n) {
+  long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < n) d[t] = TD(s[t]);
+}
+
+}  // namespace sgs

@@ -1,0 +1,374 @@
+// Host-side hierarchy construction; see setup.hpp.
+//
+// Follows the reference's set-up sequence: page activation and the SIMP map
+// (solver/SPGrid_CPU_Solver.cpp:100-145), the Dirichlet node->cell rule (:147-192),
+// cell/node flags and the boundary band (solver/CPU_Kernels/Flaging.h:31-173),
+// the coarse levels (solver/MG/Multigrid_Hierarchy.h:122-214) and the padding
+// check (:145-157).
+#include "setup.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <unordered_set>
+
+namespace sgs {
+
+uint64_t page_key(int bi, int bj, int bk) {
+  uint64_t key = 0;
+  for (int m = 0; m < 21; ++m) {
+    key |= uint64_t((bj >> m) & 1) << (3 * m);
+    key |= uint64_t((bi >> m) & 1) << (3 * m + 1);
+    key |= uint64_t((bk >> m) & 1) << (3 * m + 2);
+  }
+  return key;
+}
+
+static inline int node_slot(int x, int y, int z) { return (x & 3) * 32 + (y & 3) * 8 + (z & 7); }
+
+long HostLevel::cell(int x, int y, int z) const {
+  if (x < 0 || y < 0 || z < 0) return -1;
+  int bi = x >> 2, bj = y >> 2, bk = z >> 3;
+  if (bi >= grid[0] || bj >= grid[1] || bk >= grid[2]) return -1;
+  return (long(bi) * grid[1] + bj) * grid[2] + bk;
+}
+
+int HostLevel::block_at(int x, int y, int z) const {
+  long c = cell(x, y, z);
+  return c < 0 ? -1 : bgrid[c];
+}
+
+int HostLevel::active_block_at(int x, int y, int z) const {
+  int b = block_at(x, y, z);
+  return (b >= 0 && b < nb) ? b : -1;
+}
+
+int HostLevel::touch(int x, int y, int z) {
+  long c = cell(x, y, z);
+  if (c < 0) return -1;
+  int b = bgrid[c];
+  if (b < 0) {
+    b = int(coords.size() / 3);
+    bgrid[c] = b;
+    coords.push_back(x & ~3);
+    coords.push_back(y & ~3);
+    coords.push_back(z & ~7);
+    flags.resize(flags.size() + NODES_PER_BLOCK, 0u);
+  }
+  return b;
+}
+
+namespace {
+
+// A level under construction: blocks are created in touch order, then the
+// active ones are renumbered into page order.
+struct Builder {
+  HostLevel L;
+  std::vector<double> scratch;  // per-slot payload riding along with the blocks (E on level 0)
+
+  void init(int sx, int sy, int sz) {
+    L.size[0] = sx; L.size[1] = sy; L.size[2] = sz;
+    L.grid[0] = sx / BLK_X + 3; L.grid[1] = sy / BLK_Y + 3; L.grid[2] = sz / BLK_Z + 3;
+    L.bgrid.assign(size_t(L.grid[0]) * L.grid[1] * L.grid[2], -1);
+    L.active_page.assign(L.bgrid.size(), 0);
+  }
+  int set_page(int x, int y, int z) {
+    long c = L.cell(x, y, z);
+    if (c < 0) return -1;
+    int b = L.touch(x, y, z);
+    L.active_page[c] = 1;
+    return b;
+  }
+  bool test_page(int x, int y, int z) const {
+    long c = L.cell(x, y, z);
+    return c >= 0 && L.active_page[c];
+  }
+  uint32_t* flag(int x, int y, int z) {
+    int b = L.touch(x, y, z);
+    return b < 0 ? nullptr : &L.flags[size_t(b) * NODES_PER_BLOCK + node_slot(x, y, z)];
+  }
+  // Renumber: active blocks in page order first, ghosts after; returns old->new map.
+  std::vector<int32_t> finalize() {
+    const int n_all = int(L.coords.size() / 3);
+    std::vector<std::pair<uint64_t, int>> act;
+    std::vector<int> ghost;
+    for (int b = 0; b < n_all; ++b) {
+      int x = L.coords[3 * b], y = L.coords[3 * b + 1], z = L.coords[3 * b + 2];
+      if (L.active_page[L.cell(x, y, z)]) act.push_back({page_key(x >> 2, y >> 2, z >> 3), b});
+      else ghost.push_back(b);
+    }
+    std::sort(act.begin(), act.end());
+    std::vector<int32_t> order;
+    for (auto& a : act) order.push_back(a.second);
+    for (int g : ghost) order.push_back(g);
+    std::vector<int32_t> remap(n_all);
+    for (int i = 0; i < n_all; ++i) remap[order[i]] = i;
+    std::vector<int32_t> coords(L.coords.size());
+    std::vector<uint32_t> flags(L.flags.size());
+    std::vector<double> sc(scratch.size());
+    for (int i = 0; i < n_all; ++i) {
+      int o = order[i];
+      for (int v = 0; v < 3; ++v) coords[3 * i + v] = L.coords[3 * o + v];
+      std::copy(&L.flags[size_t(o) * NODES_PER_BLOCK], &L.flags[size_t(o) * NODES_PER_BLOCK] + NODES_PER_BLOCK,
+                &flags[size_t(i) * NODES_PER_BLOCK]);
+      if (!scratch.empty())
+        std::copy(&scratch[size_t(o) * NODES_PER_BLOCK], &scratch[size_t(o) * NODES_PER_BLOCK] + NODES_PER_BLOCK,
+                  &sc[size_t(i) * NODES_PER_BLOCK]);
+    }
+    L.coords.swap(coords);
+    L.flags.swap(flags);
+    scratch.swap(sc);
+    for (auto& g : L.bgrid)
+      if (g >= 0) g = remap[g];
+    L.nb = int(act.size());
+    return remap;
+  }
+};
+
+void flag_nodes(HostLevel& L) {
+  // Flaging.h:65-80 — OR each cell's (flags >> 4) into its 8 corner nodes.  Runs
+  // serially like the reference; writes may create ghost blocks.
+  for (int b = 0; b < L.nb; ++b) {
+    const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
+    for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+      uint32_t nf = (L.flags[size_t(b) * NODES_PER_BLOCK + e] & (F_ACTIVE_CELL | F_DIRICHLET_CELL)) >> 4;
+      if (!nf) continue;
+      int x = bx + (e >> 5), y = by + ((e >> 3) & 3), z = bz + (e & 7);
+      for (int c = 0; c < 8; ++c) {
+        int nx = x + (c >> 2), ny = y + ((c >> 1) & 1), nz = z + (c & 1);
+        int nbk = L.touch(nx, ny, nz);
+        if (nbk >= 0) L.flags[size_t(nbk) * NODES_PER_BLOCK + node_slot(nx, ny, nz)] |= nf;
+      }
+    }
+  }
+}
+
+void flag_boundary(HostLevel& L, int band = 3) {
+  // Flaging.h:93-147: three Jacobi-style passes growing a band of active,
+  // non-Dirichlet nodes around the Dirichlet nodes.
+  auto flag_at = [&](int x, int y, int z) -> uint32_t {
+    int b = L.block_at(x, y, z);
+    return b < 0 ? 0u : L.flags[size_t(b) * NODES_PER_BLOCK + node_slot(x, y, z)];
+  };
+  for (int pass = 0; pass < band; ++pass) {
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < L.nb; ++b) {
+      const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
+      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+        uint32_t& f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
+        if ((f & F_DIRICHLET_NODE) || !(f & F_ACTIVE_NODE)) continue;
+        int x = bx + (e >> 5), y = by + ((e >> 3) & 3), z = bz + (e & 7);
+        bool hit = false;
+        for (int d = 0; d < 27 && !hit; ++d)
+          hit = flag_at(x + d / 9 - 1, y + (d / 3) % 3 - 1, z + d % 3 - 1) & (F_DIRICHLET_NODE | F_BOUNDARY_NODE);
+        if (hit) f |= F_BOUNDARY_TEMP;
+      }
+    }
+    for (size_t i = 0; i < size_t(L.nb) * NODES_PER_BLOCK; ++i)
+      if (L.flags[i] & F_BOUNDARY_TEMP) L.flags[i] = (L.flags[i] & ~F_BOUNDARY_TEMP) | F_BOUNDARY_NODE;
+  }
+  L.boundary.clear();
+  for (int b = 0; b < L.nb; ++b)
+    for (int e = 0; e < NODES_PER_BLOCK; ++e)
+      if (L.flags[size_t(b) * NODES_PER_BLOCK + e] & F_BOUNDARY_NODE) {
+        L.boundary.push_back(b);
+        break;
+      }
+}
+
+void finish_level(HostLevel& L) {
+  for (int v = 0; v < 3; ++v) L.dirichlet[v].clear();
+  for (int b = 0; b < L.nb; ++b)
+    for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+      uint32_t f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
+      for (int v = 0; v < 3; ++v)
+        if (f & (F_DIRICHLET_NODE_X << v)) L.dirichlet[v].push_back(b * NODES_PER_BLOCK + e);
+    }
+  L.nbr.assign(size_t(L.nb) * 27, -1);
+  for (int b = 0; b < L.nb; ++b) {
+    const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
+    for (int d = 0; d < 27; ++d)
+      L.nbr[size_t(b) * 27 + d] = L.active_block_at(bx + (d / 9 - 1) * BLK_X, by + ((d / 3) % 3 - 1) * BLK_Y,
+                                                    bz + (d % 3 - 1) * BLK_Z);
+  }
+}
+
+}  // namespace
+
+std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
+  char msg[256];
+  auto fail = [&](int code, const char* m) {
+    *error_code = code;
+    return std::string(m);
+  };
+  *error_code = 0;
+  if (!in.use_density_only) return fail(2, "Unsupported mode: only use_density_only=true inputs are accepted");
+  if (in.mg_level == 2) return fail(3, "mg_level = 2 is not supported (the caller bumps it to 3)");
+  for (int v = 0; v < 3; ++v)
+    if (in.resolution[v] <= 0 || in.resolution[v] > (1 << 20)) return fail(4, "resolution out of range");
+  P.resolution[0] = in.resolution[0]; P.resolution[1] = in.resolution[1]; P.resolution[2] = in.resolution[2];
+  P.dx = in.dx;
+  P.mu0 = in.global_mu;
+  P.lambda0 = in.global_lambda;
+  P.disable_mg = in.mg_level <= 0;
+  P.mg_levels = in.mg_level <= 0 ? 1 : in.mg_level;
+  P.smoothing = in.pre_and_post_smoothing_iter;
+  P.boundary_smoothing = in.get_int("boundary_smoothing", 5);
+  P.tolerance = in.krylov.tolerance;
+  const double penalty = in.get_double("penalty", 0.0), emin = in.get_double("minimum_stiffness", 0.0),
+               rho_min = in.get_double("minimum_density", 0.0);
+  P.penalty = penalty;
+  P.minimum_stiffness = emin;
+
+  // ---- level 0: page activation and stiffness (SPGrid_CPU_Solver.cpp:102-136)
+  Builder b0;
+  b0.init(in.resolution[0], in.resolution[1], in.resolution[2]);
+  const size_t nin = in.density.num_blocks();
+  struct CellE { int x, y, z; double E; };
+  std::vector<CellE> cells;
+  for (size_t b = 0; b < nin; ++b) {
+    int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
+    if ((x & 3) || (y & 3) || (z & 3)) return fail(4, "density block base is not a multiple of 4");
+    if (b0.set_page(x, y, z) < 0) return fail(4, "density block outside the grid");
+    for (int e = 0; e < 64; ++e) {
+      double d = in.density.data[b * 64 + e];
+      if (d > 0) {
+        double E = penalty ? (1 - emin) * std::pow(std::max(rho_min, d), penalty) + emin : d;
+        cells.push_back({x + (e >> 4), y + ((e >> 2) & 3), z + (e & 3), E});
+      }
+    }
+  }
+  // material slots ride along with the blocks through the renumbering
+  b0.scratch.assign(b0.L.coords.size() / 3 * NODES_PER_BLOCK, 0.0);
+  for (auto& c : cells) {
+    int bk = b0.L.block_at(c.x, c.y, c.z);
+    if (bk < 0) return fail(4, "material cell outside the grid");
+    b0.scratch[size_t(bk) * NODES_PER_BLOCK + node_slot(c.x, c.y, c.z)] = c.E;
+  }
+  // Validate_With_Density (solver/CPU_Kernels/Validate_Blocks.h:311-335): every
+  // material cell needs its +1 neighbour pages.
+  for (auto& c : cells)
+    if (c.E * P.mu0 > 0)
+      for (int n = 1; n < 8; ++n)
+        if (!b0.test_page(c.x + (n >> 2), c.y + ((n >> 1) & 1), c.z + (n & 1))) {
+          std::snprintf(msg, sizeof msg, "Block activation check failed at cell (%d, %d, %d)", c.x, c.y, c.z);
+          return fail(5, msg);
+        }
+  // ACTIVE_CELL where mu != 0 (Flaging.h:31-44); written before renumbering
+  for (auto& c : cells)
+    if (c.E * P.mu0 != 0) *b0.flag(c.x, c.y, c.z) |= F_ACTIVE_CELL;
+  // Dirichlet node -> cell: a cell is fixed on axis v when all 8 corners are
+  // listed on axis v (SPGrid_CPU_Solver.cpp:169-192)
+  for (int v = 0; v < 3; ++v) {
+    std::unordered_set<uint64_t> set;
+    auto key = [](int x, int y, int z) {
+      return (uint64_t(uint32_t(x) & 0x1fffff) << 42) | (uint64_t(uint32_t(y) & 0x1fffff) << 21) | (uint32_t(z) & 0x1fffff);
+    };
+    for (auto& d : in.dirichlet_nodes)
+      if (d.axis == v) set.insert(key(d.coord[0], d.coord[1], d.coord[2]));
+    for (auto& d : in.dirichlet_nodes) {
+      if (d.axis != v) continue;
+      bool all = true;
+      for (int n = 1; n < 8 && all; ++n)
+        all = set.count(key(d.coord[0] + (n >> 2), d.coord[1] + ((n >> 1) & 1), d.coord[2] + (n & 1))) > 0;
+      if (all) {
+        uint32_t* f = b0.flag(d.coord[0], d.coord[1], d.coord[2]);
+        if (f) *f |= (F_DIRICHLET_CELL_X << v);
+      }
+    }
+  }
+  for (auto& d : in.dirichlet_nodes)
+    if (d.axis < 0 || d.axis > 2) return fail(4, "Dirichlet axis out of range");
+  b0.finalize();
+  P.levels.clear();
+  P.levels.push_back(std::move(b0.L));
+  P.E.assign(b0.scratch.begin(), b0.scratch.begin() + size_t(P.levels[0].nb) * NODES_PER_BLOCK);
+
+  // ---- coarse levels (Multigrid_Hierarchy.h:122-195)
+  const int pad[3] = {2 * BLK_X, 2 * BLK_Y, 2 * BLK_Z};
+  for (int lev = 1; lev < P.mg_levels; ++lev) {
+    HostLevel& F = P.levels[lev - 1];
+    int sz[3];
+    for (int v = 0; v < 3; ++v) {
+      int fine = F.size[v] + 1 - pad[v];
+      sz[v] = pad[v] + fine / 2 + (fine % 2 ? 1 : 0);
+    }
+    Builder bc;
+    bc.init(sz[0], sz[1], sz[2]);
+    for (int b = 0; b < F.nb; ++b) {
+      const int bx = F.coords[3 * b], by = F.coords[3 * b + 1], bz = F.coords[3 * b + 2];
+      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+        uint32_t ff = F.flags[size_t(b) * NODES_PER_BLOCK + e];
+        if (!(ff & (F_ACTIVE_CELL | F_DIRICHLET_CELL))) continue;
+        int x = bx + (e >> 5), y = by + ((e >> 3) & 3), z = bz + (e & 7);
+        int cx = (x + BLK_X) >> 1, cy = (y + BLK_Y) >> 1, cz = (z + BLK_Z) >> 1;
+        if (ff & F_ACTIVE_CELL) {
+          if (uint32_t* f = bc.flag(cx, cy, cz)) *f |= F_ACTIVE_CELL;
+          for (int n = 0; n < 8; ++n) bc.set_page(cx + (n >> 2), cy + ((n >> 1) & 1), cz + (n & 1));
+        }
+        for (int v = 0; v < 3; ++v)
+          if (ff & (F_DIRICHLET_CELL_X << v)) {
+            if (uint32_t* f = bc.flag(cx, cy, cz)) *f |= (F_DIRICHLET_CELL_X << v);
+            for (int n = 1; n < 8; ++n) bc.set_page(cx + (n >> 2), cy + ((n >> 1) & 1), cz + (n & 1));
+          }
+      }
+    }
+    bc.finalize();
+    P.levels.push_back(std::move(bc.L));
+  }
+  for (auto& L : P.levels) flag_nodes(L);
+  for (auto& L : P.levels) flag_boundary(L);
+  for (auto& L : P.levels) finish_level(L);
+
+  // ---- padding check (Multigrid_Hierarchy.h:145-157)
+  {
+    HostLevel& L = P.levels[0];
+    const int bs[3] = {BLK_X, BLK_Y, BLK_Z};
+    for (int b = 0; b < L.nb; ++b)
+      for (int v = 0; v < 3; ++v) {
+        int c = L.coords[3 * b + v];
+        if (c < bs[v] || c >= L.size[v] - 2 * bs[v]) {
+          std::snprintf(msg, sizeof msg, "Padding violated by block (%d, %d, %d)", L.coords[3 * b], L.coords[3 * b + 1],
+                        L.coords[3 * b + 2]);
+          return fail(6, msg);
+        }
+      }
+  }
+
+  // ---- input-block map, forces and the Dirichlet lift on level 0
+  HostLevel& L0 = P.levels[0];
+  P.in_block.resize(nin);
+  P.in_zoff.resize(nin);
+  P.in_base.assign(in.density.base.begin(), in.density.base.end());
+  for (size_t b = 0; b < nin; ++b) {
+    int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
+    P.in_block[b] = L0.active_block_at(x, y, z);
+    P.in_zoff[b] = z & 4;
+  }
+  // forces are assigned, the last entry of a node wins (SPGrid_CPU_Solver.cpp:290-296)
+  P.force_node.clear();
+  P.force_val.clear();
+  for (auto& f : in.forces) {
+    int bk = L0.active_block_at(f.coord[0], f.coord[1], f.coord[2]);
+    if (bk < 0) continue;  // outside the active pages: the projections zero it
+    P.force_node.push_back(bk * NODES_PER_BLOCK + node_slot(f.coord[0], f.coord[1], f.coord[2]));
+    for (int v = 0; v < 3; ++v) {
+      if (!std::isfinite(f.f[v])) return fail(4, "non-finite force");
+      P.force_val.push_back(f.f[v]);
+    }
+  }
+  P.lift_node.clear();
+  P.lift_axis.clear();
+  P.lift_val.clear();
+  for (auto& d : in.dirichlet_nodes) {
+    int bk = L0.active_block_at(d.coord[0], d.coord[1], d.coord[2]);
+    if (bk < 0) continue;  // values on inactive pages never reach an active cell
+    if (!std::isfinite(d.value)) return fail(4, "non-finite Dirichlet value");
+    P.lift_node.push_back(bk * NODES_PER_BLOCK + node_slot(d.coord[0], d.coord[1], d.coord[2]));
+    P.lift_axis.push_back(d.axis);
+    P.lift_val.push_back(d.value);
+  }
+  return std::string();
+}
+
+}  // namespace sgs

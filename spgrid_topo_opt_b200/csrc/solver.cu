@@ -1,0 +1,1267 @@
+// Narrow-band SPGrid linear-elasticity MGPCG on one B200.
+//
+// Host orchestration of the kernels in kernels.cuh / setup_kernels.cuh and the
+// C ABI declared in include/spgrid_fem.h.  The solve follows the reference's
+// fem_solve (solver/SPGrid_CPU_Solver.cpp:26-409): Dirichlet lift, PCG with one
+// V-cycle per iteration (solver/CG/CONJUGATE_GRADIENT.cpp:21-61,
+// solver/MG/Multigrid_Hierarchy.h:569-619), L-infinity stopping rule relative
+// to the zero-guess residual, output packing per input block.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/spgrid_fem.h"
+#include "kernels.cuh"
+#include "setup.hpp"
+#include "setup_kernels.cuh"
+#include "wire.hpp"
+
+namespace sgs {
+
+// ---------------------------------------------------------------------------
+// small utilities
+// ---------------------------------------------------------------------------
+struct CudaError : std::runtime_error {
+  int code;
+  CudaError(const std::string& m, int c) : std::runtime_error(m), code(c) {}
+};
+
+#define SGS_CUDA(x)                                                                                     \
+  do {                                                                                                  \
+    cudaError_t e_ = (x);                                                                               \
+    if (e_ != cudaSuccess)                                                                              \
+      throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_), SGS_ERR_CUDA);                   \
+  } while (0)
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) SGS_CUDA(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) SGS_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
+  void zero(cudaStream_t s) {
+    if (n) SGS_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+};
+
+static inline unsigned blocks_for(long n, int t) { return unsigned((n + t - 1) / t); }
+
+// Element stiffness of the Q1 hex on the unit cube: K_mu = int(delta_ij grad Na.grad Nb
+// + d_j Na d_i Nb), K_la = int d_i Na d_j Nb; node index a = 4x + 2y + z.  These are
+// the exact rationals k/72 of solver/CPU_Kernels/Stiffness_Matrices.h.
+static void element_tables(double Kmu[8][8][3][3], double Kla[8][8][3][3]) {
+  const int M[2][2] = {{2, 1}, {1, 2}}, D[2][2] = {{-3, -3}, {3, 3}}, S[2][2] = {{6, -6}, {-6, 6}};
+  auto g = [&](int a, int b, int i, int j) {
+    long v = 1;
+    for (int ax = 0; ax < 3; ++ax) {
+      int pa = (a >> (2 - ax)) & 1, pb = (b >> (2 - ax)) & 1;
+      bool da = ax == i, db = ax == j;
+      v *= (da && db) ? S[pa][pb] : da ? D[pa][pb] : db ? D[pb][pa] : M[pa][pb];
+    }
+    return v;  // 216 * integral
+  };
+  for (int a = 0; a < 8; ++a)
+    for (int b = 0; b < 8; ++b)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          long lam = g(a, b, i, j), mu = g(a, b, j, i);
+          if (i == j)
+            for (int k = 0; k < 3; ++k) mu += g(a, b, k, k);
+          Kla[a][b][i][j] = double(lam / 3) / 72.0;
+          Kmu[a][b][i][j] = double(mu / 3) / 72.0;
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Device level
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Level {
+  int nb = 0;
+  long N = 0;
+  DevBuf<int> coords, nbr, bgrid, boundary, dir[3];
+  DevBuf<uint32_t> flags, spokes;
+  GridView grid{};
+  int nbound = 0, ndir[3] = {0, 0, 0};
+  DevBuf<T> u, b, r;   // [3N] each
+  DevBuf<T> A;         // [243][N] stencils (levels with Galerkin operators)
+  bool has_matrix = false;
+};
+
+struct Bottom {
+  int ndof_nodes = 0;
+  long n = 0, ld = 0;
+  DevBuf<int> dof_node, node_dof;
+  DevBuf<double> Minv, xb, xs;
+};
+
+enum Precision { PREC_REFERENCE = 0, PREC_FP64 = 1, PREC_MIXED = 2 };
+
+// ---------------------------------------------------------------------------
+// The solver: device hierarchy + PCG
+// ---------------------------------------------------------------------------
+class Solver {
+ public:
+  Problem P;
+  int precision = PREC_REFERENCE;
+  cudaStream_t stream = nullptr;
+  // level data (double for reference/fp64, float for the mixed V-cycle)
+  std::vector<std::unique_ptr<Level<double>>> L64;
+  std::vector<std::unique_ptr<Level<float>>> L32;
+  Bottom bottom;
+  DevBuf<double> E64;
+  DevBuf<float> E32;
+  // CG vectors [3N0]
+  DevBuf<double> x, f, s, q, ubk, scratch;
+  DevBuf<int> lift_node, lift_axis, force_node;
+  DevBuf<double> lift_val, force_val;
+  DevBuf<double> red;      // reduction partials
+  DevBuf<double> scal;     // device scalars: 0 rho, 1 rho_old, 2 sq, 3 norm, 4 beta, 5 alpha, 6 -alpha, 7 breakdown
+  double* h_scal = nullptr;  // pinned mirror
+  // input block map for packing
+  DevBuf<int> in_block, in_zoff;
+  DevBuf<double> out_disp;
+  // stats
+  int iterations = 0;
+  double initial_residual = 0, final_residual = 0, setup_seconds = 0, solve_seconds = 0;
+  std::vector<double> history;
+  std::string error;
+  int error_code = 0;
+  // graph of one PCG iteration
+  cudaGraphExec_t iter_graph = nullptr;
+  long launches_per_iteration = 0;
+  long launch_counter = 0;
+
+  ~Solver() {
+    if (iter_graph) cudaGraphExecDestroy(iter_graph);
+    if (h_scal) cudaFreeHost(h_scal);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  long N0() const { return long(P.levels[0].nb) * NODES_PER_BLOCK; }
+  bool mixed() const { return precision == PREC_MIXED; }
+  bool round_ref() const { return precision == PREC_REFERENCE; }
+  int nlev() const { return int(P.levels.size()); }
+
+  void init(int prec) {
+    precision = prec;
+    SGS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    SGS_CUDA(cudaMallocHost(&h_scal, 16 * sizeof(double)));
+    auto t0 = std::chrono::steady_clock::now();
+    upload_constants();
+    build_levels();
+    build_operators();
+    build_bottom();
+    alloc_cg();
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  void upload_constants() {
+    double Kmu[8][8][3][3], Kla[8][8][3][3];
+    element_tables(Kmu, Kla);
+    double kc64[576];
+    float kc32[576];
+    for (int I = 0; I < 8; ++I)
+      for (int J = 0; J < 8; ++J)
+        for (int v = 0; v < 3; ++v)
+          for (int w = 0; w < 3; ++w) {
+            double val = P.mu0 * Kmu[I][J][v][w] + P.lambda0 * Kla[I][J][v][w];
+            kc64[(I * 8 + J) * 9 + v * 3 + w] = val;
+            kc32[(I * 8 + J) * 9 + v * 3 + w] = float(val);
+          }
+    SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kc64, kc64, sizeof(kc64), 0, cudaMemcpyHostToDevice, stream));
+    SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kc32, kc32, sizeof(kc32), 0, cudaMemcpyHostToDevice, stream));
+  }
+
+  template <typename T>
+  void upload_level(Level<T>& d, const HostLevel& h) {
+    d.nb = h.nb;
+    d.N = long(h.nb) * NODES_PER_BLOCK;
+    d.coords.upload(h.coords.data(), size_t(h.nb) * 3, stream);
+    d.nbr.upload(h.nbr, stream);
+    d.flags.upload(h.flags.data(), size_t(d.N), stream);
+    std::vector<int32_t> g(h.bgrid.size());
+    for (size_t i = 0; i < g.size(); ++i) g[i] = (h.bgrid[i] >= 0 && h.bgrid[i] < h.nb) ? h.bgrid[i] : -1;
+    d.bgrid.upload(g, stream);
+    d.grid = GridView{d.bgrid.p, h.grid[0], h.grid[1], h.grid[2]};
+    d.boundary.upload(h.boundary, stream);
+    d.nbound = int(h.boundary.size());
+    for (int v = 0; v < 3; ++v) {
+      std::vector<int32_t> lst(h.dirichlet[v].begin(), h.dirichlet[v].end());
+      for (auto& i : lst) i += v * int(d.N);  // index into the [3][N] planes
+      d.dir[v].upload(lst, stream);
+      d.ndir[v] = int(lst.size());
+    }
+    d.u.alloc(3 * d.N);
+    d.b.alloc(3 * d.N);
+    d.r.alloc(3 * d.N);
+    d.u.zero(stream);
+    d.b.zero(stream);
+    d.r.zero(stream);
+  }
+
+  void build_levels() {
+    for (auto& h : P.levels) {
+      L64.emplace_back(new Level<double>());
+      upload_level(*L64.back(), h);
+      if (mixed()) {
+        L32.emplace_back(new Level<float>());
+        upload_level(*L32.back(), h);
+      }
+    }
+    E64.upload(P.E, stream);
+    if (mixed()) {
+      E32.alloc(P.E.size());
+      convert_kernel<float, double><<<blocks_for(long(P.E.size()), 256), 256, 0, stream>>>(E32.p, E64.p, long(P.E.size()));
+    }
+  }
+
+  // Galerkin tables for one depth: table[p][a][b][v][w]
+  std::vector<double> galerkin_table(int depth) {
+    double Kmu[8][8][3][3], Kla[8][8][3][3];
+    element_tables(Kmu, Kla);
+    const int side = 1 << depth;
+    const long npos = long(side) * side * side;
+    std::vector<double> tab(size_t(npos) * 576, 0.0);
+    double Kc[8][8][9];
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j)
+        for (int vw = 0; vw < 9; ++vw) Kc[i][j][vw] = P.mu0 * Kmu[i][j][vw / 3][vw % 3] + P.lambda0 * Kla[i][j][vw / 3][vw % 3];
+    for (long p = 0; p < npos; ++p) {
+      const int pc[3] = {int(p / (long(side) * side)), int((p / side) % side), int(p % side)};
+      double W[8][8];  // W[i][a]
+      for (int i = 0; i < 8; ++i)
+        for (int a = 0; a < 8; ++a) {
+          double w = 1;
+          for (int ax = 0; ax < 3; ++ax) {
+            double tpos = double(pc[ax] + ((i >> (2 - ax)) & 1)) / side;
+            w *= ((a >> (2 - ax)) & 1) ? tpos : 1 - tpos;
+          }
+          W[i][a] = w;
+        }
+      double* out = &tab[size_t(p) * 576];
+      for (int a = 0; a < 8; ++a)
+        for (int b = 0; b < 8; ++b)
+          for (int vw = 0; vw < 9; ++vw) {
+            double s = 0;
+            for (int i = 0; i < 8; ++i) {
+              if (W[i][a] == 0) continue;
+              for (int j = 0; j < 8; ++j) s += W[i][a] * W[j][b] * Kc[i][j][vw];
+            }
+            out[(a * 8 + b) * 9 + vw] = s;
+          }
+    }
+    return tab;
+  }
+
+  void build_operators() {
+    if (P.disable_mg) return;
+    const int n = nlev();
+    const int first = (n == 1) ? 0 : P.explicit_level;
+    for (int lev = first; lev < n; ++lev) {
+      Level<double>& d = *L64[lev];
+      if (lev > 6) throw CudaError("multigrid depth above 6 is not supported", SGS_ERR_INPUT);
+      std::vector<double> tab = galerkin_table(lev);
+      DevBuf<double> dtab;
+      dtab.upload(tab, stream);
+      d.A.alloc(243 * size_t(d.N));
+      d.A.zero(stream);
+      d.spokes.alloc(size_t(d.N));
+      d.spokes.zero(stream);
+      d.has_matrix = true;
+      if (d.N > 0) {
+        galerkin_kernel<<<unsigned(d.N), 576, 0, stream>>>(d.coords.p, d.flags.p, lev, L64[0]->grid, E64.p, dtab.p, d.A.p,
+                                                          d.spokes.p, d.N, P.dx);
+        SGS_CUDA(cudaGetLastError());
+        delete_dirichlet_kernel<<<blocks_for(d.N, 128), 128, 0, stream>>>(d.nb, d.coords.p, d.flags.p, d.spokes.p, d.grid,
+                                                                         d.A.p, d.N);
+        SGS_CUDA(cudaGetLastError());
+      }
+      SGS_CUDA(cudaStreamSynchronize(stream));  // dtab goes out of scope
+      if (mixed()) {
+        Level<float>& m = *L32[lev];
+        m.A.alloc(243 * size_t(d.N));
+        convert_kernel<float, double><<<blocks_for(243 * d.N, 256), 256, 0, stream>>>(m.A.p, d.A.p, 243 * d.N);
+        m.spokes.alloc(size_t(d.N));
+        SGS_CUDA(cudaMemcpyAsync(m.spokes.p, d.spokes.p, d.N * 4, cudaMemcpyDeviceToDevice, stream));
+        m.has_matrix = true;
+      }
+    }
+  }
+
+  void build_bottom() {
+    if (P.disable_mg) return;
+    Level<double>& d = *L64[nlev() - 1];
+    std::vector<uint32_t> sp(size_t(d.N));
+    if (d.N) SGS_CUDA(cudaMemcpyAsync(sp.data(), d.spokes.p, d.N * 4, cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    std::vector<int32_t> dof_node, node_dof(size_t(d.N), -1);
+    for (long i = 0; i < d.N; ++i)
+      if (sp[i] & 0x07ffffffu) {
+        node_dof[i] = int(dof_node.size());
+        dof_node.push_back(int(i));
+      }
+    bottom.ndof_nodes = int(dof_node.size());
+    bottom.n = 3L * bottom.ndof_nodes;
+    bottom.ld = ((bottom.n + GJ - 1) / GJ) * GJ;
+    const long max_dense = 24576;  // 4.8 GB of FP64
+    if (bottom.n > max_dense) {
+      char m[160];
+      std::snprintf(m, sizeof m, "bottom level has %ld unknowns; the dense bottom solve supports at most %ld (raise mg_level)",
+                    bottom.n, max_dense);
+      throw CudaError(m, SGS_ERR_INPUT);
+    }
+    bottom.dof_node.upload(dof_node, stream);
+    bottom.node_dof.upload(node_dof, stream);
+    bottom.xb.alloc(size_t(bottom.ld));
+    bottom.xs.alloc(size_t(bottom.ld));
+    bottom.xb.zero(stream);
+    bottom.xs.zero(stream);
+    if (bottom.n == 0) return;
+    bottom.Minv.alloc(size_t(bottom.ld) * bottom.ld);
+    bottom.Minv.zero(stream);
+    bottom_assemble_kernel<<<blocks_for(bottom.ndof_nodes, 128), 128, 0, stream>>>(
+        bottom.ndof_nodes, bottom.dof_node.p, bottom.node_dof.p, d.coords.p, d.flags.p, d.spokes.p, d.grid, d.A.p, d.N,
+        bottom.Minv.p, bottom.ld);
+    if (bottom.ld > bottom.n)
+      identity_pad_kernel<<<blocks_for(bottom.ld - bottom.n, 64), 64, 0, stream>>>(bottom.Minv.p, bottom.ld, bottom.n);
+    SGS_CUDA(cudaGetLastError());
+    invert_dense(bottom.Minv.p, bottom.ld);
+  }
+
+  void invert_dense(double* M, long ld) {
+    const int nt = int(ld / GJ);
+    DevBuf<double> pinv;
+    pinv.alloc(GJ * GJ);
+    DevBuf<int> bad;
+    bad.alloc(1);
+    bad.zero(stream);
+    const size_t tile_smem = 2 * GJ * 65 * sizeof(double);
+    SGS_CUDA(cudaFuncSetAttribute(gj_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tile_smem)));
+    for (int K = 0; K < nt; ++K) {
+      gj_pivot_kernel<<<1, 256, GJ * 65 * sizeof(double), stream>>>(M, ld, K, pinv.p, bad.p);
+      gj_tile_kernel<<<nt, 256, tile_smem, stream>>>(M, ld, K, pinv.p, 0);
+      gj_tile_kernel<<<dim3(nt, nt), 256, tile_smem, stream>>>(M, ld, K, pinv.p, 1);
+      gj_tile_kernel<<<nt, 256, tile_smem, stream>>>(M, ld, K, pinv.p, 2);
+      gj_store_pivot_kernel<<<1, 256, 0, stream>>>(M, ld, K, pinv.p);
+    }
+    SGS_CUDA(cudaGetLastError());
+    int hbad = 0;
+    SGS_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    if (hbad) throw CudaError("bottom operator is not positive definite", SGS_ERR_BREAKDOWN);
+  }
+
+  void alloc_cg() {
+    const long n3 = 3 * N0();
+    for (DevBuf<double>* v : {&x, &f, &s, &q, &ubk, &scratch}) {
+      v->alloc(size_t(n3));
+      v->zero(stream);
+    }
+    lift_node.upload(P.lift_node, stream);
+    lift_axis.upload(P.lift_axis, stream);
+    lift_val.upload(P.lift_val, stream);
+    force_node.upload(P.force_node, stream);
+    force_val.upload(P.force_val, stream);
+    red.alloc(1024);
+    scal.alloc(16);
+    scal.zero(stream);
+    in_block.upload(P.in_block, stream);
+    in_zoff.upload(P.in_zoff, stream);
+    out_disp.alloc(P.in_block.size() * 64 * 4);
+  }
+
+  // ------------------------------------------------------------------ kernels
+  template <typename T>
+  Level<T>& lev(int l);
+
+  template <typename T>
+  const T* Edev();
+
+  template <typename T>
+  void project(Level<T>& d, T* v) {
+    for (int c = 0; c < 3; ++c)
+      if (d.ndir[c]) {
+        zero_list_kernel<T><<<blocks_for(d.ndir[c], 256), 256, 0, stream>>>(v, d.dir[c].p, d.ndir[c]);
+        ++launch_counter;
+      }
+  }
+
+  template <typename T>
+  void project_null(Level<T>& d, T* v) {
+    project_null_kernel<T><<<blocks_for(d.N, 256), 256, 0, stream>>>(v, d.flags.p, d.N);
+    ++launch_counter;
+  }
+
+  template <typename T>
+  void round3(Level<T>& d, T* v) {
+    round_float_kernel<T><<<blocks_for(3 * d.N, 256), 256, 0, stream>>>(v, 3 * d.N);
+    ++launch_counter;
+  }
+
+  template <typename T, int OP>
+  void level0(const int* list, int count, const T* u, T* uo, const T* b, T* out, int color, int boundary) {
+    Level<T>& d = lev<T>(0);
+    if (count <= 0) return;
+    level0_op_kernel<T, OP><<<count, 128, 0, stream>>>(list, count, d.nbr.p, Edev<T>(), u, uo, b, out, d.flags.p, d.N,
+                                                      T(P.dx), color, boundary);
+    ++launch_counter;
+  }
+
+  template <typename T, int OP>
+  void stencil(int l, const int* list, int count, const T* u, T* uo, const T* b, T* out, int color, int boundary,
+               int round_out) {
+    Level<T>& d = lev<T>(l);
+    if (count <= 0) return;
+    const int per = OP == SOP_GS ? 16 : 128;
+    stencil_op_kernel<T, OP><<<blocks_for(long(count) * per, 128), 128, 0, stream>>>(
+        list, count, d.coords.p, d.grid, d.A.p, d.flags.p, u, uo, b, out, d.N, color, boundary, round_out);
+    ++launch_counter;
+  }
+
+  // one full smoothing sweep (8 colours) of level l on u given b
+  template <typename T>
+  void sweep(int l, T* u, const T* b, bool forward, bool boundary) {
+    Level<T>& d = lev<T>(l);
+    const int* list = boundary ? d.boundary.p : nullptr;
+    const int count = boundary ? d.nbound : d.nb;
+    if (count == 0) return;
+    if (l == 0) {
+      for (int k = 0; k < 8; ++k) {
+        const int c = forward ? k : 7 - k;
+        level0<T, OP_GS>(list, count, u, u, b, nullptr, c, boundary ? 1 : 0);
+      }
+      return;
+    }
+    static const int order[2][8] = {{1, 5, 4, 6, 7, 3, 2, 0}, {0, 2, 3, 7, 6, 4, 5, 1}};
+    for (int k = 0; k < 8; ++k)
+      stencil<T, SOP_GS>(l, list, count, u, u, b, nullptr, forward ? order[0][k] : order[1][k], boundary ? 1 : 0, 0);
+  }
+
+  template <typename T>
+  void sweeps(int l, T* u, const T* b, bool forward) {
+    const bool rr = round_ref();
+    for (int t = 0; t < P.boundary_smoothing; ++t) {
+      sweep<T>(l, u, b, forward, true);
+      if (rr) round3(lev<T>(l), u);
+    }
+    for (int t = 0; t < P.smoothing; ++t) {
+      sweep<T>(l, u, b, forward, false);
+      if (rr) round3(lev<T>(l), u);
+    }
+    for (int t = 0; t < P.boundary_smoothing; ++t) {
+      sweep<T>(l, u, b, forward, true);
+      if (rr) round3(lev<T>(l), u);
+    }
+  }
+
+  template <typename T>
+  void restrict_to(int lc, const T* fine_field) {
+    Level<T>& c = lev<T>(lc);
+    Level<T>& fl = lev<T>(lc - 1);
+    if (c.N == 0) return;
+    restrict_kernel<T><<<blocks_for(c.N, 128), 128, 0, stream>>>(c.nb, c.coords.p, c.flags.p, fl.grid, fine_field, fl.N,
+                                                                c.b.p, c.N);
+    ++launch_counter;
+  }
+
+  template <typename T>
+  void prolongate_to(int lf, T* fine_u) {
+    Level<T>& fl = lev<T>(lf);
+    Level<T>& c = lev<T>(lf + 1);
+    if (fl.N == 0) return;
+    prolongate_kernel<T><<<blocks_for(fl.N, 128), 128, 0, stream>>>(fl.nb, fl.coords.p, fl.flags.p, c.grid, c.u.p, c.N,
+                                                                   fine_u, fl.N, round_ref() ? 1 : 0);
+    ++launch_counter;
+  }
+
+  template <typename T>
+  void bottom_solve(int l) {
+    Level<T>& d = lev<T>(l);
+    // nodes without unknowns keep b (the reference copies b in and out)
+    SGS_CUDA(cudaMemcpyAsync(d.u.p, d.b.p, 3 * d.N * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+    if (bottom.ndof_nodes > 0) {
+      bottom_gather_kernel<T><<<blocks_for(bottom.ndof_nodes, 128), 128, 0, stream>>>(bottom.ndof_nodes, bottom.dof_node.p,
+                                                                                     d.b.p, d.N, bottom.xb.p);
+      gemv_kernel<<<blocks_for(bottom.ld * 32, 256), 256, 0, stream>>>(bottom.Minv.p, bottom.ld, bottom.ld, bottom.xb.p,
+                                                                      bottom.xs.p);
+      bottom_scatter_kernel<T><<<blocks_for(bottom.ndof_nodes, 128), 128, 0, stream>>>(bottom.ndof_nodes,
+                                                                                      bottom.dof_node.p, bottom.xs.p,
+                                                                                      d.u.p, d.N);
+      launch_counter += 3;
+    }
+    if (round_ref()) round3(d, d.u.p);
+  }
+
+  // V-cycle (Run_VCycle): level-0 right-hand side b0, correction written to u0.
+  template <typename T>
+  void vcycle(const T* b0, T* u0) {
+    const int n = nlev();
+    const int ex = P.explicit_level;
+    const bool rr = round_ref();
+    Level<T>& l0 = lev<T>(0);
+    SGS_CUDA(cudaMemsetAsync(u0, 0, 3 * l0.N * sizeof(T), stream));
+    if (n == 1) {
+      // single level: exact solve on level 0 (its b is the given right-hand side)
+      SGS_CUDA(cudaMemcpyAsync(l0.b.p, b0, 3 * l0.N * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+      bottom_solve<T>(0);
+      SGS_CUDA(cudaMemcpyAsync(u0, l0.u.p, 3 * l0.N * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+      return;
+    }
+    auto U = [&](int l) -> T* { return l == 0 ? u0 : lev<T>(l).u.p; };
+    auto B = [&](int l) -> const T* { return l == 0 ? b0 : lev<T>(l).b.p; };
+    for (int l = 0; l < n - 1; ++l) {
+      const bool smooth = l == 0 || l >= ex;
+      if (smooth) sweeps<T>(l, U(l), B(l), true);
+      Level<T>& c = lev<T>(l + 1);
+      SGS_CUDA(cudaMemsetAsync(c.u.p, 0, 3 * c.N * sizeof(T), stream));
+      SGS_CUDA(cudaMemsetAsync(c.b.p, 0, 3 * c.N * sizeof(T), stream));
+      Level<T>& d = lev<T>(l);
+      if (smooth) {
+        if (l == 0) {
+          level0<T, OP_RES>(nullptr, d.nb, U(0), nullptr, B(0), d.r.p, 0, 0);
+          if (rr) round3(d, d.r.p);
+        } else {
+          stencil<T, SOP_RES>(l, nullptr, d.nb, U(l), nullptr, B(l), d.r.p, 0, 0, rr ? 1 : 0);
+        }
+        restrict_to<T>(l + 1, d.r.p);
+      } else {
+        restrict_to<T>(l + 1, B(l));
+      }
+    }
+    bottom_solve<T>(n - 1);
+    for (int l = n - 2; l >= 0; --l) {
+      prolongate_to<T>(l, U(l));
+      if (l == 0 || l >= ex) sweeps<T>(l, U(l), B(l), false);
+    }
+  }
+
+  // ------------------------------------------------------------------ PCG
+  void dot(const double* a, const double* b, double* out);
+  void linf(const double* a, double* out);
+  void axpy(double* dst, double sign, int coef_slot, const double* xv, const double* yv);
+  void precondition();
+  void record_iteration();
+  void solve();
+  void pack_outputs(std::vector<double>& disp);
+  double sensitivity(const double* rho, double penalty, double emin, double* dc, double* se);
+};
+
+template <>
+Level<double>& Solver::lev<double>(int l) { return *L64[l]; }
+template <>
+Level<float>& Solver::lev<float>(int l) { return *L32[l]; }
+template <>
+const double* Solver::Edev<double>() { return E64.p; }
+template <>
+const float* Solver::Edev<float>() { return E32.p; }
+
+// ---------------------------------------------------------------------------
+// CG vector kernels
+// ---------------------------------------------------------------------------
+constexpr int RED_BLOCKS = 592, RED_THREADS = 256;  // 4 CTAs per SM on 148 SMs
+
+__global__ void dot_partial_kernel(const double* __restrict__ a, const double* __restrict__ b, long n,
+                                   double* __restrict__ part) {
+  __shared__ double sm[RED_THREADS / 32];
+  double s = 0;
+  for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) s += a[i] * b[i];
+  for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t += sm[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void linf_partial_kernel(const double* __restrict__ a, long n, double* __restrict__ part) {
+  __shared__ double sm[RED_THREADS / 32];
+  double s = 0;
+  for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) s = fmax(s, fabs(a[i]));
+  for (int o = 16; o; o >>= 1) s = fmax(s, __shfl_down_sync(0xffffffffu, s, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t = fmax(t, sm[w]);
+    part[blockIdx.x] = t;
+  }
+}
+
+// Fixed-order final reduction; op 0 = sum, 1 = max.  Also derives the PCG scalars:
+// what = 0: rho -> beta = rho/rho_old;  what = 1: sq -> alpha, -alpha, breakdown flag;
+// what = 2: norm.
+__global__ void finish_reduce_kernel(const double* __restrict__ part, int np, int op, double* scal, int what) {
+  __shared__ double sm[32];
+  double s = 0;
+  for (int i = threadIdx.x; i < np; i += 32) s = op ? fmax(s, part[i]) : s + part[i];
+  sm[threadIdx.x] = s;
+  __syncwarp();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < 32; ++w) t = op ? fmax(t, sm[w]) : t + sm[w];
+    if (what == 0) {
+      scal[0] = t;               // rho
+      scal[4] = t / scal[1];     // beta = rho / rho_old
+    } else if (what == 1) {
+      scal[2] = t;               // s.q
+      if (!(t > 0)) scal[7] = 1;  // indefinite or singular (CONJUGATE_GRADIENT.cpp:49-52)
+      scal[5] = scal[0] / t;     // alpha
+      scal[6] = -scal[5];
+    } else if (what == 2) {
+      scal[3] = t;
+    } else {
+      scal[8] = t;
+    }
+  }
+}
+
+__global__ void rho_shift_kernel(double* scal) { scal[1] = scal[0]; }
+
+// dst = c*x + y, c = scal[slot]; optionally in single precision like the
+// reference's float-rounded CG_VECTOR::Copy (CG_VECTOR.cpp:96-114)
+__global__ void axpy_kernel(double* dst, const double* __restrict__ scal, int slot, const double* xv, const double* yv,
+                            long n, int float_round) {
+  long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double c = scal[slot];
+  if (float_round) dst[i] = double(__fadd_rn(__fmul_rn(float(c), float(xv[i])), float(yv[i])));
+  else dst[i] = c * xv[i] + yv[i];
+}
+
+// r = r - q with optional float rounding (CG_VECTOR::operator-=, CG_VECTOR.cpp:35-52)
+__global__ void sub_kernel(double* r, const double* __restrict__ q, long n, int float_round) {
+  long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (float_round) r[i] = double(__fsub_rn(float(r[i]), float(q[i])));
+  else r[i] -= q[i];
+}
+
+__global__ void scatter_lift_kernel(double* u, const int* __restrict__ node, const int* __restrict__ axis,
+                                    const double* __restrict__ val, int n, long N) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) u[node[i] + axis[i] * N] = val[i];
+}
+
+__global__ void scatter_force_kernel(double* s, const int* __restrict__ node, const double* __restrict__ val, int n, long N) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int v = 0; v < 3; ++v) s[node[i] + v * N] = val[3 * i + v];
+}
+
+__global__ void add_kernel(double* a, const double* __restrict__ b, long n) {
+  long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) a[i] += b[i];
+}
+
+// Output packing (SPGrid_CPU_Solver.cpp:343-364): per input block node
+// (u_x, u_y, u_z, max_v |r_v|)
+__global__ void pack_kernel(int nin, const int* __restrict__ in_block, const int* __restrict__ in_zoff,
+                            const double* __restrict__ u, const double* __restrict__ r, long N, double* __restrict__ out) {
+  long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nin) * 64) return;
+  int b = int(t >> 6), e = int(t & 63);
+  int blk = in_block[b];
+  double* o = out + t * 4;
+  if (blk < 0) {
+    o[0] = o[1] = o[2] = o[3] = 0;
+    return;
+  }
+  int ii = e >> 4, jj = (e >> 2) & 3, kk = e & 3;
+  long n = long(blk) * 128 + ii * 32 + jj * 8 + (kk + in_zoff[b]);
+  double m = 0;
+  for (int v = 0; v < 3; ++v) {
+    o[v] = u[n + v * N];
+    m = fmax(m, fabs(r[n + v * N]));
+  }
+  o[3] = m;
+}
+
+// SIMP sensitivity per input-block cell (topo_opt/objective/minimal_compliance.cpp:86-146):
+// s_e = u_e^T (mu0 K_mu + lambda0 K_la) u_e (no dx), dc = p rho^(p-1) (1-Emin) s_e,
+// objective term s_e (Emin + rho^p (1-Emin)).
+__global__ void sensitivity_kernel(int nin, const int* __restrict__ in_block, const int* __restrict__ in_zoff,
+                                   const int* __restrict__ nbr, const double* __restrict__ u, long N,
+                                   const double* __restrict__ rho, double penalty, double emin, double* __restrict__ dc,
+                                   double* __restrict__ se, double* __restrict__ obj_part) {
+  long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  double objv = 0;
+  if (t < long(nin) * 64) {
+    int b = int(t >> 6), e = int(t & 63);
+    int blk = in_block[b];
+    double r = rho[t], s = 0;
+    if (blk >= 0 && r > 0) {
+      int x = e >> 4, y = (e >> 2) & 3, z = (e & 3) + in_zoff[b];
+      double ue[8][3];
+      for (int a = 0; a < 8; ++a) {
+        int nx = x + (a >> 2), ny = y + ((a >> 1) & 1), nz = z + (a & 1);
+        int d = (nx > 3 ? 2 : 1) * 9 + (ny > 3 ? 2 : 1) * 3 + (nz > 7 ? 2 : 1);
+        int nb = nbr[long(blk) * 27 + d];
+        for (int v = 0; v < 3; ++v)
+          ue[a][v] = nb < 0 ? 0.0 : u[long(nb) * 128 + ((nx & 3) << 5) + ((ny & 3) << 3) + (nz & 7) + v * N];
+      }
+      for (int a = 0; a < 8; ++a)
+        for (int bb = 0; bb < 8; ++bb) {
+          const int k = (a * 8 + bb) * 9;
+          for (int i = 0; i < 3; ++i)
+            s += ue[a][i] * (c_Kc64[k + i * 3] * ue[bb][0] + c_Kc64[k + i * 3 + 1] * ue[bb][1] + c_Kc64[k + i * 3 + 2] * ue[bb][2]);
+        }
+      dc[t] = s * pow(r, penalty - 1.0) * penalty * (1 - emin);
+      objv = s * (emin + pow(r, penalty) * (1 - emin));
+    } else {
+      dc[t] = 0;
+    }
+    se[t] = s;
+  }
+  // block partial of the objective (fixed order)
+  __shared__ double sm[256];
+  sm[threadIdx.x] = objv;
+  __syncthreads();
+  for (int o = 128; o; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) obj_part[blockIdx.x] = sm[0];
+}
+
+void Solver::dot(const double* a, const double* b, double* out_unused) {
+  (void)out_unused;
+  dot_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, stream>>>(a, b, 3 * N0(), red.p);
+  launch_counter += 1;
+}
+
+void Solver::linf(const double* a, double*) {
+  linf_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, stream>>>(a, 3 * N0(), red.p);
+  finish_reduce_kernel<<<1, 32, 0, stream>>>(red.p, RED_BLOCKS, 1, scal.p, 2);
+  launch_counter += 2;
+}
+
+void Solver::axpy(double* dst, double, int slot, const double* xv, const double* yv) {
+  axpy_kernel<<<blocks_for(3 * N0(), 256), 256, 0, stream>>>(dst, scal.p, slot, xv, yv, 3 * N0(), round_ref() ? 1 : 0);
+  ++launch_counter;
+}
+
+// z = M^-1 r into q (z and q share storage, SPGrid_CPU_Solver.cpp:91-92), then
+// Project and Project_Nullspace (KRYLOV_SYSTEM_BASE.cpp:25-31)
+void Solver::precondition() {
+  Level<double>& l0 = *L64[0];
+  const long N = l0.N;
+  if (P.disable_mg) {
+    SGS_CUDA(cudaMemcpyAsync(q.p, f.p, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  } else if (mixed()) {
+    Level<float>& m0 = *L32[0];
+    convert_kernel<float, double><<<blocks_for(3 * N, 256), 256, 0, stream>>>(m0.b.p, f.p, 3 * N);
+    vcycle<float>(m0.b.p, m0.u.p);
+    convert_kernel<double, float><<<blocks_for(3 * N, 256), 256, 0, stream>>>(q.p, m0.u.p, 3 * N);
+    launch_counter += 2;
+  } else {
+    vcycle<double>(f.p, q.p);
+  }
+  project<double>(l0, q.p);
+  project_null<double>(l0, q.p);
+}
+
+// One PCG iteration after the convergence test (CONJUGATE_GRADIENT.cpp:41-57) plus
+// the next iteration's Project_Nullspace and norm (:32-33).
+void Solver::record_iteration() {
+  Level<double>& l0 = *L64[0];
+  precondition();
+  dot_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, stream>>>(q.p, f.p, 3 * N0(), red.p);
+  finish_reduce_kernel<<<1, 32, 0, stream>>>(red.p, RED_BLOCKS, 0, scal.p, 0);
+  axpy(s.p, 1, 4, s.p, q.p);  // s = beta*s + z
+  level0<double, OP_KU>(nullptr, l0.nb, s.p, nullptr, nullptr, q.p, 0, 0);
+  project<double>(l0, q.p);
+  dot_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, stream>>>(s.p, q.p, 3 * N0(), red.p);
+  finish_reduce_kernel<<<1, 32, 0, stream>>>(red.p, RED_BLOCKS, 0, scal.p, 1);
+  axpy(x.p, 1, 5, s.p, x.p);   // x = alpha*s + x
+  axpy(f.p, 1, 6, q.p, f.p);   // r = -alpha*q + r
+  rho_shift_kernel<<<1, 1, 0, stream>>>(scal.p);
+  project_null<double>(l0, f.p);
+  linf(f.p, nullptr);
+  launch_counter += 5;
+}
+
+void Solver::solve() {
+  Level<double>& l0 = *L64[0];
+  const long N = l0.N, n3 = 3 * N;
+  const int fr = round_ref() ? 1 : 0;
+  history.clear();
+  iterations = 0;
+  // u = g on the listed Dirichlet nodes (SPGrid_CPU_Solver.cpp:241-285)
+  x.zero(stream);
+  if (!P.lift_node.empty())
+    scatter_lift_kernel<<<blocks_for(long(P.lift_node.size()), 128), 128, 0, stream>>>(
+        x.p, lift_node.p, lift_axis.p, lift_val.p, int(P.lift_node.size()), N);
+  // s = forces; Project; Project_Nullspace; f = s - K u; Project (:287-301)
+  s.zero(stream);
+  if (!P.force_node.empty())
+    scatter_force_kernel<<<blocks_for(long(P.force_node.size()), 128), 128, 0, stream>>>(
+        s.p, force_node.p, force_val.p, int(P.force_node.size()), N);
+  project<double>(l0, s.p);
+  project_null<double>(l0, s.p);
+  level0<double, OP_RES>(nullptr, l0.nb, x.p, nullptr, s.p, f.p, 0, 0);
+  project<double>(l0, f.p);
+  SGS_CUDA(cudaMemcpyAsync(ubk.p, x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  q.zero(stream);
+  s.zero(stream);
+  linf(f.p, nullptr);
+  SGS_CUDA(cudaMemcpyAsync(h_scal, scal.p, 16 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  initial_residual = h_scal[3];
+  const double tol = P.tolerance * initial_residual;
+  auto t0 = std::chrono::steady_clock::now();
+  x.zero(stream);
+  // CONJUGATE_GRADIENT_4Ch::Solve: q = K x (= 0); r -= q; Project(r)
+  level0<double, OP_KU>(nullptr, l0.nb, x.p, nullptr, nullptr, q.p, 0, 0);
+  sub_kernel<<<blocks_for(n3, 256), 256, 0, stream>>>(f.p, q.p, n3, fr);
+  project<double>(l0, f.p);
+  double init_scal[16] = {0};
+  init_scal[1] = 3.40282346638528859811704183484516925440e+38;  // FLT_MAX (rho_old)
+  SGS_CUDA(cudaMemcpyAsync(scal.p, init_scal, sizeof(init_scal), cudaMemcpyHostToDevice, stream));
+  project_null<double>(l0, f.p);
+  linf(f.p, nullptr);
+  // capture one iteration as a CUDA graph
+  if (!iter_graph) {
+    cudaGraph_t g;
+    long before = launch_counter;
+    SGS_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    record_iteration();
+    SGS_CUDA(cudaStreamEndCapture(stream, &g));
+    SGS_CUDA(cudaGraphInstantiate(&iter_graph, g, 0));
+    SGS_CUDA(cudaGraphDestroy(g));
+    launches_per_iteration = launch_counter - before;
+  }
+  const double* norm_slot = scal.p + 3;
+  for (int it = 0;; ++it) {
+    SGS_CUDA(cudaMemcpyAsync(h_scal, scal.p, 16 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    (void)norm_slot;
+    const double norm = h_scal[3];
+    history.push_back(norm);
+    if (h_scal[7] != 0) {
+      iterations = it;
+      final_residual = norm;
+      throw CudaError("CG detected an indefinite or singular operator", SGS_ERR_BREAKDOWN);
+    }
+    if (!std::isfinite(norm)) {
+      iterations = it;
+      throw CudaError("non-finite residual", SGS_ERR_BREAKDOWN);
+    }
+    if (norm <= tol || it == P.max_iterations) {
+      iterations = it;
+      final_residual = norm;
+      break;
+    }
+    SGS_CUDA(cudaGraphLaunch(iter_graph, stream));
+  }
+  add_kernel<<<blocks_for(n3, 256), 256, 0, stream>>>(x.p, ubk.p, n3);
+  SGS_CUDA(cudaGetLastError());
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void Solver::pack_outputs(std::vector<double>& disp) {
+  const long nin = long(P.in_block.size());
+  disp.assign(size_t(nin) * 256, 0.0);
+  if (nin == 0) return;
+  pack_kernel<<<blocks_for(nin * 64, 256), 256, 0, stream>>>(int(nin), in_block.p, in_zoff.p, x.p, f.p, N0(), out_disp.p);
+  SGS_CUDA(cudaMemcpyAsync(disp.data(), out_disp.p, disp.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+double Solver::sensitivity(const double* rho_host, double penalty, double emin, double* dc_host, double* se_host) {
+  const long nin = long(P.in_block.size());
+  if (nin == 0) return 0;
+  DevBuf<double> rho, dc, se, part;
+  rho.upload(rho_host, size_t(nin) * 64, stream);
+  dc.alloc(size_t(nin) * 64);
+  se.alloc(size_t(nin) * 64);
+  const unsigned nblk = blocks_for(nin * 64, 256);
+  part.alloc(nblk);
+  sensitivity_kernel<<<nblk, 256, 0, stream>>>(int(nin), in_block.p, in_zoff.p, L64[0]->nbr.p, x.p, N0(), rho.p, penalty,
+                                               emin, dc.p, se.p, part.p);
+  std::vector<double> hp(nblk);
+  SGS_CUDA(cudaMemcpyAsync(dc_host, dc.p, nin * 64 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  if (se_host) SGS_CUDA(cudaMemcpyAsync(se_host, se.p, nin * 64 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaMemcpyAsync(hp.data(), part.p, nblk * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  double obj = 0;
+  for (double v : hp) obj += v;
+  return obj;
+}
+
+}  // namespace sgs
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace sgs;
+
+struct sgs_session {
+  std::unique_ptr<Solver> solver;
+  std::string error;
+};
+
+static void set_err(char* buf, int len, const std::string& m) {
+  if (buf && len > 0) std::snprintf(buf, size_t(len), "%s", m.c_str());
+}
+
+static int session_from_inputs(const FEMInputs& in, int precision, sgs_session** out, std::string* err) {
+  std::unique_ptr<sgs_session> h(new sgs_session());
+  h->solver.reset(new Solver());
+  int code = 0;
+  std::string m = build_problem(in, h->solver->P, &code);
+  if (!m.empty()) {
+    *err = m;
+    return code ? code : SGS_ERR_INPUT;
+  }
+  h->solver->P.max_iterations = 500;  // the reference hard-codes 500 (SPGrid_CPU_Solver.cpp:326)
+  if (in.get_int("sgs_honor_max_iterations", 0)) h->solver->P.max_iterations = in.krylov.max_iterations;
+  if (precision == SGS_HOST_SETUP_ONLY) {  // inspection of the host-side hierarchy, no device work
+    h->solver->precision = precision;
+    *out = h.release();
+    return 0;
+  }
+  try {
+    h->solver->init(precision);
+  } catch (const CudaError& e) {
+    *err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    *err = e.what();
+    return SGS_ERR_INTERNAL;
+  }
+  *out = h.release();
+  return 0;
+}
+
+// host compact [3][N] <-> device level field
+template <typename T>
+static void put_field(Solver& S, T* dst, const double* src, long N) {
+  std::vector<T> tmp(size_t(3 * N));
+  for (long i = 0; i < 3 * N; ++i) tmp[i] = T(src[i]);
+  SGS_CUDA(cudaMemcpyAsync(dst, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice, S.stream));
+  SGS_CUDA(cudaStreamSynchronize(S.stream));
+}
+template <typename T>
+static void get_field(Solver& S, double* dst, const T* src, long N) {
+  std::vector<T> tmp(size_t(3 * N));
+  SGS_CUDA(cudaMemcpyAsync(tmp.data(), src, tmp.size() * sizeof(T), cudaMemcpyDeviceToHost, S.stream));
+  SGS_CUDA(cudaStreamSynchronize(S.stream));
+  for (long i = 0; i < 3 * N; ++i) dst[i] = double(tmp[i]);
+}
+
+template <typename T>
+static int apply_op(Solver& S, int op, int level, int arg, const double* in, const double* in2, double* out) {
+  const int n = S.nlev();
+  if (level < 0 || level >= n) return SGS_ERR_INPUT;
+  Level<T>& d = S.lev<T>(level);
+  const long N = d.N;
+  switch (op) {
+    case 0:
+    case 1:
+      if (level != 0) return SGS_ERR_INPUT;
+      put_field<T>(S, d.u.p, in, N);
+      if (op == 1) put_field<T>(S, d.b.p, in2, N);
+      if (op == 0) S.level0<T, OP_KU>(nullptr, d.nb, d.u.p, nullptr, nullptr, d.r.p, 0, 0);
+      else S.level0<T, OP_RES>(nullptr, d.nb, d.u.p, nullptr, d.b.p, d.r.p, 0, 0);
+      get_field<T>(S, out, d.r.p, N);
+      return 0;
+    case 2:
+      if (level != 0 && !d.has_matrix) return SGS_ERR_INPUT;
+      put_field<T>(S, d.u.p, in, N);
+      put_field<T>(S, d.b.p, in2, N);
+      S.sweep<T>(level, d.u.p, d.b.p, arg & 1, (arg >> 1) & 1);
+      get_field<T>(S, out, d.u.p, N);
+      return 0;
+    case 3:
+      if (level + 1 >= n) return SGS_ERR_INPUT;
+      put_field<T>(S, d.r.p, in, N);
+      S.restrict_to<T>(level + 1, d.r.p);
+      get_field<T>(S, out, S.lev<T>(level + 1).b.p, S.lev<T>(level + 1).N);
+      return 0;
+    case 4:
+      if (level + 1 >= n) return SGS_ERR_INPUT;
+      put_field<T>(S, S.lev<T>(level + 1).u.p, in, S.lev<T>(level + 1).N);
+      put_field<T>(S, d.r.p, in2, N);
+      S.prolongate_to<T>(level, d.r.p);
+      get_field<T>(S, out, d.r.p, N);
+      return 0;
+    case 5:
+      if (!d.has_matrix) return SGS_ERR_INPUT;
+      put_field<T>(S, d.u.p, in, N);
+      S.stencil<T, SOP_MUL>(level, nullptr, d.nb, d.u.p, nullptr, nullptr, d.r.p, 0, 0, 0);
+      get_field<T>(S, out, d.r.p, N);
+      return 0;
+    case 6:
+      if (level != n - 1 || S.P.disable_mg) return SGS_ERR_INPUT;
+      put_field<T>(S, d.b.p, in, N);
+      S.bottom_solve<T>(level);
+      get_field<T>(S, out, d.u.p, N);
+      return 0;
+    case 7: {
+      if (level != 0) return SGS_ERR_INPUT;
+      std::vector<double> tmp(in, in + 3 * N);
+      SGS_CUDA(cudaMemcpyAsync(S.f.p, tmp.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+      S.precondition();
+      SGS_CUDA(cudaMemcpyAsync(out, S.q.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+      SGS_CUDA(cudaStreamSynchronize(S.stream));
+      return 0;
+    }
+  }
+  return SGS_ERR_INPUT;
+}
+
+extern "C" {
+
+SGS_API int sgs_create(const void* input_blob, int precision, sgs_session** out, char* err, int errlen) {
+  if (!input_blob || !out) return SGS_ERR_INPUT;
+  *out = nullptr;
+  if (precision < 0 || precision > SGS_HOST_SETUP_ONLY) {
+    set_err(err, errlen, "precision must be 0 (reference), 1 (fp64), 2 (mixed) or 3 (host set-up only)");
+    return SGS_ERR_INPUT;
+  }
+  try {
+    FEMInputs in = decode_inputs(input_blob);
+    std::string m;
+    int rc = session_from_inputs(in, precision, out, &m);
+    if (rc) set_err(err, errlen, m);
+    return rc;
+  } catch (const WireError& e) {
+    set_err(err, errlen, std::string("malformed input blob: ") + e.what());
+    return SGS_ERR_WIRE;
+  } catch (const std::exception& e) {
+    set_err(err, errlen, e.what());
+    return SGS_ERR_INTERNAL;
+  }
+}
+
+SGS_API void sgs_destroy(sgs_session* h) { delete h; }
+
+SGS_API const char* sgs_last_error(sgs_session* h) { return h ? h->error.c_str() : ""; }
+
+static bool host_only(sgs_session* h) { return h->solver->precision == SGS_HOST_SETUP_ONLY; }
+
+SGS_API int sgs_solve(sgs_session* h, double tolerance, int max_iterations, sgs_stats* stats) {
+  if (!h || host_only(h)) return SGS_ERR_INPUT;
+  Solver& S = *h->solver;
+  if (tolerance > 0) S.P.tolerance = tolerance;
+  if (max_iterations > 0) S.P.max_iterations = max_iterations;
+  int rc = 0;
+  try {
+    S.solve();
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    rc = e.code;
+  } catch (const std::exception& e) {
+    h->error = e.what();
+    rc = SGS_ERR_INTERNAL;
+  }
+  if (stats) {
+    stats->iterations = S.iterations;
+    stats->levels = S.nlev();
+    stats->initial_residual = S.initial_residual;
+    stats->final_residual = S.final_residual;
+    stats->setup_seconds = S.setup_seconds;
+    stats->solve_seconds = S.solve_seconds;
+    stats->launches_per_iteration = S.launches_per_iteration;
+    stats->dof = 3 * S.N0();
+    stats->bottom_unknowns = S.bottom.n;
+  }
+  return rc;
+}
+
+SGS_API int sgs_residual_history(sgs_session* h, double* out, int cap) {
+  if (!h) return 0;
+  int n = int(h->solver->history.size());
+  for (int i = 0; i < n && i < cap; ++i) out[i] = h->solver->history[i];
+  return n;
+}
+
+SGS_API int sgs_displacements(sgs_session* h, double* out) {
+  if (!h || !out || host_only(h)) return SGS_ERR_INPUT;
+  try {
+    std::vector<double> d;
+    h->solver->pack_outputs(d);
+    std::memcpy(out, d.data(), d.size() * sizeof(double));
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+SGS_API double sgs_sensitivity(sgs_session* h, const double* density, double* dc, double* element_energy) {
+  if (!h || !density || !dc || host_only(h)) return std::nan("");
+  try {
+    return h->solver->sensitivity(density, h->solver->P.penalty, h->solver->P.minimum_stiffness, dc, element_energy);
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return std::nan("");
+  }
+}
+
+SGS_API int sgs_level_count(sgs_session* h) { return h ? h->solver->nlev() : 0; }
+
+SGS_API int sgs_level_blocks(sgs_session* h, int level, int32_t* coords) {
+  if (!h || level < 0 || level >= h->solver->nlev()) return -1;
+  const HostLevel& L = h->solver->P.levels[level];
+  if (coords) std::memcpy(coords, L.coords.data(), size_t(L.nb) * 3 * sizeof(int32_t));
+  return L.nb;
+}
+
+SGS_API int sgs_level_flags(sgs_session* h, int level, uint32_t* flags) {
+  if (!h || level < 0 || level >= h->solver->nlev()) return -1;
+  const HostLevel& L = h->solver->P.levels[level];
+  std::memcpy(flags, L.flags.data(), size_t(L.nb) * NODES_PER_BLOCK * sizeof(uint32_t));
+  return 0;
+}
+
+SGS_API int sgs_boundary_blocks(sgs_session* h, int level, int32_t* ordinals) {
+  if (!h || level < 0 || level >= h->solver->nlev()) return -1;
+  const HostLevel& L = h->solver->P.levels[level];
+  if (ordinals) std::memcpy(ordinals, L.boundary.data(), L.boundary.size() * sizeof(int32_t));
+  return int(L.boundary.size());
+}
+
+SGS_API int sgs_apply(sgs_session* h, int op, int level, int arg, const double* in, const double* in2, double* out) {
+  if (!h || !in || !out || host_only(h)) return SGS_ERR_INPUT;
+  try {
+    if (op == 7) return apply_op<double>(*h->solver, op, level, arg, in, in2, out);
+    return h->solver->mixed() ? apply_op<float>(*h->solver, op, level, arg, in, in2, out)
+                              : apply_op<double>(*h->solver, op, level, arg, in, in2, out);
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+}
+
+SGS_API int sgs_level_stencils(sgs_session* h, int level, double* out, uint32_t* spokes) {
+  if (!h || host_only(h) || level < 0 || level >= h->solver->nlev()) return SGS_ERR_INPUT;
+  Level<double>& d = *h->solver->L64[level];
+  if (!d.has_matrix) return SGS_ERR_INPUT;
+  try {
+    std::vector<double> planes(size_t(243) * d.N);
+    SGS_CUDA(cudaMemcpyAsync(planes.data(), d.A.p, planes.size() * sizeof(double), cudaMemcpyDeviceToHost, h->solver->stream));
+    if (spokes) SGS_CUDA(cudaMemcpyAsync(spokes, d.spokes.p, d.N * 4, cudaMemcpyDeviceToHost, h->solver->stream));
+    SGS_CUDA(cudaStreamSynchronize(h->solver->stream));
+    for (long n = 0; n < d.N; ++n)
+      for (int k = 0; k < 243; ++k) out[n * 243 + k] = planes[size_t(k) * d.N + n];
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+// Drop-in entry (see include/spgrid_fem.h).
+SGS_API void fem_solve(void* input, void* output) {
+  if (!output) return;
+  void** out_ptr = reinterpret_cast<void**>(output);
+  *out_ptr = nullptr;
+  FEMOutputs outs;
+  outs.success = false;
+  try {
+    FEMInputs in = decode_inputs(input);
+    for (int v = 0; v < 3; ++v) outs.displacements.resolution[v] = in.resolution[v];
+    const int precision = in.get_int("sgs_precision", PREC_REFERENCE);
+    sgs_session* h = nullptr;
+    std::string err;
+    int rc = (precision < 0 || precision > 2) ? SGS_ERR_INPUT : session_from_inputs(in, precision, &h, &err);
+    if (rc) {
+      outs.error_code = rc;
+      outs.info = err.empty() ? "invalid sgs_precision" : err;
+    } else {
+      std::unique_ptr<sgs_session> guard(h);
+      sgs_stats st{};
+      rc = sgs_solve(h, 0, 0, &st);
+      outs.residuals = h->solver->history;
+      outs.extra_ints["iterations"] = st.iterations;
+      outs.extra_doubles["initial_residual"] = st.initial_residual;
+      outs.extra_doubles["final_residual"] = st.final_residual;
+      outs.extra_doubles["setup_seconds"] = st.setup_seconds;
+      outs.extra_doubles["solve_seconds"] = st.solve_seconds;
+      if (rc) {
+        outs.error_code = rc;
+        outs.info = h->error;
+      } else {
+        const size_t nin = in.density.num_blocks();
+        outs.displacements.base.assign(in.density.base.begin(), in.density.base.end());
+        outs.displacements.data.resize(nin * 256);
+        rc = sgs_displacements(h, outs.displacements.data.data());
+        if (rc) {
+          outs.displacements.base.clear();
+          outs.displacements.data.clear();
+          outs.error_code = rc;
+          outs.info = h->error;
+        } else {
+          outs.success = true;
+          char m[200];
+          std::snprintf(m, sizeof m, "converged in %d iterations, L-inf residual %.6g of %.6g", st.iterations,
+                        st.final_residual, st.initial_residual);
+          outs.info = m;
+        }
+      }
+    }
+  } catch (const WireError& e) {
+    outs.error_code = SGS_ERR_WIRE;
+    outs.info = std::string("malformed input blob: ") + e.what();
+  } catch (const std::exception& e) {
+    outs.error_code = SGS_ERR_INTERNAL;
+    outs.info = e.what();
+  }
+  try {
+    *out_ptr = encode_outputs(outs, nullptr);
+  } catch (...) {
+    *out_ptr = nullptr;
+  }
+}
+
+SGS_API void fem_solve_free(void* blob) { delete[] static_cast<char*>(blob); }
+
+SGS_API int sgs_codec_roundtrip(const void* blob, int which, void** out) {
+  if (!blob || !out) return SGS_ERR_INPUT;
+  *out = nullptr;
+  try {
+    if (which == 0) {
+      std::vector<uint8_t> b = encode_inputs(decode_inputs(blob));
+      char* o = new char[b.size()];
+      std::memcpy(o, b.data(), b.size());
+      *out = o;
+    } else {
+      *out = encode_outputs(decode_outputs(blob), nullptr);
+    }
+  } catch (const WireError&) {
+    return SGS_ERR_WIRE;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,224 @@
+"""ctypes binding of libspgrid_gpu_solver.so (the C ABI of include/spgrid_fem.h).
+
+There is no CPU fallback: if the CUDA library is missing or no GPU is present,
+the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import fem_interface as fi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libspgrid_gpu_solver.so")
+
+PRECISION_REFERENCE, PRECISION_FP64, PRECISION_MIXED, HOST_SETUP_ONLY = 0, 1, 2, 3
+OP_KU, OP_RESIDUAL, OP_SMOOTH, OP_RESTRICT, OP_PROLONG, OP_STENCIL, OP_BOTTOM, OP_VCYCLE = range(8)
+
+EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", "sgs_last_error", "sgs_solve",
+                    "sgs_residual_history", "sgs_displacements", "sgs_sensitivity", "sgs_level_count",
+                    "sgs_level_blocks", "sgs_level_flags", "sgs_boundary_blocks", "sgs_apply", "sgs_level_stencils",
+                    "sgs_codec_roundtrip")
+
+
+class SolverError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class Stats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("levels", C.c_int32), ("initial_residual", C.c_double),
+                ("final_residual", C.c_double), ("setup_seconds", C.c_double), ("solve_seconds", C.c_double),
+                ("launches_per_iteration", C.c_int64), ("dof", C.c_int64), ("bottom_unknowns", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load(build_if_missing: bool = False):
+    """Load the CUDA library; raises if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if build_if_missing:
+            from .build import build
+            build()
+        else:
+            raise ImportError(f"{LIB_PATH} is not built; run `python -m spgrid_topo_opt_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    L.fem_solve.argtypes = [P, P]
+    L.fem_solve.restype = None
+    L.fem_solve_free.argtypes = [P]
+    L.sgs_create.argtypes = [P, C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
+    L.sgs_create.restype = C.c_int
+    L.sgs_destroy.argtypes = [P]
+    L.sgs_last_error.argtypes = [P]
+    L.sgs_last_error.restype = C.c_char_p
+    L.sgs_solve.argtypes = [P, C.c_double, C.c_int, C.POINTER(Stats)]
+    L.sgs_residual_history.argtypes = [P, P, C.c_int]
+    L.sgs_displacements.argtypes = [P, P]
+    L.sgs_sensitivity.argtypes = [P, P, P, P]
+    L.sgs_sensitivity.restype = C.c_double
+    L.sgs_level_count.argtypes = [P]
+    L.sgs_level_blocks.argtypes = [P, C.c_int, P]
+    L.sgs_level_flags.argtypes = [P, C.c_int, P]
+    L.sgs_boundary_blocks.argtypes = [P, C.c_int, P]
+    L.sgs_apply.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P, P]
+    L.sgs_level_stencils.argtypes = [P, C.c_int, P, P]
+    L.sgs_codec_roundtrip.argtypes = [P, C.c_int, C.POINTER(C.c_void_p)]
+    _lib = L
+    return L
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def fem_solve_blob(blob: bytes) -> bytes:
+    """Call the drop-in ``fem_solve`` entry with a serialized FEMInputs blob and
+    return the serialized FEMOutputs blob (ownership handled as the reference's
+    FEMInterface::run does, fem_interface.h:464-478)."""
+    L = load()
+    buf = C.create_string_buffer(bytes(blob), len(blob))
+    out = C.c_void_p(0)
+    L.fem_solve(C.cast(buf, C.c_void_p), C.cast(C.pointer(out), C.c_void_p))
+    if not out.value:
+        raise SolverError(11, "fem_solve returned no output blob")
+    try:
+        n = C.cast(out, C.POINTER(C.c_uint64))[0]
+        data = C.string_at(out.value, n)
+    finally:
+        L.fem_solve_free(out)
+    return data
+
+
+def codec_roundtrip(blob: bytes, which: int = 0) -> bytes:
+    """Decode and re-encode a blob with the C++ codec (0 inputs, 1 outputs)."""
+    L = load()
+    buf = C.create_string_buffer(bytes(blob), len(blob))
+    out = C.c_void_p(0)
+    rc = L.sgs_codec_roundtrip(C.cast(buf, C.c_void_p), which, C.byref(out))
+    if rc != 0:
+        raise SolverError(rc, "codec rejected the blob")
+    try:
+        n = C.cast(out, C.POINTER(C.c_uint64))[0]
+        return C.string_at(out.value, n)
+    finally:
+        L.fem_solve_free(out)
+
+
+def fem_solve(inputs: fi.FEMInputs) -> fi.FEMOutputs:
+    """Serialize, solve on the GPU, deserialize (FEMInterface::run equivalent)."""
+    return fi.deserialize_outputs(fem_solve_blob(fi.serialize_inputs(inputs)))
+
+
+class Session:
+    """A problem resident on the GPU: set-up once, solve, read back."""
+
+    def __init__(self, inputs, precision: int = PRECISION_REFERENCE):
+        L = load()
+        blob = inputs if isinstance(inputs, (bytes, bytearray)) else fi.serialize_inputs(inputs)
+        self.inputs = inputs if not isinstance(inputs, (bytes, bytearray)) else fi.deserialize_inputs(blob)
+        self._blob = C.create_string_buffer(bytes(blob), len(blob))
+        h = C.c_void_p(0)
+        err = C.create_string_buffer(512)
+        rc = L.sgs_create(C.cast(self._blob, C.c_void_p), precision, C.byref(h), err, 512)
+        if rc != 0:
+            raise SolverError(rc, err.value.decode(errors="replace"))
+        self.h = h
+        self.precision = precision
+        self.stats: Optional[dict] = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().sgs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise SolverError(rc, load().sgs_last_error(self.h).decode(errors="replace"))
+
+    def solve(self, tolerance: float = 0.0, max_iterations: int = 0) -> dict:
+        st = Stats()
+        self._check(load().sgs_solve(self.h, tolerance, max_iterations, C.byref(st)))
+        self.stats = st.as_dict()
+        return self.stats
+
+    def history(self) -> np.ndarray:
+        out = np.zeros(1024)
+        n = load().sgs_residual_history(self.h, _ptr(out), 1024)
+        return out[:min(n, 1024)].copy()
+
+    def displacements(self) -> np.ndarray:
+        nb = self.inputs.density.base.shape[0]
+        out = np.zeros((nb, 64, 4))
+        self._check(load().sgs_displacements(self.h, _ptr(out)))
+        return out
+
+    def sensitivity(self, density: Optional[np.ndarray] = None):
+        rho = np.ascontiguousarray(self.inputs.density.data if density is None else density, np.float64)
+        dc = np.zeros(rho.shape)
+        se = np.zeros(rho.shape)
+        obj = load().sgs_sensitivity(self.h, _ptr(rho), _ptr(dc), _ptr(se))
+        if not np.isfinite(obj):
+            raise SolverError(10, load().sgs_last_error(self.h).decode(errors="replace"))
+        return obj, dc, se
+
+    # ---- inspection / unit operators
+    @property
+    def levels(self) -> int:
+        return load().sgs_level_count(self.h)
+
+    def blocks(self, level: int) -> np.ndarray:
+        n = load().sgs_level_blocks(self.h, level, None)
+        out = np.zeros((n, 3), np.int32)
+        load().sgs_level_blocks(self.h, level, _ptr(out))
+        return out
+
+    def flags(self, level: int) -> np.ndarray:
+        n = self.blocks(level).shape[0]
+        out = np.zeros(n * 128, np.uint32)
+        load().sgs_level_flags(self.h, level, _ptr(out))
+        return out
+
+    def boundary_blocks(self, level: int) -> np.ndarray:
+        n = load().sgs_boundary_blocks(self.h, level, None)
+        out = np.zeros(n, np.int32)
+        load().sgs_boundary_blocks(self.h, level, _ptr(out))
+        return out
+
+    def apply(self, op: int, level: int, x: np.ndarray, x2: Optional[np.ndarray] = None, arg: int = 0,
+              out_level: Optional[int] = None) -> np.ndarray:
+        ol = level if out_level is None else out_level
+        n = self.blocks(ol).shape[0] * 128
+        out = np.zeros((3, n))
+        x = np.ascontiguousarray(x, np.float64)
+        x2 = None if x2 is None else np.ascontiguousarray(x2, np.float64)
+        self._check(load().sgs_apply(self.h, op, level, arg, _ptr(x), _ptr(x2), _ptr(out)))
+        return out
+
+    def stencils(self, level: int):
+        n = self.blocks(level).shape[0] * 128
+        out = np.zeros((n, 243))
+        sp = np.zeros(n, np.uint32)
+        self._check(load().sgs_level_stencils(self.h, level, _ptr(out), _ptr(sp)))
+        return out, sp

@@ -1,0 +1,79 @@
+"""Host-side pieces of the CUDA library, checked without a GPU: the exported C ABI,
+the C++ codec against the reference's golden blobs, the error paths of fem_solve
+that fail before any device work, and the host-built hierarchy (page order,
+flags, boundary band) against the oracle."""
+import gzip
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, MODE_FP64
+from spgrid_topo_opt_b200 import configs, native
+from spgrid_topo_opt_b200 import fem_interface as fi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+def test_library_exports_every_declared_symbol(native_lib):
+    header = open(os.path.join(ROOT, "include", "spgrid_fem.h")).read()
+    declared = set(re.findall(r"SGS_API\s+[\w\s\*]+?\b(\w+)\s*\(", header))
+    assert {"fem_solve", "fem_solve_free", "sgs_create", "sgs_apply"} <= declared
+    for name in declared:
+        assert hasattr(native_lib, name), name
+    assert set(native.EXPORTED_SYMBOLS) == declared
+
+
+@pytest.mark.parametrize("name,which", [("kat_inputs.bin.gz", 0), ("kat_outputs.bin.gz", 1)])
+def test_cpp_codec_is_byte_compatible(native_lib, name, which):
+    blob = gzip.open(os.path.join(GOLD, name)).read()
+    assert native.codec_roundtrip(blob, which) == blob
+
+
+def _fem_outputs(blob):
+    return fi.deserialize_outputs(native.fem_solve_blob(blob))
+
+
+def test_fem_solve_reports_malformed_blob(native_lib):
+    blob = bytearray(gzip.open(os.path.join(GOLD, "kat_inputs.bin.gz")).read())
+    blob[8] = 9  # version_major
+    out = _fem_outputs(bytes(blob))
+    assert not out.success and out.error_code == 9 and "malformed" in out.info
+
+
+def test_fem_solve_rejects_mg_level_two(native_lib):
+    inp = configs.to_inputs(configs.cantilever_box(8), mg_level=2)
+    out = _fem_outputs(fi.serialize_inputs(inp))
+    assert not out.success and out.error_code == 3
+
+
+def test_fem_solve_rejects_padding_violation(native_lib):
+    inp = configs.to_inputs(configs.cantilever_box(8))
+    inp.resolution = [24, 24, 24]  # blocks now sit on the upper padding
+    out = _fem_outputs(fi.serialize_inputs(inp))
+    assert not out.success and out.error_code in (4, 6)
+
+
+def test_fem_solve_rejects_missing_neighbour_blocks(native_lib):
+    inp = configs.to_inputs(configs.cantilever_box(8))
+    keep = ~np.all(inp.density.base == inp.density.base.max(axis=0), axis=1)
+    inp.density.base = inp.density.base[keep]
+    inp.density.data = inp.density.data[keep]
+    inp.density.data[:] = np.where(inp.density.data > 0, inp.density.data, 0.1)  # material up to the edge
+    out = _fem_outputs(fi.serialize_inputs(inp))
+    assert not out.success and out.error_code == 5
+
+
+@pytest.mark.parametrize("problem", ["cantilever", "shell"])
+def test_host_hierarchy_matches_oracle(native_lib, problem):
+    prob = configs.cantilever_box(16, bottom_size=4) if problem == "cantilever" else configs.sphere_shell(24, bottom_size=4)
+    inp = configs.to_inputs(prob)
+    ref = Oracle(inp, mode=MODE_FP64)
+    ses = native.Session(inp, precision=native.HOST_SETUP_ONLY)
+    assert ses.levels == ref.levels
+    for lev in range(ref.levels):
+        assert np.array_equal(ses.blocks(lev), ref.blocks(lev)), lev
+        assert np.array_equal(ses.flags(lev), ref.flags(lev)), lev
+        assert np.array_equal(ses.boundary_blocks(lev), ref.boundary_blocks(lev)), lev
