@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark: MGPCG time-to-solution and MDOF/s to a relative L-inf residual of
+1e-6 on one B200, mixed precision (FP32 V-cycle, FP64 outer PCG) against the
+same GPU's plain FP64 MGPCG, on the narrow-band sphere-shell workload (256^3
+grid, shell radii 0.4-0.5, seeded smoothed-noise density).
+
+One step = one complete PCG solve (first residual to convergence) of the
+resident problem; set-up (flags, Galerkin operators, bottom inverse) is done
+once before the timed region and reported separately.  MDOF/s = 3 * nodes of
+the active level-0 blocks / solve time / 1e6.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs (torchrun, one process per GPU) solve an independent replica per
+rank: the solve does not shard ("replicas only"), so per-GPU work is fixed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MGPCG time & MDOF/s to rel.res 1e-6: mixed-prec vs FP64, same B200"
+TOL = 1e-6
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256, help="grid size of the shell workload")
+    ap.add_argument("--bottom-size", type=int, default=8)
+    ap.add_argument("--cpu-sample-n", type=int, default=64, help="grid size of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n: int, bottom: int):
+    from spgrid_topo_opt_b200 import configs
+    prob = configs.sphere_shell(n, bottom_size=bottom)
+    inp = configs.to_inputs(prob, tolerance=TOL)
+    return prob, inp
+
+
+def config_dict(args, inp, extra=None):
+    d = {"workload": f"sphere_shell{args.n}", "grid": [args.n] * 3, "shell_radii": [0.4, 0.5],
+         "density": "clamp(0.5+0.3*smoothed uniform noise, 1e-3, 1), seed 1234", "mg_level": int(inp.mg_level),
+         "smoothing": [int(inp.pre_and_post_smoothing_iter), int(inp.extra_ints["boundary_smoothing"])],
+         "tolerance": TOL, "stopping_rule": "L-inf residual <= tol * zero-guess L-inf residual",
+         "blocks": int(inp.density.base.shape[0]), "l2": "flushed (256 MiB write) before every timed solve"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(args):
+    """The oracle port (CPU restatement of the reference solver, FP64) timed on a
+    bounded sample of the same workload: a complete solve of the same shell
+    generator at a smaller grid, all host threads."""
+    from oracle.oracle import Oracle, MODE_REF
+    prob, inp = workload(args.cpu_sample_n, 4)
+    cores = os.cpu_count() or 1
+    o = Oracle(inp, mode=MODE_REF, tolerance=TOL, threads=cores)
+    t0 = time.perf_counter()
+    r = o.solve()
+    t = time.perf_counter() - t0
+    dof = 3 * o.blocks(0).shape[0] * 128
+    return {"value": dof / t / 1e6, "unit": "MDOF/s", "cores": cores, "kind": "port",
+            "sample": f"complete REF-mode solve of sphere_shell{args.cpu_sample_n} ({dof} DOF, {r['iterations']} "
+                      f"iterations, {t:.2f} s, tol {TOL})"}
+
+
+def flush_l2(buf):
+    if buf is not None:
+        buf.fill_(1.0)
+
+
+def run_ours(args, rank, world):
+    import torch
+    from spgrid_topo_opt_b200 import fem_interface as fi
+    from spgrid_topo_opt_b200 import native
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    native.load(build_if_missing=(rank == 0))
+    prob, inp = workload(args.n, args.bottom_size)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def timed_solves(ses, steps, warmup):
+        for _ in range(warmup):
+            ses.solve(tolerance=TOL)
+        times, iters, launches = [], [], 0
+        for _ in range(steps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            st = ses.solve(tolerance=TOL)
+            times.append(st["solve_device_seconds"])
+            iters.append(st["iterations"])
+            launches += st["kernel_launches"]
+        return times, iters, launches, st
+
+    # mixed precision (the headline) and the FP64 reference arm on the same GPU
+    mixed = native.Session(inp, precision=native.PRECISION_MIXED)
+    fp64 = native.Session(inp, precision=native.PRECISION_FP64)
+    gpu_index = torch.cuda.current_device()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(gpu_index) as clocks:
+        t_mix, it_mix, launches, st_mix = timed_solves(mixed, args.steps, args.warmup)
+        if dist:
+            dist.barrier()
+    t_64, it_64, _, st_64 = timed_solves(fp64, max(2, args.steps // 2), 1)
+    dof = st_mix["dof"]
+    per_step = float(np.mean(t_mix))
+    if dist:
+        tt = torch.tensor([per_step], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        per_step = float(tt.item())
+    value = world * dof / per_step / 1e6
+
+    # dominant kernel: the level-0 smoothing sweep (8 colour launches); its
+    # algorithmic bytes per node are u read+write (6w) + b (3w) + E (w) + flags (4 B)
+    sweep_ms = mixed.time_op(2, reps=20)
+    ku_ms = mixed.time_op(0, reps=20)
+    vcyc_ms = mixed.time_op(3, reps=5)
+    nodes = dof // 3
+    peak, peak_kind = measured_peaks()
+    sweep_bytes = nodes * (10 * 4 + 4)
+    achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9
+    ku_bytes = nodes * 7 * 4
+    roofline = {"bound": "hbm", "kernel": "level0 Gauss-Seidel sweep (8 colour launches, FP32)",
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch_set": sweep_bytes, "sweep_ms": round(sweep_ms, 4),
+                "ku_ms": round(ku_ms, 4), "ku_achieved_gbs": round(ku_bytes / (ku_ms * 1e-3) / 1e9, 1),
+                "vcycle_ms": round(vcyc_ms, 4)}
+
+    # end to end through the drop-in C ABI: serialize on the host, fem_solve (set-up,
+    # H2D, solve, D2H), deserialize; mixed precision selected through extra_ints
+    e2e_inp = fi.deserialize_inputs(fi.serialize_inputs(inp))
+    e2e_inp.extra_ints["sgs_precision"] = native.PRECISION_MIXED
+    blob = fi.serialize_inputs(e2e_inp)
+    e2e_times, h2d, d2h = [], 0.0, 0.0
+    for i in range(2 + max(1, args.steps // 2)):
+        t0 = time.perf_counter()
+        out = fi.deserialize_outputs(native.fem_solve_blob(blob))
+        dt = time.perf_counter() - t0
+        if not out.success:
+            raise RuntimeError(out.info)
+        if i >= 2:
+            e2e_times.append(dt)
+            h2d, d2h = out.extra_doubles.get("h2d_bytes", 0), out.extra_doubles.get("d2h_bytes", 0)
+    e2e_s = float(np.mean(e2e_times))
+
+    result = None
+    if rank == 0:
+        cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(args)
+        result = {
+            "metric": METRIC, "value": round(value, 3), "unit": "MDOF/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 V-cycle / f64 PCG", "data": "synthetic (seeded)",
+            "config": config_dict(args, inp, {"dof": int(dof), "iterations_mixed": int(np.median(it_mix)),
+                                              "iterations_fp64": int(np.median(it_64)),
+                                              "parallelism": "replicas" if world > 1 else "single GPU"}),
+            "fp64": {"ms_per_step": round(float(np.mean(t_64)) * 1e3, 3),
+                     "value": round(dof / float(np.mean(t_64)) / 1e6, 3), "unit": "MDOF/s",
+                     "iterations": int(np.median(it_64))},
+            "mixed_over_fp64_speedup": round(float(np.mean(t_64)) / per_step, 3),
+            "setup_seconds": round(st_mix["setup_seconds"], 3),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(world * dof / e2e_s / 1e6, 3), "unit": "MDOF/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "seconds_per_step": round(e2e_s, 4),
+                    "path": "fem_solve C ABI: decode, set-up, H2D, solve, pack, D2H, encode"},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+        }
+    mixed.close()
+    fp64.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference solver cannot be built here (ICC-only C++ and
+    MKL PARDISO), so its CPU restatement (the oracle, reference-rounding mode) is
+    timed on the host cores on a bounded sample of the same workload."""
+    if rank != 0:
+        return None
+    from oracle.oracle import Oracle, MODE_REF
+    prob, inp = workload(args.cpu_sample_n, 4)
+    cores = os.cpu_count() or 1
+    o = Oracle(inp, mode=MODE_REF, tolerance=TOL, threads=cores)
+    dof = 3 * o.blocks(0).shape[0] * 128
+    for _ in range(max(0, min(args.warmup, 1))):
+        o.solve()
+    times, iters = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = o.solve()
+        times.append(time.perf_counter() - t0)
+        iters.append(r["iterations"])
+    t = float(np.mean(times))
+    value = dof / t / 1e6
+    sample = (f"complete REF-mode solve of sphere_shell{args.cpu_sample_n} ({dof} DOF, {int(np.median(iters))} "
+              f"iterations) per step; the reference needs ICC and MKL PARDISO and is not built, its CPU "
+              f"restatement (oracle/spgrid_oracle.cpp) is timed instead")
+    return {"metric": METRIC, "value": round(value, 4), "unit": "MDOF/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (float-rounded CG updates, as the reference)", "data": "synthetic (seeded)",
+            "config": config_dict(args, inp, {"workload": f"sphere_shell{args.cpu_sample_n} (bounded CPU sample of "
+                                                          f"sphere_shell{args.n})"}),
+            "impl": "reference",
+            "cpu_baseline": {"value": round(value, 4), "unit": "MDOF/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "MDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    else:
+        res = run_ours(args, rank, world)
+    if rank == 0 and res is not None:
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

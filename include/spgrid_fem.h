@@ -62,6 +62,9 @@ typedef struct {
   int64_t launches_per_iteration;
   int64_t dof;             /* 3 * nodes of the active level-0 blocks */
   int64_t bottom_unknowns;
+  double solve_device_seconds; /* PCG, CUDA events on the solver stream */
+  int64_t kernel_launches;     /* kernels executed by the last solve */
+  double h2d_bytes, d2h_bytes; /* host<->device bytes moved by the library so far */
 } sgs_stats;
 
 /* Build a session from an FEMInputs blob.  precision: 0 reference, 1 fp64, 2 mixed,
@@ -106,6 +109,11 @@ SGS_API int sgs_apply(sgs_session* s, int op, int level, int arg, const double* 
 /* Galerkin stencils of a level as [nblocks*128][243] (row node, comp v; column
  * neighbour (i,j,k)-1, comp w at ((i*3+j)*3+k)*9 + v*3 + w) and spoke masks. */
 SGS_API int sgs_level_stencils(sgs_session* s, int level, double* out, uint32_t* spokes);
+
+/* Average device time (ms, CUDA events) of `reps` back-to-back runs of a level-0
+ * operator on the session's resident data: 0 K*u, 1 residual, 2 one smoothing
+ * sweep (8 colours), 3 one preconditioner application (V-cycle). */
+SGS_API int sgs_time_op(sgs_session* s, int op, int reps, double* ms);
 
 /* Decode a blob and encode it again with this library's codec (which = 0 for
  * FEMInputs, 1 for FEMOutputs); *out receives a new[] blob for fem_solve_free.

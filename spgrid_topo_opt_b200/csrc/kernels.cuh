@@ -180,6 +180,9 @@ enum { SOP_MUL = 0, SOP_RES = 1, SOP_GS = 2 };
 
 // One thread per node; GS updates only colour-`color` nodes.  Reads neighbours
 // through the block grid.  Results with a Dirichlet flag are zeroed (Project).
+// The reference projects the whole level after every colour; here only updated
+// nodes are projected, which is the same because the V-cycle keeps u zero on
+// Dirichlet components (cleared levels, projected transfers and updates).
 template <typename T, int OP>
 __global__ void stencil_op_kernel(const int* __restrict__ block_list, int nblocks, const int* __restrict__ coords,
                                   GridView g, const T* __restrict__ A, const uint32_t* __restrict__ flags,

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -40,6 +41,10 @@ struct CudaError : std::runtime_error {
       throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_), SGS_ERR_CUDA);                   \
   } while (0)
 
+// Host<->device bytes moved by this library (uploads, read-backs); sessions and
+// fem_solve report the difference across a call.
+static std::atomic<unsigned long long> g_h2d_bytes{0}, g_d2h_bytes{0};
+
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
@@ -61,6 +66,7 @@ struct DevBuf {
   void upload(const T* h, size_t count, cudaStream_t s) {
     alloc(count);
     if (count) SGS_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    g_h2d_bytes += count * sizeof(T);
   }
   void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
   void zero(cudaStream_t s) {
@@ -154,9 +160,14 @@ class Solver {
   // graph of one PCG iteration
   cudaGraphExec_t iter_graph = nullptr;
   long launches_per_iteration = 0;
-  long launch_counter = 0;
+  long launch_counter = 0;   // kernels launched (or captured) by this solver
+  long solve_launches = 0;   // kernels executed by the last solve
+  double solve_device_seconds = 0;
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr;
 
   ~Solver() {
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_end) cudaEventDestroy(ev_end);
     if (iter_graph) cudaGraphExecDestroy(iter_graph);
     if (h_scal) cudaFreeHost(h_scal);
     if (stream) cudaStreamDestroy(stream);
@@ -814,6 +825,13 @@ void Solver::solve() {
   const int fr = round_ref() ? 1 : 0;
   history.clear();
   iterations = 0;
+  solve_launches = 0;
+  const long launches_before = launch_counter;
+  if (!ev_start) {
+    SGS_CUDA(cudaEventCreate(&ev_start));
+    SGS_CUDA(cudaEventCreate(&ev_end));
+  }
+  SGS_CUDA(cudaEventRecord(ev_start, stream));
   // u = g on the listed Dirichlet nodes (SPGrid_CPU_Solver.cpp:241-285)
   x.zero(stream);
   if (!P.lift_node.empty())
@@ -848,6 +866,7 @@ void Solver::solve() {
   project_null<double>(l0, f.p);
   linf(f.p, nullptr);
   // capture one iteration as a CUDA graph
+  long capture_launches = 0;
   if (!iter_graph) {
     cudaGraph_t g;
     long before = launch_counter;
@@ -857,12 +876,12 @@ void Solver::solve() {
     SGS_CUDA(cudaGraphInstantiate(&iter_graph, g, 0));
     SGS_CUDA(cudaGraphDestroy(g));
     launches_per_iteration = launch_counter - before;
+    capture_launches = launches_per_iteration;
   }
-  const double* norm_slot = scal.p + 3;
   for (int it = 0;; ++it) {
     SGS_CUDA(cudaMemcpyAsync(h_scal, scal.p, 16 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    g_d2h_bytes += 16 * sizeof(double);
     SGS_CUDA(cudaStreamSynchronize(stream));
-    (void)norm_slot;
     const double norm = h_scal[3];
     history.push_back(norm);
     if (h_scal[7] != 0) {
@@ -880,11 +899,18 @@ void Solver::solve() {
       break;
     }
     SGS_CUDA(cudaGraphLaunch(iter_graph, stream));
+    solve_launches += launches_per_iteration;
   }
   add_kernel<<<blocks_for(n3, 256), 256, 0, stream>>>(x.p, ubk.p, n3);
+  ++launch_counter;
+  SGS_CUDA(cudaEventRecord(ev_end, stream));
   SGS_CUDA(cudaGetLastError());
   SGS_CUDA(cudaStreamSynchronize(stream));
   solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  float ms = 0;
+  SGS_CUDA(cudaEventElapsedTime(&ms, ev_start, ev_end));
+  solve_device_seconds = ms * 1e-3;
+  solve_launches += launch_counter - launches_before - (capture_launches);
 }
 
 void Solver::pack_outputs(std::vector<double>& disp) {
@@ -893,6 +919,7 @@ void Solver::pack_outputs(std::vector<double>& disp) {
   if (nin == 0) return;
   pack_kernel<<<blocks_for(nin * 64, 256), 256, 0, stream>>>(int(nin), in_block.p, in_zoff.p, x.p, f.p, N0(), out_disp.p);
   SGS_CUDA(cudaMemcpyAsync(disp.data(), out_disp.p, disp.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  g_d2h_bytes += disp.size() * sizeof(double);
   SGS_CUDA(cudaStreamSynchronize(stream));
 }
 
@@ -1039,6 +1066,30 @@ static int apply_op(Solver& S, int op, int level, int arg, const double* in, con
   return SGS_ERR_INPUT;
 }
 
+template <typename T>
+static double time_op(Solver& S, int op, int reps) {
+  Level<T>& d = S.lev<T>(0);
+  cudaEvent_t a, b;
+  SGS_CUDA(cudaEventCreate(&a));
+  SGS_CUDA(cudaEventCreate(&b));
+  auto run = [&]() {
+    if (op == 0) S.level0<T, OP_KU>(nullptr, d.nb, d.u.p, nullptr, nullptr, d.r.p, 0, 0);
+    else if (op == 1) S.level0<T, OP_RES>(nullptr, d.nb, d.u.p, nullptr, d.b.p, d.r.p, 0, 0);
+    else if (op == 2) S.sweep<T>(0, d.u.p, d.b.p, true, false);
+    else if (op == 3) S.precondition();
+  };
+  run();
+  SGS_CUDA(cudaEventRecord(a, S.stream));
+  for (int i = 0; i < reps; ++i) run();
+  SGS_CUDA(cudaEventRecord(b, S.stream));
+  SGS_CUDA(cudaEventSynchronize(b));
+  float ms = 0;
+  SGS_CUDA(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return double(ms) / reps;
+}
+
 extern "C" {
 
 SGS_API int sgs_create(const void* input_blob, int precision, sgs_session** out, char* err, int errlen) {
@@ -1094,6 +1145,10 @@ SGS_API int sgs_solve(sgs_session* h, double tolerance, int max_iterations, sgs_
     stats->launches_per_iteration = S.launches_per_iteration;
     stats->dof = 3 * S.N0();
     stats->bottom_unknowns = S.bottom.n;
+    stats->solve_device_seconds = S.solve_device_seconds;
+    stats->kernel_launches = S.solve_launches;
+    stats->h2d_bytes = double(g_h2d_bytes.load());
+    stats->d2h_bytes = double(g_d2h_bytes.load());
   }
   return rc;
 }
@@ -1192,6 +1247,7 @@ SGS_API void fem_solve(void* input, void* output) {
     FEMInputs in = decode_inputs(input);
     for (int v = 0; v < 3; ++v) outs.displacements.resolution[v] = in.resolution[v];
     const int precision = in.get_int("sgs_precision", PREC_REFERENCE);
+    const unsigned long long h2d0 = g_h2d_bytes.load(), d2h0 = g_d2h_bytes.load();
     sgs_session* h = nullptr;
     std::string err;
     int rc = (precision < 0 || precision > 2) ? SGS_ERR_INPUT : session_from_inputs(in, precision, &h, &err);
@@ -1216,6 +1272,10 @@ SGS_API void fem_solve(void* input, void* output) {
         outs.displacements.base.assign(in.density.base.begin(), in.density.base.end());
         outs.displacements.data.resize(nin * 256);
         rc = sgs_displacements(h, outs.displacements.data.data());
+        outs.extra_doubles["h2d_bytes"] = double(g_h2d_bytes.load() - h2d0);
+        outs.extra_doubles["d2h_bytes"] = double(g_d2h_bytes.load() - d2h0);
+        outs.extra_doubles["solve_device_seconds"] = st.solve_device_seconds;
+        outs.extra_ints["kernel_launches"] = int(st.kernel_launches);
         if (rc) {
           outs.displacements.base.clear();
           outs.displacements.data.clear();
@@ -1245,6 +1305,17 @@ SGS_API void fem_solve(void* input, void* output) {
 }
 
 SGS_API void fem_solve_free(void* blob) { delete[] static_cast<char*>(blob); }
+
+SGS_API int sgs_time_op(sgs_session* h, int op, int reps, double* ms) {
+  if (!h || !ms || host_only(h) || reps <= 0 || op < 0 || op > 3) return SGS_ERR_INPUT;
+  try {
+    *ms = h->solver->mixed() && op != 3 ? time_op<float>(*h->solver, op, reps) : time_op<double>(*h->solver, op, reps);
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
 
 SGS_API int sgs_codec_roundtrip(const void* blob, int which, void** out) {
   if (!blob || !out) return SGS_ERR_INPUT;

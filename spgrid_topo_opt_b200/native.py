@@ -22,7 +22,7 @@ OP_KU, OP_RESIDUAL, OP_SMOOTH, OP_RESTRICT, OP_PROLONG, OP_STENCIL, OP_BOTTOM, O
 EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", "sgs_last_error", "sgs_solve",
                     "sgs_residual_history", "sgs_displacements", "sgs_sensitivity", "sgs_level_count",
                     "sgs_level_blocks", "sgs_level_flags", "sgs_boundary_blocks", "sgs_apply", "sgs_level_stencils",
-                    "sgs_codec_roundtrip")
+                    "sgs_codec_roundtrip", "sgs_time_op")
 
 
 class SolverError(RuntimeError):
@@ -34,7 +34,9 @@ class SolverError(RuntimeError):
 class Stats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("levels", C.c_int32), ("initial_residual", C.c_double),
                 ("final_residual", C.c_double), ("setup_seconds", C.c_double), ("solve_seconds", C.c_double),
-                ("launches_per_iteration", C.c_int64), ("dof", C.c_int64), ("bottom_unknowns", C.c_int64)]
+                ("launches_per_iteration", C.c_int64), ("dof", C.c_int64), ("bottom_unknowns", C.c_int64),
+                ("solve_device_seconds", C.c_double), ("kernel_launches", C.c_int64), ("h2d_bytes", C.c_double),
+                ("d2h_bytes", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -76,6 +78,7 @@ def load(build_if_missing: bool = False):
     L.sgs_apply.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P, P]
     L.sgs_level_stencils.argtypes = [P, C.c_int, P, P]
     L.sgs_codec_roundtrip.argtypes = [P, C.c_int, C.POINTER(C.c_void_p)]
+    L.sgs_time_op.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_double)]
     _lib = L
     return L
 
@@ -182,6 +185,13 @@ class Session:
         if not np.isfinite(obj):
             raise SolverError(10, load().sgs_last_error(self.h).decode(errors="replace"))
         return obj, dc, se
+
+    def time_op(self, op: int, reps: int = 20) -> float:
+        """Average device milliseconds of a level-0 operator (0 K*u, 1 residual,
+        2 smoothing sweep, 3 V-cycle) on the resident data."""
+        ms = C.c_double(0)
+        self._check(load().sgs_time_op(self.h, op, reps, C.byref(ms)))
+        return ms.value
 
     # ---- inspection / unit operators
     @property
