@@ -5,7 +5,7 @@
 // A 3-vector field is stored as three planes of N = nb*128 values ([3][N]).
 // Level 0 carries the per-cell stiffness scale E (cell = its min-corner node,
 // 0 = empty); the element matrix of a cell is E * (mu0*K_mu + lambda0*K_la).
-// Coarse levels carry 27-point Galerkin stencils in planes [243][N], entry
+// Coarse levels carry 27-point Galerkin stencils node-major, [N][243], entry
 // ((i*3+j)*3+k)*9 + v*3 + w = row (node, v), column (node + (i,j,k) - 1, w).
 #pragma once
 #include <cstdint>
@@ -162,6 +162,103 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// Level-0 Gauss-Seidel colour pass (solver/CPU_Kernels/SPGrid_Gauss_Seidel.h:876-1180):
+// 8 blocks per CTA, the 16 colour-`color` nodes of each block one per thread.
+// Neighbours are read through L1; the residual is accumulated neighbour by
+// neighbour, A_d = sum over the cells shared with neighbour d of E_c Kc[I][J].
+// Same-colour nodes never share a cell, so a pass updates in place.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) gs0_kernel(const int* __restrict__ block_list, int nblocks,
+                                                  const int* __restrict__ nbr, const T* __restrict__ E, T* u,
+                                                  const T* __restrict__ b, const uint32_t* __restrict__ flags, long N,
+                                                  T dx, int color, int boundary_only) {
+  __shared__ int snb[8][27];
+  for (int i = threadIdx.x; i < 8 * 27; i += 128) {
+    const long bb = long(blockIdx.x) * 8 + i / 27;
+    int v = -1;
+    if (bb < nblocks) v = nbr[long(block_list ? block_list[bb] : int(bb)) * 27 + i % 27];
+    snb[i / 27][i % 27] = v;
+  }
+  __syncthreads();
+  const int slot = threadIdx.x >> 4, q = threadIdx.x & 15;
+  const long bidx = long(blockIdx.x) * 8 + slot;
+  if (bidx >= nblocks) return;
+  const int bi = block_list ? block_list[bidx] : int(bidx);
+  const int x = (q >> 3) * 2 + ((color >> 2) & 1), y = ((q >> 2) & 1) * 2 + ((color >> 1) & 1), z = (q & 3) * 2 + (color & 1);
+  const long gidx = long(bi) * 128 + (x << 5) + (y << 3) + z;
+  const uint32_t fl = flags[gidx];
+  const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
+  if (!((fl & ACTIVE_NODE) && (!boundary_only || (fl & BOUNDARY_NODE)))) {
+    // inactive (or out-of-band) nodes keep u; Dirichlet components are cleared
+    if (fx) u[gidx] = T(0);
+    if (fy) u[gidx + N] = T(0);
+    if (fz) u[gidx + 2 * N] = T(0);
+    return;
+  }
+  const int* nb = snb[slot];
+  // E of the 8 cells around the node (cell = node - I)
+  T Ec[8];
+#pragma unroll
+  for (int I = 0; I < 8; ++I) {
+    const int cx = x - (I >> 2), cy = y - ((I >> 1) & 1), cz = z - (I & 1);
+    const int nbk = nb[(cx < 0 ? 0 : 1) * 9 + (cy < 0 ? 0 : 1) * 3 + (cz < 0 ? 0 : 1)];
+    Ec[I] = nbk >= 0 ? E[long(nbk) * 128 + ((cx & 3) << 5) + ((cy & 3) << 3) + (cz & 7)] : T(0);
+  }
+  T f0 = 0, f1 = 0, f2 = 0, d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, uc0 = 0, uc1 = 0, uc2 = 0;
+#pragma unroll
+  for (int d = 0; d < 27; ++d) {
+    const int ox = d / 9 - 1, oy = (d / 3) % 3 - 1, oz = d % 3 - 1;
+    const int nx = x + ox, ny = y + oy, nz = z + oz;
+    const int nbk = nb[(nx < 0 ? 0 : (nx > 3 ? 2 : 1)) * 9 + (ny < 0 ? 0 : (ny > 3 ? 2 : 1)) * 3 + (nz < 0 ? 0 : (nz > 7 ? 2 : 1))];
+    T ux = 0, uy = 0, uz = 0;
+    if (nbk >= 0) {
+      const long n = long(nbk) * 128 + ((nx & 3) << 5) + ((ny & 3) << 3) + (nz & 7);
+      ux = u[n];
+      uy = u[n + N];
+      uz = u[n + 2 * N];
+    }
+    T a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int I = 0; I < 8; ++I) {
+      const int Jx = (I >> 2) + ox, Jy = ((I >> 1) & 1) + oy, Jz = (I & 1) + oz;
+      if (Jx < 0 || Jx > 1 || Jy < 0 || Jy > 1 || Jz < 0 || Jz > 1) continue;
+      const int k = (I * 8 + ((Jx << 2) | (Jy << 1) | Jz)) * 9;
+#pragma unroll
+      for (int m = 0; m < 9; ++m) a[m] += Ec[I] * kc<T>(k + m);
+    }
+    f0 += a[0] * ux + a[1] * uy + a[2] * uz;
+    f1 += a[3] * ux + a[4] * uy + a[5] * uz;
+    f2 += a[6] * ux + a[7] * uy + a[8] * uz;
+    if (d == 13) {
+      d0 = a[0]; d1 = a[4]; d2 = a[8]; d3 = a[1]; d4 = a[2]; d5 = a[5];
+      uc0 = ux; uc1 = uy; uc2 = uz;
+    }
+  }
+  const T r0 = b[gidx] - f0 * dx, r1 = b[gidx + N] - f1 * dx, r2 = b[gidx + 2 * N] - f2 * dx;
+  d0 *= dx; d1 *= dx; d2 *= dx; d3 *= dx; d4 *= dx; d5 *= dx;
+  if (fx) { d0 = 1; d3 = 0; d4 = 0; }
+  if (fy) { d1 = 1; d3 = 0; d5 = 0; }
+  if (fz) { d2 = 1; d4 = 0; d5 = 0; }
+  const T m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
+  const T m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
+  const T inv = T(1) / (d0 * m11 + d3 * m12 + d4 * m13);
+  T a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
+  if (fx) { a0 = 0; a3 = 0; a4 = 0; }
+  if (fy) { a1 = 0; a3 = 0; a5 = 0; }
+  if (fz) { a2 = 0; a4 = 0; a5 = 0; }
+  T v0 = uc0 + r0 * a0 + r1 * a3 + r2 * a4;
+  T v1 = uc1 + r0 * a3 + r1 * a1 + r2 * a5;
+  T v2 = uc2 + r0 * a4 + r1 * a5 + r2 * a2;
+  if (fx) v0 = 0;
+  if (fy) v1 = 0;
+  if (fz) v2 = 0;
+  u[gidx] = v0;
+  u[gidx + N] = v1;
+  u[gidx + 2 * N] = v2;
+}
+
+// ---------------------------------------------------------------------------
 // Coarse-level stencil operators (solver/MG/SPGrid_Stencil_Multiply.h:15-280)
 // ---------------------------------------------------------------------------
 struct GridView {
@@ -178,28 +275,34 @@ struct GridView {
 
 enum { SOP_MUL = 0, SOP_RES = 1, SOP_GS = 2 };
 
-// One thread per node; GS updates only colour-`color` nodes.  Reads neighbours
-// through the block grid.  Results with a Dirichlet flag are zeroed (Project).
-// The reference projects the whole level after every colour; here only updated
-// nodes are projected, which is the same because the V-cycle keeps u zero on
-// Dirichlet components (cleared levels, projected transfers and updates).
+// One warp per node: lane q < 27 multiplies the 3x3 block of spoke q with the
+// neighbour's u, the warp sums the three components.  Stencils are node-major,
+// A[node*243 + q*9 + v*3 + w], so a warp reads one node's coefficients in one
+// coalesced sweep.  GS updates only colour-`color` nodes (16 per block).
+// Results on Dirichlet components are zeroed (Project).  The reference
+// projects the whole level after every colour; here only updated nodes are
+// projected, which is the same because the V-cycle keeps u zero on Dirichlet
+// components (cleared levels, projected transfers and updates).
 template <typename T, int OP>
-__global__ void stencil_op_kernel(const int* __restrict__ block_list, int nblocks, const int* __restrict__ coords,
-                                  GridView g, const T* __restrict__ A, const uint32_t* __restrict__ flags,
-                                  const T* u, T* out_u, const T* __restrict__ b, T* __restrict__ out, long N,
-                                  int color, int boundary_only, int round_out) {
+__global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__ block_list, int nblocks,
+                                                         const int* __restrict__ coords, GridView g,
+                                                         const T* __restrict__ A, const uint32_t* __restrict__ flags,
+                                                         const T* u, T* out_u, const T* __restrict__ b,
+                                                         T* __restrict__ out, long N, int color, int boundary_only,
+                                                         int round_out) {
   const int per = (OP == SOP_GS) ? 16 : 128;
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  const long blk = t / per;
+  const long w = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;  // one warp per node
+  const int lane = threadIdx.x & 31;
+  const long blk = w / per;
   if (blk >= nblocks) return;
   const int bi = block_list ? block_list[blk] : int(blk);
   int e;
   if (OP == SOP_GS) {
-    const int q = int(t % per);  // 16 nodes of the colour: (x/2, y/2, z/2) in 2x2x4
+    const int q = int(w % per);  // 16 nodes of the colour: (x/2, y/2, z/2) in 2x2x4
     const int px = (color >> 2) & 1, py = (color >> 1) & 1, pz = color & 1;
     e = (((q >> 3) * 2 + px) << 5) + ((((q >> 2) & 1) * 2 + py) << 3) + ((q & 3) * 2 + pz);
   } else {
-    e = int(t % per);
+    e = int(w % per);
   }
   const long gidx = long(bi) * 128 + e;
   const uint32_t fl = flags[gidx];
@@ -207,18 +310,25 @@ __global__ void stencil_op_kernel(const int* __restrict__ block_list, int nblock
     if (!(fl & ACTIVE_NODE)) return;
     if (boundary_only && !(fl & BOUNDARY_NODE)) return;
   }
-  const int x = coords[3 * bi] + (e >> 5), y = coords[3 * bi + 1] + ((e >> 3) & 3), z = coords[3 * bi + 2] + (e & 7);
   T f0 = 0, f1 = 0, f2 = 0;
-#pragma unroll 3
-  for (int q = 0; q < 27; ++q) {
-    const long n = g.node(x + q / 9 - 1, y + (q / 3) % 3 - 1, z + q % 3 - 1);
-    if (n < 0) continue;
-    const T ux = u[n], uy = u[n + N], uz = u[n + 2 * N];
-    const T* a = A + long(q) * 9 * N + gidx;
-    f0 += a[0] * ux + a[N] * uy + a[2 * N] * uz;
-    f1 += a[3 * N] * ux + a[4 * N] * uy + a[5 * N] * uz;
-    f2 += a[6 * N] * ux + a[7 * N] * uy + a[8 * N] * uz;
+  if (lane < 27) {
+    const int x = coords[3 * bi] + (e >> 5), y = coords[3 * bi + 1] + ((e >> 3) & 3), z = coords[3 * bi + 2] + (e & 7);
+    const long n = g.node(x + lane / 9 - 1, y + (lane / 3) % 3 - 1, z + lane % 3 - 1);
+    if (n >= 0) {
+      const T ux = u[n], uy = u[n + N], uz = u[n + 2 * N];
+      const T* a = A + gidx * 243 + lane * 9;
+      f0 = a[0] * ux + a[1] * uy + a[2] * uz;
+      f1 = a[3] * ux + a[4] * uy + a[5] * uz;
+      f2 = a[6] * ux + a[7] * uy + a[8] * uz;
+    }
   }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    f0 += __shfl_down_sync(0xffffffffu, f0, o);
+    f1 += __shfl_down_sync(0xffffffffu, f1, o);
+    f2 += __shfl_down_sync(0xffffffffu, f2, o);
+  }
+  if (lane != 0) return;
   if (OP == SOP_MUL) {
     out[gidx] = (fl & DIR_X) ? T(0) : f0;
     out[gidx + N] = (fl & DIR_Y) ? T(0) : f1;
@@ -234,8 +344,8 @@ __global__ void stencil_op_kernel(const int* __restrict__ block_list, int nblock
     out[gidx + 2 * N] = o2;
     return;
   }
-  const T* c = A + long(13) * 9 * N + gidx;
-  T d0 = c[0], d1 = c[4 * N], d2 = c[8 * N], d3 = c[N], d4 = c[2 * N], d5 = c[5 * N];
+  const T* c = A + gidx * 243 + 13 * 9;
+  T d0 = c[0], d1 = c[4], d2 = c[8], d3 = c[1], d4 = c[2], d5 = c[5];
   const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
   if (fx) { d0 = 1; d3 = 0; d4 = 0; }
   if (fy) { d1 = 1; d3 = 0; d5 = 0; }

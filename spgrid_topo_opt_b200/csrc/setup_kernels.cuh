@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(576) galerkin_kernel(const int* __restrict__ c
       if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
       s += contrib[cc][((bx << 2) | (by << 1) | bz) * 9 + w9];
     }
-    A[(long(q) * 9 + w9) * N + gidx] = s * dx;
+    A[gidx * 243 + q * 9 + w9] = s * dx;
   }
   if (t < 27) {
     const int qi = t / 9, qj = (t / 3) % 3, qk = t % 3;
@@ -105,7 +105,7 @@ __global__ void delete_dirichlet_kernel(int nb, const int* __restrict__ coords, 
     const uint32_t nf = n >= 0 ? flags[n] : 0u;
     for (int v = 0; v < 3; ++v)
       for (int w = 0; w < 3; ++w) {
-        double* a = A + (long(q) * 9 + v * 3 + w) * N + gidx;
+        double* a = A + gidx * 243 + q * 9 + v * 3 + w;
         if (fl & (DIR_X << v)) *a = (v == w && q == 13) ? 1.0 : 0.0;
         else if ((nf & ACTIVE_NODE) && (nf & (DIR_X << w))) *a = 0.0;
       }
@@ -137,7 +137,7 @@ __global__ void bottom_assemble_kernel(int ndof_nodes, const int* __restrict__ d
       for (int w = 0; w < 3; ++w) {
         const long r = 3L * i + v, c = 3L * j + w;
         if (r > c) continue;
-        double val = A[(long(q) * 9 + v * 3 + w) * N + gidx];
+        double val = A[gidx * 243 + q * 9 + v * 3 + w];
         const bool dr = fact && (fl & (DIR_X << v));
         const bool dc = (nf & ACTIVE_NODE) && (nf & (DIR_X << w));
         if (dr || dc) val = (r == c) ? 1.0 : 0.0;

@@ -450,7 +450,7 @@ class Solver {
     Level<T>& d = lev<T>(l);
     if (count <= 0) return;
     const int per = OP == SOP_GS ? 16 : 128;
-    stencil_op_kernel<T, OP><<<blocks_for(long(count) * per, 128), 128, 0, stream>>>(
+    stencil_op_kernel<T, OP><<<blocks_for(long(count) * per * 32, 256), 256, 0, stream>>>(
         list, count, d.coords.p, d.grid, d.A.p, d.flags.p, u, uo, b, out, d.N, color, boundary, round_out);
     ++launch_counter;
   }
@@ -465,7 +465,9 @@ class Solver {
     if (l == 0) {
       for (int k = 0; k < 8; ++k) {
         const int c = forward ? k : 7 - k;
-        level0<T, OP_GS>(list, count, u, u, b, nullptr, c, boundary ? 1 : 0);
+        gs0_kernel<T><<<blocks_for(count, 8), 128, 0, stream>>>(list, count, d.nbr.p, Edev<T>(), u, b, d.flags.p, d.N,
+                                                                T(P.dx), c, boundary ? 1 : 0);
+        ++launch_counter;
       }
       return;
     }
@@ -1223,12 +1225,9 @@ SGS_API int sgs_level_stencils(sgs_session* h, int level, double* out, uint32_t*
   Level<double>& d = *h->solver->L64[level];
   if (!d.has_matrix) return SGS_ERR_INPUT;
   try {
-    std::vector<double> planes(size_t(243) * d.N);
-    SGS_CUDA(cudaMemcpyAsync(planes.data(), d.A.p, planes.size() * sizeof(double), cudaMemcpyDeviceToHost, h->solver->stream));
+    SGS_CUDA(cudaMemcpyAsync(out, d.A.p, size_t(243) * d.N * sizeof(double), cudaMemcpyDeviceToHost, h->solver->stream));
     if (spokes) SGS_CUDA(cudaMemcpyAsync(spokes, d.spokes.p, d.N * 4, cudaMemcpyDeviceToHost, h->solver->stream));
     SGS_CUDA(cudaStreamSynchronize(h->solver->stream));
-    for (long n = 0; n < d.N; ++n)
-      for (int k = 0; k < 243; ++k) out[n * 243 + k] = planes[size_t(k) * d.N + n];
   } catch (const CudaError& e) {
     h->error = e.what();
     return e.code;
