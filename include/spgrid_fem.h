@@ -92,6 +92,24 @@ SGS_API int sgs_displacements(sgs_session* s, double* out);
  * Returns the objective sum u_e^T K0 u_e (Emin + rho^p (1 - Emin)). */
 SGS_API double sgs_sensitivity(sgs_session* s, const double* density, double* dc, double* element_energy);
 
+/* No counterpart in the reference.  Allocation-free variant of sgs_sensitivity
+ * for callers that cannot allocate device memory while they run (frameworks
+ * that own the allocator, code that must not call cudaMalloc/cudaFree once it
+ * has started).  All arrays are caller-owned DEVICE buffers on the session's
+ * device: density_dev[nblocks][64] in, dc_dev and element_energy_dev
+ * [nblocks][64] out, objective_dev one double out.  The only scratch, the
+ * per-CTA partial sums of the objective, lives in a static device array of
+ * SGS_SENSITIVITY_STATIC_MAX_PARTIALS doubles that every GPU loading the
+ * library holds until exit; problems with more than that many 256-cell CTAs
+ * (nblocks * 64 > MAX * 256) are rejected with SGS_ERR_INPUT.  The first call
+ * on a device looks the array's device address up, so make that first call
+ * before any stream capture.  Every call reuses the same array: calls that
+ * overlap on the GPU (other host threads, other sessions on the device) race.
+ * Synchronous; returns 0 or an error code (message in sgs_last_error). */
+#define SGS_SENSITIVITY_STATIC_MAX_PARTIALS 16384
+SGS_API int sgs_sensitivity_static(sgs_session* s, const double* density_dev, double* dc_dev,
+                                   double* element_energy_dev, double* objective_dev);
+
 /* ---- inspection and unit operators (tests) ------------------------------ */
 SGS_API int sgs_level_count(sgs_session* s);
 /* Active blocks of a level in SPGrid page order; coords may be null. */

@@ -1185,6 +1185,68 @@ SGS_API double sgs_sensitivity(sgs_session* h, const double* density, double* dc
   }
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free sensitivity.  Some callers cannot allocate device memory
+// while they run (an allocator locked down by a framework, a region that must
+// not call cudaMalloc/cudaFree, a memory budget that is fixed after start-up).
+// This variant takes caller-owned device buffers and keeps the only scratch it
+// needs, the per-CTA partial sums of the objective, in a fixed static device
+// array of SGS_SENSITIVITY_STATIC_MAX_PARTIALS doubles (128 KiB, held by every
+// GPU that loads the library until the process exits).
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_sensitivity_partials[SGS_SENSITIVITY_STATIC_MAX_PARTIALS];
+static double* g_sensitivity_partials_addr[128] = {nullptr};  // device address per device ordinal
+
+// Sum the partials in index order, the order sgs_sensitivity uses on the host.
+__global__ void sum_in_order_kernel(const double* __restrict__ part, int n, double* __restrict__ out) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double s = 0;
+    for (int i = 0; i < n; ++i) s += part[i];
+    *out = s;
+  }
+}
+
+SGS_API int sgs_sensitivity_static(sgs_session* h, const double* density_dev, double* dc_dev,
+                                   double* element_energy_dev, double* objective_dev) {
+  if (!h || host_only(h) || !density_dev || !dc_dev || !element_energy_dev || !objective_dev) return SGS_ERR_INPUT;
+  Solver& S = *h->solver;
+  const long nin = long(S.P.in_block.size());
+  const long ncta = (nin * 64 + 255) / 256;
+  if (ncta > SGS_SENSITIVITY_STATIC_MAX_PARTIALS) {
+    char m[200];
+    std::snprintf(m, sizeof m, "sgs_sensitivity_static handles at most %d x 256 cells (%ld input blocks given)",
+                  SGS_SENSITIVITY_STATIC_MAX_PARTIALS, nin);
+    h->error = m;
+    return SGS_ERR_INPUT;
+  }
+  try {
+    int dev = 0;
+    SGS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) throw CudaError("device ordinal out of range", SGS_ERR_CUDA);
+    if (!g_sensitivity_partials_addr[dev]) {
+      // the symbol's host-side name is not a device address: resolve it once per device
+      void* p = nullptr;
+      SGS_CUDA(cudaGetSymbolAddress(&p, g_sensitivity_partials));
+      g_sensitivity_partials_addr[dev] = static_cast<double*>(p);
+    }
+    double* part = g_sensitivity_partials_addr[dev];
+    if (nin == 0) {
+      SGS_CUDA(cudaMemsetAsync(objective_dev, 0, sizeof(double), S.stream));
+    } else {
+      sensitivity_kernel<<<unsigned(ncta), 256, 0, S.stream>>>(int(nin), S.in_block.p, S.in_zoff.p, S.L64[0]->nbr.p, S.x.p,
+                                                              S.N0(), density_dev, S.P.penalty, S.P.minimum_stiffness,
+                                                              dc_dev, element_energy_dev, part);
+      sum_in_order_kernel<<<1, 32, 0, S.stream>>>(part, int(ncta), objective_dev);
+    }
+    SGS_CUDA(cudaGetLastError());
+    SGS_CUDA(cudaStreamSynchronize(S.stream));
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
 SGS_API int sgs_level_count(sgs_session* h) { return h ? h->solver->nlev() : 0; }
 
 SGS_API int sgs_level_blocks(sgs_session* h, int level, int32_t* coords) {

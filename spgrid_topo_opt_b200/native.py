@@ -22,7 +22,7 @@ OP_KU, OP_RESIDUAL, OP_SMOOTH, OP_RESTRICT, OP_PROLONG, OP_STENCIL, OP_BOTTOM, O
 EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", "sgs_last_error", "sgs_solve",
                     "sgs_residual_history", "sgs_displacements", "sgs_sensitivity", "sgs_level_count",
                     "sgs_level_blocks", "sgs_level_flags", "sgs_boundary_blocks", "sgs_apply", "sgs_level_stencils",
-                    "sgs_codec_roundtrip", "sgs_time_op")
+                    "sgs_codec_roundtrip", "sgs_time_op", "sgs_sensitivity_static")
 
 
 class SolverError(RuntimeError):
@@ -79,6 +79,8 @@ def load(build_if_missing: bool = False):
     L.sgs_level_stencils.argtypes = [P, C.c_int, P, P]
     L.sgs_codec_roundtrip.argtypes = [P, C.c_int, C.POINTER(C.c_void_p)]
     L.sgs_time_op.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.sgs_sensitivity_static.argtypes = [P, P, P, P, P]
+    L.sgs_sensitivity_static.restype = C.c_int
     _lib = L
     return L
 
