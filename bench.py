@@ -41,21 +41,46 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=256, help="grid size of the shell workload")
-    ap.add_argument("--bottom-size", type=int, default=8)
+    ap.add_argument("--workload", choices=["shell", "band"], default="shell",
+                    help="shell: sphere shell (BASELINE config 1); band: narrow band of 8 spheres (config 4)")
+    ap.add_argument("--n", type=int, default=None, help="grid size (default 256 shell, 1024 band)")
+    ap.add_argument("--bottom-size", type=int, default=None)
     ap.add_argument("--cpu-sample-n", type=int, default=64, help="grid size of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-iterations", type=int, default=0,
+                    help="profiling mode: set up, warm up, then one solve of this many PCG iterations "
+                         "between cudaProfilerStart/Stop (for ncu --profile-from-start off); prints stats only")
+    ap.add_argument("--precision", choices=["mixed", "fp64", "reference"], default="mixed",
+                    help="precision of the profiled solve")
+    args = ap.parse_args()
+    if args.n is None:
+        args.n = 256 if args.workload == "shell" else 1024
+    if args.bottom_size is None:
+        args.bottom_size = 8 if args.workload == "shell" else 16
+    return args
 
 
-def workload(n: int, bottom: int):
+def workload(n: int, bottom: int, kind: str = "shell"):
     from spgrid_topo_opt_b200 import configs
+    if kind == "band":
+        return None, configs.spheres_band_inputs(n, bottom_size=bottom, tolerance=TOL)
     prob = configs.sphere_shell(n, bottom_size=bottom)
     inp = configs.to_inputs(prob, tolerance=TOL)
     return prob, inp
 
 
 def config_dict(args, inp, extra=None):
+    if args.workload == "band":
+        d = {"workload": f"spheres_band{args.n}", "grid": [args.n] * 3,
+             "band": "12-voxel shell around the union of 8 seeded spheres (radii 0.1-0.3), seed 7",
+             "density": "uniform [1e-3, 1], seeded", "mg_level": int(inp.mg_level),
+             "smoothing": [int(inp.pre_and_post_smoothing_iter), int(inp.extra_ints["boundary_smoothing"])],
+             "tolerance": TOL, "stopping_rule": "L-inf residual <= tol * zero-guess L-inf residual",
+             "blocks": int(inp.density.base.shape[0]), "l2": "flushed (256 MiB write) before every timed solve"}
+        if extra:
+            d.update(extra)
+        return d
     d = {"workload": f"sphere_shell{args.n}", "grid": [args.n] * 3, "shell_radii": [0.4, 0.5],
          "density": "clamp(0.5+0.3*smoothed uniform noise, 1e-3, 1), seed 1234", "mg_level": int(inp.mg_level),
          "smoothing": [int(inp.pre_and_post_smoothing_iter), int(inp.extra_ints["boundary_smoothing"])],
@@ -133,7 +158,7 @@ def cpu_baseline(args):
     bounded sample of the same workload: a complete solve of the same shell
     generator at a smaller grid, all host threads."""
     from oracle.oracle import Oracle, MODE_REF
-    prob, inp = workload(args.cpu_sample_n, 4)
+    prob, inp = workload(args.cpu_sample_n, 4, args.workload)
     cores = os.cpu_count() or 1
     o = Oracle(inp, mode=MODE_REF, tolerance=TOL, threads=cores)
     t0 = time.perf_counter()
@@ -162,7 +187,18 @@ def run_ours(args, rank, world):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     native.load(build_if_missing=(rank == 0))
-    prob, inp = workload(args.n, args.bottom_size)
+    prob, inp = workload(args.n, args.bottom_size, args.workload)
+    if args.profile_iterations > 0:
+        prec = {"mixed": native.PRECISION_MIXED, "fp64": native.PRECISION_FP64,
+                "reference": native.PRECISION_REFERENCE}[args.precision]
+        with native.Session(inp, precision=prec) as ses:
+            ses.solve(tolerance=TOL, max_iterations=args.profile_iterations)
+            torch.cuda.synchronize()
+            torch.cuda.cudart().cudaProfilerStart()
+            st = ses.solve(tolerance=TOL, max_iterations=args.profile_iterations)
+            torch.cuda.synchronize()
+            torch.cuda.cudart().cudaProfilerStop()
+        return {"profile": True, "stats": st} if rank == 0 else None
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def timed_solves(ses, steps, warmup):
@@ -221,7 +257,7 @@ def run_ours(args, rank, world):
     e2e_inp.extra_ints["sgs_precision"] = native.PRECISION_MIXED
     blob = fi.serialize_inputs(e2e_inp)
     e2e_times, h2d, d2h = [], 0.0, 0.0
-    for i in range(2 + max(1, args.steps // 2)):
+    for i in range(0 if args.no_e2e else 2 + max(1, args.steps // 2)):
         t0 = time.perf_counter()
         out = fi.deserialize_outputs(native.fem_solve_blob(blob))
         dt = time.perf_counter() - t0
@@ -230,7 +266,7 @@ def run_ours(args, rank, world):
         if i >= 2:
             e2e_times.append(dt)
             h2d, d2h = out.extra_doubles.get("h2d_bytes", 0), out.extra_doubles.get("d2h_bytes", 0)
-    e2e_s = float(np.mean(e2e_times))
+    e2e_s = float(np.mean(e2e_times)) if e2e_times else float("nan")
 
     result = None
     if rank == 0:
@@ -249,7 +285,7 @@ def run_ours(args, rank, world):
             "setup_seconds": round(st_mix["setup_seconds"], 3),
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": {"value": round(world * dof / e2e_s / 1e6, 3), "unit": "MDOF/s",
+            "e2e": None if args.no_e2e else {"value": round(world * dof / e2e_s / 1e6, 3), "unit": "MDOF/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "seconds_per_step": round(e2e_s, 4),
                     "path": "fem_solve C ABI: decode, set-up, H2D, solve, pack, D2H, encode"},
@@ -271,7 +307,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     from oracle.oracle import Oracle, MODE_REF
-    prob, inp = workload(args.cpu_sample_n, 4)
+    prob, inp = workload(args.cpu_sample_n, 4, args.workload)
     cores = os.cpu_count() or 1
     o = Oracle(inp, mode=MODE_REF, tolerance=TOL, threads=cores)
     dof = 3 * o.blocks(0).shape[0] * 128

@@ -110,6 +110,12 @@ SGS_API double sgs_sensitivity(sgs_session* s, const double* density, double* dc
 SGS_API int sgs_sensitivity_static(sgs_session* s, const double* density_dev, double* dc_dev,
                                    double* element_energy_dev, double* objective_dev);
 
+/* Replace the densities of a resident problem ([nblocks][64], input block
+ * order) keeping its material pattern (cells with density > 0): E, the Galerkin
+ * operators and the bottom inverse are rebuilt, the hierarchy is kept.  Returns
+ * SGS_ERR_INPUT when a cell's material status would change. */
+SGS_API int sgs_set_density(sgs_session* s, const double* density);
+
 /* ---- inspection and unit operators (tests) ------------------------------ */
 SGS_API int sgs_level_count(sgs_session* s);
 /* Active blocks of a level in SPGrid page order; coords may be null. */

@@ -200,34 +200,81 @@ def sphere_shell(n: int = 256, r_in: float = 0.4, r_out: float = 0.5, seed: int 
     return Problem(f"shell{n}", (n, n, n), rho, dcells, f, 1.0 / n, mg_level_for(n, bottom_size))
 
 
-def spheres_band(n: int = 1024, nspheres: int = 8, thickness: int = 12, seed: int = 7,
-                 bottom_size: int = 64) -> Problem:
-    """Narrow band: a ``thickness``-voxel shell around the union of seeded random
-    spheres (radii 0.1-0.3 of the box); density uniform[1e-3,1]; the lowest
-    material node plane is fixed (as whole cells); 16 seeded unit point loads."""
+def spheres_band_inputs(n: int = 1024, nspheres: int = 8, thickness: int = 12, seed: int = 7,
+                        bottom_size: int = 16, **solver_kw) -> FEMInputs:
+    """Narrow band of an n^3 grid, built block by block (no dense n^3 arrays): a
+    ``thickness``-voxel shell around the union of ``nspheres`` seeded random
+    spheres (centres in [0.3,0.7]^3, radii 0.1-0.3 of the box); cell density
+    uniform [1e-3, 1] (seeded); every band cell of the lowest band cell layer is
+    fixed (whole cells, xyz); 16 seeded unit point loads on band nodes."""
     rng = np.random.default_rng(seed)
     centres = rng.uniform(0.3, 0.7, size=(nspheres, 3))
     radii = rng.uniform(0.1, 0.3, size=nspheres)
-    band = np.zeros((n, n, n), bool)
-    c = (np.arange(n) + 0.5) / n
     half = thickness / (2.0 * n)
-    for z0 in range(0, n, 64):
-        cz = c[z0:z0 + 64]
-        sdf = np.full((n, n, len(cz)), np.inf)
+    nb = n // 4
+
+    def sdf(p):  # p: [..., 3] in unit-box coordinates
+        d = np.full(p.shape[:-1], np.inf)
         for ctr, rad in zip(centres, radii):
-            d = np.sqrt((c[:, None, None] - ctr[0]) ** 2 + (c[None, :, None] - ctr[1]) ** 2 +
-                        (cz[None, None, :] - ctr[2]) ** 2) - rad
-            sdf = np.minimum(sdf, d)
-        band[:, :, z0:z0 + 64] = np.abs(sdf) <= half
-    rho = np.where(band, rng.uniform(1e-3, 1.0, size=(n, n, n)), 0.0)
-    ys = np.argwhere(band)[:, 1]
-    ymin = ys.min()
-    dcells = np.argwhere(band[:, ymin:ymin + 1, :]).astype(np.int32)
-    dcells[:, 1] += ymin
-    cells = np.argwhere(band)
-    pick = cells[rng.choice(len(cells), 16, replace=False)] + 1
+            d = np.minimum(d, np.sqrt(((p - ctr) ** 2).sum(-1)) - rad)
+        return d
+
+    # candidate blocks: block centre within half + block half-diagonal of the surface
+    g = (np.arange(nb) * 4 + 2.0) / n
+    cand = []
+    margin = half + np.sqrt(3) * 2.0 / n
+    for bi in range(nb):
+        pts = np.stack(np.broadcast_arrays(g[bi], g[:, None], g[None, :]), -1)
+        near = np.abs(sdf(pts)) <= margin
+        jj, kk = np.nonzero(near)
+        if len(jj):
+            cand.append(np.stack([np.full(len(jj), bi), jj, kk], 1))
+    cand = np.concatenate(cand).astype(np.int64)
+    # cell-level band test inside the candidate blocks
+    off = np.array([[i, j, k] for i in range(4) for j in range(4) for k in range(4)], np.int64)  # i*16+j*4+k
+    cells = cand[:, None, :] * 4 + off[None]                 # [nc, 64, 3] container cell coords
+    band = np.abs(sdf((cells + 0.5) / n)) <= half
+    keep = band.any(1)
+    mat_blocks, band = cand[keep], band[keep]
+    rho = np.where(band, rng.uniform(1e-3, 1.0, size=band.shape), 0.0)
+    # node blocks: the +x/+y/+z neighbours of material blocks (zero density)
+    fwd = np.array([[a, b, c] for a in (0, 1) for b in (0, 1) for c in (0, 1)], np.int64)
+    allb = np.unique((mat_blocks[:, None, :] + fwd[None]).reshape(-1, 3), axis=0)
+    key = lambda b: (b[:, 0] * nb + b[:, 1]) * nb + b[:, 2]
+    mk = key(mat_blocks)
+    order = np.argsort(mk)
+    pos = np.searchsorted(mk[order], key(allb))
+    pos = np.minimum(pos, len(mk) - 1)
+    is_mat = mk[order][pos] == key(allb)
+    data = np.zeros((len(allb), 64))
+    data[is_mat] = rho[order][pos[is_mat]]
+    base = (allb * 4 + PADDING).astype(np.int32)
+    # Dirichlet: every band cell of the lowest band cell layer
+    bc = (mat_blocks[:, None, :] * 4 + off[None])[band]
+    ymin = bc[:, 1].min()
+    dcells = bc[bc[:, 1] == ymin].astype(np.int32) + PADDING
+    # loads: 16 seeded band cells, load on the cell's (1,1,1) corner node
+    pick = bc[rng.choice(len(bc), 16, replace=False)] + 1 + PADDING
     f = np.zeros(16, FORCE_DTYPE)
     f["coord"] = pick
     v = rng.normal(size=(16, 3))
     f["f"] = v / np.linalg.norm(v, axis=1, keepdims=True)
-    return Problem(f"band{n}", (n, n, n), rho, dcells, f, 1.0 / n, mg_level_for(n, bottom_size))
+    kw = dict(tolerance=1e-6)
+    kw.update(solver_kw)
+    mu, lam = lame(kw.pop("E", 1e6), kw.pop("nu", 0.3))
+    p = FEMInputs()
+    p.resolution = [n + 7 * PADDING] * 3
+    p.dx = 1.0 / n
+    p.global_mu, p.global_lambda = mu, lam
+    p.density = BlockedGrid(resolution=list(p.resolution), base=base, data=data)
+    p.krylov = KrylovSolverParameters(kw.get("tolerance", 1e-6), kw.get("max_iterations", 50), 0, False)
+    p.extra_doubles.update({"penalty": kw.get("penalty", 3.0), "minimum_stiffness": kw.get("minimum_stiffness", 1e-9),
+                            "min_fraction": 0.0})
+    p.extra_ints.update({"boundary_smoothing": kw.get("boundary_smoothing", 3), "keep_state": 0, "forced_reuse": 1})
+    p.mg_level = kw.get("mg_level", mg_level_for(n, bottom_size))
+    p.pre_and_post_smoothing_iter = kw.get("smoothing", 1)
+    p.dirichlet_nodes = dirichlet_nodes_from_cells(dcells)
+    p.forces = f
+    p.caller_method = "spgrid_topo_opt_b200"
+    p.preserve_output(base.shape[0])
+    return p

@@ -219,6 +219,7 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
                rho_min = in.get_double("minimum_density", 0.0);
   P.penalty = penalty;
   P.minimum_stiffness = emin;
+  P.minimum_density = rho_min;
 
   // ---- level 0: page activation and stiffness (SPGrid_CPU_Solver.cpp:102-136)
   Builder b0;

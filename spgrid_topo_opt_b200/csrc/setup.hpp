@@ -46,7 +46,7 @@ struct Problem {
   // inputs
   int resolution[3] = {0, 0, 0};
   double dx = 1, mu0 = 0, lambda0 = 0;
-  double penalty = 0, minimum_stiffness = 0;  // SIMP parameters (fem_interface.h:318-353)
+  double penalty = 0, minimum_stiffness = 0, minimum_density = 0;  // SIMP parameters (fem_interface.h:318-353)
   int mg_levels = 3;          // levels after the mg_level=0 rewrite
   bool disable_mg = false;
   int explicit_level = 2;

@@ -8,84 +8,148 @@ namespace sgs {
 // ---------------------------------------------------------------------------
 // Galerkin operator of a coarse level at `depth` (solver/MG/Galerkin_Coarsen.h:40-100).
 // The reference prolongates a unit vector cell by cell down to the finest level,
-// applies the finest element matrices and restricts back.  Here the same
-// quantity is assembled directly: for coarse cell C and fine cell p inside it,
-// table[p][a][b][v][w] = sum_ij W_p[i][a] W_p[j][b] Kc[i][j][v][w] with W_p the
-// trilinear weights of C's corners at p's nodes, so
-//     K_C[(a,v),(b,w)] = sum_p E_p * table[p][a][b][v][w].
-// One CTA (576 threads: 8 cells x 8 corners x 9 components) per coarse node.
+// applies the finest element matrices and restricts back.  The same quantity is
+// assembled here in two steps.  For a coarse cell C and a finest cell p inside
+// it, table[p][a][b][v][w] = sum_ij W_p[i][a] W_p[j][b] Kc[i][j][v][w] (W_p: the
+// trilinear weights of C's corners at p's nodes), so the 24x24 cell matrix is
+//     K_C[(a,v),(b,w)] = sum_p E_p * table[p][a][b][v][w],
+// one row of a GEMM [cells x 8^depth] x [8^depth x 576].  Each active coarse
+// node then sums the row blocks of its corner from its 8 incident cells.
 // ---------------------------------------------------------------------------
-constexpr int GAL_CHUNK = 64;
 
-__global__ void __launch_bounds__(576) galerkin_kernel(const int* __restrict__ coords, const uint32_t* __restrict__ flags,
-                                                       int depth, GridView g0, const double* __restrict__ E0,
-                                                       const double* __restrict__ table, double* __restrict__ A,
-                                                       uint32_t* __restrict__ spokes, long N, double dx) {
-  __shared__ double sE[8][GAL_CHUNK];
-  __shared__ double contrib[8][72];
-  __shared__ int sorigin[8][3];
+// table[p][(a*8+b)*9 + v*3 + w], one thread per (p, a, b)
+__global__ void galerkin_table_kernel(int depth, double* __restrict__ table) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int side = 1 << depth;
+  const long npos = long(side) * side * side;
+  if (t >= npos * 64) return;
+  const long p = t >> 6;
+  const int a = int(t >> 3) & 7, b = int(t) & 7;
+  const int pc[3] = {int(p / (long(side) * side)), int((p / side) % side), int(p % side)};
+  double Wa[8], Wb[8];
+  for (int i = 0; i < 8; ++i) {
+    double wa = 1, wb = 1;
+    for (int ax = 0; ax < 3; ++ax) {
+      const double tpos = double(pc[ax] + ((i >> (2 - ax)) & 1)) / side;
+      wa *= ((a >> (2 - ax)) & 1) ? tpos : 1 - tpos;
+      wb *= ((b >> (2 - ax)) & 1) ? tpos : 1 - tpos;
+    }
+    Wa[i] = wa;
+    Wb[i] = wb;
+  }
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < 8; ++i) {
+    if (Wa[i] == 0) continue;
+    for (int j = 0; j < 8; ++j) {
+      const double w = Wa[i] * Wb[j];
+      if (w == 0) continue;
+      for (int m = 0; m < 9; ++m) acc[m] += w * c_Kc64[(i * 8 + j) * 9 + m];
+    }
+  }
+  double* out = table + p * 576 + (a * 8 + b) * 9;
+  for (int m = 0; m < 9; ++m) out[m] = acc[m];
+}
+
+// Cell matrices: C[cell][576] = sum_p E(origin_cell + p) * table[p][576], 64x64
+// output tiles, the E operand gathered from the finest level on the fly.
+constexpr int GT = 64;
+__global__ void __launch_bounds__(256) galerkin_cell_kernel(int ncells, const int* __restrict__ origin, int depth,
+                                                           GridView g0, const double* __restrict__ E0,
+                                                           const double* __restrict__ table, double* __restrict__ C) {
+  extern __shared__ double gsm[];
+  double* sA = gsm;            // [64 cells][65]
+  double* sB = gsm + GT * 65;  // [64 p][65]
+  const int col0 = blockIdx.x * GT;
+  const int cell0 = blockIdx.y * GT;
+  const int side = 1 << depth;
+  const long npos = long(side) * side * side;
+  const int t = threadIdx.x, ty = t / 16, tx = t % 16;
+  double acc[4][4] = {};
+  for (long p0 = 0; p0 < npos; p0 += GT) {
+    for (int i = t; i < GT * GT; i += 256) {
+      const int r = i / GT, k = i % GT;
+      const int cell = cell0 + r;
+      const long p = p0 + k;
+      double ev = 0;
+      if (cell < ncells && p < npos) {
+        const int px = int(p / (long(side) * side)), py = int((p / side) % side), pz = int(p % side);
+        const long n = g0.node(origin[3 * cell] + px, origin[3 * cell + 1] + py, origin[3 * cell + 2] + pz);
+        if (n >= 0) ev = E0[n];
+      }
+      sA[r * 65 + k] = ev;
+    }
+    __syncthreads();
+    for (int i = t; i < GT * GT; i += 256) {
+      const int k = i / GT, c = i % GT;
+      const long p = p0 + k;
+      sB[k * 65 + c] = p < npos ? table[p * 576 + col0 + c] : 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < GT; ++k) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) av[r] = sA[(ty + 16 * r) * 65 + k];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) bv[s] = sB[k * 65 + tx + 16 * s];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) acc[r][s] += av[r] * bv[s];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int cell = cell0 + ty + 16 * r;
+    if (cell >= ncells) continue;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) C[long(cell) * 576 + col0 + tx + 16 * s] = acc[r][s];
+  }
+}
+
+// Node stencils from the cell matrices: entry (q, v, w) sums the (corner, neighbour)
+// blocks of the incident cells in a fixed order; spoke q is active when any of
+// those blocks has a non-zero entry (Galerkin_Coarsen.h:79-93).  One CTA per node.
+__global__ void __launch_bounds__(256) galerkin_assemble_kernel(const int* __restrict__ coords,
+                                                               const uint32_t* __restrict__ flags,
+                                                               const int* __restrict__ cell_of_slot, GridView g,
+                                                               const double* __restrict__ C, double* __restrict__ A,
+                                                               uint32_t* __restrict__ spokes, double dx) {
+  __shared__ int scell[8];
   const long gidx = blockIdx.x;
   if (!(flags[gidx] & ACTIVE_NODE)) return;
   const int bi = int(gidx >> 7), e = int(gidx & 127);
   const int x = coords[3 * bi] + (e >> 5), y = coords[3 * bi + 1] + ((e >> 3) & 3), z = coords[3 * bi + 2] + (e & 7);
   const int t = threadIdx.x;
-  const int c = t / 72, b = (t / 9) % 8, vw = t % 9;
-  const int a = 7 - c;
-  const int side = 1 << depth;
   if (t < 8) {
-    // min corner of coarse cell t on the finest level: 2^d * cell - (2^d - 1) * (4,4,8)
-    const int ccx = x + (t >> 2) - 1, ccy = y + ((t >> 1) & 1) - 1, ccz = z + (t & 1) - 1;
-    sorigin[t][0] = side * ccx - (side - 1) * 4;
-    sorigin[t][1] = side * ccy - (side - 1) * 4;
-    sorigin[t][2] = side * ccz - (side - 1) * 8;
+    const long n = g.node(x + (t >> 2) - 1, y + ((t >> 1) & 1) - 1, z + (t & 1) - 1);
+    scell[t] = n >= 0 ? cell_of_slot[n] : -1;
   }
-  __syncthreads();
-  const long npos = long(side) * side * side;
-  double acc = 0;
-  for (long p0 = 0; p0 < npos; p0 += GAL_CHUNK) {
-    if (t < 8 * GAL_CHUNK) {
-      const int cc = t / GAL_CHUNK;
-      const long p = p0 + t % GAL_CHUNK;
-      double ev = 0;
-      if (p < npos) {
-        const int px = int(p / (long(side) * side)), py = int((p / side) % side), pz = int(p % side);
-        const long n = g0.node(sorigin[cc][0] + px, sorigin[cc][1] + py, sorigin[cc][2] + pz);
-        if (n >= 0) ev = E0[n];
-      }
-      sE[cc][t % GAL_CHUNK] = ev;
-    }
-    __syncthreads();
-    const int np = int(min(long(GAL_CHUNK), npos - p0));
-    const double* tb = table + ((p0 * 8 + a) * 8 + b) * 9 + vw;
-    for (int q = 0; q < np; ++q) {
-      const double ev = sE[c][q];
-      if (ev != 0) acc += ev * tb[long(q) * 576];
-    }
-    __syncthreads();
-  }
-  contrib[c][b * 9 + vw] = acc;
   __syncthreads();
   if (t < 243) {
-    const int q = t / 9, w9 = t % 9;
+    const int q = t / 9, vw = t % 9;
     const int qi = q / 9, qj = (q / 3) % 3, qk = q % 3;
     double s = 0;
-    for (int cc = 0; cc < 8; ++cc) {
-      const int bx = qi - (cc >> 2), by = qj - ((cc >> 1) & 1), bz = qk - (cc & 1);
-      if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
-      s += contrib[cc][((bx << 2) | (by << 1) | bz) * 9 + w9];
+    for (int c = 0; c < 8; ++c) {
+      const int bx = qi - (c >> 2), by = qj - ((c >> 1) & 1), bz = qk - (c & 1);
+      if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1 || scell[c] < 0) continue;
+      s += C[long(scell[c]) * 576 + ((7 - c) * 8 + ((bx << 2) | (by << 1) | bz)) * 9 + vw];
     }
-    A[gidx * 243 + q * 9 + w9] = s * dx;
+    A[gidx * 243 + t] = s * dx;
   }
-  if (t < 27) {
-    const int qi = t / 9, qj = (t / 3) % 3, qk = t % 3;
+  if (t < 32) {
     bool nz = false;
-    for (int cc = 0; cc < 8; ++cc) {
-      const int bx = qi - (cc >> 2), by = qj - ((cc >> 1) & 1), bz = qk - (cc & 1);
-      if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
-      for (int k = 0; k < 9; ++k) nz |= contrib[cc][((bx << 2) | (by << 1) | bz) * 9 + k] != 0.0;
+    if (t < 27) {
+      const int qi = t / 9, qj = (t / 3) % 3, qk = t % 3;
+      for (int c = 0; c < 8; ++c) {
+        const int bx = qi - (c >> 2), by = qj - ((c >> 1) & 1), bz = qk - (c & 1);
+        if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1 || scell[c] < 0) continue;
+        const double* blk = C + long(scell[c]) * 576 + ((7 - c) * 8 + ((bx << 2) | (by << 1) | bz)) * 9;
+        for (int k = 0; k < 9; ++k) nz |= blk[k] != 0.0;
+      }
     }
-    unsigned m = __ballot_sync(0x07ffffffu, nz);
-    if (t == 0) spokes[gidx] = m;
+    const unsigned m = __ballot_sync(0xffffffffu, nz);
+    if (t == 0) spokes[gidx] = m & 0x07ffffffu;
   }
 }
 

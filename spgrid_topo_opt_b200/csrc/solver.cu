@@ -252,44 +252,9 @@ class Solver {
     }
   }
 
-  // Galerkin tables for one depth: table[p][a][b][v][w]
-  std::vector<double> galerkin_table(int depth) {
-    double Kmu[8][8][3][3], Kla[8][8][3][3];
-    element_tables(Kmu, Kla);
-    const int side = 1 << depth;
-    const long npos = long(side) * side * side;
-    std::vector<double> tab(size_t(npos) * 576, 0.0);
-    double Kc[8][8][9];
-    for (int i = 0; i < 8; ++i)
-      for (int j = 0; j < 8; ++j)
-        for (int vw = 0; vw < 9; ++vw) Kc[i][j][vw] = P.mu0 * Kmu[i][j][vw / 3][vw % 3] + P.lambda0 * Kla[i][j][vw / 3][vw % 3];
-    for (long p = 0; p < npos; ++p) {
-      const int pc[3] = {int(p / (long(side) * side)), int((p / side) % side), int(p % side)};
-      double W[8][8];  // W[i][a]
-      for (int i = 0; i < 8; ++i)
-        for (int a = 0; a < 8; ++a) {
-          double w = 1;
-          for (int ax = 0; ax < 3; ++ax) {
-            double tpos = double(pc[ax] + ((i >> (2 - ax)) & 1)) / side;
-            w *= ((a >> (2 - ax)) & 1) ? tpos : 1 - tpos;
-          }
-          W[i][a] = w;
-        }
-      double* out = &tab[size_t(p) * 576];
-      for (int a = 0; a < 8; ++a)
-        for (int b = 0; b < 8; ++b)
-          for (int vw = 0; vw < 9; ++vw) {
-            double s = 0;
-            for (int i = 0; i < 8; ++i) {
-              if (W[i][a] == 0) continue;
-              for (int j = 0; j < 8; ++j) s += W[i][a] * W[j][b] * Kc[i][j][vw];
-            }
-            out[(a * 8 + b) * 9 + vw] = s;
-          }
-    }
-    return tab;
-  }
-
+  // Galerkin operators of the levels >= explicit_level (all on the GPU):
+  // table of the depth, cell matrices as a GEMM over the finest cells, node
+  // stencils, Dirichlet deletion (Multigrid_Hierarchy.h:215-226).
   void build_operators() {
     if (P.disable_mg) return;
     const int n = nlev();
@@ -297,23 +262,45 @@ class Solver {
     for (int lev = first; lev < n; ++lev) {
       Level<double>& d = *L64[lev];
       if (lev > 6) throw CudaError("multigrid depth above 6 is not supported", SGS_ERR_INPUT);
-      std::vector<double> tab = galerkin_table(lev);
-      DevBuf<double> dtab;
-      dtab.upload(tab, stream);
+      const HostLevel& h = P.levels[lev];
+      const int side = 1 << lev;
+      const long npos = long(side) * side * side;
+      // active coarse cells (the only ones with finest material) and their finest origin
+      std::vector<int32_t> origin, cell_of_slot(size_t(d.N), -1);
+      int ncells = 0;
+      const int B[3] = {BLK_X, BLK_Y, BLK_Z};
+      for (long slot = 0; slot < d.N; ++slot) {
+        if (!(h.flags[slot] & F_ACTIVE_CELL)) continue;
+        const int b = int(slot / NODES_PER_BLOCK), e = int(slot % NODES_PER_BLOCK);
+        const int c[3] = {h.coords[3 * b] + (e >> 5), h.coords[3 * b + 1] + ((e >> 3) & 3), h.coords[3 * b + 2] + (e & 7)};
+        for (int v = 0; v < 3; ++v) origin.push_back(side * c[v] - (side - 1) * B[v]);
+        cell_of_slot[slot] = ncells++;
+      }
       d.A.alloc(243 * size_t(d.N));
       d.A.zero(stream);
       d.spokes.alloc(size_t(d.N));
       d.spokes.zero(stream);
       d.has_matrix = true;
-      if (d.N > 0) {
-        galerkin_kernel<<<unsigned(d.N), 576, 0, stream>>>(d.coords.p, d.flags.p, lev, L64[0]->grid, E64.p, dtab.p, d.A.p,
-                                                          d.spokes.p, d.N, P.dx);
+      if (ncells > 0) {
+        DevBuf<double> table, cellmat;
+        DevBuf<int32_t> dorigin, dcell;
+        table.alloc(size_t(npos) * 576);
+        galerkin_table_kernel<<<blocks_for(npos * 64, 128), 128, 0, stream>>>(lev, table.p);
+        dorigin.upload(origin, stream);
+        dcell.upload(cell_of_slot, stream);
+        cellmat.alloc(size_t(ncells) * 576);
+        const size_t smem = 2 * GT * 65 * sizeof(double);
+        SGS_CUDA(cudaFuncSetAttribute(galerkin_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        galerkin_cell_kernel<<<dim3(576 / GT, (ncells + GT - 1) / GT), 256, smem, stream>>>(
+            ncells, dorigin.p, lev, L64[0]->grid, E64.p, table.p, cellmat.p);
+        galerkin_assemble_kernel<<<unsigned(d.N), 256, 0, stream>>>(d.coords.p, d.flags.p, dcell.p, d.grid, cellmat.p, d.A.p,
+                                                                   d.spokes.p, P.dx);
         SGS_CUDA(cudaGetLastError());
         delete_dirichlet_kernel<<<blocks_for(d.N, 128), 128, 0, stream>>>(d.nb, d.coords.p, d.flags.p, d.spokes.p, d.grid,
                                                                          d.A.p, d.N);
         SGS_CUDA(cudaGetLastError());
+        SGS_CUDA(cudaStreamSynchronize(stream));  // the temporaries go out of scope
       }
-      SGS_CUDA(cudaStreamSynchronize(stream));  // dtab goes out of scope
       if (mixed()) {
         Level<float>& m = *L32[lev];
         m.A.alloc(243 * size_t(d.N));
@@ -583,6 +570,43 @@ class Solver {
   void solve();
   void pack_outputs(std::vector<double>& disp);
   double sensitivity(const double* rho, double penalty, double emin, double* dc, double* se);
+
+  // New densities for the same material pattern: E, the Galerkin operators and
+  // the bottom inverse are rebuilt, the hierarchy and flags are kept.
+  std::string update_density(const double* rho) {
+    const size_t nin = P.in_block.size();
+    std::vector<double> E = P.E;
+    for (size_t b = 0; b < nin; ++b) {
+      const int blk = P.in_block[b];
+      if (blk < 0) continue;
+      for (int e = 0; e < 64; ++e) {
+        const double d = rho[b * 64 + e];
+        double val = 0;
+        if (d > 0)
+          val = P.penalty ? (1 - P.minimum_stiffness) * std::pow(std::max(P.minimum_density, d), P.penalty) +
+                                P.minimum_stiffness
+                          : d;
+        if (!std::isfinite(val)) return "non-finite density";
+        const size_t slot = size_t(blk) * NODES_PER_BLOCK + (e >> 4) * 32 + ((e >> 2) & 3) * 8 + (e & 3) + P.in_zoff[b];
+        if ((val * P.mu0 != 0) != (P.E[slot] * P.mu0 != 0))
+          return "the set of material cells changed; create a new session";
+        E[slot] = val;
+      }
+    }
+    P.E.swap(E);
+    SGS_CUDA(cudaMemcpyAsync(E64.p, P.E.data(), P.E.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    g_h2d_bytes += P.E.size() * sizeof(double);
+    if (mixed())
+      convert_kernel<float, double><<<blocks_for(long(P.E.size()), 256), 256, 0, stream>>>(E32.p, E64.p, long(P.E.size()));
+    if (iter_graph) {  // the captured iteration refers to the old operator buffers
+      SGS_CUDA(cudaGraphExecDestroy(iter_graph));
+      iter_graph = nullptr;
+    }
+    build_operators();
+    build_bottom();
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    return std::string();
+  }
 };
 
 template <>
@@ -1240,6 +1264,21 @@ SGS_API int sgs_sensitivity_static(sgs_session* h, const double* density_dev, do
     }
     SGS_CUDA(cudaGetLastError());
     SGS_CUDA(cudaStreamSynchronize(S.stream));
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+SGS_API int sgs_set_density(sgs_session* h, const double* density) {
+  if (!h || !density || host_only(h)) return SGS_ERR_INPUT;
+  try {
+    std::string m = h->solver->update_density(density);
+    if (!m.empty()) {
+      h->error = m;
+      return SGS_ERR_INPUT;
+    }
   } catch (const CudaError& e) {
     h->error = e.what();
     return e.code;

@@ -22,7 +22,7 @@ OP_KU, OP_RESIDUAL, OP_SMOOTH, OP_RESTRICT, OP_PROLONG, OP_STENCIL, OP_BOTTOM, O
 EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", "sgs_last_error", "sgs_solve",
                     "sgs_residual_history", "sgs_displacements", "sgs_sensitivity", "sgs_level_count",
                     "sgs_level_blocks", "sgs_level_flags", "sgs_boundary_blocks", "sgs_apply", "sgs_level_stencils",
-                    "sgs_codec_roundtrip", "sgs_time_op", "sgs_sensitivity_static")
+                    "sgs_codec_roundtrip", "sgs_time_op", "sgs_sensitivity_static", "sgs_set_density")
 
 
 class SolverError(RuntimeError):
@@ -81,6 +81,7 @@ def load(build_if_missing: bool = False):
     L.sgs_time_op.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.sgs_sensitivity_static.argtypes = [P, P, P, P, P]
     L.sgs_sensitivity_static.restype = C.c_int
+    L.sgs_set_density.argtypes = [P, P]
     _lib = L
     return L
 
@@ -187,6 +188,14 @@ class Session:
         if not np.isfinite(obj):
             raise SolverError(10, load().sgs_last_error(self.h).decode(errors="replace"))
         return obj, dc, se
+
+    def set_density(self, density: np.ndarray) -> None:
+        """New densities for the same material pattern (operators are rebuilt)."""
+        rho = np.ascontiguousarray(density, np.float64).reshape(-1, 64)
+        if rho.shape[0] != self.inputs.density.base.shape[0]:
+            raise ValueError("density must have one row of 64 values per input block")
+        self._check(load().sgs_set_density(self.h, _ptr(rho)))
+        self.inputs.density.data = rho.copy()
 
     def time_op(self, op: int, reps: int = 20) -> float:
         """Average device milliseconds of a level-0 operator (0 K*u, 1 residual,
