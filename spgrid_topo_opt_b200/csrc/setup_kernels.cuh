@@ -313,6 +313,7 @@ __global__ void gj_store_pivot_kernel(double* M, long ld, int K, const double* _
 template <typename T>
 __global__ void bottom_gather_kernel(int ndof, const int* __restrict__ dof_node, const T* __restrict__ b, long N,
                                      double* __restrict__ xb) {
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ndof) return;
   long n = dof_node[i];
@@ -324,6 +325,7 @@ __global__ void bottom_gather_kernel(int ndof, const int* __restrict__ dof_node,
 // y = M x, one warp per row
 __global__ void gemv_kernel(const double* __restrict__ M, long ld, long n, const double* __restrict__ x,
                             double* __restrict__ y) {
+  pdl_wait();
   const long row = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (row >= n) return;
@@ -337,6 +339,7 @@ __global__ void gemv_kernel(const double* __restrict__ M, long ld, long n, const
 template <typename T>
 __global__ void bottom_scatter_kernel(int ndof, const int* __restrict__ dof_node, const double* __restrict__ xs,
                                       T* __restrict__ u, long N) {
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ndof) return;
   long n = dof_node[i];

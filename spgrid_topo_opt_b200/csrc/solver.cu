@@ -174,6 +174,24 @@ class Solver {
   }
 
   long N0() const { return long(P.levels[0].nb) * NODES_PER_BLOCK; }
+
+  // Launch on the solver stream with programmatic stream serialization (the
+  // kernel begins with pdl_wait(), so it may be scheduled while its
+  // predecessor finishes).
+  template <typename... KArgs, typename... Args>
+  void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SGS_CUDA(cudaLaunchKernelEx(&cfg, kernel, KArgs(args)...));
+  }
   bool mixed() const { return precision == PREC_MIXED; }
   bool round_ref() const { return precision == PREC_REFERENCE; }
   int nlev() const { return int(P.levels.size()); }
@@ -248,7 +266,7 @@ class Solver {
     E64.upload(P.E, stream);
     if (mixed()) {
       E32.alloc(P.E.size());
-      convert_kernel<float, double><<<blocks_for(long(P.E.size()), 256), 256, 0, stream>>>(E32.p, E64.p, long(P.E.size()));
+      launch(convert_kernel<float, double>, blocks_for(long(P.E.size()), 256), 256, 0, E32.p, E64.p, long(P.E.size()));
     }
   }
 
@@ -304,7 +322,7 @@ class Solver {
       if (mixed()) {
         Level<float>& m = *L32[lev];
         m.A.alloc(243 * size_t(d.N));
-        convert_kernel<float, double><<<blocks_for(243 * d.N, 256), 256, 0, stream>>>(m.A.p, d.A.p, 243 * d.N);
+        launch(convert_kernel<float, double>, blocks_for(243 * d.N, 256), 256, 0, m.A.p, d.A.p, 243 * d.N);
         m.spokes.alloc(size_t(d.N));
         SGS_CUDA(cudaMemcpyAsync(m.spokes.p, d.spokes.p, d.N * 4, cudaMemcpyDeviceToDevice, stream));
         m.has_matrix = true;
@@ -405,20 +423,20 @@ class Solver {
   void project(Level<T>& d, T* v) {
     for (int c = 0; c < 3; ++c)
       if (d.ndir[c]) {
-        zero_list_kernel<T><<<blocks_for(d.ndir[c], 256), 256, 0, stream>>>(v, d.dir[c].p, d.ndir[c]);
+        launch(zero_list_kernel<T>, blocks_for(d.ndir[c], 256), 256, 0, v, d.dir[c].p, d.ndir[c]);
         ++launch_counter;
       }
   }
 
   template <typename T>
   void project_null(Level<T>& d, T* v) {
-    project_null_kernel<T><<<blocks_for(d.N, 256), 256, 0, stream>>>(v, d.flags.p, d.N);
+    launch(project_null_kernel<T>, blocks_for(d.N, 256), 256, 0, v, d.flags.p, d.N);
     ++launch_counter;
   }
 
   template <typename T>
   void round3(Level<T>& d, T* v) {
-    round_float_kernel<T><<<blocks_for(3 * d.N, 256), 256, 0, stream>>>(v, 3 * d.N);
+    launch(round_float_kernel<T>, blocks_for(3 * d.N, 256), 256, 0, v, 3 * d.N);
     ++launch_counter;
   }
 
@@ -426,7 +444,7 @@ class Solver {
   void level0(const int* list, int count, const T* u, T* uo, const T* b, T* out, int color, int boundary) {
     Level<T>& d = lev<T>(0);
     if (count <= 0) return;
-    level0_op_kernel<T, OP><<<count, 128, 0, stream>>>(list, count, d.nbr.p, Edev<T>(), u, uo, b, out, d.flags.p, d.N,
+    launch(level0_op_kernel<T, OP>, count, 128, 0, list, count, d.nbr.p, Edev<T>(), u, uo, b, out, d.flags.p, d.N,
                                                       T(P.dx), color, boundary);
     ++launch_counter;
   }
@@ -437,7 +455,7 @@ class Solver {
     Level<T>& d = lev<T>(l);
     if (count <= 0) return;
     const int per = OP == SOP_GS ? 16 : 128;
-    stencil_op_kernel<T, OP><<<blocks_for(long(count) * per * 32, 256), 256, 0, stream>>>(
+    launch(stencil_op_kernel<T, OP>, blocks_for(long(count) * per * 32, 256), 256, 0, 
         list, count, d.coords.p, d.grid, d.A.p, d.flags.p, u, uo, b, out, d.N, color, boundary, round_out);
     ++launch_counter;
   }
@@ -452,8 +470,12 @@ class Solver {
     if (l == 0) {
       for (int k = 0; k < 8; ++k) {
         const int c = forward ? k : 7 - k;
-        gs0_kernel<T><<<blocks_for(count, 8), 128, 0, stream>>>(list, count, d.nbr.p, Edev<T>(), u, b, d.flags.p, d.N,
-                                                                T(P.dx), c, boundary ? 1 : 0);
+        if constexpr (sizeof(T) == 4)
+          launch(gs0_f32_kernel, blocks_for(count, 8), 128, 0, list, count, d.nbr.p, Edev<T>(), u, b, d.flags.p, d.N,
+                 T(P.dx), c, boundary ? 1 : 0);
+        else
+          launch(gs0_kernel<T>, blocks_for(count, 8), 128, 0, list, count, d.nbr.p, Edev<T>(), u, b, d.flags.p, d.N,
+                 T(P.dx), c, boundary ? 1 : 0);
         ++launch_counter;
       }
       return;
@@ -485,7 +507,7 @@ class Solver {
     Level<T>& c = lev<T>(lc);
     Level<T>& fl = lev<T>(lc - 1);
     if (c.N == 0) return;
-    restrict_kernel<T><<<blocks_for(c.N, 128), 128, 0, stream>>>(c.nb, c.coords.p, c.flags.p, fl.grid, fine_field, fl.N,
+    launch(restrict_kernel<T>, blocks_for(c.N, 128), 128, 0, c.nb, c.coords.p, c.flags.p, fl.grid, fine_field, fl.N,
                                                                 c.b.p, c.N);
     ++launch_counter;
   }
@@ -495,7 +517,7 @@ class Solver {
     Level<T>& fl = lev<T>(lf);
     Level<T>& c = lev<T>(lf + 1);
     if (fl.N == 0) return;
-    prolongate_kernel<T><<<blocks_for(fl.N, 128), 128, 0, stream>>>(fl.nb, fl.coords.p, fl.flags.p, c.grid, c.u.p, c.N,
+    launch(prolongate_kernel<T>, blocks_for(fl.N, 128), 128, 0, fl.nb, fl.coords.p, fl.flags.p, c.grid, c.u.p, c.N,
                                                                    fine_u, fl.N, round_ref() ? 1 : 0);
     ++launch_counter;
   }
@@ -506,11 +528,11 @@ class Solver {
     // nodes without unknowns keep b (the reference copies b in and out)
     SGS_CUDA(cudaMemcpyAsync(d.u.p, d.b.p, 3 * d.N * sizeof(T), cudaMemcpyDeviceToDevice, stream));
     if (bottom.ndof_nodes > 0) {
-      bottom_gather_kernel<T><<<blocks_for(bottom.ndof_nodes, 128), 128, 0, stream>>>(bottom.ndof_nodes, bottom.dof_node.p,
+      launch(bottom_gather_kernel<T>, blocks_for(bottom.ndof_nodes, 128), 128, 0, bottom.ndof_nodes, bottom.dof_node.p,
                                                                                      d.b.p, d.N, bottom.xb.p);
-      gemv_kernel<<<blocks_for(bottom.ld * 32, 256), 256, 0, stream>>>(bottom.Minv.p, bottom.ld, bottom.ld, bottom.xb.p,
+      launch(gemv_kernel, blocks_for(bottom.ld * 32, 256), 256, 0, bottom.Minv.p, bottom.ld, bottom.ld, bottom.xb.p,
                                                                       bottom.xs.p);
-      bottom_scatter_kernel<T><<<blocks_for(bottom.ndof_nodes, 128), 128, 0, stream>>>(bottom.ndof_nodes,
+      launch(bottom_scatter_kernel<T>, blocks_for(bottom.ndof_nodes, 128), 128, 0, bottom.ndof_nodes,
                                                                                       bottom.dof_node.p, bottom.xs.p,
                                                                                       d.u.p, d.N);
       launch_counter += 3;
@@ -597,7 +619,7 @@ class Solver {
     SGS_CUDA(cudaMemcpyAsync(E64.p, P.E.data(), P.E.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
     g_h2d_bytes += P.E.size() * sizeof(double);
     if (mixed())
-      convert_kernel<float, double><<<blocks_for(long(P.E.size()), 256), 256, 0, stream>>>(E32.p, E64.p, long(P.E.size()));
+      launch(convert_kernel<float, double>, blocks_for(long(P.E.size()), 256), 256, 0, E32.p, E64.p, long(P.E.size()));
     if (iter_graph) {  // the captured iteration refers to the old operator buffers
       SGS_CUDA(cudaGraphExecDestroy(iter_graph));
       iter_graph = nullptr;
@@ -625,6 +647,7 @@ constexpr int RED_BLOCKS = 592, RED_THREADS = 256;  // 4 CTAs per SM on 148 SMs
 
 __global__ void dot_partial_kernel(const double* __restrict__ a, const double* __restrict__ b, long n,
                                    double* __restrict__ part) {
+  pdl_wait();
   __shared__ double sm[RED_THREADS / 32];
   double s = 0;
   for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) s += a[i] * b[i];
@@ -639,6 +662,7 @@ __global__ void dot_partial_kernel(const double* __restrict__ a, const double* _
 }
 
 __global__ void linf_partial_kernel(const double* __restrict__ a, long n, double* __restrict__ part) {
+  pdl_wait();
   __shared__ double sm[RED_THREADS / 32];
   double s = 0;
   for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) s = fmax(s, fabs(a[i]));
@@ -656,6 +680,7 @@ __global__ void linf_partial_kernel(const double* __restrict__ a, long n, double
 // what = 0: rho -> beta = rho/rho_old;  what = 1: sq -> alpha, -alpha, breakdown flag;
 // what = 2: norm.
 __global__ void finish_reduce_kernel(const double* __restrict__ part, int np, int op, double* scal, int what) {
+  pdl_wait();
   __shared__ double sm[32];
   double s = 0;
   for (int i = threadIdx.x; i < np; i += 32) s = op ? fmax(s, part[i]) : s + part[i];
@@ -680,12 +705,14 @@ __global__ void finish_reduce_kernel(const double* __restrict__ part, int np, in
   }
 }
 
-__global__ void rho_shift_kernel(double* scal) { scal[1] = scal[0]; }
+__global__ void rho_shift_kernel(double* scal) {
+  pdl_wait(); scal[1] = scal[0]; }
 
 // dst = c*x + y, c = scal[slot]; optionally in single precision like the
 // reference's float-rounded CG_VECTOR::Copy (CG_VECTOR.cpp:96-114)
 __global__ void axpy_kernel(double* dst, const double* __restrict__ scal, int slot, const double* xv, const double* yv,
                             long n, int float_round) {
+  pdl_wait();
   long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double c = scal[slot];
@@ -695,6 +722,7 @@ __global__ void axpy_kernel(double* dst, const double* __restrict__ scal, int sl
 
 // r = r - q with optional float rounding (CG_VECTOR::operator-=, CG_VECTOR.cpp:35-52)
 __global__ void sub_kernel(double* r, const double* __restrict__ q, long n, int float_round) {
+  pdl_wait();
   long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (float_round) r[i] = double(__fsub_rn(float(r[i]), float(q[i])));
@@ -703,17 +731,20 @@ __global__ void sub_kernel(double* r, const double* __restrict__ q, long n, int 
 
 __global__ void scatter_lift_kernel(double* u, const int* __restrict__ node, const int* __restrict__ axis,
                                     const double* __restrict__ val, int n, long N) {
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) u[node[i] + axis[i] * N] = val[i];
 }
 
 __global__ void scatter_force_kernel(double* s, const int* __restrict__ node, const double* __restrict__ val, int n, long N) {
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int v = 0; v < 3; ++v) s[node[i] + v * N] = val[3 * i + v];
 }
 
 __global__ void add_kernel(double* a, const double* __restrict__ b, long n) {
+  pdl_wait();
   long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) a[i] += b[i];
 }
@@ -722,6 +753,7 @@ __global__ void add_kernel(double* a, const double* __restrict__ b, long n) {
 // (u_x, u_y, u_z, max_v |r_v|)
 __global__ void pack_kernel(int nin, const int* __restrict__ in_block, const int* __restrict__ in_zoff,
                             const double* __restrict__ u, const double* __restrict__ r, long N, double* __restrict__ out) {
+  pdl_wait();
   long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= long(nin) * 64) return;
   int b = int(t >> 6), e = int(t & 63);
@@ -790,18 +822,18 @@ __global__ void sensitivity_kernel(int nin, const int* __restrict__ in_block, co
 
 void Solver::dot(const double* a, const double* b, double* out_unused) {
   (void)out_unused;
-  dot_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, stream>>>(a, b, 3 * N0(), red.p);
+  launch(dot_partial_kernel, RED_BLOCKS, RED_THREADS, 0, a, b, 3 * N0(), red.p);
   launch_counter += 1;
 }
 
 void Solver::linf(const double* a, double*) {
-  linf_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, stream>>>(a, 3 * N0(), red.p);
-  finish_reduce_kernel<<<1, 32, 0, stream>>>(red.p, RED_BLOCKS, 1, scal.p, 2);
+  launch(linf_partial_kernel, RED_BLOCKS, RED_THREADS, 0, a, 3 * N0(), red.p);
+  launch(finish_reduce_kernel, 1, 32, 0, red.p, RED_BLOCKS, 1, scal.p, 2);
   launch_counter += 2;
 }
 
 void Solver::axpy(double* dst, double, int slot, const double* xv, const double* yv) {
-  axpy_kernel<<<blocks_for(3 * N0(), 256), 256, 0, stream>>>(dst, scal.p, slot, xv, yv, 3 * N0(), round_ref() ? 1 : 0);
+  launch(axpy_kernel, blocks_for(3 * N0(), 256), 256, 0, dst, scal.p, slot, xv, yv, 3 * N0(), round_ref() ? 1 : 0);
   ++launch_counter;
 }
 
@@ -814,9 +846,9 @@ void Solver::precondition() {
     SGS_CUDA(cudaMemcpyAsync(q.p, f.p, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
   } else if (mixed()) {
     Level<float>& m0 = *L32[0];
-    convert_kernel<float, double><<<blocks_for(3 * N, 256), 256, 0, stream>>>(m0.b.p, f.p, 3 * N);
+    launch(convert_kernel<float, double>, blocks_for(3 * N, 256), 256, 0, m0.b.p, f.p, 3 * N);
     vcycle<float>(m0.b.p, m0.u.p);
-    convert_kernel<double, float><<<blocks_for(3 * N, 256), 256, 0, stream>>>(q.p, m0.u.p, 3 * N);
+    launch(convert_kernel<double, float>, blocks_for(3 * N, 256), 256, 0, q.p, m0.u.p, 3 * N);
     launch_counter += 2;
   } else {
     vcycle<double>(f.p, q.p);
@@ -830,16 +862,16 @@ void Solver::precondition() {
 void Solver::record_iteration() {
   Level<double>& l0 = *L64[0];
   precondition();
-  dot_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, stream>>>(q.p, f.p, 3 * N0(), red.p);
-  finish_reduce_kernel<<<1, 32, 0, stream>>>(red.p, RED_BLOCKS, 0, scal.p, 0);
+  launch(dot_partial_kernel, RED_BLOCKS, RED_THREADS, 0, q.p, f.p, 3 * N0(), red.p);
+  launch(finish_reduce_kernel, 1, 32, 0, red.p, RED_BLOCKS, 0, scal.p, 0);
   axpy(s.p, 1, 4, s.p, q.p);  // s = beta*s + z
   level0<double, OP_KU>(nullptr, l0.nb, s.p, nullptr, nullptr, q.p, 0, 0);
   project<double>(l0, q.p);
-  dot_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, stream>>>(s.p, q.p, 3 * N0(), red.p);
-  finish_reduce_kernel<<<1, 32, 0, stream>>>(red.p, RED_BLOCKS, 0, scal.p, 1);
+  launch(dot_partial_kernel, RED_BLOCKS, RED_THREADS, 0, s.p, q.p, 3 * N0(), red.p);
+  launch(finish_reduce_kernel, 1, 32, 0, red.p, RED_BLOCKS, 0, scal.p, 1);
   axpy(x.p, 1, 5, s.p, x.p);   // x = alpha*s + x
   axpy(f.p, 1, 6, q.p, f.p);   // r = -alpha*q + r
-  rho_shift_kernel<<<1, 1, 0, stream>>>(scal.p);
+  launch(rho_shift_kernel, 1, 1, 0, scal.p);
   project_null<double>(l0, f.p);
   linf(f.p, nullptr);
   launch_counter += 5;
@@ -861,12 +893,12 @@ void Solver::solve() {
   // u = g on the listed Dirichlet nodes (SPGrid_CPU_Solver.cpp:241-285)
   x.zero(stream);
   if (!P.lift_node.empty())
-    scatter_lift_kernel<<<blocks_for(long(P.lift_node.size()), 128), 128, 0, stream>>>(
+    launch(scatter_lift_kernel, blocks_for(long(P.lift_node.size()), 128), 128, 0, 
         x.p, lift_node.p, lift_axis.p, lift_val.p, int(P.lift_node.size()), N);
   // s = forces; Project; Project_Nullspace; f = s - K u; Project (:287-301)
   s.zero(stream);
   if (!P.force_node.empty())
-    scatter_force_kernel<<<blocks_for(long(P.force_node.size()), 128), 128, 0, stream>>>(
+    launch(scatter_force_kernel, blocks_for(long(P.force_node.size()), 128), 128, 0, 
         s.p, force_node.p, force_val.p, int(P.force_node.size()), N);
   project<double>(l0, s.p);
   project_null<double>(l0, s.p);
@@ -884,7 +916,7 @@ void Solver::solve() {
   x.zero(stream);
   // CONJUGATE_GRADIENT_4Ch::Solve: q = K x (= 0); r -= q; Project(r)
   level0<double, OP_KU>(nullptr, l0.nb, x.p, nullptr, nullptr, q.p, 0, 0);
-  sub_kernel<<<blocks_for(n3, 256), 256, 0, stream>>>(f.p, q.p, n3, fr);
+  launch(sub_kernel, blocks_for(n3, 256), 256, 0, f.p, q.p, n3, fr);
   project<double>(l0, f.p);
   double init_scal[16] = {0};
   init_scal[1] = 3.40282346638528859811704183484516925440e+38;  // FLT_MAX (rho_old)
@@ -927,7 +959,7 @@ void Solver::solve() {
     SGS_CUDA(cudaGraphLaunch(iter_graph, stream));
     solve_launches += launches_per_iteration;
   }
-  add_kernel<<<blocks_for(n3, 256), 256, 0, stream>>>(x.p, ubk.p, n3);
+  launch(add_kernel, blocks_for(n3, 256), 256, 0, x.p, ubk.p, n3);
   ++launch_counter;
   SGS_CUDA(cudaEventRecord(ev_end, stream));
   SGS_CUDA(cudaGetLastError());
@@ -943,7 +975,7 @@ void Solver::pack_outputs(std::vector<double>& disp) {
   const long nin = long(P.in_block.size());
   disp.assign(size_t(nin) * 256, 0.0);
   if (nin == 0) return;
-  pack_kernel<<<blocks_for(nin * 64, 256), 256, 0, stream>>>(int(nin), in_block.p, in_zoff.p, x.p, f.p, N0(), out_disp.p);
+  launch(pack_kernel, blocks_for(nin * 64, 256), 256, 0, int(nin), in_block.p, in_zoff.p, x.p, f.p, N0(), out_disp.p);
   SGS_CUDA(cudaMemcpyAsync(disp.data(), out_disp.p, disp.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
   g_d2h_bytes += disp.size() * sizeof(double);
   SGS_CUDA(cudaStreamSynchronize(stream));
