@@ -168,82 +168,118 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// Level-0 Gauss-Seidel colour pass (solver/CPU_Kernels/SPGrid_Gauss_Seidel.h:876-1180):
-// 8 blocks per CTA, the 16 colour-`color` nodes of each block one per thread.
-// Neighbours are read through L1; the residual is accumulated neighbour by
-// neighbour, A_d = sum over the cells shared with neighbour d of E_c Kc[I][J].
-// Same-colour nodes never share a cell, so a pass updates in place.
+// Level-0 Gauss-Seidel colour pass over a compact list of the colour's nodes
+// (solver/CPU_Kernels/SPGrid_Gauss_Seidel.h:876-1180), one node per thread.
+// The residual is accumulated cell by cell, g_I = sum_J Kc[I][J] u_J over the
+// node's 8 cells and f = sum_I E_I g_I, visiting the 27 neighbours one x-plane
+// (9 nodes) at a time; a cell is folded into f after its last plane.  Same-
+// colour nodes share no cell, so a pass updates u in place.  List entries
+// ~node (negative) name nodes the pass does not update: only their Dirichlet
+// components are cleared.  MINB bounds the registers (resident CTAs per SM):
+// the pass is latency-bound, so occupancy is worth a few spilled registers.
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(128) gs0_kernel(const int* __restrict__ block_list, int nblocks,
-                                                  const int* __restrict__ nbr, const T* __restrict__ E, T* u,
-                                                  const T* __restrict__ b, const uint32_t* __restrict__ flags, long N,
-                                                  T dx, int color, int boundary_only) {
-  pdl_wait();
-  __shared__ int snb[8][27];
-  for (int i = threadIdx.x; i < 8 * 27; i += 128) {
-    const long bb = long(blockIdx.x) * 8 + i / 27;
-    int v = -1;
-    if (bb < nblocks) v = nbr[long(block_list ? block_list[bb] : int(bb)) * 27 + i % 27];
-    snb[i / 27][i % 27] = v;
+
+// Addressing of the 3x3x3 neighbourhood of a level-0 node: per axis, the terms
+// of the neighbour-block selector (into the block's 27-entry nbr row) and of the
+// slot inside that block, for the offsets -1, 0, +1.
+struct Nbhd {
+  const int* nb;
+  int sx[3], sy[3], sz[3], lx[3], ly[3], lz[3];
+  __device__ __forceinline__ void init(const int* __restrict__ nbr, int g) {
+    const int bi = g >> 7, e = g & 127;
+    const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
+    nb = nbr + long(bi) * 27;
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+      const int xx = x + o - 1, yy = y + o - 1, zz = z + o - 1;
+      sx[o] = (xx < 0 ? 0 : (xx > 3 ? 2 : 1)) * 9;
+      sy[o] = (yy < 0 ? 0 : (yy > 3 ? 2 : 1)) * 3;
+      sz[o] = zz < 0 ? 0 : (zz > 7 ? 2 : 1);
+      lx[o] = (xx & 3) << 5;
+      ly[o] = (yy & 3) << 3;
+      lz[o] = zz & 7;
+    }
   }
-  __syncthreads();
-  const int slot = threadIdx.x >> 4, q = threadIdx.x & 15;
-  const long bidx = long(blockIdx.x) * 8 + slot;
-  if (bidx >= nblocks) return;
-  const int bi = block_list ? block_list[bidx] : int(bidx);
-  const int x = (q >> 3) * 2 + ((color >> 2) & 1), y = ((q >> 2) & 1) * 2 + ((color >> 1) & 1), z = (q & 3) * 2 + (color & 1);
-  const long gidx = long(bi) * 128 + (x << 5) + (y << 3) + z;
-  const uint32_t fl = flags[gidx];
+  // global index of the neighbour at offset (ix-1, iy-1, iz-1), -1 if its block is not active
+  __device__ __forceinline__ int at(int ix, int iy, int iz) const {
+    const int b = __ldg(nb + sx[ix] + sy[iy] + sz[iz]);
+    return b < 0 ? -1 : (b << 7) + lx[ix] + ly[iy] + lz[iz];
+  }
+};
+
+template <typename T, int MINB>
+__global__ void __launch_bounds__(128, MINB) gs0_list_kernel(const int* __restrict__ list, int n,
+                                                             const int* __restrict__ nbr, const T* __restrict__ E,
+                                                             T* u, const T* __restrict__ b,
+                                                             const uint32_t* __restrict__ flags, int N, T dx) {
+  pdl_wait();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int raw = list[t];
+  const int g = raw >= 0 ? raw : ~raw;
+  const uint32_t fl = flags[g];
   const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
-  if (!((fl & ACTIVE_NODE) && (!boundary_only || (fl & BOUNDARY_NODE)))) {
-    // inactive (or out-of-band) nodes keep u; Dirichlet components are cleared
-    if (fx) u[gidx] = T(0);
-    if (fy) u[gidx + N] = T(0);
-    if (fz) u[gidx + 2 * N] = T(0);
+  if (raw < 0) {
+    if (fx) u[g] = T(0);
+    if (fy) u[g + N] = T(0);
+    if (fz) u[g + 2 * N] = T(0);
     return;
   }
-  const int* nb = snb[slot];
-  // E of the 8 cells around the node (cell = node - I)
-  T Ec[8];
+  Nbhd nh;
+  nh.init(nbr, g);
+  T gc[8][3], Ec[8], uc[3];
+  T f[3] = {0, 0, 0}, dg[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-  for (int I = 0; I < 8; ++I) {
-    const int cx = x - (I >> 2), cy = y - ((I >> 1) & 1), cz = z - (I & 1);
-    const int nbk = nb[(cx < 0 ? 0 : 1) * 9 + (cy < 0 ? 0 : 1) * 3 + (cz < 0 ? 0 : 1)];
-    Ec[I] = nbk >= 0 ? E[long(nbk) * 128 + ((cx & 3) << 5) + ((cy & 3) << 3) + (cz & 7)] : T(0);
-  }
-  T f0 = 0, f1 = 0, f2 = 0, d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, uc0 = 0, uc1 = 0, uc2 = 0;
+  for (int I = 0; I < 8; ++I) gc[I][0] = gc[I][1] = gc[I][2] = T(0);
 #pragma unroll
-  for (int d = 0; d < 27; ++d) {
-    const int ox = d / 9 - 1, oy = (d / 3) % 3 - 1, oz = d % 3 - 1;
-    const int nx = x + ox, ny = y + oy, nz = z + oz;
-    const int nbk = nb[(nx < 0 ? 0 : (nx > 3 ? 2 : 1)) * 9 + (ny < 0 ? 0 : (ny > 3 ? 2 : 1)) * 3 + (nz < 0 ? 0 : (nz > 7 ? 2 : 1))];
-    T ux = 0, uy = 0, uz = 0;
-    if (nbk >= 0) {
-      const long n = long(nbk) * 128 + ((nx & 3) << 5) + ((ny & 3) << 3) + (nz & 7);
-      ux = u[n];
-      uy = u[n + N];
-      uz = u[n + 2 * N];
+  for (int px = 0; px < 3; ++px) {
+    T up[9][3];
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+      const int iy = p / 3, iz = p % 3;
+      const int i = (px == 1 && p == 4) ? g : nh.at(px, iy, iz);
+      up[p][0] = i < 0 ? T(0) : u[i];
+      up[p][1] = i < 0 ? T(0) : u[i + N];
+      up[p][2] = i < 0 ? T(0) : u[i + 2 * N];
+      // the cell of corner I (min corner = node - I) sits at offset -I
+      if (px <= 1 && iy <= 1 && iz <= 1) Ec[(1 - px) * 4 + (1 - iy) * 2 + (1 - iz)] = i < 0 ? T(0) : E[i];
     }
-    T a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (px == 1) {
+      uc[0] = up[4][0];
+      uc[1] = up[4][1];
+      uc[2] = up[4][2];
+    }
 #pragma unroll
     for (int I = 0; I < 8; ++I) {
-      const int Jx = (I >> 2) + ox, Jy = ((I >> 1) & 1) + oy, Jz = (I & 1) + oz;
-      if (Jx < 0 || Jx > 1 || Jy < 0 || Jy > 1 || Jz < 0 || Jz > 1) continue;
-      const int k = (I * 8 + ((Jx << 2) | (Jy << 1) | Jz)) * 9;
+      const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
+      const int Jx = px - 1 + Ix;
+      if (Jx < 0 || Jx > 1) continue;
 #pragma unroll
-      for (int m = 0; m < 9; ++m) a[m] += Ec[I] * kc<T>(k + m);
-    }
-    f0 += a[0] * ux + a[1] * uy + a[2] * uz;
-    f1 += a[3] * ux + a[4] * uy + a[5] * uz;
-    f2 += a[6] * ux + a[7] * uy + a[8] * uz;
-    if (d == 13) {
-      d0 = a[0]; d1 = a[4]; d2 = a[8]; d3 = a[1]; d4 = a[2]; d5 = a[5];
-      uc0 = ux; uc1 = uy; uc2 = uz;
+      for (int q = 0; q < 4; ++q) {
+        const int Jy = q >> 1, Jz = q & 1;
+        const int p = (Jy - Iy + 1) * 3 + (Jz - Iz + 1);
+        const int k = (I * 8 + Jx * 4 + Jy * 2 + Jz) * 9;
+#pragma unroll
+        for (int v = 0; v < 3; ++v)
+#pragma unroll
+          for (int w = 0; w < 3; ++w) gc[I][v] = fma(kc<T>(k + v * 3 + w), up[p][w], gc[I][v]);
+      }
+      if (Jx == 1) {  // last plane of this cell
+#pragma unroll
+        for (int v = 0; v < 3; ++v) f[v] = fma(Ec[I], gc[I][v], f[v]);
+        const int kd = (I * 8 + I) * 9;
+        dg[0] = fma(kc<T>(kd + 0), Ec[I], dg[0]);
+        dg[1] = fma(kc<T>(kd + 4), Ec[I], dg[1]);
+        dg[2] = fma(kc<T>(kd + 8), Ec[I], dg[2]);
+        dg[3] = fma(kc<T>(kd + 1), Ec[I], dg[3]);
+        dg[4] = fma(kc<T>(kd + 2), Ec[I], dg[4]);
+        dg[5] = fma(kc<T>(kd + 5), Ec[I], dg[5]);
+      }
     }
   }
-  const T r0 = b[gidx] - f0 * dx, r1 = b[gidx + N] - f1 * dx, r2 = b[gidx + 2 * N] - f2 * dx;
-  d0 *= dx; d1 *= dx; d2 *= dx; d3 *= dx; d4 *= dx; d5 *= dx;
+  // u += D^{-1} (b - K u), Dirichlet rows replaced by the identity
+  const T r0 = b[g] - f[0] * dx, r1 = b[g + N] - f[1] * dx, r2 = b[g + 2 * N] - f[2] * dx;
+  T d0 = dg[0] * dx, d1 = dg[1] * dx, d2 = dg[2] * dx, d3 = dg[3] * dx, d4 = dg[4] * dx, d5 = dg[5] * dx;
   if (fx) { d0 = 1; d3 = 0; d4 = 0; }
   if (fy) { d1 = 1; d3 = 0; d5 = 0; }
   if (fz) { d2 = 1; d4 = 0; d5 = 0; }
@@ -254,111 +290,15 @@ __global__ void __launch_bounds__(128) gs0_kernel(const int* __restrict__ block_
   if (fx) { a0 = 0; a3 = 0; a4 = 0; }
   if (fy) { a1 = 0; a3 = 0; a5 = 0; }
   if (fz) { a2 = 0; a4 = 0; a5 = 0; }
-  T v0 = uc0 + r0 * a0 + r1 * a3 + r2 * a4;
-  T v1 = uc1 + r0 * a3 + r1 * a1 + r2 * a5;
-  T v2 = uc2 + r0 * a4 + r1 * a5 + r2 * a2;
+  T v0 = uc[0] + r0 * a0 + r1 * a3 + r2 * a4;
+  T v1 = uc[1] + r0 * a3 + r1 * a1 + r2 * a5;
+  T v2 = uc[2] + r0 * a4 + r1 * a5 + r2 * a2;
   if (fx) v0 = 0;
   if (fy) v1 = 0;
   if (fz) v2 = 0;
-  u[gidx] = v0;
-  u[gidx + N] = v1;
-  u[gidx + 2 * N] = v2;
-}
-
-// Single-precision variant of gs0_kernel: the 27 neighbours' displacements are
-// loaded into registers first (81 floats), then the residual is accumulated cell
-// by cell, g_I = sum_J Kc[I][J] u_J and f += E_I g_I (600 FMA instead of 819,
-// and one address computation per neighbour).
-__global__ void __launch_bounds__(128) gs0_f32_kernel(const int* __restrict__ block_list, int nblocks,
-                                                      const int* __restrict__ nbr, const float* __restrict__ E, float* u,
-                                                      const float* __restrict__ b, const uint32_t* __restrict__ flags,
-                                                      long N, float dx, int color, int boundary_only) {
-  pdl_wait();
-  __shared__ int snb[8][27];
-  for (int i = threadIdx.x; i < 8 * 27; i += 128) {
-    const long bb = long(blockIdx.x) * 8 + i / 27;
-    int v = -1;
-    if (bb < nblocks) v = nbr[long(block_list ? block_list[bb] : int(bb)) * 27 + i % 27];
-    snb[i / 27][i % 27] = v;
-  }
-  __syncthreads();
-  const int slot = threadIdx.x >> 4, q = threadIdx.x & 15;
-  const long bidx = long(blockIdx.x) * 8 + slot;
-  if (bidx >= nblocks) return;
-  const int bi = block_list ? block_list[bidx] : int(bidx);
-  const int x = (q >> 3) * 2 + ((color >> 2) & 1), y = ((q >> 2) & 1) * 2 + ((color >> 1) & 1), z = (q & 3) * 2 + (color & 1);
-  const long gidx = long(bi) * 128 + (x << 5) + (y << 3) + z;
-  const uint32_t fl = flags[gidx];
-  const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
-  if (!((fl & ACTIVE_NODE) && (!boundary_only || (fl & BOUNDARY_NODE)))) {
-    if (fx) u[gidx] = 0.f;
-    if (fy) u[gidx + N] = 0.f;
-    if (fz) u[gidx + 2 * N] = 0.f;
-    return;
-  }
-  const int* nb = snb[slot];
-  float un[27][3];
-#pragma unroll
-  for (int d = 0; d < 27; ++d) {
-    const int nx = x + d / 9 - 1, ny = y + (d / 3) % 3 - 1, nz = z + d % 3 - 1;
-    const int nbk = nb[(nx < 0 ? 0 : (nx > 3 ? 2 : 1)) * 9 + (ny < 0 ? 0 : (ny > 3 ? 2 : 1)) * 3 + (nz < 0 ? 0 : (nz > 7 ? 2 : 1))];
-    if (nbk >= 0) {
-      const long n = long(nbk) * 128 + ((nx & 3) << 5) + ((ny & 3) << 3) + (nz & 7);
-      un[d][0] = u[n];
-      un[d][1] = u[n + N];
-      un[d][2] = u[n + 2 * N];
-    } else {
-      un[d][0] = un[d][1] = un[d][2] = 0.f;
-    }
-  }
-  float f0 = 0, f1 = 0, f2 = 0, d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0;
-#pragma unroll
-  for (int I = 0; I < 8; ++I) {
-    const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
-    const int cx = x - Ix, cy = y - Iy, cz = z - Iz;
-    const int nbk = nb[(cx < 0 ? 0 : 1) * 9 + (cy < 0 ? 0 : 1) * 3 + (cz < 0 ? 0 : 1)];
-    const float Ec = nbk >= 0 ? E[long(nbk) * 128 + ((cx & 3) << 5) + ((cy & 3) << 3) + (cz & 7)] : 0.f;
-    float g0 = 0, g1 = 0, g2 = 0;
-#pragma unroll
-    for (int J = 0; J < 8; ++J) {
-      const int d = (((J >> 2) - Ix + 1) * 3 + (((J >> 1) & 1) - Iy + 1)) * 3 + ((J & 1) - Iz + 1);
-      const int k = (I * 8 + J) * 9;
-      g0 += kc<float>(k + 0) * un[d][0] + kc<float>(k + 1) * un[d][1] + kc<float>(k + 2) * un[d][2];
-      g1 += kc<float>(k + 3) * un[d][0] + kc<float>(k + 4) * un[d][1] + kc<float>(k + 5) * un[d][2];
-      g2 += kc<float>(k + 6) * un[d][0] + kc<float>(k + 7) * un[d][1] + kc<float>(k + 8) * un[d][2];
-    }
-    f0 += Ec * g0;
-    f1 += Ec * g1;
-    f2 += Ec * g2;
-    const int kd = (I * 8 + I) * 9;
-    d0 += Ec * kc<float>(kd + 0);
-    d1 += Ec * kc<float>(kd + 4);
-    d2 += Ec * kc<float>(kd + 8);
-    d3 += Ec * kc<float>(kd + 1);
-    d4 += Ec * kc<float>(kd + 2);
-    d5 += Ec * kc<float>(kd + 5);
-  }
-  const float r0 = b[gidx] - f0 * dx, r1 = b[gidx + N] - f1 * dx, r2 = b[gidx + 2 * N] - f2 * dx;
-  d0 *= dx; d1 *= dx; d2 *= dx; d3 *= dx; d4 *= dx; d5 *= dx;
-  if (fx) { d0 = 1; d3 = 0; d4 = 0; }
-  if (fy) { d1 = 1; d3 = 0; d5 = 0; }
-  if (fz) { d2 = 1; d4 = 0; d5 = 0; }
-  const float m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
-  const float m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
-  const float inv = 1.f / (d0 * m11 + d3 * m12 + d4 * m13);
-  float a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
-  if (fx) { a0 = 0; a3 = 0; a4 = 0; }
-  if (fy) { a1 = 0; a3 = 0; a5 = 0; }
-  if (fz) { a2 = 0; a4 = 0; a5 = 0; }
-  float v0 = un[13][0] + r0 * a0 + r1 * a3 + r2 * a4;
-  float v1 = un[13][1] + r0 * a3 + r1 * a1 + r2 * a5;
-  float v2 = un[13][2] + r0 * a4 + r1 * a5 + r2 * a2;
-  if (fx) v0 = 0;
-  if (fy) v1 = 0;
-  if (fz) v2 = 0;
-  u[gidx] = v0;
-  u[gidx + N] = v1;
-  u[gidx + 2 * N] = v2;
+  u[g] = v0;
+  u[g + N] = v1;
+  u[g + 2 * N] = v2;
 }
 
 // ---------------------------------------------------------------------------

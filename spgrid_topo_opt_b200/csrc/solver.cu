@@ -116,6 +116,10 @@ struct Level {
   DevBuf<T> u, b, r;   // [3N] each
   DevBuf<T> A;         // [243][N] stencils (levels with Galerkin operators)
   bool has_matrix = false;
+  // level 0: node lists of the Gauss-Seidel passes, full sweep colours 0..7
+  // then boundary sweep colours 8..15, concatenated; list k is gs_off[k]..gs_off[k+1]
+  DevBuf<int> gs_list;
+  int gs_off[17] = {0};
 };
 
 struct Bottom {
@@ -254,13 +258,60 @@ class Solver {
     d.r.zero(stream);
   }
 
+  // Node lists of the level-0 Gauss-Seidel passes.  A node's colour is the
+  // parity of its coordinates (blocks have even extents, so the slot's parity
+  // is the global one).  A pass visits the colour's nodes of all blocks (full
+  // sweep) or of the boundary blocks (boundary sweep), updates the active
+  // (active boundary-band) ones and clears the Dirichlet components of the
+  // rest; those come last in a list, encoded as ~node.  Lists ascend, so a
+  // warp's threads work on neighbouring nodes of few blocks.
+  static void colour_lists(const HostLevel& h, std::vector<int32_t>& out, int off[17]) {
+    std::vector<int32_t> upd[16], clr[16];
+    std::vector<char> in_boundary(size_t(h.nb), 0);
+    for (int b : h.boundary) in_boundary[size_t(b)] = 1;
+    const long N = long(h.nb) * NODES_PER_BLOCK;
+    for (long g = 0; g < N; ++g) {
+      const uint32_t fl = h.flags[size_t(g)];
+      const int e = int(g & 127);
+      const int c = ((e >> 5) & 1) << 2 | ((e >> 3) & 1) << 1 | (e & 1);
+      const bool act = fl & ACTIVE_NODE, dir = fl & (DIR_X | DIR_Y | DIR_Z);
+      if (act) upd[c].push_back(int32_t(g));
+      else if (dir) clr[c].push_back(~int32_t(g));
+      if (!in_boundary[size_t(g >> 7)]) continue;
+      if (act && (fl & BOUNDARY_NODE)) upd[8 + c].push_back(int32_t(g));
+      else if (dir) clr[8 + c].push_back(~int32_t(g));
+    }
+    out.clear();
+    off[0] = 0;
+    for (int k = 0; k < 16; ++k) {
+      out.insert(out.end(), upd[k].begin(), upd[k].end());
+      out.insert(out.end(), clr[k].begin(), clr[k].end());
+      off[k + 1] = int(out.size());
+    }
+  }
+
   void build_levels() {
+    // the level-0 kernels index the [3][N] planes with 32-bit integers
+    if (3 * long(P.levels[0].nb) * NODES_PER_BLOCK >= long(INT32_MAX))
+      throw CudaError("the finest level has too many blocks for 32-bit node indices", SGS_ERR_INPUT);
+    std::vector<int32_t> gsl;
+    int off[17];
+    colour_lists(P.levels[0], gsl, off);
     for (auto& h : P.levels) {
+      const bool first = &h == &P.levels[0];
       L64.emplace_back(new Level<double>());
       upload_level(*L64.back(), h);
+      if (first) {
+        L64.back()->gs_list.upload(gsl, stream);
+        std::copy(off, off + 17, L64.back()->gs_off);
+      }
       if (mixed()) {
         L32.emplace_back(new Level<float>());
         upload_level(*L32.back(), h);
+        if (first) {
+          L32.back()->gs_list.upload(gsl, stream);
+          std::copy(off, off + 17, L32.back()->gs_off);
+        }
       }
     }
     E64.upload(P.E, stream);
@@ -469,13 +520,16 @@ class Solver {
     if (count == 0) return;
     if (l == 0) {
       for (int k = 0; k < 8; ++k) {
-        const int c = forward ? k : 7 - k;
+        const int c = (boundary ? 8 : 0) + (forward ? k : 7 - k);
+        const int lo = d.gs_off[c], cnt = d.gs_off[c + 1] - lo;
+        if (cnt == 0) continue;
+        // single precision: 80 registers, 6 CTAs per SM; double: 128, 4 per SM
         if constexpr (sizeof(T) == 4)
-          launch(gs0_f32_kernel, blocks_for(count, 8), 128, 0, list, count, d.nbr.p, Edev<T>(), u, b, d.flags.p, d.N,
-                 T(P.dx), c, boundary ? 1 : 0);
+          launch(gs0_list_kernel<T, 6>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbr.p, Edev<T>(), u, b,
+                 d.flags.p, int(d.N), T(P.dx));
         else
-          launch(gs0_kernel<T>, blocks_for(count, 8), 128, 0, list, count, d.nbr.p, Edev<T>(), u, b, d.flags.p, d.N,
-                 T(P.dx), c, boundary ? 1 : 0);
+          launch(gs0_list_kernel<T, 4>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbr.p, Edev<T>(), u, b,
+                 d.flags.p, int(d.N), T(P.dx));
         ++launch_counter;
       }
       return;
