@@ -57,7 +57,8 @@ def parse():
     if args.n is None:
         args.n = 256 if args.workload == "shell" else 1024
     if args.bottom_size is None:
-        args.bottom_size = 8 if args.workload == "shell" else 16
+        # mg_bottom_size 16, the value of the reference's dense-box configuration
+        args.bottom_size = 16
     return args
 
 
