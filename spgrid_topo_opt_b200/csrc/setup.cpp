@@ -125,47 +125,111 @@ struct Builder {
   }
 };
 
+// The 27 blocks (active or ghost) around block b, -1 where there is none;
+// entry (dx+1)*9 + (dy+1)*3 + (dz+1).
+static void block_ring(const HostLevel& L, int b, int ring[27]) {
+  const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
+  for (int d = 0; d < 27; ++d)
+    ring[d] = L.block_at(bx + (d / 9 - 1) * BLK_X, by + ((d / 3) % 3 - 1) * BLK_Y, bz + (d % 3 - 1) * BLK_Z);
+}
+
 void flag_nodes(HostLevel& L) {
-  // Flaging.h:65-80 — OR each cell's (flags >> 4) into its 8 corner nodes.  Runs
-  // serially like the reference; writes may create ghost blocks.
+  // Flaging.h:65-80 — each active block's cells OR (flags >> 4) into their 8
+  // corner nodes; nodes in untouched pages get ghost blocks.  The OR is order
+  // free, so it runs as a gather: first the ghost blocks that some cell of an
+  // active block reaches are created (serially), then every node ORs the bits
+  // of its 8 incident cells in active blocks (in parallel).
+  const uint32_t CELL = F_ACTIVE_CELL | F_DIRICHLET_CELL;
+  std::vector<uint8_t> reach(size_t(L.nb), 0);  // bit (dx*4+dy*2+dz): a cell on that +face combination
+#pragma omp parallel for schedule(static)
   for (int b = 0; b < L.nb; ++b) {
-    const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
+    uint8_t m = 0;
     for (int e = 0; e < NODES_PER_BLOCK; ++e) {
-      uint32_t nf = (L.flags[size_t(b) * NODES_PER_BLOCK + e] & (F_ACTIVE_CELL | F_DIRICHLET_CELL)) >> 4;
-      if (!nf) continue;
-      int x = bx + (e >> 5), y = by + ((e >> 3) & 3), z = bz + (e & 7);
+      if (!(L.flags[size_t(b) * NODES_PER_BLOCK + e] & CELL)) continue;
+      const int kx = (e >> 5) == 3, ky = ((e >> 3) & 3) == 3, kz = (e & 7) == 7;
+      for (int c = 1; c < 8; ++c)
+        if ((!(c & 4) || kx) && (!(c & 2) || ky) && (!(c & 1) || kz)) m |= uint8_t(1u << c);
+    }
+    reach[size_t(b)] = m;
+  }
+  for (int b = 0; b < L.nb; ++b)
+    for (int c = 1; c < 8; ++c)
+      if (reach[size_t(b)] >> c & 1)
+        L.touch(L.coords[3 * b] + (c >> 2) * BLK_X, L.coords[3 * b + 1] + ((c >> 1) & 1) * BLK_Y,
+                L.coords[3 * b + 2] + (c & 1) * BLK_Z);
+  const int nall = int(L.coords.size() / 3);
+  std::vector<uint32_t> add(size_t(nall) * NODES_PER_BLOCK, 0u);
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < nall; ++b) {
+    int ring[27];
+    block_ring(L, b, ring);
+    for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+      const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
+      uint32_t acc = 0;
       for (int c = 0; c < 8; ++c) {
-        int nx = x + (c >> 2), ny = y + ((c >> 1) & 1), nz = z + (c & 1);
-        int nbk = L.touch(nx, ny, nz);
-        if (nbk >= 0) L.flags[size_t(nbk) * NODES_PER_BLOCK + node_slot(nx, ny, nz)] |= nf;
+        const int cx = x - (c >> 2), cy = y - ((c >> 1) & 1), cz = z - (c & 1);
+        const int nb = ring[(cx < 0 ? 0 : 1) * 9 + (cy < 0 ? 0 : 1) * 3 + (cz < 0 ? 0 : 1)];
+        if (nb < 0 || nb >= L.nb) continue;  // only cells of active blocks spread their flags
+        acc |= (L.flags[size_t(nb) * NODES_PER_BLOCK + node_slot(cx, cy, cz)] & CELL) >> 4;
       }
+      add[size_t(b) * NODES_PER_BLOCK + e] = acc;
     }
   }
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < long(add.size()); ++i) L.flags[size_t(i)] |= add[size_t(i)];
 }
 
 void flag_boundary(HostLevel& L, int band = 3) {
   // Flaging.h:93-147: three Jacobi-style passes growing a band of active,
-  // non-Dirichlet nodes around the Dirichlet nodes.
-  auto flag_at = [&](int x, int y, int z) -> uint32_t {
-    int b = L.block_at(x, y, z);
-    return b < 0 ? 0u : L.flags[size_t(b) * NODES_PER_BLOCK + node_slot(x, y, z)];
+  // non-Dirichlet nodes around the Dirichlet nodes.  A pass can only reach
+  // blocks next to a block that already holds a Dirichlet or band node, so
+  // each pass visits those blocks alone.
+  const uint32_t SEED = F_DIRICHLET_NODE | F_BOUNDARY_NODE;
+  const int nall = int(L.coords.size() / 3);
+  std::vector<std::array<int, 27>> rings(size_t(L.nb));
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < L.nb; ++b) block_ring(L, b, rings[size_t(b)].data());
+  auto flag_at = [&](const int* ring, int x, int y, int z) -> uint32_t {
+    const int nb = ring[(x < 0 ? 0 : (x > 3 ? 2 : 1)) * 9 + (y < 0 ? 0 : (y > 3 ? 2 : 1)) * 3 + (z < 0 ? 0 : (z > 7 ? 2 : 1))];
+    return nb < 0 ? 0u : L.flags[size_t(nb) * NODES_PER_BLOCK + node_slot(x, y, z)];
   };
+  std::vector<uint8_t> seeded(static_cast<size_t>(nall), 0);
+  std::vector<int> cand;
   for (int pass = 0; pass < band; ++pass) {
 #pragma omp parallel for schedule(static)
-    for (int b = 0; b < L.nb; ++b) {
-      const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
+    for (int b = 0; b < nall; ++b) {
+      uint8_t s = 0;
+      for (int e = 0; e < NODES_PER_BLOCK && !s; ++e) s = (L.flags[size_t(b) * NODES_PER_BLOCK + e] & SEED) != 0;
+      seeded[size_t(b)] = s;
+    }
+    cand.clear();
+    for (int b = 0; b < L.nb; ++b)
+      for (int d = 0; d < 27; ++d) {
+        const int nb = rings[size_t(b)][d];
+        if (nb >= 0 && seeded[size_t(nb)]) {
+          cand.push_back(b);
+          break;
+        }
+      }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long k = 0; k < long(cand.size()); ++k) {
+      const int b = cand[size_t(k)];
+      const int* ring = rings[size_t(b)].data();
       for (int e = 0; e < NODES_PER_BLOCK; ++e) {
         uint32_t& f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
         if ((f & F_DIRICHLET_NODE) || !(f & F_ACTIVE_NODE)) continue;
-        int x = bx + (e >> 5), y = by + ((e >> 3) & 3), z = bz + (e & 7);
+        const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
         bool hit = false;
-        for (int d = 0; d < 27 && !hit; ++d)
-          hit = flag_at(x + d / 9 - 1, y + (d / 3) % 3 - 1, z + d % 3 - 1) & (F_DIRICHLET_NODE | F_BOUNDARY_NODE);
+        for (int d = 0; d < 27 && !hit; ++d) hit = flag_at(ring, x + d / 9 - 1, y + (d / 3) % 3 - 1, z + d % 3 - 1) & SEED;
         if (hit) f |= F_BOUNDARY_TEMP;
       }
     }
-    for (size_t i = 0; i < size_t(L.nb) * NODES_PER_BLOCK; ++i)
-      if (L.flags[i] & F_BOUNDARY_TEMP) L.flags[i] = (L.flags[i] & ~F_BOUNDARY_TEMP) | F_BOUNDARY_NODE;
+#pragma omp parallel for schedule(static)
+    for (long k = 0; k < long(cand.size()); ++k)
+      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+        uint32_t& f = L.flags[size_t(cand[size_t(k)]) * NODES_PER_BLOCK + e];
+        if (f & F_BOUNDARY_TEMP) f = (f & ~F_BOUNDARY_TEMP) | F_BOUNDARY_NODE;
+      }
   }
   L.boundary.clear();
   for (int b = 0; b < L.nb; ++b)
@@ -225,39 +289,71 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   Builder b0;
   b0.init(in.resolution[0], in.resolution[1], in.resolution[2]);
   const size_t nin = in.density.num_blocks();
-  struct CellE { int x, y, z; double E; };
-  std::vector<CellE> cells;
-  for (size_t b = 0; b < nin; ++b) {
-    int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
-    if ((x & 3) || (y & 3) || (z & 3)) return fail(4, "density block base is not a multiple of 4");
-    if (b0.set_page(x, y, z) < 0) return fail(4, "density block outside the grid");
-    for (int e = 0; e < 64; ++e) {
-      double d = in.density.data[b * 64 + e];
-      if (d > 0) {
-        double E = penalty ? (1 - emin) * std::pow(std::max(rho_min, d), penalty) + emin : d;
-        cells.push_back({x + (e >> 4), y + ((e >> 2) & 3), z + (e & 3), E});
-      }
+  // Each 4x4x4 input block fills one z half of a 4x4x8 solver block.  Pages are
+  // set serially (block creation order); the per-cell work then runs per input
+  // block in parallel, which writes disjoint slots unless an input block is
+  // repeated: then the cells go in input order, the last write winning.
+  std::vector<int32_t> in_slot(nin);
+  bool repeated = false;
+  {
+    std::vector<uint8_t> halves;
+    for (size_t b = 0; b < nin; ++b) {
+      int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
+      if ((x & 3) || (y & 3) || (z & 3)) return fail(4, "density block base is not a multiple of 4");
+      const int bk = b0.set_page(x, y, z);
+      if (bk < 0) return fail(4, "density block outside the grid");
+      in_slot[b] = bk * NODES_PER_BLOCK + node_slot(x, y, z);
+      if (halves.size() <= size_t(bk)) halves.resize(size_t(bk) + 1, 0);
+      const uint8_t h = uint8_t(1u << ((z >> 2) & 1));
+      repeated |= (halves[size_t(bk)] & h) != 0;
+      halves[size_t(bk)] |= h;
     }
   }
   // material slots ride along with the blocks through the renumbering
   b0.scratch.assign(b0.L.coords.size() / 3 * NODES_PER_BLOCK, 0.0);
-  for (auto& c : cells) {
-    int bk = b0.L.block_at(c.x, c.y, c.z);
-    if (bk < 0) return fail(4, "material cell outside the grid");
-    b0.scratch[size_t(bk) * NODES_PER_BLOCK + node_slot(c.x, c.y, c.z)] = c.E;
-  }
+  auto cell_E = [&](size_t b, int e) {
+    const double d = in.density.data[b * 64 + e];
+    return d > 0 ? (penalty ? (1 - emin) * std::pow(std::max(rho_min, d), penalty) + emin : d) : 0.0;
+  };
+  // input cell e = i*16 + j*4 + k sits at slot offset i*32 + j*8 + k from the block's slot
+  auto cell_slot = [](int e) { return (e >> 4) * 32 + ((e >> 2) & 3) * 8 + (e & 3); };
+#pragma omp parallel for schedule(static) if (!repeated)
+  for (long b = 0; b < long(nin); ++b)
+    for (int e = 0; e < 64; ++e)
+      if (in.density.data[size_t(b) * 64 + e] > 0) b0.scratch[size_t(in_slot[size_t(b)] + cell_slot(e))] = cell_E(size_t(b), e);
   // Validate_With_Density (solver/CPU_Kernels/Validate_Blocks.h:311-335): every
-  // material cell needs its +1 neighbour pages.
-  for (auto& c : cells)
-    if (c.E * P.mu0 > 0)
-      for (int n = 1; n < 8; ++n)
-        if (!b0.test_page(c.x + (n >> 2), c.y + ((n >> 1) & 1), c.z + (n & 1))) {
-          std::snprintf(msg, sizeof msg, "Block activation check failed at cell (%d, %d, %d)", c.x, c.y, c.z);
-          return fail(5, msg);
-        }
+  // material cell needs its +1 neighbour pages; the first failure in input order is reported.
+  long first_bad = -1;
+  {
+    std::vector<long> bad(nin, -1);
+#pragma omp parallel for schedule(static)
+    for (long b = 0; b < long(nin); ++b) {
+      const int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
+      for (int e = 0; e < 64 && bad[size_t(b)] < 0; ++e) {
+        if (!(cell_E(size_t(b), e) * P.mu0 > 0)) continue;
+        const int cx = x + (e >> 4), cy = y + ((e >> 2) & 3), cz = z + (e & 3);
+        for (int n = 1; n < 8; ++n)
+          if (!b0.test_page(cx + (n >> 2), cy + ((n >> 1) & 1), cz + (n & 1))) {
+            bad[size_t(b)] = long(b) * 64 + e;
+            break;
+          }
+      }
+    }
+    for (size_t b = 0; b < nin && first_bad < 0; ++b) first_bad = bad[b];
+  }
+  if (first_bad >= 0) {
+    const size_t b = size_t(first_bad / 64);
+    const int e = int(first_bad % 64);
+    std::snprintf(msg, sizeof msg, "Block activation check failed at cell (%d, %d, %d)", in.density.base[3 * b] + (e >> 4),
+                  in.density.base[3 * b + 1] + ((e >> 2) & 3), in.density.base[3 * b + 2] + (e & 3));
+    return fail(5, msg);
+  }
   // ACTIVE_CELL where mu != 0 (Flaging.h:31-44); written before renumbering
-  for (auto& c : cells)
-    if (c.E * P.mu0 != 0) *b0.flag(c.x, c.y, c.z) |= F_ACTIVE_CELL;
+#pragma omp parallel for schedule(static) if (!repeated)
+  for (long b = 0; b < long(nin); ++b)
+    for (int e = 0; e < 64; ++e)
+      if (in.density.data[size_t(b) * 64 + e] > 0 && cell_E(size_t(b), e) * P.mu0 != 0)
+        b0.L.flags[size_t(in_slot[size_t(b)] + cell_slot(e))] |= F_ACTIVE_CELL;
   // Dirichlet node -> cell: a cell is fixed on axis v when all 8 corners are
   // listed on axis v (SPGrid_CPU_Solver.cpp:169-192)
   for (int v = 0; v < 3; ++v) {
@@ -303,14 +399,24 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
         if (!(ff & (F_ACTIVE_CELL | F_DIRICHLET_CELL))) continue;
         int x = bx + (e >> 5), y = by + ((e >> 3) & 3), z = bz + (e & 7);
         int cx = (x + BLK_X) >> 1, cy = (y + BLK_Y) >> 1, cz = (z + BLK_Z) >> 1;
+        // the pages of the corners cx + n: a +1 offset leaves the cell's page
+        // only on an axis where the cell is on the page's last layer, so each
+        // distinct page is set once (n = 0 excluded for Dirichlet cells)
+        const int kx = (cx & 3) == 3, ky = (cy & 3) == 3, kz = (cz & 7) == 7;
+        auto pages = [&](bool with_self) {
+          for (int dx = 0; dx <= kx; ++dx)
+            for (int dy = 0; dy <= ky; ++dy)
+              for (int dz = 0; dz <= kz; ++dz)
+                if (with_self || dx || dy || dz || !(kx && ky && kz)) bc.set_page(cx + dx, cy + dy, cz + dz);
+        };
         if (ff & F_ACTIVE_CELL) {
           if (uint32_t* f = bc.flag(cx, cy, cz)) *f |= F_ACTIVE_CELL;
-          for (int n = 0; n < 8; ++n) bc.set_page(cx + (n >> 2), cy + ((n >> 1) & 1), cz + (n & 1));
+          pages(true);
         }
         for (int v = 0; v < 3; ++v)
           if (ff & (F_DIRICHLET_CELL_X << v)) {
             if (uint32_t* f = bc.flag(cx, cy, cz)) *f |= (F_DIRICHLET_CELL_X << v);
-            for (int n = 1; n < 8; ++n) bc.set_page(cx + (n >> 2), cy + ((n >> 1) & 1), cz + (n & 1));
+            pages(false);
           }
       }
     }
