@@ -260,7 +260,7 @@ def run_ours(args, rank, world):
     e2e_times, h2d, d2h = [], 0.0, 0.0
     for i in range(0 if args.no_e2e else 2 + max(1, args.steps // 2)):
         t0 = time.perf_counter()
-        out = fi.deserialize_outputs(native.fem_solve_blob(blob))
+        out = native.fem_solve_outputs(blob)
         dt = time.perf_counter() - t0
         if not out.success:
             raise RuntimeError(out.info)

@@ -644,7 +644,7 @@ class Solver {
   void precondition();
   void record_iteration();
   void solve();
-  void pack_outputs(std::vector<double>& disp);
+  void pack_outputs(double* disp);
   double sensitivity(const double* rho, double penalty, double emin, double* dc, double* se);
 
   // New densities for the same material pattern: E, the Galerkin operators and
@@ -1025,13 +1025,15 @@ void Solver::solve() {
   solve_launches += launch_counter - launches_before - (capture_launches);
 }
 
-void Solver::pack_outputs(std::vector<double>& disp) {
+// The output field, [input block][64 nodes][4] doubles, copied straight into
+// the caller's buffer.
+void Solver::pack_outputs(double* disp) {
   const long nin = long(P.in_block.size());
-  disp.assign(size_t(nin) * 256, 0.0);
   if (nin == 0) return;
   launch(pack_kernel, blocks_for(nin * 64, 256), 256, 0, int(nin), in_block.p, in_zoff.p, x.p, f.p, N0(), out_disp.p);
-  SGS_CUDA(cudaMemcpyAsync(disp.data(), out_disp.p, disp.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
-  g_d2h_bytes += disp.size() * sizeof(double);
+  const size_t bytes = size_t(nin) * 256 * sizeof(double);
+  SGS_CUDA(cudaMemcpyAsync(disp, out_disp.p, bytes, cudaMemcpyDeviceToHost, stream));
+  g_d2h_bytes += bytes;
   SGS_CUDA(cudaStreamSynchronize(stream));
 }
 
@@ -1275,9 +1277,7 @@ SGS_API int sgs_residual_history(sgs_session* h, double* out, int cap) {
 SGS_API int sgs_displacements(sgs_session* h, double* out) {
   if (!h || !out || host_only(h)) return SGS_ERR_INPUT;
   try {
-    std::vector<double> d;
-    h->solver->pack_outputs(d);
-    std::memcpy(out, d.data(), d.size() * sizeof(double));
+    h->solver->pack_outputs(out);
   } catch (const CudaError& e) {
     h->error = e.what();
     return e.code;
@@ -1429,14 +1429,20 @@ SGS_API void fem_solve(void* input, void* output) {
   *out_ptr = nullptr;
   FEMOutputs outs;
   outs.success = false;
+  using clk = std::chrono::steady_clock;
+  auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
   try {
+    const auto t0 = clk::now();
     FEMInputs in = decode_inputs(input);
     for (int v = 0; v < 3; ++v) outs.displacements.resolution[v] = in.resolution[v];
     const int precision = in.get_int("sgs_precision", PREC_REFERENCE);
     const unsigned long long h2d0 = g_h2d_bytes.load(), d2h0 = g_d2h_bytes.load();
     sgs_session* h = nullptr;
     std::string err;
+    const auto t1 = clk::now();
     int rc = (precision < 0 || precision > 2) ? SGS_ERR_INPUT : session_from_inputs(in, precision, &h, &err);
+    outs.extra_doubles["decode_seconds"] = secs(t0, t1);
+    outs.extra_doubles["session_seconds"] = secs(t1, clk::now());
     if (rc) {
       outs.error_code = rc;
       outs.info = err.empty() ? "invalid sgs_precision" : err;
@@ -1457,7 +1463,9 @@ SGS_API void fem_solve(void* input, void* output) {
         const size_t nin = in.density.num_blocks();
         outs.displacements.base.assign(in.density.base.begin(), in.density.base.end());
         outs.displacements.data.resize(nin * 256);
+        const auto t2 = clk::now();
         rc = sgs_displacements(h, outs.displacements.data.data());
+        outs.extra_doubles["output_seconds"] = secs(t2, clk::now());
         outs.extra_doubles["h2d_bytes"] = double(g_h2d_bytes.load() - h2d0);
         outs.extra_doubles["d2h_bytes"] = double(g_d2h_bytes.load() - d2h0);
         outs.extra_doubles["solve_device_seconds"] = st.solve_device_seconds;
@@ -1475,6 +1483,9 @@ SGS_API void fem_solve(void* input, void* output) {
           outs.info = m;
         }
       }
+      const auto t3 = clk::now();
+      guard.reset();
+      outs.extra_doubles["teardown_seconds"] = secs(t3, clk::now());
     }
   } catch (const WireError& e) {
     outs.error_code = SGS_ERR_WIRE;

@@ -6,13 +6,14 @@
 namespace sgs {
 namespace {
 
+// Writes a record into a caller-sized buffer; with no buffer it only counts
+// bytes, so an encoder runs once to size its output and once to fill it.
 class Writer {
  public:
-  Writer() { buf_.resize(8, 0); }
+  explicit Writer(uint8_t* dst = nullptr) : dst_(dst) {}
   void bytes(const void* p, size_t n) {
-    size_t h = buf_.size();
-    buf_.resize(h + n);
-    if (n) std::memcpy(buf_.data() + h, p, n);
+    if (dst_ && n) std::memcpy(dst_ + pos_, p, n);
+    pos_ += n;
   }
   template <typename T>
   void pod(const T& v) { bytes(&v, sizeof(T)); }
@@ -29,24 +30,31 @@ class Writer {
       val(kv.second);
     }
   }
+  // records of {int base[3]; double data[64*width]}, copied block-parallel
   void grid(const BlockedGrid& g, int width) {
     for (int v = 0; v < 3; ++v) pod<int32_t>(g.resolution[v]);
-    size_t n = g.num_blocks();
+    const size_t n = g.num_blocks(), payload = sizeof(double) * 64 * size_t(width), rec = 12 + payload;
     if (g.data.size() != n * 64 * size_t(width)) throw WireError("grid payload size mismatch");
     count(n);
-    for (size_t b = 0; b < n; ++b) {
-      bytes(&g.base[3 * b], 12);
-      bytes(&g.data[b * 64 * width], sizeof(double) * 64 * width);
+    if (dst_) {
+      uint8_t* at = dst_ + pos_;
+#pragma omp parallel for schedule(static) if (n > 4096)
+      for (long b = 0; b < long(n); ++b) {
+        std::memcpy(at + size_t(b) * rec, &g.base[3 * size_t(b)], 12);
+        std::memcpy(at + size_t(b) * rec + 12, &g.data[size_t(b) * 64 * width], payload);
+      }
     }
+    pos_ += n * rec;
   }
-  std::vector<uint8_t>& finish() {
-    uint64_t n = buf_.size();
-    std::memcpy(buf_.data(), &n, 8);
-    return buf_;
+  size_t size() const { return pos_; }
+  void finish() {
+    const uint64_t n = pos_;
+    if (dst_) std::memcpy(dst_, &n, 8);
   }
 
  private:
-  std::vector<uint8_t> buf_;
+  uint8_t* dst_;
+  size_t pos_ = 8;  // the length header comes first
 };
 
 class Reader {
@@ -94,10 +102,14 @@ class Reader {
     size_t n = count(rec);
     g.base.resize(n * 3);
     g.data.resize(n * 64 * width);
-    for (size_t b = 0; b < n; ++b) {
-      bytes(&g.base[3 * b], 12);
-      bytes(&g.data[b * 64 * width], sizeof(double) * 64 * width);
+    const uint8_t* at = p_ + head_;
+    const size_t payload = rec - 12;
+#pragma omp parallel for schedule(static) if (n > 4096)
+    for (long b = 0; b < long(n); ++b) {
+      std::memcpy(&g.base[3 * size_t(b)], at + size_t(b) * rec, 12);
+      std::memcpy(&g.data[size_t(b) * 64 * width], at + size_t(b) * rec + 12, payload);
     }
+    head_ += n * rec;
   }
   void done() const {
     if (head_ != total_) throw WireError("trailing bytes after the record");
@@ -214,8 +226,7 @@ FEMInputs decode_inputs(const void* blob) {
   return p;
 }
 
-std::vector<uint8_t> encode_inputs(const FEMInputs& p) {
-  Writer w;
+static void write_inputs(Writer& w, const FEMInputs& p) {
   write_base(w, p);
   w.pod(p.dx);
   w.pod(p.preserved_buffer_size);
@@ -242,11 +253,19 @@ std::vector<uint8_t> encode_inputs(const FEMInputs& p) {
   w.pod(p.krylov.restart_iterations);
   w.pod<uint8_t>(p.krylov.print_residuals ? 1 : 0);
   w.str(p.caller_method);
-  return w.finish();
 }
 
-char* encode_outputs(const FEMOutputs& o, size_t* length) {
-  Writer w;
+std::vector<uint8_t> encode_inputs(const FEMInputs& p) {
+  Writer sizer;
+  write_inputs(sizer, p);
+  std::vector<uint8_t> out(sizer.size());
+  Writer w(out.data());
+  write_inputs(w, p);
+  w.finish();
+  return out;
+}
+
+static void write_outputs(Writer& w, const FEMOutputs& o) {
   write_base(w, o);
   w.grid(o.displacements, 4);
   w.grid(o.residual_field, 1);
@@ -255,10 +274,16 @@ char* encode_outputs(const FEMOutputs& o, size_t* length) {
   w.bytes(o.residuals.data(), sizeof(double) * o.residuals.size());
   w.pod(o.error_code);
   w.pod<uint8_t>(o.success ? 1 : 0);
-  auto& buf = w.finish();
-  char* out = new char[buf.size()];
-  std::memcpy(out, buf.data(), buf.size());
-  if (length) *length = buf.size();
+}
+
+char* encode_outputs(const FEMOutputs& o, size_t* length) {
+  Writer sizer;
+  write_outputs(sizer, o);
+  char* out = new char[sizer.size()];
+  Writer w(reinterpret_cast<uint8_t*>(out));
+  write_outputs(w, o);
+  w.finish();
+  if (length) *length = sizer.size();
   return out;
 }
 

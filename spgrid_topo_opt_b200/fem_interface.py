@@ -317,7 +317,9 @@ def serialize_outputs(o: FEMOutputs) -> bytes:
 # --------------------------------------------------------------------------
 class _Reader:
     def __init__(self, blob) -> None:
-        self.buf = memoryview(bytes(blob))
+        # any contiguous buffer (bytes, bytearray, a view of foreign memory) is
+        # read in place; arrays are copied out of it
+        self.buf = memoryview(blob).cast("B")
         if len(self.buf) < 8:
             raise WireFormatError("blob shorter than its length header")
         (self.total,) = struct.unpack_from("<Q", self.buf, 0)
@@ -363,7 +365,7 @@ class _Reader:
         rec = np.dtype([("base", "<i4", (3,)), ("data", "<f8", (per,))])
         if n > (self.total - self.head) // rec.itemsize:
             raise WireFormatError("block count exceeds blob size")
-        arr = np.frombuffer(bytes(self.take(n * rec.itemsize)), rec, count=n)
+        arr = np.frombuffer(self.take(n * rec.itemsize), rec, count=n)
         data = arr["data"].copy()
         data = data.reshape(n, _BLOCK_VOLUME, 4) if vector else data.reshape(n, _BLOCK_VOLUME)
         return BlockedGrid(resolution=res, base=arr["base"].copy(), data=data)
@@ -372,7 +374,7 @@ class _Reader:
         n = self.u64()
         if n > (self.total - self.head) // dtype.itemsize:
             raise WireFormatError("record count exceeds blob size")
-        return np.frombuffer(bytes(self.take(n * dtype.itemsize)), dtype, count=n).copy()
+        return np.frombuffer(self.take(n * dtype.itemsize), dtype, count=n).copy()
 
     def done(self) -> None:
         if self.head != self.total:
@@ -426,7 +428,7 @@ def deserialize_outputs(blob) -> FEMOutputs:
     o.residual_field = r.grid(vector=False)
     o.info = r.string()
     n = r.u64()
-    o.residuals = np.frombuffer(bytes(r.take(8 * n)), "<f8").copy()
+    o.residuals = np.frombuffer(r.take(8 * n), "<f8").copy()
     o.error_code = r.i32()
     o.success = r.boolean()
     r.done()

@@ -95,9 +95,9 @@ def fem_solve_blob(blob: bytes) -> bytes:
     return the serialized FEMOutputs blob (ownership handled as the reference's
     FEMInterface::run does, fem_interface.h:464-478)."""
     L = load()
-    buf = C.create_string_buffer(bytes(blob), len(blob))
+    blob = bytes(blob)  # fem_solve only reads the input: pass the bytes object's own buffer
     out = C.c_void_p(0)
-    L.fem_solve(C.cast(buf, C.c_void_p), C.cast(C.pointer(out), C.c_void_p))
+    L.fem_solve(C.cast(C.c_char_p(blob), C.c_void_p), C.cast(C.pointer(out), C.c_void_p))
     if not out.value:
         raise SolverError(11, "fem_solve returned no output blob")
     try:
@@ -106,6 +106,25 @@ def fem_solve_blob(blob: bytes) -> bytes:
     finally:
         L.fem_solve_free(out)
     return data
+
+
+def fem_solve_outputs(blob: bytes):
+    """``fem_solve`` on a serialized FEMInputs blob, returning the decoded
+    FEMOutputs.  The output blob is read in place before it is released, so the
+    displacement field is copied once (into the returned arrays)."""
+    from . import fem_interface as fi
+
+    L = load()
+    blob = bytes(blob)  # fem_solve only reads the input: pass the bytes object's own buffer
+    out = C.c_void_p(0)
+    L.fem_solve(C.cast(C.c_char_p(blob), C.c_void_p), C.cast(C.pointer(out), C.c_void_p))
+    if not out.value:
+        raise SolverError(11, "fem_solve returned no output blob")
+    try:
+        n = C.cast(out, C.POINTER(C.c_uint64))[0]
+        return fi.deserialize_outputs((C.c_char * n).from_address(out.value))
+    finally:
+        L.fem_solve_free(out)
 
 
 def codec_roundtrip(blob: bytes, which: int = 0) -> bytes:

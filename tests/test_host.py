@@ -33,7 +33,11 @@ def test_cpp_codec_is_byte_compatible(native_lib, name, which):
 
 
 def _fem_outputs(blob):
-    return fi.deserialize_outputs(native.fem_solve_blob(blob))
+    out = fi.deserialize_outputs(native.fem_solve_blob(blob))
+    # the in-place decoder must read the same record as the byte-copy path
+    direct = native.fem_solve_outputs(blob)
+    assert (direct.success, direct.error_code, direct.info) == (out.success, out.error_code, out.info)
+    return out
 
 
 def test_fem_solve_reports_malformed_blob(native_lib):
