@@ -28,9 +28,15 @@ __device__ __forceinline__ float kc<float>(int idx) { return c_Kc32[idx]; }
 __device__ __forceinline__ double round_to_float(double v) { return double(float(v)); }
 
 // Programmatic dependent launch: kernels of the solve are launched so that they
-// may start while their predecessor drains; each waits here, before touching
-// memory, until the predecessor has completed and its writes are visible.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// may start while their predecessor drains.  Each waits here until the
+// predecessor has completed and its writes are visible, then lets its own
+// successor be scheduled; code before the wait (a prologue) reads only data
+// that no kernel of the solve writes (lists, neighbour tables, flags, E,
+// stencils), since the predecessor may still be running.
+__device__ __forceinline__ void pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 // ---------------------------------------------------------------------------
 // Level-0 matrix-free operator on one block per CTA (128 threads, one node each)
@@ -212,22 +218,32 @@ __global__ void __launch_bounds__(128, MINB) gs0_list_kernel(const int* __restri
                                                              const int* __restrict__ nbr, const T* __restrict__ E,
                                                              T* u, const T* __restrict__ b,
                                                              const uint32_t* __restrict__ flags, int N, T dx) {
-  pdl_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
+  if (t >= n) {
+    pdl_wait();
+    return;
+  }
+  // prologue: list, flags, neighbour table and E do not change during a solve
   const int raw = list[t];
   const int g = raw >= 0 ? raw : ~raw;
   const uint32_t fl = flags[g];
   const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
+  Nbhd nh;
+  nh.init(nbr, g);
+  T Ec[8];
+#pragma unroll
+  for (int I = 0; I < 8; ++I) {  // the cell of corner I (min corner = node - I) sits at offset -I
+    const int i = nh.at(1 - (I >> 2), 1 - ((I >> 1) & 1), 1 - (I & 1));
+    Ec[I] = (raw < 0 || i < 0) ? T(0) : E[i];
+  }
+  pdl_wait();
   if (raw < 0) {
     if (fx) u[g] = T(0);
     if (fy) u[g + N] = T(0);
     if (fz) u[g + 2 * N] = T(0);
     return;
   }
-  Nbhd nh;
-  nh.init(nbr, g);
-  T gc[8][3], Ec[8], uc[3];
+  T gc[8][3], uc[3];
   T f[3] = {0, 0, 0}, dg[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
   for (int I = 0; I < 8; ++I) gc[I][0] = gc[I][1] = gc[I][2] = T(0);
@@ -241,8 +257,6 @@ __global__ void __launch_bounds__(128, MINB) gs0_list_kernel(const int* __restri
       up[p][0] = i < 0 ? T(0) : u[i];
       up[p][1] = i < 0 ? T(0) : u[i + N];
       up[p][2] = i < 0 ? T(0) : u[i + 2 * N];
-      // the cell of corner I (min corner = node - I) sits at offset -I
-      if (px <= 1 && iy <= 1 && iz <= 1) Ec[(1 - px) * 4 + (1 - iy) * 2 + (1 - iz)] = i < 0 ? T(0) : E[i];
     }
     if (px == 1) {
       uc[0] = up[4][0];
@@ -333,12 +347,14 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__
                                                          const T* u, T* out_u, const T* __restrict__ b,
                                                          T* __restrict__ out, long N, int color, int boundary_only,
                                                          int round_out) {
-  pdl_wait();
   const int per = (OP == SOP_GS) ? 16 : 128;
   const long w = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;  // one warp per node
   const int lane = threadIdx.x & 31;
   const long blk = w / per;
-  if (blk >= nblocks) return;
+  if (blk >= nblocks) {
+    pdl_wait();
+    return;
+  }
   const int bi = block_list ? block_list[blk] : int(blk);
   int e;
   if (OP == SOP_GS) {
@@ -351,20 +367,33 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__
   const long gidx = long(bi) * 128 + e;
   const uint32_t fl = flags[gidx];
   if (OP == SOP_GS) {
-    if (!(fl & ACTIVE_NODE)) return;
-    if (boundary_only && !(fl & BOUNDARY_NODE)) return;
+    if (!(fl & ACTIVE_NODE) || (boundary_only && !(fl & BOUNDARY_NODE))) {
+      pdl_wait();
+      return;
+    }
   }
-  T f0 = 0, f1 = 0, f2 = 0;
+  // prologue: the stencil row (and the neighbour's index) does not change during a solve
+  long n = -1;
+  T a[9];
   if (lane < 27) {
     const int x = coords[3 * bi] + (e >> 5), y = coords[3 * bi + 1] + ((e >> 3) & 3), z = coords[3 * bi + 2] + (e & 7);
-    const long n = g.node(x + lane / 9 - 1, y + (lane / 3) % 3 - 1, z + lane % 3 - 1);
-    if (n >= 0) {
-      const T ux = u[n], uy = u[n + N], uz = u[n + 2 * N];
-      const T* a = A + gidx * 243 + lane * 9;
-      f0 = a[0] * ux + a[1] * uy + a[2] * uz;
-      f1 = a[3] * ux + a[4] * uy + a[5] * uz;
-      f2 = a[6] * ux + a[7] * uy + a[8] * uz;
-    }
+    n = g.node(x + lane / 9 - 1, y + (lane / 3) % 3 - 1, z + lane % 3 - 1);
+    const T* ap = A + gidx * 243 + lane * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = n >= 0 ? ap[k] : T(0);
+  }
+  T d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0;
+  if (OP == SOP_GS && lane == 0) {
+    const T* c = A + gidx * 243 + 13 * 9;
+    d0 = c[0]; d1 = c[4]; d2 = c[8]; d3 = c[1]; d4 = c[2]; d5 = c[5];
+  }
+  pdl_wait();
+  T f0 = 0, f1 = 0, f2 = 0;
+  if (n >= 0) {
+    const T ux = u[n], uy = u[n + N], uz = u[n + 2 * N];
+    f0 = a[0] * ux + a[1] * uy + a[2] * uz;
+    f1 = a[3] * ux + a[4] * uy + a[5] * uz;
+    f2 = a[6] * ux + a[7] * uy + a[8] * uz;
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) {
@@ -388,8 +417,6 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__
     out[gidx + 2 * N] = o2;
     return;
   }
-  const T* c = A + gidx * 243 + 13 * 9;
-  T d0 = c[0], d1 = c[4], d2 = c[8], d3 = c[1], d4 = c[2], d5 = c[5];
   const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
   if (fx) { d0 = 1; d3 = 0; d4 = 0; }
   if (fy) { d1 = 1; d3 = 0; d5 = 0; }
