@@ -31,6 +31,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MGPCG time & MDOF/s to rel.res 1e-6: mixed-prec vs FP64, same B200"
+ACTIVE_NODE = 0x10  # node flag of an active node (solver/Flags.h); DOF = 3 x active nodes
 TOL = 1e-6
 L2_BYTES = 126 * 1024 * 1024
 
@@ -165,7 +166,7 @@ def cpu_baseline(args):
     t0 = time.perf_counter()
     r = o.solve()
     t = time.perf_counter() - t0
-    dof = 3 * o.blocks(0).shape[0] * 128
+    dof = 3 * int(np.count_nonzero(o.flags(0) & ACTIVE_NODE))
     return {"value": dof / t / 1e6, "unit": "MDOF/s", "cores": cores, "kind": "port",
             "sample": f"complete REF-mode solve of sphere_shell{args.cpu_sample_n} ({dof} DOF, {r['iterations']} "
                       f"iterations, {t:.2f} s, tol {TOL})"}
@@ -311,7 +312,7 @@ def run_reference(args, rank, world):
     prob, inp = workload(args.cpu_sample_n, 4, args.workload)
     cores = os.cpu_count() or 1
     o = Oracle(inp, mode=MODE_REF, tolerance=TOL, threads=cores)
-    dof = 3 * o.blocks(0).shape[0] * 128
+    dof = 3 * int(np.count_nonzero(o.flags(0) & ACTIVE_NODE))
     for _ in range(max(0, min(args.warmup, 1))):
         o.solve()
     times, iters = [], []

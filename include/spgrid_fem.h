@@ -60,7 +60,7 @@ typedef struct {
   double setup_seconds;
   double solve_seconds;    /* PCG only, host wall clock */
   int64_t launches_per_iteration;
-  int64_t dof;             /* 3 * nodes of the active level-0 blocks */
+  int64_t dof;             /* 3 * active level-0 nodes (the unknowns of the problem) */
   int64_t bottom_unknowns;
   double solve_device_seconds; /* PCG, CUDA events on the solver stream */
   int64_t kernel_launches;     /* kernels executed by the last solve */

@@ -178,6 +178,7 @@ class Solver {
   }
 
   long N0() const { return long(P.levels[0].nb) * NODES_PER_BLOCK; }
+  long active_nodes0 = 0;  // level-0 nodes flagged active: the problem has 3x as many DOF
 
   // Launch on the solver stream with programmatic stream serialization (the
   // kernel begins with pdl_wait(), so it may be scheduled while its
@@ -294,6 +295,8 @@ class Solver {
     // the level-0 kernels index the [3][N] planes with 32-bit integers
     if (3 * long(P.levels[0].nb) * NODES_PER_BLOCK >= long(INT32_MAX))
       throw CudaError("the finest level has too many blocks for 32-bit node indices", SGS_ERR_INPUT);
+    active_nodes0 = 0;
+    for (long i = 0; i < N0(); ++i) active_nodes0 += (P.levels[0].flags[size_t(i)] & ACTIVE_NODE) ? 1 : 0;
     std::vector<int32_t> gsl;
     int off[17];
     colour_lists(P.levels[0], gsl, off);
@@ -1257,7 +1260,7 @@ SGS_API int sgs_solve(sgs_session* h, double tolerance, int max_iterations, sgs_
     stats->setup_seconds = S.setup_seconds;
     stats->solve_seconds = S.solve_seconds;
     stats->launches_per_iteration = S.launches_per_iteration;
-    stats->dof = 3 * S.N0();
+    stats->dof = 3 * S.active_nodes0;
     stats->bottom_unknowns = S.bottom.n;
     stats->solve_device_seconds = S.solve_device_seconds;
     stats->kernel_launches = S.solve_launches;
