@@ -39,11 +39,14 @@ __device__ __forceinline__ void pdl_wait() {
 }
 
 // ---------------------------------------------------------------------------
-// Level-0 matrix-free operator on one block per CTA (128 threads, one node each)
-// OP_KU: out = dx*K*u, OP_RES: out = b - dx*K*u, OP_GS: colour-`color` Gauss-Seidel
-// update of u in place (solver/CPU_Kernels/SPGrid_Gauss_Seidel.h:876-1180).
+// Level-0 matrix-free operator on one block per CTA (128 threads, one node each;
+// solver/CPU_Kernels/SPGrid_Linear_Elasticity.h:96-344): OP_KU: out = dx*K*u,
+// OP_RES: out = b - dx*K*u.  u of the block plus a one-node halo and E of the
+// cells around it are staged in shared memory; each node sums its 8 cells,
+// g_I = sum_J Kc[I][J] u_J scaled by E_I.  Empty cells (E = 0) are skipped,
+// which saves the work wherever a warp's nodes share them (band edges).
 // ---------------------------------------------------------------------------
-enum { OP_KU = 0, OP_RES = 1, OP_GS = 2 };
+enum { OP_KU = 0, OP_RES = 1 };
 
 // halo geometry: nodes [-1,4]x[-1,4]x[-1,8] (6x6x10), cells [-1,3]x[-1,3]x[-1,7] (5x5x9)
 constexpr int HU = 360, HE = 225;
@@ -51,9 +54,8 @@ constexpr int HU = 360, HE = 225;
 template <typename T, int OP>
 __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ block_list, int nblocks,
                                                         const int* __restrict__ nbr, const T* __restrict__ E,
-                                                        const T* u, T* out_u, const T* __restrict__ b,
-                                                        T* __restrict__ out, const uint32_t* __restrict__ flags,
-                                                        long N, T dx, int color, int boundary_only) {
+                                                        const T* u, const T* __restrict__ b, T* __restrict__ out,
+                                                        long N, T dx) {
   pdl_wait();
   __shared__ T su[3][HU];
   __shared__ T sE[HE];
@@ -89,26 +91,13 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
   const int e = threadIdx.x;
   const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
   const long gidx = long(bi) * 128 + e;
-  uint32_t fl = 0;
-  if (OP == OP_GS) {
-    if (((x & 1) << 2 | (y & 1) << 1 | (z & 1)) != color) return;
-    fl = flags[gidx];
-    const bool act = (fl & ACTIVE_NODE) && (!boundary_only || (fl & BOUNDARY_NODE));
-    if (!act) {
-      // inactive nodes keep u; Dirichlet components are still cleared
-      if (fl & DIR_X) out_u[gidx] = T(0);
-      if (fl & DIR_Y) out_u[gidx + N] = T(0);
-      if (fl & DIR_Z) out_u[gidx + 2 * N] = T(0);
-      return;
-    }
-  }
   T f0 = 0, f1 = 0, f2 = 0;
-  T d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0;
 #pragma unroll
   for (int I = 0; I < 8; ++I) {
     const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
     const int cx = x - Ix, cy = y - Iy, cz = z - Iz;  // cell, in [-1,3]x[-1,3]x[-1,7]
     const T Ec = sE[((cx + 1) * 5 + (cy + 1)) * 9 + (cz + 1)];
+    if (Ec == T(0)) continue;
     T g0 = 0, g1 = 0, g2 = 0;
 #pragma unroll
     for (int J = 0; J < 8; ++J) {
@@ -119,14 +108,6 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
       g0 += kc<T>(k + 0) * ux + kc<T>(k + 1) * uy + kc<T>(k + 2) * uz;
       g1 += kc<T>(k + 3) * ux + kc<T>(k + 4) * uy + kc<T>(k + 5) * uz;
       g2 += kc<T>(k + 6) * ux + kc<T>(k + 7) * uy + kc<T>(k + 8) * uz;
-      if (OP == OP_GS && J == I) {
-        d0 += Ec * kc<T>(k + 0);
-        d1 += Ec * kc<T>(k + 4);
-        d2 += Ec * kc<T>(k + 8);
-        d3 += Ec * kc<T>(k + 1);
-        d4 += Ec * kc<T>(k + 2);
-        d5 += Ec * kc<T>(k + 5);
-      }
     }
     f0 += Ec * g0;
     f1 += Ec * g1;
@@ -139,38 +120,11 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
     out[gidx] = f0;
     out[gidx + N] = f1;
     out[gidx + 2 * N] = f2;
-    return;
-  }
-  if (OP == OP_RES) {
+  } else {
     out[gidx] = b[gidx] - f0;
     out[gidx + N] = b[gidx + N] - f1;
     out[gidx + 2 * N] = b[gidx + 2 * N] - f2;
-    return;
   }
-  // Gauss-Seidel update: u += D^{-1} (b - K u) with Dirichlet rows replaced by identity
-  const T r0 = b[gidx] - f0, r1 = b[gidx + N] - f1, r2 = b[gidx + 2 * N] - f2;
-  d0 *= dx; d1 *= dx; d2 *= dx; d3 *= dx; d4 *= dx; d5 *= dx;
-  const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
-  if (fx) { d0 = 1; d3 = 0; d4 = 0; }
-  if (fy) { d1 = 1; d3 = 0; d5 = 0; }
-  if (fz) { d2 = 1; d4 = 0; d5 = 0; }
-  const T m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
-  const T m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
-  const T inv = T(1) / (d0 * m11 + d3 * m12 + d4 * m13);
-  T a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
-  if (fx) { a0 = 0; a3 = 0; a4 = 0; }
-  if (fy) { a1 = 0; a3 = 0; a5 = 0; }
-  if (fz) { a2 = 0; a4 = 0; a5 = 0; }
-  const int hc = ((x + 1) * 6 + (y + 1)) * 10 + (z + 1);
-  T u0 = su[0][hc] + r0 * a0 + r1 * a3 + r2 * a4;
-  T u1 = su[1][hc] + r0 * a3 + r1 * a1 + r2 * a5;
-  T u2 = su[2][hc] + r0 * a4 + r1 * a5 + r2 * a2;
-  if (fx) u0 = 0;
-  if (fy) u1 = 0;
-  if (fz) u2 = 0;
-  out_u[gidx] = u0;
-  out_u[gidx + N] = u1;
-  out_u[gidx + 2 * N] = u2;
 }
 
 // ---------------------------------------------------------------------------

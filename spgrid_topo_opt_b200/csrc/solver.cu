@@ -494,12 +494,12 @@ class Solver {
     ++launch_counter;
   }
 
+  // out = dx K u (OP_KU) or b - dx K u (OP_RES) over all level-0 blocks
   template <typename T, int OP>
-  void level0(const int* list, int count, const T* u, T* uo, const T* b, T* out, int color, int boundary) {
+  void level0(const T* u, const T* b, T* out) {
     Level<T>& d = lev<T>(0);
-    if (count <= 0) return;
-    launch(level0_op_kernel<T, OP>, count, 128, 0, list, count, d.nbr.p, Edev<T>(), u, uo, b, out, d.flags.p, d.N,
-                                                      T(P.dx), color, boundary);
+    if (d.nb <= 0) return;
+    launch(level0_op_kernel<T, OP>, d.nb, 128, 0, nullptr, d.nb, d.nbr.p, Edev<T>(), u, b, out, d.N, T(P.dx));
     ++launch_counter;
   }
 
@@ -623,7 +623,7 @@ class Solver {
       Level<T>& d = lev<T>(l);
       if (smooth) {
         if (l == 0) {
-          level0<T, OP_RES>(nullptr, d.nb, U(0), nullptr, B(0), d.r.p, 0, 0);
+          level0<T, OP_RES>(U(0), B(0), d.r.p);
           if (rr) round3(d, d.r.p);
         } else {
           stencil<T, SOP_RES>(l, nullptr, d.nb, U(l), nullptr, B(l), d.r.p, 0, 0, rr ? 1 : 0);
@@ -922,7 +922,7 @@ void Solver::record_iteration() {
   launch(dot_partial_kernel, RED_BLOCKS, RED_THREADS, 0, q.p, f.p, 3 * N0(), red.p);
   launch(finish_reduce_kernel, 1, 32, 0, red.p, RED_BLOCKS, 0, scal.p, 0);
   axpy(s.p, 1, 4, s.p, q.p);  // s = beta*s + z
-  level0<double, OP_KU>(nullptr, l0.nb, s.p, nullptr, nullptr, q.p, 0, 0);
+  level0<double, OP_KU>(s.p, nullptr, q.p);
   project<double>(l0, q.p);
   launch(dot_partial_kernel, RED_BLOCKS, RED_THREADS, 0, s.p, q.p, 3 * N0(), red.p);
   launch(finish_reduce_kernel, 1, 32, 0, red.p, RED_BLOCKS, 0, scal.p, 1);
@@ -959,7 +959,7 @@ void Solver::solve() {
         s.p, force_node.p, force_val.p, int(P.force_node.size()), N);
   project<double>(l0, s.p);
   project_null<double>(l0, s.p);
-  level0<double, OP_RES>(nullptr, l0.nb, x.p, nullptr, s.p, f.p, 0, 0);
+  level0<double, OP_RES>(x.p, s.p, f.p);
   project<double>(l0, f.p);
   SGS_CUDA(cudaMemcpyAsync(ubk.p, x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
   q.zero(stream);
@@ -972,7 +972,7 @@ void Solver::solve() {
   auto t0 = std::chrono::steady_clock::now();
   x.zero(stream);
   // CONJUGATE_GRADIENT_4Ch::Solve: q = K x (= 0); r -= q; Project(r)
-  level0<double, OP_KU>(nullptr, l0.nb, x.p, nullptr, nullptr, q.p, 0, 0);
+  level0<double, OP_KU>(x.p, nullptr, q.p);
   launch(sub_kernel, blocks_for(n3, 256), 256, 0, f.p, q.p, n3, fr);
   project<double>(l0, f.p);
   double init_scal[16] = {0};
@@ -1134,8 +1134,8 @@ static int apply_op(Solver& S, int op, int level, int arg, const double* in, con
       if (level != 0) return SGS_ERR_INPUT;
       put_field<T>(S, d.u.p, in, N);
       if (op == 1) put_field<T>(S, d.b.p, in2, N);
-      if (op == 0) S.level0<T, OP_KU>(nullptr, d.nb, d.u.p, nullptr, nullptr, d.r.p, 0, 0);
-      else S.level0<T, OP_RES>(nullptr, d.nb, d.u.p, nullptr, d.b.p, d.r.p, 0, 0);
+      if (op == 0) S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);
+      else S.level0<T, OP_RES>(d.u.p, d.b.p, d.r.p);
       get_field<T>(S, out, d.r.p, N);
       return 0;
     case 2:
@@ -1190,8 +1190,8 @@ static double time_op(Solver& S, int op, int reps) {
   SGS_CUDA(cudaEventCreate(&a));
   SGS_CUDA(cudaEventCreate(&b));
   auto run = [&]() {
-    if (op == 0) S.level0<T, OP_KU>(nullptr, d.nb, d.u.p, nullptr, nullptr, d.r.p, 0, 0);
-    else if (op == 1) S.level0<T, OP_RES>(nullptr, d.nb, d.u.p, nullptr, d.b.p, d.r.p, 0, 0);
+    if (op == 0) S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);
+    else if (op == 1) S.level0<T, OP_RES>(d.u.p, d.b.p, d.r.p);
     else if (op == 2) S.sweep<T>(0, d.u.p, d.b.p, true, false);
     else if (op == 3) S.precondition();
   };
