@@ -46,7 +46,7 @@ __device__ __forceinline__ void pdl_wait() {
 // g_I = sum_J Kc[I][J] u_J scaled by E_I.  Empty cells (E = 0) are skipped,
 // which saves the work wherever a warp's nodes share them (band edges).
 // ---------------------------------------------------------------------------
-enum { OP_KU = 0, OP_RES = 1 };
+enum { OP_KU = 0, OP_RES = 1, OP_KUP = 2 };  // OP_KUP: K u with Project, and the CTA's partial u.(Ku)
 
 // halo geometry: nodes [-1,4]x[-1,4]x[-1,8] (6x6x10), cells [-1,3]x[-1,3]x[-1,7] (5x5x9)
 constexpr int HU = 360, HE = 225;
@@ -55,7 +55,8 @@ template <typename T, int OP>
 __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ block_list, int nblocks,
                                                         const int* __restrict__ nbr, const T* __restrict__ E,
                                                         const T* u, const T* __restrict__ b, T* __restrict__ out,
-                                                        long N, T dx) {
+                                                        long N, T dx, const uint32_t* __restrict__ flags,
+                                                        double* __restrict__ part) {
   pdl_wait();
   __shared__ T su[3][HU];
   __shared__ T sE[HE];
@@ -120,10 +121,27 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
     out[gidx] = f0;
     out[gidx + N] = f1;
     out[gidx + 2 * N] = f2;
-  } else {
+  } else if (OP == OP_RES) {
     out[gidx] = b[gidx] - f0;
     out[gidx + N] = b[gidx + N] - f1;
     out[gidx + 2 * N] = b[gidx + 2 * N] - f2;
+  } else {
+    // the PCG matvec q = K s: Dirichlet components zeroed, and s.q summed per CTA
+    const uint32_t fl = flags[gidx];
+    if (fl & DIR_X) f0 = 0;
+    if (fl & DIR_Y) f1 = 0;
+    if (fl & DIR_Z) f2 = 0;
+    out[gidx] = f0;
+    out[gidx + N] = f1;
+    out[gidx + 2 * N] = f2;
+    const int hc = ((x + 1) * 6 + (y + 1)) * 10 + (z + 1);
+    double d = double(su[0][hc]) * double(f0) + double(su[1][hc]) * double(f1) + double(su[2][hc]) * double(f2);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+    __shared__ double sd[4];
+    if ((threadIdx.x & 31) == 0) sd[threadIdx.x >> 5] = d;
+    __syncthreads();
+    if (threadIdx.x == 0) part[blockIdx.x] = (sd[0] + sd[1]) + (sd[2] + sd[3]);
   }
 }
 

@@ -458,7 +458,7 @@ class Solver {
     lift_val.upload(P.lift_val, stream);
     force_node.upload(P.force_node, stream);
     force_val.upload(P.force_val, stream);
-    red.alloc(1024);
+    red.alloc(size_t(std::max<long>(1024, P.levels[0].nb)));  // reduction partials (one per level-0 block at most)
     scal.alloc(16);
     scal.zero(stream);
     in_block.upload(P.in_block, stream);
@@ -494,12 +494,14 @@ class Solver {
     ++launch_counter;
   }
 
-  // out = dx K u (OP_KU) or b - dx K u (OP_RES) over all level-0 blocks
+  // out = dx K u (OP_KU), b - dx K u (OP_RES) or the projected PCG matvec with
+  // per-block partial products u.out in red (OP_KUP) over all level-0 blocks
   template <typename T, int OP>
   void level0(const T* u, const T* b, T* out) {
     Level<T>& d = lev<T>(0);
     if (d.nb <= 0) return;
-    launch(level0_op_kernel<T, OP>, d.nb, 128, 0, nullptr, d.nb, d.nbr.p, Edev<T>(), u, b, out, d.N, T(P.dx));
+    launch(level0_op_kernel<T, OP>, d.nb, 128, 0, nullptr, d.nb, d.nbr.p, Edev<T>(), u, b, out, d.N, T(P.dx),
+           d.flags.p, red.p);
     ++launch_counter;
   }
 
@@ -645,6 +647,7 @@ class Solver {
   void linf(const double* a, double* out);
   void axpy(double* dst, double sign, int coef_slot, const double* xv, const double* yv);
   void precondition();
+  void stage_residual();
   void record_iteration();
   void solve();
   void pack_outputs(double* disp);
@@ -733,19 +736,24 @@ __global__ void linf_partial_kernel(const double* __restrict__ a, long n, double
   }
 }
 
-// Fixed-order final reduction; op 0 = sum, 1 = max.  Also derives the PCG scalars:
-// what = 0: rho -> beta = rho/rho_old;  what = 1: sq -> alpha, -alpha, breakdown flag;
-// what = 2: norm.
+// Fixed-order final reduction by one CTA of FIN_THREADS; op 0 = sum, 1 = max.
+// Also derives the PCG scalars: what = 0: rho -> beta = rho/rho_old;
+// what = 1: sq -> alpha, -alpha, breakdown flag; what = 2: norm; what = 4: norm
+// and rho_old = rho (the end of an iteration).
+constexpr int FIN_THREADS = 256;
 __global__ void finish_reduce_kernel(const double* __restrict__ part, int np, int op, double* scal, int what) {
   pdl_wait();
-  __shared__ double sm[32];
+  __shared__ double sm[FIN_THREADS];
   double s = 0;
-  for (int i = threadIdx.x; i < np; i += 32) s = op ? fmax(s, part[i]) : s + part[i];
+  for (int i = threadIdx.x; i < np; i += FIN_THREADS) s = op ? fmax(s, part[i]) : s + part[i];
   sm[threadIdx.x] = s;
-  __syncwarp();
+  __syncthreads();
+  for (int w = FIN_THREADS / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sm[threadIdx.x] = op ? fmax(sm[threadIdx.x], sm[threadIdx.x + w]) : sm[threadIdx.x] + sm[threadIdx.x + w];
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
-    double t = 0;
-    for (int w = 0; w < 32; ++w) t = op ? fmax(t, sm[w]) : t + sm[w];
+    const double t = sm[0];
     if (what == 0) {
       scal[0] = t;               // rho
       scal[4] = t / scal[1];     // beta = rho / rho_old
@@ -756,9 +764,81 @@ __global__ void finish_reduce_kernel(const double* __restrict__ part, int np, in
       scal[6] = -scal[5];
     } else if (what == 2) {
       scal[3] = t;
+    } else if (what == 4) {
+      scal[3] = t;
+      scal[1] = scal[0];
     } else {
       scal[8] = t;
     }
+  }
+}
+
+// The V-cycle's z into q with Project and Project_Nullspace (KRYLOV_SYSTEM_BASE.cpp:25-31),
+// and per-CTA partials of rho = q.r (CONJUGATE_GRADIENT.cpp:41); z may alias q.
+template <typename TS>
+__global__ void precond_out_kernel(const TS* z, double* q, const double* __restrict__ f,
+                                   const uint32_t* __restrict__ flags, long N, double* __restrict__ part) {
+  pdl_wait();
+  __shared__ double sm[RED_THREADS / 32];
+  double s = 0;
+  for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += long(gridDim.x) * blockDim.x) {
+    const uint32_t fl = flags[i];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const long k = i + v * N;
+      const double val = ((fl & ACTIVE_NODE) && !(fl & (DIR_X << v))) ? double(z[k]) : 0.0;
+      q[k] = val;
+      s += val * f[k];
+    }
+  }
+  for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t += sm[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+// End of a PCG iteration (CONJUGATE_GRADIENT.cpp:54-57, 32-33): x += alpha s,
+// r -= alpha q (float-rounded like CG_VECTOR in the reference mode), then
+// Project_Nullspace(r), per-CTA partials of |r|_inf and, when b32 is given, the
+// single-precision copy of r that the next V-cycle starts from.
+__global__ void cg_update_kernel(double* x, const double* __restrict__ s, double* f, const double* __restrict__ q,
+                                 const double* __restrict__ scal, const uint32_t* __restrict__ flags, long N,
+                                 int float_round, float* __restrict__ b32, double* __restrict__ part) {
+  pdl_wait();
+  __shared__ double sm[RED_THREADS / 32];
+  const double a = scal[5], na = scal[6];
+  double m = 0;
+  for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += long(gridDim.x) * blockDim.x) {
+    const bool act = flags[i] & ACTIVE_NODE;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const long k = i + v * N;
+      double xv, fv;
+      if (float_round) {
+        xv = double(__fadd_rn(__fmul_rn(float(a), float(s[k])), float(x[k])));
+        fv = double(__fadd_rn(__fmul_rn(float(na), float(q[k])), float(f[k])));
+      } else {
+        xv = a * s[k] + x[k];
+        fv = na * q[k] + f[k];
+      }
+      if (!act) fv = 0;
+      x[k] = xv;
+      f[k] = fv;
+      if (b32) b32[k] = float(fv);
+      m = fmax(m, fabs(fv));
+    }
+  }
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t = fmax(t, sm[w]);
+    part[blockIdx.x] = t;
   }
 }
 
@@ -885,7 +965,7 @@ void Solver::dot(const double* a, const double* b, double* out_unused) {
 
 void Solver::linf(const double* a, double*) {
   launch(linf_partial_kernel, RED_BLOCKS, RED_THREADS, 0, a, 3 * N0(), red.p);
-  launch(finish_reduce_kernel, 1, 32, 0, red.p, RED_BLOCKS, 1, scal.p, 2);
+  launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, RED_BLOCKS, 1, scal.p, 2);
   launch_counter += 2;
 }
 
@@ -895,43 +975,48 @@ void Solver::axpy(double* dst, double, int slot, const double* xv, const double*
 }
 
 // z = M^-1 r into q (z and q share storage, SPGrid_CPU_Solver.cpp:91-92), then
-// Project and Project_Nullspace (KRYLOV_SYSTEM_BASE.cpp:25-31)
+// Project and Project_Nullspace (KRYLOV_SYSTEM_BASE.cpp:25-31), fused with the
+// partial sums of rho = q.r.  In mixed precision the V-cycle starts from the
+// FP32 copy of r in level 0's b, written by stage_residual() or by the previous
+// iteration's update.
 void Solver::precondition() {
   Level<double>& l0 = *L64[0];
   const long N = l0.N;
   if (P.disable_mg) {
     SGS_CUDA(cudaMemcpyAsync(q.p, f.p, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    launch(precond_out_kernel<double>, RED_BLOCKS, RED_THREADS, 0, q.p, q.p, f.p, l0.flags.p, N, red.p);
   } else if (mixed()) {
     Level<float>& m0 = *L32[0];
-    launch(convert_kernel<float, double>, blocks_for(3 * N, 256), 256, 0, m0.b.p, f.p, 3 * N);
     vcycle<float>(m0.b.p, m0.u.p);
-    launch(convert_kernel<double, float>, blocks_for(3 * N, 256), 256, 0, q.p, m0.u.p, 3 * N);
-    launch_counter += 2;
+    launch(precond_out_kernel<float>, RED_BLOCKS, RED_THREADS, 0, m0.u.p, q.p, f.p, l0.flags.p, N, red.p);
   } else {
     vcycle<double>(f.p, q.p);
+    launch(precond_out_kernel<double>, RED_BLOCKS, RED_THREADS, 0, q.p, q.p, f.p, l0.flags.p, N, red.p);
   }
-  project<double>(l0, q.p);
-  project_null<double>(l0, q.p);
+  ++launch_counter;
+}
+
+// the FP32 copy of the residual for the mixed V-cycle
+void Solver::stage_residual() {
+  if (!mixed() || P.disable_mg) return;
+  const long n3 = 3 * N0();
+  launch(convert_kernel<float, double>, blocks_for(n3, 256), 256, 0, L32[0]->b.p, f.p, n3);
+  ++launch_counter;
 }
 
 // One PCG iteration after the convergence test (CONJUGATE_GRADIENT.cpp:41-57) plus
 // the next iteration's Project_Nullspace and norm (:32-33).
 void Solver::record_iteration() {
   Level<double>& l0 = *L64[0];
-  precondition();
-  launch(dot_partial_kernel, RED_BLOCKS, RED_THREADS, 0, q.p, f.p, 3 * N0(), red.p);
-  launch(finish_reduce_kernel, 1, 32, 0, red.p, RED_BLOCKS, 0, scal.p, 0);
-  axpy(s.p, 1, 4, s.p, q.p);  // s = beta*s + z
-  level0<double, OP_KU>(s.p, nullptr, q.p);
-  project<double>(l0, q.p);
-  launch(dot_partial_kernel, RED_BLOCKS, RED_THREADS, 0, s.p, q.p, 3 * N0(), red.p);
-  launch(finish_reduce_kernel, 1, 32, 0, red.p, RED_BLOCKS, 0, scal.p, 1);
-  axpy(x.p, 1, 5, s.p, x.p);   // x = alpha*s + x
-  axpy(f.p, 1, 6, q.p, f.p);   // r = -alpha*q + r
-  launch(rho_shift_kernel, 1, 1, 0, scal.p);
-  project_null<double>(l0, f.p);
-  linf(f.p, nullptr);
-  launch_counter += 5;
+  precondition();                                                        // q = z, rho partials
+  launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, RED_BLOCKS, 0, scal.p, 0);  // rho, beta
+  axpy(s.p, 1, 4, s.p, q.p);                                             // s = beta*s + z
+  level0<double, OP_KUP>(s.p, nullptr, q.p);                             // q = K s, Project, s.q partials
+  launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, l0.nb, 0, scal.p, 1);       // alpha
+  launch(cg_update_kernel, RED_BLOCKS, RED_THREADS, 0, x.p, s.p, f.p, q.p, scal.p, l0.flags.p, l0.N,
+         round_ref() ? 1 : 0, (mixed() && !P.disable_mg) ? L32[0]->b.p : (float*)nullptr, red.p);
+  launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, RED_BLOCKS, 1, scal.p, 4);  // |r|_inf, rho_old
+  launch_counter += 4;
 }
 
 void Solver::solve() {
@@ -980,6 +1065,7 @@ void Solver::solve() {
   SGS_CUDA(cudaMemcpyAsync(scal.p, init_scal, sizeof(init_scal), cudaMemcpyHostToDevice, stream));
   project_null<double>(l0, f.p);
   linf(f.p, nullptr);
+  stage_residual();
   // capture one iteration as a CUDA graph
   long capture_launches = 0;
   if (!iter_graph) {
@@ -1174,6 +1260,7 @@ static int apply_op(Solver& S, int op, int level, int arg, const double* in, con
       if (level != 0) return SGS_ERR_INPUT;
       std::vector<double> tmp(in, in + 3 * N);
       SGS_CUDA(cudaMemcpyAsync(S.f.p, tmp.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+      S.stage_residual();
       S.precondition();
       SGS_CUDA(cudaMemcpyAsync(out, S.q.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
       SGS_CUDA(cudaStreamSynchronize(S.stream));
