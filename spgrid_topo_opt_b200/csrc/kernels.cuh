@@ -288,6 +288,190 @@ __global__ void __launch_bounds__(128, MINB) gs0_list_kernel(const int* __restri
 }
 
 // ---------------------------------------------------------------------------
+// Packed level 0 of the single-precision V-cycle.  The iterate of level 0 is
+// one float4 per node, (u_x, u_y, u_z, E of the node's cell): the 27-point
+// gathers of the smoother and the halo staging of the residual then read a
+// node's displacement and its cell's stiffness scale in one 16-byte load, the
+// same bytes as three planes of u plus the E plane.
+// ---------------------------------------------------------------------------
+
+// u4 = (0, 0, 0, E): the zero start of the V-cycle's level-0 correction
+__global__ void reset_u4_kernel(float4* __restrict__ u4, const float* __restrict__ E, long N) {
+  pdl_wait();
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < N) u4[i] = make_float4(0.f, 0.f, 0.f, E[i]);
+}
+
+// planar fields <-> packed iterate (for the unit operators on a packed level)
+__global__ void pack_u4_kernel(float4* __restrict__ u4, const float* __restrict__ u, const float* __restrict__ E,
+                               long N) {
+  pdl_wait();
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < N) u4[i] = make_float4(u[i], u[i + N], u[i + 2 * N], E[i]);
+}
+__global__ void unpack_u4_kernel(float* __restrict__ u, const float4* __restrict__ u4, long N) {
+  pdl_wait();
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float4 v = u4[i];
+  u[i] = v.x;
+  u[i + N] = v.y;
+  u[i + 2 * N] = v.z;
+}
+
+// gs0_list_kernel on the packed iterate (one float4 gather per neighbour; the
+// cells' E come with the nodes at offsets -I).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restrict__ list, int n,
+                                                              const int* __restrict__ nbr, float4* u4,
+                                                              const float* __restrict__ b,
+                                                              const uint32_t* __restrict__ flags, int N, float dx) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) {
+    pdl_wait();
+    return;
+  }
+  const int raw = list[t];
+  const int g = raw >= 0 ? raw : ~raw;
+  const uint32_t fl = flags[g];
+  const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
+  Nbhd nh;
+  nh.init(nbr, g);
+  pdl_wait();
+  if (raw < 0) {
+    float4 v = u4[g];
+    if (fx) v.x = 0.f;
+    if (fy) v.y = 0.f;
+    if (fz) v.z = 0.f;
+    u4[g] = v;
+    return;
+  }
+  float gc[8][3], Ec[8], uc[3];
+  float f[3] = {0.f, 0.f, 0.f}, dg[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int I = 0; I < 8; ++I) gc[I][0] = gc[I][1] = gc[I][2] = 0.f;
+#pragma unroll
+  for (int px = 0; px < 3; ++px) {
+    float up[9][3];
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+      const int iy = p / 3, iz = p % 3;
+      const int i = (px == 1 && p == 4) ? g : nh.at(px, iy, iz);
+      const float4 v = i < 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : u4[i];
+      up[p][0] = v.x;
+      up[p][1] = v.y;
+      up[p][2] = v.z;
+      if (px <= 1 && iy <= 1 && iz <= 1) Ec[(1 - px) * 4 + (1 - iy) * 2 + (1 - iz)] = v.w;
+    }
+    if (px == 1) {
+      uc[0] = up[4][0];
+      uc[1] = up[4][1];
+      uc[2] = up[4][2];
+    }
+#pragma unroll
+    for (int I = 0; I < 8; ++I) {
+      const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
+      const int Jx = px - 1 + Ix;
+      if (Jx < 0 || Jx > 1) continue;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int Jy = q >> 1, Jz = q & 1;
+        const int p = (Jy - Iy + 1) * 3 + (Jz - Iz + 1);
+        const int k = (I * 8 + Jx * 4 + Jy * 2 + Jz) * 9;
+#pragma unroll
+        for (int v = 0; v < 3; ++v)
+#pragma unroll
+          for (int w = 0; w < 3; ++w) gc[I][v] = fmaf(kc<float>(k + v * 3 + w), up[p][w], gc[I][v]);
+      }
+      if (Jx == 1) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) f[v] = fmaf(Ec[I], gc[I][v], f[v]);
+        const int kd = (I * 8 + I) * 9;
+        dg[0] = fmaf(kc<float>(kd + 0), Ec[I], dg[0]);
+        dg[1] = fmaf(kc<float>(kd + 4), Ec[I], dg[1]);
+        dg[2] = fmaf(kc<float>(kd + 8), Ec[I], dg[2]);
+        dg[3] = fmaf(kc<float>(kd + 1), Ec[I], dg[3]);
+        dg[4] = fmaf(kc<float>(kd + 2), Ec[I], dg[4]);
+        dg[5] = fmaf(kc<float>(kd + 5), Ec[I], dg[5]);
+      }
+    }
+  }
+  const float r0 = b[g] - f[0] * dx, r1 = b[g + N] - f[1] * dx, r2 = b[g + 2 * N] - f[2] * dx;
+  float d0 = dg[0] * dx, d1 = dg[1] * dx, d2 = dg[2] * dx, d3 = dg[3] * dx, d4 = dg[4] * dx, d5 = dg[5] * dx;
+  if (fx) { d0 = 1; d3 = 0; d4 = 0; }
+  if (fy) { d1 = 1; d3 = 0; d5 = 0; }
+  if (fz) { d2 = 1; d4 = 0; d5 = 0; }
+  const float m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
+  const float m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
+  const float inv = 1.f / (d0 * m11 + d3 * m12 + d4 * m13);
+  float a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
+  if (fx) { a0 = 0; a3 = 0; a4 = 0; }
+  if (fy) { a1 = 0; a3 = 0; a5 = 0; }
+  if (fz) { a2 = 0; a4 = 0; a5 = 0; }
+  float v0 = uc[0] + r0 * a0 + r1 * a3 + r2 * a4;
+  float v1 = uc[1] + r0 * a3 + r1 * a1 + r2 * a5;
+  float v2 = uc[2] + r0 * a4 + r1 * a5 + r2 * a2;
+  if (fx) v0 = 0;
+  if (fy) v1 = 0;
+  if (fz) v2 = 0;
+  u4[g] = make_float4(v0, v1, v2, Ec[0]);  // corner I = 0: the node's own cell
+}
+
+// level0_op_kernel<float, OP_RES> on the packed iterate: r = b - dx K u
+__global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int* __restrict__ nbr,
+                                                          const float4* __restrict__ u4, const float* __restrict__ b,
+                                                          float* __restrict__ out, long N, float dx) {
+  pdl_wait();
+  __shared__ float su[3][HU];
+  __shared__ float sE[HU];
+  __shared__ int snb[27];
+  const int bi = blockIdx.x;
+  if (threadIdx.x < 27) snb[threadIdx.x] = nbr[long(bi) * 27 + threadIdx.x];
+  __syncthreads();
+  for (int h = threadIdx.x; h < HU; h += 128) {
+    const int sx = h / 60, sy = (h / 10) % 6, sz = h % 10;
+    const int lx = sx - 1, ly = sy - 1, lz = sz - 1;
+    const int dxb = lx < 0 ? 0 : (lx > 3 ? 2 : 1), dyb = ly < 0 ? 0 : (ly > 3 ? 2 : 1), dzb = lz < 0 ? 0 : (lz > 7 ? 2 : 1);
+    const int nb = snb[dxb * 9 + dyb * 3 + dzb];
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (nb >= 0) v = u4[long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7)];
+    su[0][h] = v.x;
+    su[1][h] = v.y;
+    su[2][h] = v.z;
+    sE[h] = v.w;
+  }
+  __syncthreads();
+  const int e = threadIdx.x;
+  const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
+  const long gidx = long(bi) * 128 + e;
+  float f0 = 0, f1 = 0, f2 = 0;
+#pragma unroll
+  for (int I = 0; I < 8; ++I) {
+    const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
+    const int cx = x - Ix, cy = y - Iy, cz = z - Iz;  // cell = its min-corner node, in the halo
+    const float Ec = sE[((cx + 1) * 6 + (cy + 1)) * 10 + (cz + 1)];
+    if (Ec == 0.f) continue;
+    float g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+    for (int J = 0; J < 8; ++J) {
+      const int nx = cx + (J >> 2) + 1, ny = cy + ((J >> 1) & 1) + 1, nz = cz + (J & 1) + 1;
+      const int h = (nx * 6 + ny) * 10 + nz;
+      const float ux = su[0][h], uy = su[1][h], uz = su[2][h];
+      const int k = (I * 8 + J) * 9;
+      g0 += kc<float>(k + 0) * ux + kc<float>(k + 1) * uy + kc<float>(k + 2) * uz;
+      g1 += kc<float>(k + 3) * ux + kc<float>(k + 4) * uy + kc<float>(k + 5) * uz;
+      g2 += kc<float>(k + 6) * ux + kc<float>(k + 7) * uy + kc<float>(k + 8) * uz;
+    }
+    f0 += Ec * g0;
+    f1 += Ec * g1;
+    f2 += Ec * g2;
+  }
+  out[gidx] = b[gidx] - f0 * dx;
+  out[gidx + N] = b[gidx + N] - f1 * dx;
+  out[gidx + 2 * N] = b[gidx + 2 * N] - f2 * dx;
+}
+
+// ---------------------------------------------------------------------------
 // Coarse-level stencil operators (solver/MG/SPGrid_Stencil_Multiply.h:15-280)
 // ---------------------------------------------------------------------------
 struct GridView {
@@ -478,6 +662,38 @@ __global__ void prolongate_kernel(int nb, const int* __restrict__ coords, const 
   fu[t] = v0;
   fu[t + Nf] = v1;
   fu[t + 2 * Nf] = v2;
+}
+
+// prolongate_kernel into the packed level-0 iterate (E in .w is kept)
+__global__ void prolongate4_kernel(int nb, const int* __restrict__ coords, const uint32_t* __restrict__ fflags,
+                                   GridView coarse, const float* __restrict__ cin, long Nc, float4* __restrict__ fu4) {
+  pdl_wait();
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nb) * 128) return;
+  const int bi = int(t >> 7), e = int(t & 127);
+  const int lx = e >> 5, ly = (e >> 3) & 3, lz = e & 7;
+  const int x = coords[3 * bi] + lx, y = coords[3 * bi + 1] + ly, z = coords[3 * bi + 2] + lz;
+  const int cx = (x + 4) >> 1, cy = (y + 4) >> 1, cz = (z + 8) >> 1;
+  float4 v = fu4[t];
+  for (int q = 0; q < 8; ++q) {
+    const int ii = q >> 2, jj = (q >> 1) & 1, kk = q & 1;
+    const double wx = (lx & 1) ? 0.5 : (ii ? 0.0 : 1.0);
+    const double wy = (ly & 1) ? 0.5 : (jj ? 0.0 : 1.0);
+    const double wz = (lz & 1) ? 0.5 : (kk ? 0.0 : 1.0);
+    const float w = float(wx * wy * wz);
+    if (!(w > 0.f)) continue;
+    const long n = coarse.node(cx + ii, cy + jj, cz + kk);
+    if (n < 0) continue;
+    v.x += w * cin[n];
+    v.y += w * cin[n + Nc];
+    v.z += w * cin[n + 2 * Nc];
+  }
+  const uint32_t fl = fflags[t];
+  if (fl & DIR_X) v.x = 0;
+  if (fl & DIR_Y) v.y = 0;
+  if (fl & DIR_Z) v.z = 0;
+  if (!(fl & ACTIVE_NODE)) v.x = v.y = v.z = 0;
+  fu4[t] = v;
 }
 
 // ---------------------------------------------------------------------------

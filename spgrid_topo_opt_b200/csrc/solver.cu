@@ -120,6 +120,8 @@ struct Level {
   // then boundary sweep colours 8..15, concatenated; list k is gs_off[k]..gs_off[k+1]
   DevBuf<int> gs_list;
   int gs_off[17] = {0};
+  // level 0 of the single-precision V-cycle: the iterate packed as (u, E) per node
+  DevBuf<float4> u4;
 };
 
 struct Bottom {
@@ -198,6 +200,8 @@ class Solver {
     SGS_CUDA(cudaLaunchKernelEx(&cfg, kernel, KArgs(args)...));
   }
   bool mixed() const { return precision == PREC_MIXED; }
+  // the mixed V-cycle keeps its level-0 iterate packed (see reset_u4_kernel)
+  bool packed0() const { return mixed() && nlev() > 1; }
   bool round_ref() const { return precision == PREC_REFERENCE; }
   int nlev() const { return int(P.levels.size()); }
 
@@ -314,6 +318,7 @@ class Solver {
         if (first) {
           L32.back()->gs_list.upload(gsl, stream);
           std::copy(off, off + 17, L32.back()->gs_off);
+          if (P.levels.size() > 1) L32.back()->u4.alloc(size_t(L32.back()->N));
         }
       }
     }
@@ -528,6 +533,14 @@ class Solver {
         const int c = (boundary ? 8 : 0) + (forward ? k : 7 - k);
         const int lo = d.gs_off[c], cnt = d.gs_off[c + 1] - lo;
         if (cnt == 0) continue;
+        if constexpr (sizeof(T) == 4) {
+          if (!u) {  // the packed iterate of the mixed V-cycle
+            launch(gs0_list4_kernel<6>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbr.p, d.u4.p, b,
+                   d.flags.p, int(d.N), T(P.dx));
+            ++launch_counter;
+            continue;
+          }
+        }
         // single precision: 80 registers, 6 CTAs per SM; double: 128, 4 per SM
         if constexpr (sizeof(T) == 4)
           launch(gs0_list_kernel<T, 6>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbr.p, Edev<T>(), u, b,
@@ -576,6 +589,14 @@ class Solver {
     Level<T>& fl = lev<T>(lf);
     Level<T>& c = lev<T>(lf + 1);
     if (fl.N == 0) return;
+    if constexpr (sizeof(T) == 4) {
+      if (!fine_u) {  // into the packed level-0 iterate
+        launch(prolongate4_kernel, blocks_for(fl.N, 128), 128, 0, fl.nb, fl.coords.p, fl.flags.p, c.grid, c.u.p, c.N,
+               fl.u4.p);
+        ++launch_counter;
+        return;
+      }
+    }
     launch(prolongate_kernel<T>, blocks_for(fl.N, 128), 128, 0, fl.nb, fl.coords.p, fl.flags.p, c.grid, c.u.p, c.N,
                                                                    fine_u, fl.N, round_ref() ? 1 : 0);
     ++launch_counter;
@@ -606,7 +627,17 @@ class Solver {
     const int ex = P.explicit_level;
     const bool rr = round_ref();
     Level<T>& l0 = lev<T>(0);
-    SGS_CUDA(cudaMemsetAsync(u0, 0, 3 * l0.N * sizeof(T), stream));
+    // u0 == nullptr: single precision with the packed level-0 iterate l0.u4
+    bool packed = false;
+    if constexpr (sizeof(T) == 4) packed = u0 == nullptr;
+    if (packed) {
+      if constexpr (sizeof(T) == 4) {
+        launch(reset_u4_kernel, blocks_for(l0.N, 256), 256, 0, l0.u4.p, E32.p, l0.N);
+        ++launch_counter;
+      }
+    } else {
+      SGS_CUDA(cudaMemsetAsync(u0, 0, 3 * l0.N * sizeof(T), stream));
+    }
     if (n == 1) {
       // single level: exact solve on level 0 (its b is the given right-hand side)
       SGS_CUDA(cudaMemcpyAsync(l0.b.p, b0, 3 * l0.N * sizeof(T), cudaMemcpyDeviceToDevice, stream));
@@ -625,7 +656,14 @@ class Solver {
       Level<T>& d = lev<T>(l);
       if (smooth) {
         if (l == 0) {
-          level0<T, OP_RES>(U(0), B(0), d.r.p);
+          if (packed) {
+            if constexpr (sizeof(T) == 4) {
+              launch(level0_res4_kernel, d.nb, 128, 0, d.nb, d.nbr.p, d.u4.p, B(0), d.r.p, d.N, T(P.dx));
+              ++launch_counter;
+            }
+          } else {
+            level0<T, OP_RES>(U(0), B(0), d.r.p);
+          }
           if (rr) round3(d, d.r.p);
         } else {
           stencil<T, SOP_RES>(l, nullptr, d.nb, U(l), nullptr, B(l), d.r.p, 0, 0, rr ? 1 : 0);
@@ -787,6 +825,34 @@ __global__ void precond_out_kernel(const TS* z, double* q, const double* __restr
     for (int v = 0; v < 3; ++v) {
       const long k = i + v * N;
       const double val = ((fl & ACTIVE_NODE) && !(fl & (DIR_X << v))) ? double(z[k]) : 0.0;
+      q[k] = val;
+      s += val * f[k];
+    }
+  }
+  for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t += sm[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+// precond_out_kernel for the packed single-precision level-0 iterate
+__global__ void precond_out4_kernel(const float4* __restrict__ z4, double* q, const double* __restrict__ f,
+                                    const uint32_t* __restrict__ flags, long N, double* __restrict__ part) {
+  pdl_wait();
+  __shared__ double sm[RED_THREADS / 32];
+  double s = 0;
+  for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += long(gridDim.x) * blockDim.x) {
+    const uint32_t fl = flags[i];
+    const float4 z = z4[i];
+    const float zc[3] = {z.x, z.y, z.z};
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const long k = i + v * N;
+      const double val = ((fl & ACTIVE_NODE) && !(fl & (DIR_X << v))) ? double(zc[v]) : 0.0;
       q[k] = val;
       s += val * f[k];
     }
@@ -987,8 +1053,13 @@ void Solver::precondition() {
     launch(precond_out_kernel<double>, RED_BLOCKS, RED_THREADS, 0, q.p, q.p, f.p, l0.flags.p, N, red.p);
   } else if (mixed()) {
     Level<float>& m0 = *L32[0];
-    vcycle<float>(m0.b.p, m0.u.p);
-    launch(precond_out_kernel<float>, RED_BLOCKS, RED_THREADS, 0, m0.u.p, q.p, f.p, l0.flags.p, N, red.p);
+    if (packed0()) {
+      vcycle<float>(m0.b.p, nullptr);
+      launch(precond_out4_kernel, RED_BLOCKS, RED_THREADS, 0, m0.u4.p, q.p, f.p, l0.flags.p, N, red.p);
+    } else {
+      vcycle<float>(m0.b.p, m0.u.p);
+      launch(precond_out_kernel<float>, RED_BLOCKS, RED_THREADS, 0, m0.u.p, q.p, f.p, l0.flags.p, N, red.p);
+    }
   } else {
     vcycle<double>(f.p, q.p);
     launch(precond_out_kernel<double>, RED_BLOCKS, RED_THREADS, 0, q.p, q.p, f.p, l0.flags.p, N, red.p);
@@ -1276,11 +1347,24 @@ static double time_op(Solver& S, int op, int reps) {
   cudaEvent_t a, b;
   SGS_CUDA(cudaEventCreate(&a));
   SGS_CUDA(cudaEventCreate(&b));
+  // in a mixed session the residual and the sweep run on the packed iterate, as in its V-cycle
+  const bool packed = sizeof(T) == 4 && S.packed0();
   auto run = [&]() {
-    if (op == 0) S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);
-    else if (op == 1) S.level0<T, OP_RES>(d.u.p, d.b.p, d.r.p);
-    else if (op == 2) S.sweep<T>(0, d.u.p, d.b.p, true, false);
-    else if (op == 3) S.precondition();
+    if (op == 0) {
+      S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);
+    } else if (op == 1) {
+      if constexpr (sizeof(T) == 4) {
+        if (packed) {
+          S.launch(level0_res4_kernel, d.nb, 128, 0, d.nb, d.nbr.p, d.u4.p, d.b.p, d.r.p, d.N, T(S.P.dx));
+          return;
+        }
+      }
+      S.level0<T, OP_RES>(d.u.p, d.b.p, d.r.p);
+    } else if (op == 2) {
+      S.sweep<T>(0, packed ? nullptr : d.u.p, d.b.p, true, false);
+    } else if (op == 3) {
+      S.precondition();
+    }
   };
   run();
   SGS_CUDA(cudaEventRecord(a, S.stream));
