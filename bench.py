@@ -33,6 +33,9 @@ sys.path.insert(0, ROOT)
 METRIC = "MGPCG time & MDOF/s to rel.res 1e-6: mixed-prec vs FP64, same B200"
 ACTIVE_NODE = 0x10  # node flag of an active node (solver/Flags.h); DOF = 3 x active nodes
 TOL = 1e-6
+# ncu-measured DRAM traffic of one level-0 sweep per workload
+# (profiles/gs0_list4_kernel_sphere_shell256.md)
+SWEEP_DRAM_BYTES = {"sphere_shell256": 1.125e9}
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -79,7 +82,7 @@ def config_dict(args, inp, extra=None):
              "density": "uniform [1e-3, 1], seeded", "mg_level": int(inp.mg_level),
              "smoothing": [int(inp.pre_and_post_smoothing_iter), int(inp.extra_ints["boundary_smoothing"])],
              "tolerance": TOL, "stopping_rule": "L-inf residual <= tol * zero-guess L-inf residual",
-             "blocks": int(inp.density.base.shape[0]), "l2": "flushed (256 MiB write) before every timed solve"}
+             "input_blocks_4x4x4": int(inp.density.base.shape[0]), "l2": "flushed (256 MiB write) before every timed solve"}
         if extra:
             d.update(extra)
         return d
@@ -87,7 +90,7 @@ def config_dict(args, inp, extra=None):
          "density": "clamp(0.5+0.3*smoothed uniform noise, 1e-3, 1), seed 1234", "mg_level": int(inp.mg_level),
          "smoothing": [int(inp.pre_and_post_smoothing_iter), int(inp.extra_ints["boundary_smoothing"])],
          "tolerance": TOL, "stopping_rule": "L-inf residual <= tol * zero-guess L-inf residual",
-         "blocks": int(inp.density.base.shape[0]), "l2": "flushed (256 MiB write) before every timed solve"}
+         "input_blocks_4x4x4": int(inp.density.base.shape[0]), "l2": "flushed (256 MiB write) before every timed solve"}
     if extra:
         d.update(extra)
     return d
@@ -246,9 +249,12 @@ def run_ours(args, rank, world):
     sweep_bytes = nodes * (10 * 4 + 4)
     achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9
     ku_bytes = nodes * 7 * 4
-    roofline = {"bound": "hbm", "kernel": "level0 Gauss-Seidel sweep (8 colour launches, FP32)",
+    # DRAM bytes of one full sweep (dram__bytes_read.sum + dram__bytes_write.sum over its 8
+    # colour-pass launches) from the ncu launch list of this workload, where one was taken
+    traffic = SWEEP_DRAM_BYTES.get(config_dict(args, inp, {})["workload"])
+    roofline = {"bound": "hbm", "kernel": "level0 Gauss-Seidel sweep (8 colour launches of gs0_list4_kernel, FP32)",
                 "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "peak_kind": peak_kind, "traffic": None,
+                "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch_set": sweep_bytes, "sweep_ms": round(sweep_ms, 4),
                 "ku_ms": round(ku_ms, 4), "ku_achieved_gbs": round(ku_bytes / (ku_ms * 1e-3) / 1e9, 1),
                 "vcycle_ms": round(vcyc_ms, 4)}
