@@ -183,6 +183,10 @@ struct Nbhd {
     const int b = __ldg(nb + sx[ix] + sy[iy] + sz[iz]);
     return b < 0 ? -1 : (b << 7) + lx[ix] + ly[iy] + lz[iz];
   }
+  // the same with a neighbour table whose missing blocks name an all-zero pad block
+  __device__ __forceinline__ int at_padded(int ix, int iy, int iz) const {
+    return (__ldg(nb + sx[ix] + sy[iy] + sz[iz]) << 7) + lx[ix] + ly[iy] + lz[iz];
+  }
 };
 
 template <typename T, int MINB>
@@ -320,10 +324,11 @@ __global__ void unpack_u4_kernel(float* __restrict__ u, const float4* __restrict
 }
 
 // gs0_list_kernel on the packed iterate (one float4 gather per neighbour; the
-// cells' E come with the nodes at offsets -I).
+// cells' E come with the nodes at offsets -I).  nbrz names the zero pad block
+// (index nb) for missing neighbours, so the gathers need no test.
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restrict__ list, int n,
-                                                              const int* __restrict__ nbr, float4* u4,
+                                                              const int* __restrict__ nbrz, float4* u4,
                                                               const float* __restrict__ b,
                                                               const uint32_t* __restrict__ flags, int N, float dx) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -336,7 +341,7 @@ __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restr
   const uint32_t fl = flags[g];
   const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
   Nbhd nh;
-  nh.init(nbr, g);
+  nh.init(nbrz, g);
   pdl_wait();
   if (raw < 0) {
     float4 v = u4[g];
@@ -356,8 +361,7 @@ __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restr
 #pragma unroll
     for (int p = 0; p < 9; ++p) {
       const int iy = p / 3, iz = p % 3;
-      const int i = (px == 1 && p == 4) ? g : nh.at(px, iy, iz);
-      const float4 v = i < 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : u4[i];
+      const float4 v = u4[(px == 1 && p == 4) ? g : nh.at_padded(px, iy, iz)];
       up[p][0] = v.x;
       up[p][1] = v.y;
       up[p][2] = v.z;
@@ -418,7 +422,7 @@ __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restr
 }
 
 // level0_op_kernel<float, OP_RES> on the packed iterate: r = b - dx K u
-__global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int* __restrict__ nbrz,
                                                           const float4* __restrict__ u4, const float* __restrict__ b,
                                                           float* __restrict__ out, long N, float dx) {
   pdl_wait();
@@ -426,15 +430,14 @@ __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int
   __shared__ float sE[HU];
   __shared__ int snb[27];
   const int bi = blockIdx.x;
-  if (threadIdx.x < 27) snb[threadIdx.x] = nbr[long(bi) * 27 + threadIdx.x];
+  if (threadIdx.x < 27) snb[threadIdx.x] = nbrz[long(bi) * 27 + threadIdx.x];
   __syncthreads();
   for (int h = threadIdx.x; h < HU; h += 128) {
     const int sx = h / 60, sy = (h / 10) % 6, sz = h % 10;
     const int lx = sx - 1, ly = sy - 1, lz = sz - 1;
     const int dxb = lx < 0 ? 0 : (lx > 3 ? 2 : 1), dyb = ly < 0 ? 0 : (ly > 3 ? 2 : 1), dzb = lz < 0 ? 0 : (lz > 7 ? 2 : 1);
-    const int nb = snb[dxb * 9 + dyb * 3 + dzb];
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (nb >= 0) v = u4[long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7)];
+    const int nb = snb[dxb * 9 + dyb * 3 + dzb];  // the zero pad block where there is none
+    const float4 v = u4[long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7)];
     su[0][h] = v.x;
     su[1][h] = v.y;
     su[2][h] = v.z;

@@ -120,8 +120,10 @@ struct Level {
   // then boundary sweep colours 8..15, concatenated; list k is gs_off[k]..gs_off[k+1]
   DevBuf<int> gs_list;
   int gs_off[17] = {0};
-  // level 0 of the single-precision V-cycle: the iterate packed as (u, E) per node
+  // level 0 of the single-precision V-cycle: the iterate packed as (u, E) per node,
+  // followed by one all-zero pad block (index nb) that nbrz names for missing neighbours
   DevBuf<float4> u4;
+  DevBuf<int> nbrz;
 };
 
 struct Bottom {
@@ -318,7 +320,15 @@ class Solver {
         if (first) {
           L32.back()->gs_list.upload(gsl, stream);
           std::copy(off, off + 17, L32.back()->gs_off);
-          if (P.levels.size() > 1) L32.back()->u4.alloc(size_t(L32.back()->N));
+          if (P.levels.size() > 1) {
+            Level<float>& m0 = *L32.back();
+            m0.u4.alloc(size_t(m0.N) + NODES_PER_BLOCK);
+            SGS_CUDA(cudaMemsetAsync(m0.u4.p + m0.N, 0, NODES_PER_BLOCK * sizeof(float4), stream));
+            std::vector<int32_t> z(h.nbr);
+            for (auto& v : z)
+              if (v < 0) v = h.nb;
+            m0.nbrz.upload(z, stream);
+          }
         }
       }
     }
@@ -535,7 +545,7 @@ class Solver {
         if (cnt == 0) continue;
         if constexpr (sizeof(T) == 4) {
           if (!u) {  // the packed iterate of the mixed V-cycle
-            launch(gs0_list4_kernel<6>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbr.p, d.u4.p, b,
+            launch(gs0_list4_kernel<6>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbrz.p, d.u4.p, b,
                    d.flags.p, int(d.N), T(P.dx));
             ++launch_counter;
             continue;
@@ -658,7 +668,7 @@ class Solver {
         if (l == 0) {
           if (packed) {
             if constexpr (sizeof(T) == 4) {
-              launch(level0_res4_kernel, d.nb, 128, 0, d.nb, d.nbr.p, d.u4.p, B(0), d.r.p, d.N, T(P.dx));
+              launch(level0_res4_kernel, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, B(0), d.r.p, d.N, T(P.dx));
               ++launch_counter;
             }
           } else {
@@ -1355,7 +1365,7 @@ static double time_op(Solver& S, int op, int reps) {
     } else if (op == 1) {
       if constexpr (sizeof(T) == 4) {
         if (packed) {
-          S.launch(level0_res4_kernel, d.nb, 128, 0, d.nb, d.nbr.p, d.u4.p, d.b.p, d.r.p, d.N, T(S.P.dx));
+          S.launch(level0_res4_kernel, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, d.b.p, d.r.p, d.N, T(S.P.dx));
           return;
         }
       }
