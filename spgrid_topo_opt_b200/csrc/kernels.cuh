@@ -27,6 +27,49 @@ __device__ __forceinline__ float kc<float>(int idx) { return c_Kc32[idx]; }
 
 __device__ __forceinline__ double round_to_float(double v) { return double(float(v)); }
 
+// The element matrix in exact integers, 72 K_mu and 72 K_la of the Q1 hex on the
+// unit cube (node a = 4x + 2y + z), from the 1D integrals of the linear shape
+// functions times 6 (mass {2, 1}, derivative-mass {-3, 3}, stiffness {6, -6});
+// the same formulas as element_tables() in solver.cu.  Up to sign the 576
+// entries take 10 values (m, l), so Kc = (mu0 m + lambda0 l) / 72 is 10 numbers,
+// which the single-precision level-0 kernels keep in registers (KcReg).
+__host__ __device__ constexpr int q1_g(int a, int b, int i, int j) {
+  int v = 1;
+  for (int ax = 0; ax < 3; ++ax) {
+    const int pa = (a >> (2 - ax)) & 1, pb = (b >> (2 - ax)) & 1;
+    const bool da = ax == i, db = ax == j;
+    v *= (da && db) ? (pa == pb ? 6 : -6) : da ? (pa ? 3 : -3) : db ? (pb ? 3 : -3) : (pa == pb ? 2 : 1);
+  }
+  return v;
+}
+__host__ __device__ constexpr int q1_mu72(int a, int b, int i, int j) {
+  return (q1_g(a, b, j, i) + (i == j ? q1_g(a, b, 0, 0) + q1_g(a, b, 1, 1) + q1_g(a, b, 2, 2) : 0)) / 3;
+}
+__host__ __device__ constexpr int q1_la72(int a, int b, int i, int j) { return q1_g(a, b, i, j) / 3; }
+// class of a sign-normalised pair (m > 0, or m = 0 and l >= 0); -1 if it is none of the 10
+__host__ __device__ constexpr int q1_class(int m, int l) {
+  return (m == 3 && l == -3) ? 0 : (m == 3 && l == 3) ? 1 : (m == 4 && l == -2) ? 2 : (m == 4 && l == 4) ? 3
+       : (m == 6 && l == -6) ? 4 : (m == 6 && l == 6) ? 5 : (m == 8 && l == 2) ? 6 : (m == 8 && l == 8) ? 7
+       : (m == 10 && l == 4) ? 8 : (m == 32 && l == 8) ? 9 : -1;
+}
+constexpr int Q1_CLASS_M[10] = {3, 3, 4, 4, 6, 6, 8, 8, 10, 32}, Q1_CLASS_L[10] = {-3, 3, -2, 4, -6, 6, 2, 8, 4, 8};
+__constant__ float c_Kv32[10];  // (mu0 m_c + lambda0 l_c) / 72 per class, rounded like c_Kc32
+
+struct KcReg {
+  float v[10];
+  __device__ __forceinline__ void load() {
+#pragma unroll
+    for (int c = 0; c < 10; ++c) v[c] = c_Kv32[c];
+  }
+  // Kc[I][J][r][s]; with constant arguments this folds to one register (and a sign)
+  __device__ __forceinline__ float operator()(int I, int J, int r, int s) const {
+    const int m = q1_mu72(I, J, r, s), l = q1_la72(I, J, r, s);
+    const bool neg = m < 0 || (m == 0 && l < 0);
+    const float k = v[q1_class(neg ? -m : m, neg ? -l : l)];
+    return neg ? -k : k;
+  }
+};
+
 // Programmatic dependent launch: kernels of the solve are launched so that they
 // may start while their predecessor drains.  Each waits here until the
 // predecessor has completed and its writes are visible, then lets its own
@@ -342,6 +385,8 @@ __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restr
   const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
   Nbhd nh;
   nh.init(nbrz, g);
+  KcReg K;
+  K.load();
   pdl_wait();
   if (raw < 0) {
     float4 v = u4[g];
@@ -381,22 +426,21 @@ __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restr
       for (int q = 0; q < 4; ++q) {
         const int Jy = q >> 1, Jz = q & 1;
         const int p = (Jy - Iy + 1) * 3 + (Jz - Iz + 1);
-        const int k = (I * 8 + Jx * 4 + Jy * 2 + Jz) * 9;
+        const int J = Jx * 4 + Jy * 2 + Jz;
 #pragma unroll
         for (int v = 0; v < 3; ++v)
 #pragma unroll
-          for (int w = 0; w < 3; ++w) gc[I][v] = fmaf(kc<float>(k + v * 3 + w), up[p][w], gc[I][v]);
+          for (int w = 0; w < 3; ++w) gc[I][v] = fmaf(K(I, J, v, w), up[p][w], gc[I][v]);
       }
       if (Jx == 1) {
 #pragma unroll
         for (int v = 0; v < 3; ++v) f[v] = fmaf(Ec[I], gc[I][v], f[v]);
-        const int kd = (I * 8 + I) * 9;
-        dg[0] = fmaf(kc<float>(kd + 0), Ec[I], dg[0]);
-        dg[1] = fmaf(kc<float>(kd + 4), Ec[I], dg[1]);
-        dg[2] = fmaf(kc<float>(kd + 8), Ec[I], dg[2]);
-        dg[3] = fmaf(kc<float>(kd + 1), Ec[I], dg[3]);
-        dg[4] = fmaf(kc<float>(kd + 2), Ec[I], dg[4]);
-        dg[5] = fmaf(kc<float>(kd + 5), Ec[I], dg[5]);
+        dg[0] = fmaf(K(I, I, 0, 0), Ec[I], dg[0]);
+        dg[1] = fmaf(K(I, I, 1, 1), Ec[I], dg[1]);
+        dg[2] = fmaf(K(I, I, 2, 2), Ec[I], dg[2]);
+        dg[3] = fmaf(K(I, I, 0, 1), Ec[I], dg[3]);
+        dg[4] = fmaf(K(I, I, 0, 2), Ec[I], dg[4]);
+        dg[5] = fmaf(K(I, I, 1, 2), Ec[I], dg[5]);
       }
     }
   }
@@ -430,6 +474,8 @@ __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int
   __shared__ float sE[HU];
   __shared__ int snb[27];
   const int bi = blockIdx.x;
+  KcReg K;
+  K.load();
   if (threadIdx.x < 27) snb[threadIdx.x] = nbrz[long(bi) * 27 + threadIdx.x];
   __syncthreads();
   for (int h = threadIdx.x; h < HU; h += 128) {
@@ -460,10 +506,9 @@ __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int
       const int nx = cx + (J >> 2) + 1, ny = cy + ((J >> 1) & 1) + 1, nz = cz + (J & 1) + 1;
       const int h = (nx * 6 + ny) * 10 + nz;
       const float ux = su[0][h], uy = su[1][h], uz = su[2][h];
-      const int k = (I * 8 + J) * 9;
-      g0 += kc<float>(k + 0) * ux + kc<float>(k + 1) * uy + kc<float>(k + 2) * uz;
-      g1 += kc<float>(k + 3) * ux + kc<float>(k + 4) * uy + kc<float>(k + 5) * uz;
-      g2 += kc<float>(k + 6) * ux + kc<float>(k + 7) * uy + kc<float>(k + 8) * uz;
+      g0 += K(I, J, 0, 0) * ux + K(I, J, 0, 1) * uy + K(I, J, 0, 2) * uz;
+      g1 += K(I, J, 1, 0) * ux + K(I, J, 1, 1) * uy + K(I, J, 1, 2) * uz;
+      g2 += K(I, J, 2, 0) * ux + K(I, J, 2, 1) * uy + K(I, J, 2, 2) * uz;
     }
     f0 += Ec * g0;
     f1 += Ec * g1;

@@ -234,6 +234,23 @@ class Solver {
             kc64[(I * 8 + J) * 9 + v * 3 + w] = val;
             kc32[(I * 8 + J) * 9 + v * 3 + w] = float(val);
           }
+    // the 10 sign classes of the entries (q1_class); the integer formulas must
+    // reproduce the element tables
+    float kv[10];
+    for (int c = 0; c < 10; ++c)
+      kv[c] = float(P.mu0 * (double(Q1_CLASS_M[c]) / 72.0) + P.lambda0 * (double(Q1_CLASS_L[c]) / 72.0));
+    for (int I = 0; I < 8; ++I)
+      for (int J = 0; J < 8; ++J)
+        for (int v = 0; v < 3; ++v)
+          for (int w = 0; w < 3; ++w) {
+            const int m = q1_mu72(I, J, v, w), l = q1_la72(I, J, v, w);
+            const bool neg = m < 0 || (m == 0 && l < 0);
+            const int c = q1_class(neg ? -m : m, neg ? -l : l);
+            if (c < 0 || double(m) / 72.0 != Kmu[I][J][v][w] || double(l) / 72.0 != Kla[I][J][v][w] ||
+                (neg ? -kv[c] : kv[c]) != kc32[(I * 8 + J) * 9 + v * 3 + w])
+              throw CudaError("element table classes are inconsistent", SGS_ERR_INTERNAL);
+          }
+    SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kv32, kv, sizeof(kv), 0, cudaMemcpyHostToDevice, stream));
     SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kc64, kc64, sizeof(kc64), 0, cudaMemcpyHostToDevice, stream));
     SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kc32, kc32, sizeof(kc32), 0, cudaMemcpyHostToDevice, stream));
   }
