@@ -53,20 +53,38 @@ __host__ __device__ constexpr int q1_class(int m, int l) {
        : (m == 10 && l == 4) ? 8 : (m == 32 && l == 8) ? 9 : -1;
 }
 constexpr int Q1_CLASS_M[10] = {3, 3, 4, 4, 6, 6, 8, 8, 10, 32}, Q1_CLASS_L[10] = {-3, 3, -2, 4, -6, 6, 2, 8, 4, 8};
-__constant__ float c_Kv32[10];  // (mu0 m_c + lambda0 l_c) / 72 per class, rounded like c_Kc32
+__constant__ float c_Kv32[10];   // (mu0 m_c + lambda0 l_c) / 72 per class, rounded like c_Kc32
+__constant__ double c_Kv64[10];  // the same in double, equal to the entries of c_Kc64
 
+template <typename T>
 struct KcReg {
-  float v[10];
+  T v[10];
   __device__ __forceinline__ void load() {
 #pragma unroll
-    for (int c = 0; c < 10; ++c) v[c] = c_Kv32[c];
+    for (int c = 0; c < 10; ++c) v[c] = sizeof(T) == 4 ? T(c_Kv32[c]) : T(c_Kv64[c]);
   }
   // Kc[I][J][r][s]; with constant arguments this folds to one register (and a sign)
-  __device__ __forceinline__ float operator()(int I, int J, int r, int s) const {
+  __device__ __forceinline__ T operator()(int I, int J, int r, int s) const {
     const int m = q1_mu72(I, J, r, s), l = q1_la72(I, J, r, s);
     const bool neg = m < 0 || (m == 0 && l < 0);
-    const float k = v[q1_class(neg ? -m : m, neg ? -l : l)];
+    const T k = v[q1_class(neg ? -m : m, neg ? -l : l)];
     return neg ? -k : k;
+  }
+};
+
+// the packed node record of level 0: (u_x, u_y, u_z, E)
+template <typename T>
+struct Pack4;
+template <>
+struct Pack4<float> {
+  using type = float4;
+  static __device__ __forceinline__ float4 make(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+};
+template <>
+struct Pack4<double> {
+  using type = double4;
+  static __device__ __forceinline__ double4 make(double a, double b, double c, double d) {
+    return make_double4(a, b, c, d);
   }
 };
 
@@ -335,45 +353,30 @@ __global__ void __launch_bounds__(128, MINB) gs0_list_kernel(const int* __restri
 }
 
 // ---------------------------------------------------------------------------
-// Packed level 0 of the single-precision V-cycle.  The iterate of level 0 is
-// one float4 per node, (u_x, u_y, u_z, E of the node's cell): the 27-point
+// Packed level 0 of the V-cycle (mixed and FP64 modes).  The iterate of level 0
+// is one record per node, (u_x, u_y, u_z, E of the node's cell): the 27-point
 // gathers of the smoother and the halo staging of the residual then read a
-// node's displacement and its cell's stiffness scale in one 16-byte load, the
-// same bytes as three planes of u plus the E plane.
+// node's displacement and its cell's stiffness scale in one access (16 B in
+// FP32, 32 B in FP64), the same bytes as three planes of u plus the E plane.
 // ---------------------------------------------------------------------------
 
 // u4 = (0, 0, 0, E): the zero start of the V-cycle's level-0 correction
-__global__ void reset_u4_kernel(float4* __restrict__ u4, const float* __restrict__ E, long N) {
+template <typename T>
+__global__ void reset_u4_kernel(typename Pack4<T>::type* __restrict__ u4, const T* __restrict__ E, long N) {
   pdl_wait();
   const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < N) u4[i] = make_float4(0.f, 0.f, 0.f, E[i]);
-}
-
-// planar fields <-> packed iterate (for the unit operators on a packed level)
-__global__ void pack_u4_kernel(float4* __restrict__ u4, const float* __restrict__ u, const float* __restrict__ E,
-                               long N) {
-  pdl_wait();
-  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < N) u4[i] = make_float4(u[i], u[i + N], u[i + 2 * N], E[i]);
-}
-__global__ void unpack_u4_kernel(float* __restrict__ u, const float4* __restrict__ u4, long N) {
-  pdl_wait();
-  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const float4 v = u4[i];
-  u[i] = v.x;
-  u[i + N] = v.y;
-  u[i + 2 * N] = v.z;
+  if (i < N) u4[i] = Pack4<T>::make(T(0), T(0), T(0), E[i]);
 }
 
 // gs0_list_kernel on the packed iterate (one float4 gather per neighbour; the
 // cells' E come with the nodes at offsets -I).  nbrz names the zero pad block
 // (index nb) for missing neighbours, so the gathers need no test.
-template <int MINB>
+template <typename T, int MINB>
 __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restrict__ list, int n,
-                                                              const int* __restrict__ nbrz, float4* u4,
-                                                              const float* __restrict__ b,
-                                                              const uint32_t* __restrict__ flags, int N, float dx) {
+                                                              const int* __restrict__ nbrz,
+                                                              typename Pack4<T>::type* u4, const T* __restrict__ b,
+                                                              const uint32_t* __restrict__ flags, int N, T dx) {
+  using V = typename Pack4<T>::type;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) {
     pdl_wait();
@@ -385,28 +388,28 @@ __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restr
   const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
   Nbhd nh;
   nh.init(nbrz, g);
-  KcReg K;
+  KcReg<T> K;
   K.load();
   pdl_wait();
   if (raw < 0) {
-    float4 v = u4[g];
-    if (fx) v.x = 0.f;
-    if (fy) v.y = 0.f;
-    if (fz) v.z = 0.f;
+    V v = u4[g];
+    if (fx) v.x = T(0);
+    if (fy) v.y = T(0);
+    if (fz) v.z = T(0);
     u4[g] = v;
     return;
   }
-  float gc[8][3], Ec[8], uc[3];
-  float f[3] = {0.f, 0.f, 0.f}, dg[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  T gc[8][3], Ec[8], uc[3];
+  T f[3] = {0, 0, 0}, dg[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-  for (int I = 0; I < 8; ++I) gc[I][0] = gc[I][1] = gc[I][2] = 0.f;
+  for (int I = 0; I < 8; ++I) gc[I][0] = gc[I][1] = gc[I][2] = T(0);
 #pragma unroll
   for (int px = 0; px < 3; ++px) {
-    float up[9][3];
+    T up[9][3];
 #pragma unroll
     for (int p = 0; p < 9; ++p) {
       const int iy = p / 3, iz = p % 3;
-      const float4 v = u4[(px == 1 && p == 4) ? g : nh.at_padded(px, iy, iz)];
+      const V v = u4[(px == 1 && p == 4) ? g : nh.at_padded(px, iy, iz)];
       up[p][0] = v.x;
       up[p][1] = v.y;
       up[p][2] = v.z;
@@ -430,51 +433,52 @@ __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restr
 #pragma unroll
         for (int v = 0; v < 3; ++v)
 #pragma unroll
-          for (int w = 0; w < 3; ++w) gc[I][v] = fmaf(K(I, J, v, w), up[p][w], gc[I][v]);
+          for (int w = 0; w < 3; ++w) gc[I][v] = fma(K(I, J, v, w), up[p][w], gc[I][v]);
       }
       if (Jx == 1) {
 #pragma unroll
-        for (int v = 0; v < 3; ++v) f[v] = fmaf(Ec[I], gc[I][v], f[v]);
-        dg[0] = fmaf(K(I, I, 0, 0), Ec[I], dg[0]);
-        dg[1] = fmaf(K(I, I, 1, 1), Ec[I], dg[1]);
-        dg[2] = fmaf(K(I, I, 2, 2), Ec[I], dg[2]);
-        dg[3] = fmaf(K(I, I, 0, 1), Ec[I], dg[3]);
-        dg[4] = fmaf(K(I, I, 0, 2), Ec[I], dg[4]);
-        dg[5] = fmaf(K(I, I, 1, 2), Ec[I], dg[5]);
+        for (int v = 0; v < 3; ++v) f[v] = fma(Ec[I], gc[I][v], f[v]);
+        dg[0] = fma(K(I, I, 0, 0), Ec[I], dg[0]);
+        dg[1] = fma(K(I, I, 1, 1), Ec[I], dg[1]);
+        dg[2] = fma(K(I, I, 2, 2), Ec[I], dg[2]);
+        dg[3] = fma(K(I, I, 0, 1), Ec[I], dg[3]);
+        dg[4] = fma(K(I, I, 0, 2), Ec[I], dg[4]);
+        dg[5] = fma(K(I, I, 1, 2), Ec[I], dg[5]);
       }
     }
   }
-  const float r0 = b[g] - f[0] * dx, r1 = b[g + N] - f[1] * dx, r2 = b[g + 2 * N] - f[2] * dx;
-  float d0 = dg[0] * dx, d1 = dg[1] * dx, d2 = dg[2] * dx, d3 = dg[3] * dx, d4 = dg[4] * dx, d5 = dg[5] * dx;
+  const T r0 = b[g] - f[0] * dx, r1 = b[g + N] - f[1] * dx, r2 = b[g + 2 * N] - f[2] * dx;
+  T d0 = dg[0] * dx, d1 = dg[1] * dx, d2 = dg[2] * dx, d3 = dg[3] * dx, d4 = dg[4] * dx, d5 = dg[5] * dx;
   if (fx) { d0 = 1; d3 = 0; d4 = 0; }
   if (fy) { d1 = 1; d3 = 0; d5 = 0; }
   if (fz) { d2 = 1; d4 = 0; d5 = 0; }
-  const float m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
-  const float m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
-  const float inv = 1.f / (d0 * m11 + d3 * m12 + d4 * m13);
-  float a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
+  const T m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
+  const T m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
+  const T inv = T(1) / (d0 * m11 + d3 * m12 + d4 * m13);
+  T a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
   if (fx) { a0 = 0; a3 = 0; a4 = 0; }
   if (fy) { a1 = 0; a3 = 0; a5 = 0; }
   if (fz) { a2 = 0; a4 = 0; a5 = 0; }
-  float v0 = uc[0] + r0 * a0 + r1 * a3 + r2 * a4;
-  float v1 = uc[1] + r0 * a3 + r1 * a1 + r2 * a5;
-  float v2 = uc[2] + r0 * a4 + r1 * a5 + r2 * a2;
+  T v0 = uc[0] + r0 * a0 + r1 * a3 + r2 * a4;
+  T v1 = uc[1] + r0 * a3 + r1 * a1 + r2 * a5;
+  T v2 = uc[2] + r0 * a4 + r1 * a5 + r2 * a2;
   if (fx) v0 = 0;
   if (fy) v1 = 0;
   if (fz) v2 = 0;
-  u4[g] = make_float4(v0, v1, v2, Ec[0]);  // corner I = 0: the node's own cell
+  u4[g] = Pack4<T>::make(v0, v1, v2, Ec[0]);  // corner I = 0: the node's own cell
 }
 
-// level0_op_kernel<float, OP_RES> on the packed iterate: r = b - dx K u
+// level0_op_kernel<T, OP_RES> on the packed iterate: r = b - dx K u
+template <typename T>
 __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int* __restrict__ nbrz,
-                                                          const float4* __restrict__ u4, const float* __restrict__ b,
-                                                          float* __restrict__ out, long N, float dx) {
+                                                          const typename Pack4<T>::type* __restrict__ u4,
+                                                          const T* __restrict__ b, T* __restrict__ out, long N, T dx) {
   pdl_wait();
-  __shared__ float su[3][HU];
-  __shared__ float sE[HU];
+  __shared__ T su[3][HU];
+  __shared__ T sE[HU];
   __shared__ int snb[27];
   const int bi = blockIdx.x;
-  KcReg K;
+  KcReg<T> K;
   K.load();
   if (threadIdx.x < 27) snb[threadIdx.x] = nbrz[long(bi) * 27 + threadIdx.x];
   __syncthreads();
@@ -483,7 +487,7 @@ __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int
     const int lx = sx - 1, ly = sy - 1, lz = sz - 1;
     const int dxb = lx < 0 ? 0 : (lx > 3 ? 2 : 1), dyb = ly < 0 ? 0 : (ly > 3 ? 2 : 1), dzb = lz < 0 ? 0 : (lz > 7 ? 2 : 1);
     const int nb = snb[dxb * 9 + dyb * 3 + dzb];  // the zero pad block where there is none
-    const float4 v = u4[long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7)];
+    const auto v = u4[long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7)];
     su[0][h] = v.x;
     su[1][h] = v.y;
     su[2][h] = v.z;
@@ -493,19 +497,19 @@ __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int
   const int e = threadIdx.x;
   const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
   const long gidx = long(bi) * 128 + e;
-  float f0 = 0, f1 = 0, f2 = 0;
+  T f0 = 0, f1 = 0, f2 = 0;
 #pragma unroll
   for (int I = 0; I < 8; ++I) {
     const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
     const int cx = x - Ix, cy = y - Iy, cz = z - Iz;  // cell = its min-corner node, in the halo
-    const float Ec = sE[((cx + 1) * 6 + (cy + 1)) * 10 + (cz + 1)];
-    if (Ec == 0.f) continue;
-    float g0 = 0, g1 = 0, g2 = 0;
+    const T Ec = sE[((cx + 1) * 6 + (cy + 1)) * 10 + (cz + 1)];
+    if (Ec == T(0)) continue;
+    T g0 = 0, g1 = 0, g2 = 0;
 #pragma unroll
     for (int J = 0; J < 8; ++J) {
       const int nx = cx + (J >> 2) + 1, ny = cy + ((J >> 1) & 1) + 1, nz = cz + (J & 1) + 1;
       const int h = (nx * 6 + ny) * 10 + nz;
-      const float ux = su[0][h], uy = su[1][h], uz = su[2][h];
+      const T ux = su[0][h], uy = su[1][h], uz = su[2][h];
       g0 += K(I, J, 0, 0) * ux + K(I, J, 0, 1) * uy + K(I, J, 0, 2) * uz;
       g1 += K(I, J, 1, 0) * ux + K(I, J, 1, 1) * uy + K(I, J, 1, 2) * uz;
       g2 += K(I, J, 2, 0) * ux + K(I, J, 2, 1) * uy + K(I, J, 2, 2) * uz;
@@ -713,8 +717,10 @@ __global__ void prolongate_kernel(int nb, const int* __restrict__ coords, const 
 }
 
 // prolongate_kernel into the packed level-0 iterate (E in .w is kept)
+template <typename T>
 __global__ void prolongate4_kernel(int nb, const int* __restrict__ coords, const uint32_t* __restrict__ fflags,
-                                   GridView coarse, const float* __restrict__ cin, long Nc, float4* __restrict__ fu4) {
+                                   GridView coarse, const T* __restrict__ cin, long Nc,
+                                   typename Pack4<T>::type* __restrict__ fu4) {
   pdl_wait();
   const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= long(nb) * 128) return;
@@ -722,14 +728,14 @@ __global__ void prolongate4_kernel(int nb, const int* __restrict__ coords, const
   const int lx = e >> 5, ly = (e >> 3) & 3, lz = e & 7;
   const int x = coords[3 * bi] + lx, y = coords[3 * bi + 1] + ly, z = coords[3 * bi + 2] + lz;
   const int cx = (x + 4) >> 1, cy = (y + 4) >> 1, cz = (z + 8) >> 1;
-  float4 v = fu4[t];
+  auto v = fu4[t];
   for (int q = 0; q < 8; ++q) {
     const int ii = q >> 2, jj = (q >> 1) & 1, kk = q & 1;
     const double wx = (lx & 1) ? 0.5 : (ii ? 0.0 : 1.0);
     const double wy = (ly & 1) ? 0.5 : (jj ? 0.0 : 1.0);
     const double wz = (lz & 1) ? 0.5 : (kk ? 0.0 : 1.0);
-    const float w = float(wx * wy * wz);
-    if (!(w > 0.f)) continue;
+    const T w = T(wx * wy * wz);
+    if (!(w > T(0))) continue;
     const long n = coarse.node(cx + ii, cy + jj, cz + kk);
     if (n < 0) continue;
     v.x += w * cin[n];

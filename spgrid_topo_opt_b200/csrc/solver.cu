@@ -120,9 +120,9 @@ struct Level {
   // then boundary sweep colours 8..15, concatenated; list k is gs_off[k]..gs_off[k+1]
   DevBuf<int> gs_list;
   int gs_off[17] = {0};
-  // level 0 of the single-precision V-cycle: the iterate packed as (u, E) per node,
-  // followed by one all-zero pad block (index nb) that nbrz names for missing neighbours
-  DevBuf<float4> u4;
+  // level 0 of the V-cycle (mixed and FP64 modes): the iterate packed as (u, E) per
+  // node, followed by one all-zero pad block (index nb) that nbrz names for missing neighbours
+  DevBuf<typename Pack4<T>::type> u4;
   DevBuf<int> nbrz;
 };
 
@@ -202,8 +202,9 @@ class Solver {
     SGS_CUDA(cudaLaunchKernelEx(&cfg, kernel, KArgs(args)...));
   }
   bool mixed() const { return precision == PREC_MIXED; }
-  // the mixed V-cycle keeps its level-0 iterate packed (see reset_u4_kernel)
-  bool packed0() const { return mixed() && nlev() > 1; }
+  // the mixed and FP64 V-cycles keep their level-0 iterate packed (see
+  // reset_u4_kernel); the reference-rounding mode rounds planar fields
+  bool packed0() const { return (mixed() || precision == PREC_FP64) && nlev() > 1; }
   bool round_ref() const { return precision == PREC_REFERENCE; }
   int nlev() const { return int(P.levels.size()); }
 
@@ -237,8 +238,11 @@ class Solver {
     // the 10 sign classes of the entries (q1_class); the integer formulas must
     // reproduce the element tables
     float kv[10];
-    for (int c = 0; c < 10; ++c)
-      kv[c] = float(P.mu0 * (double(Q1_CLASS_M[c]) / 72.0) + P.lambda0 * (double(Q1_CLASS_L[c]) / 72.0));
+    double kv64[10];
+    for (int c = 0; c < 10; ++c) {
+      kv64[c] = P.mu0 * (double(Q1_CLASS_M[c]) / 72.0) + P.lambda0 * (double(Q1_CLASS_L[c]) / 72.0);
+      kv[c] = float(kv64[c]);
+    }
     for (int I = 0; I < 8; ++I)
       for (int J = 0; J < 8; ++J)
         for (int v = 0; v < 3; ++v)
@@ -247,10 +251,12 @@ class Solver {
             const bool neg = m < 0 || (m == 0 && l < 0);
             const int c = q1_class(neg ? -m : m, neg ? -l : l);
             if (c < 0 || double(m) / 72.0 != Kmu[I][J][v][w] || double(l) / 72.0 != Kla[I][J][v][w] ||
-                (neg ? -kv[c] : kv[c]) != kc32[(I * 8 + J) * 9 + v * 3 + w])
+                (neg ? -kv[c] : kv[c]) != kc32[(I * 8 + J) * 9 + v * 3 + w] ||
+                (neg ? -kv64[c] : kv64[c]) != kc64[(I * 8 + J) * 9 + v * 3 + w])
               throw CudaError("element table classes are inconsistent", SGS_ERR_INTERNAL);
           }
     SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kv32, kv, sizeof(kv), 0, cudaMemcpyHostToDevice, stream));
+    SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kv64, kv64, sizeof(kv64), 0, cudaMemcpyHostToDevice, stream));
     SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kc64, kc64, sizeof(kc64), 0, cudaMemcpyHostToDevice, stream));
     SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kc32, kc32, sizeof(kc32), 0, cudaMemcpyHostToDevice, stream));
   }
@@ -314,6 +320,17 @@ class Solver {
     }
   }
 
+  // the packed level-0 iterate with its zero pad block, and the neighbour table naming it
+  template <typename T>
+  void alloc_packed(Level<T>& d, const HostLevel& h) {
+    d.u4.alloc(size_t(d.N) + NODES_PER_BLOCK);
+    SGS_CUDA(cudaMemsetAsync(d.u4.p + d.N, 0, NODES_PER_BLOCK * sizeof(typename Pack4<T>::type), stream));
+    std::vector<int32_t> z(h.nbr);
+    for (auto& v : z)
+      if (v < 0) v = h.nb;
+    d.nbrz.upload(z, stream);
+  }
+
   void build_levels() {
     // the level-0 kernels index the [3][N] planes with 32-bit integers
     if (3 * long(P.levels[0].nb) * NODES_PER_BLOCK >= long(INT32_MAX))
@@ -330,6 +347,7 @@ class Solver {
       if (first) {
         L64.back()->gs_list.upload(gsl, stream);
         std::copy(off, off + 17, L64.back()->gs_off);
+        if (precision == PREC_FP64 && P.levels.size() > 1) alloc_packed(*L64.back(), h);
       }
       if (mixed()) {
         L32.emplace_back(new Level<float>());
@@ -337,15 +355,7 @@ class Solver {
         if (first) {
           L32.back()->gs_list.upload(gsl, stream);
           std::copy(off, off + 17, L32.back()->gs_off);
-          if (P.levels.size() > 1) {
-            Level<float>& m0 = *L32.back();
-            m0.u4.alloc(size_t(m0.N) + NODES_PER_BLOCK);
-            SGS_CUDA(cudaMemsetAsync(m0.u4.p + m0.N, 0, NODES_PER_BLOCK * sizeof(float4), stream));
-            std::vector<int32_t> z(h.nbr);
-            for (auto& v : z)
-              if (v < 0) v = h.nb;
-            m0.nbrz.upload(z, stream);
-          }
+          if (P.levels.size() > 1) alloc_packed(*L32.back(), h);
         }
       }
     }
@@ -560,13 +570,15 @@ class Solver {
         const int c = (boundary ? 8 : 0) + (forward ? k : 7 - k);
         const int lo = d.gs_off[c], cnt = d.gs_off[c + 1] - lo;
         if (cnt == 0) continue;
-        if constexpr (sizeof(T) == 4) {
-          if (!u) {  // the packed iterate of the mixed V-cycle
-            launch(gs0_list4_kernel<6>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbrz.p, d.u4.p, b,
+        if (!u) {  // the packed iterate of the V-cycle
+          if constexpr (sizeof(T) == 4)
+            launch(gs0_list4_kernel<T, 6>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbrz.p, d.u4.p, b,
                    d.flags.p, int(d.N), T(P.dx));
-            ++launch_counter;
-            continue;
-          }
+          else
+            launch(gs0_list4_kernel<T, 4>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbrz.p, d.u4.p, b,
+                   d.flags.p, int(d.N), T(P.dx));
+          ++launch_counter;
+          continue;
         }
         // single precision: 80 registers, 6 CTAs per SM; double: 128, 4 per SM
         if constexpr (sizeof(T) == 4)
@@ -616,13 +628,11 @@ class Solver {
     Level<T>& fl = lev<T>(lf);
     Level<T>& c = lev<T>(lf + 1);
     if (fl.N == 0) return;
-    if constexpr (sizeof(T) == 4) {
-      if (!fine_u) {  // into the packed level-0 iterate
-        launch(prolongate4_kernel, blocks_for(fl.N, 128), 128, 0, fl.nb, fl.coords.p, fl.flags.p, c.grid, c.u.p, c.N,
-               fl.u4.p);
-        ++launch_counter;
-        return;
-      }
+    if (!fine_u) {  // into the packed level-0 iterate
+      launch(prolongate4_kernel<T>, blocks_for(fl.N, 128), 128, 0, fl.nb, fl.coords.p, fl.flags.p, c.grid, c.u.p, c.N,
+             fl.u4.p);
+      ++launch_counter;
+      return;
     }
     launch(prolongate_kernel<T>, blocks_for(fl.N, 128), 128, 0, fl.nb, fl.coords.p, fl.flags.p, c.grid, c.u.p, c.N,
                                                                    fine_u, fl.N, round_ref() ? 1 : 0);
@@ -654,14 +664,11 @@ class Solver {
     const int ex = P.explicit_level;
     const bool rr = round_ref();
     Level<T>& l0 = lev<T>(0);
-    // u0 == nullptr: single precision with the packed level-0 iterate l0.u4
-    bool packed = false;
-    if constexpr (sizeof(T) == 4) packed = u0 == nullptr;
+    // u0 == nullptr: the packed level-0 iterate l0.u4
+    const bool packed = u0 == nullptr;
     if (packed) {
-      if constexpr (sizeof(T) == 4) {
-        launch(reset_u4_kernel, blocks_for(l0.N, 256), 256, 0, l0.u4.p, E32.p, l0.N);
-        ++launch_counter;
-      }
+      launch(reset_u4_kernel<T>, blocks_for(l0.N, 256), 256, 0, l0.u4.p, Edev<T>(), l0.N);
+      ++launch_counter;
     } else {
       SGS_CUDA(cudaMemsetAsync(u0, 0, 3 * l0.N * sizeof(T), stream));
     }
@@ -684,10 +691,8 @@ class Solver {
       if (smooth) {
         if (l == 0) {
           if (packed) {
-            if constexpr (sizeof(T) == 4) {
-              launch(level0_res4_kernel, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, B(0), d.r.p, d.N, T(P.dx));
-              ++launch_counter;
-            }
+            launch(level0_res4_kernel<T>, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, B(0), d.r.p, d.N, T(P.dx));
+            ++launch_counter;
           } else {
             level0<T, OP_RES>(U(0), B(0), d.r.p);
           }
@@ -867,15 +872,16 @@ __global__ void precond_out_kernel(const TS* z, double* q, const double* __restr
 }
 
 // precond_out_kernel for the packed single-precision level-0 iterate
-__global__ void precond_out4_kernel(const float4* __restrict__ z4, double* q, const double* __restrict__ f,
+template <typename T>
+__global__ void precond_out4_kernel(const typename Pack4<T>::type* __restrict__ z4, double* q, const double* __restrict__ f,
                                     const uint32_t* __restrict__ flags, long N, double* __restrict__ part) {
   pdl_wait();
   __shared__ double sm[RED_THREADS / 32];
   double s = 0;
   for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += long(gridDim.x) * blockDim.x) {
     const uint32_t fl = flags[i];
-    const float4 z = z4[i];
-    const float zc[3] = {z.x, z.y, z.z};
+    const auto z = z4[i];
+    const double zc[3] = {double(z.x), double(z.y), double(z.z)};
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
       const long k = i + v * N;
@@ -1082,11 +1088,14 @@ void Solver::precondition() {
     Level<float>& m0 = *L32[0];
     if (packed0()) {
       vcycle<float>(m0.b.p, nullptr);
-      launch(precond_out4_kernel, RED_BLOCKS, RED_THREADS, 0, m0.u4.p, q.p, f.p, l0.flags.p, N, red.p);
+      launch(precond_out4_kernel<float>, RED_BLOCKS, RED_THREADS, 0, m0.u4.p, q.p, f.p, l0.flags.p, N, red.p);
     } else {
       vcycle<float>(m0.b.p, m0.u.p);
       launch(precond_out_kernel<float>, RED_BLOCKS, RED_THREADS, 0, m0.u.p, q.p, f.p, l0.flags.p, N, red.p);
     }
+  } else if (packed0()) {
+    vcycle<double>(f.p, nullptr);
+    launch(precond_out4_kernel<double>, RED_BLOCKS, RED_THREADS, 0, l0.u4.p, q.p, f.p, l0.flags.p, N, red.p);
   } else {
     vcycle<double>(f.p, q.p);
     launch(precond_out_kernel<double>, RED_BLOCKS, RED_THREADS, 0, q.p, q.p, f.p, l0.flags.p, N, red.p);
@@ -1374,17 +1383,15 @@ static double time_op(Solver& S, int op, int reps) {
   cudaEvent_t a, b;
   SGS_CUDA(cudaEventCreate(&a));
   SGS_CUDA(cudaEventCreate(&b));
-  // in a mixed session the residual and the sweep run on the packed iterate, as in its V-cycle
-  const bool packed = sizeof(T) == 4 && S.packed0();
+  // with a packed level 0 the residual and the sweep run on the packed iterate, as in the V-cycle
+  const bool packed = S.packed0();
   auto run = [&]() {
     if (op == 0) {
       S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);
     } else if (op == 1) {
-      if constexpr (sizeof(T) == 4) {
-        if (packed) {
-          S.launch(level0_res4_kernel, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, d.b.p, d.r.p, d.N, T(S.P.dx));
-          return;
-        }
+      if (packed) {
+        S.launch(level0_res4_kernel<T>, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, d.b.p, d.r.p, d.N, T(S.P.dx));
+        return;
       }
       S.level0<T, OP_RES>(d.u.p, d.b.p, d.r.p);
     } else if (op == 2) {
