@@ -92,6 +92,29 @@ SGS_API int sgs_displacements(sgs_session* s, double* out);
  * Returns the objective sum u_e^T K0 u_e (Emin + rho^p (1 - Emin)). */
 SGS_API double sgs_sensitivity(sgs_session* s, const double* density, double* dc, double* element_energy);
 
+/* Density-weighted sensitivity filter of the optimizer's driver, Opt::smooth_dc
+ * (topo_opt/spgrid_topo_opt.cpp:527-579), on the input blocks of the session:
+ * dc1 = sum_n w_n dc0_n rho_n / (sum_n w_n (rho + 1e-3)) over the cells n with
+ * density > 0 inside the cube of half width floor(filter_size) (w = max(0,
+ * filter_size - |offset|)); cells with density <= 0 get 0.  dc0 follows the
+ * driver's sign (the gradient, -dc of sgs_sensitivity).  Host arrays [nblocks][64]. */
+SGS_API int sgs_filter_sensitivity(sgs_session* s, const double* density, const double* dc0, double* dc1,
+                                   double filter_size);
+
+/* One optimality-criteria density update, OptimalityCriterion::optimize
+ * (topo_opt/optimizer/optimality_criterion.cpp:19-145): bisection on the Lagrange
+ * multiplier in [1e-20, 1e20] until lower*(1+1e-7) >= upper, new density
+ * clamp(clamp(rho*sqrt(max(0, -dc0 - shift)/mid), rho -/+ step_limit),
+ * minimum_density, 1) for cells with density > 0 (shift = min(0, min -dc0) when
+ * smart_oc, else 0), fixed cells (fixed[i] != 0, may be NULL) set to fixed_density
+ * and left out of the volume when exclude_fixed; the volume target is
+ * volume_fraction x (container cells - counted fixed cells).  density
+ * [nblocks][64] is updated in place; lagrange and max_change (may be NULL)
+ * receive the multiplier and the largest density change. */
+SGS_API int sgs_oc_update(sgs_session* s, double* density, const double* dc0, const uint8_t* fixed,
+                          double volume_fraction, double step_limit, double minimum_density, double fixed_density,
+                          int smart_oc, int exclude_fixed, double* lagrange, double* max_change);
+
 /* No counterpart in the reference.  Allocation-free variant of sgs_sensitivity
  * for callers that cannot allocate device memory while they run (frameworks
  * that own the allocator, code that must not call cudaMalloc/cudaFree once it

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libspgrid_gpu_solver.so")
 SOURCES = ["solver.cu", "setup.cpp", "wire.cpp"]
-HEADERS = ["kernels.cuh", "setup_kernels.cuh", "setup.hpp", "wire.hpp"]
+HEADERS = ["kernels.cuh", "setup_kernels.cuh", "topo_kernels.cuh", "setup.hpp", "wire.hpp"]
 
 
 def nvcc() -> str:

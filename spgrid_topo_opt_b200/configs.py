@@ -278,3 +278,30 @@ def spheres_band_inputs(n: int = 1024, nspheres: int = 8, thickness: int = 12, s
     p.caller_method = "spgrid_topo_opt_b200"
     p.preserve_output(base.shape[0])
     return p
+
+
+def bridge(nx: int = 512, ny: int = 128, nz: int = 256, density: float = 0.1, support_radius: float = 0.03,
+           bottom_size: int = 16) -> Problem:
+    """A bridge-like box domain of nx x ny x nz cells (x along the span, y up): the
+    cells of the bottom layer within ``support_radius`` (a fraction of the
+    largest extent) of the four bottom corners are fixed, and a uniform downward
+    load of total magnitude 1 acts on the nodes of the top deck.  Every cell
+    starts at ``density``.  A seeded-free synthetic stand-in for the reference's
+    bridge script domain."""
+    rho = np.full((nx, ny, nz), float(density))
+    r = support_radius * max(nx, ny, nz)
+    xs, zs = np.meshgrid(np.arange(nx) + 0.5, np.arange(nz) + 0.5, indexing="ij")
+    near = np.zeros((nx, nz), bool)
+    for cx in (0.0, float(nx)):
+        for cz in (0.0, float(nz)):
+            near |= (xs - cx) ** 2 + (zs - cz) ** 2 <= r * r
+    ij = np.argwhere(near)
+    cells = np.stack([ij[:, 0], np.zeros(len(ij), np.int64), ij[:, 1]], 1).astype(np.int32)
+    top = np.argwhere(np.ones((nx + 1, nz + 1), bool))
+    f = np.zeros(len(top), FORCE_DTYPE)
+    f["coord"][:, 0] = top[:, 0]
+    f["coord"][:, 1] = ny
+    f["coord"][:, 2] = top[:, 1]
+    f["f"][:, 1] = -1.0 / len(top)
+    return Problem(f"bridge{nx}x{ny}x{nz}", (nx, ny, nz), rho, cells, f, 1.0 / max(nx, ny, nz),
+                   mg_level_for(max(nx, ny, nz), bottom_size))

@@ -22,6 +22,7 @@
 #include "kernels.cuh"
 #include "setup.hpp"
 #include "setup_kernels.cuh"
+#include "topo_kernels.cuh"
 #include "wire.hpp"
 
 namespace sgs {
@@ -722,6 +723,12 @@ class Solver {
   void solve();
   void pack_outputs(double* disp);
   double sensitivity(const double* rho, double penalty, double emin, double* dc, double* se);
+  void filter_sensitivity(const double* rho, const double* dc0, double* dc1, double filter_size);
+  double oc_update(double* rho, const double* dc0, const uint8_t* fixed, double volume_fraction, double step_limit,
+                   double minimum_density, double fixed_density, int smart_oc, int exclude_fixed, double* change);
+  // dense grid of the input 4x4x4 blocks (built on first use by the filter)
+  DevBuf<int> in_grid, in_base_d;
+  int in_gdim[3] = {0, 0, 0};
 
   // New densities for the same material pattern: E, the Galerkin operators and
   // the bottom inverse are rebuilt, the hierarchy and flags are kept.
@@ -1254,6 +1261,99 @@ double Solver::sensitivity(const double* rho_host, double penalty, double emin, 
   return obj;
 }
 
+// Sensitivity filter of the driver (topo_opt/spgrid_topo_opt.cpp:527-579) on the
+// input blocks; host arrays [input block][64].
+void Solver::filter_sensitivity(const double* rho_h, const double* dc0_h, double* dc1_h, double filter_size) {
+  const long nin = long(P.in_block.size());
+  if (nin == 0) return;
+  if (!in_grid.p) {
+    for (int v = 0; v < 3; ++v) in_gdim[v] = (P.resolution[v] + 3) / 4;
+    std::vector<int32_t> g(size_t(in_gdim[0]) * in_gdim[1] * in_gdim[2], -1);
+    for (long b = 0; b < nin; ++b)
+      g[(size_t(P.in_base[3 * b] >> 2) * in_gdim[1] + (P.in_base[3 * b + 1] >> 2)) * in_gdim[2] +
+        (P.in_base[3 * b + 2] >> 2)] = int32_t(b);
+    in_grid.upload(g, stream);
+    in_base_d.upload(P.in_base, stream);
+  }
+  DevBuf<double> rho, dc0, dc1;
+  rho.upload(rho_h, size_t(nin) * 64, stream);
+  dc0.upload(dc0_h, size_t(nin) * 64, stream);
+  dc1.alloc(size_t(nin) * 64);
+  filter_dc_kernel<<<blocks_for(nin * 64, 256), 256, 0, stream>>>(int(nin), in_base_d.p, in_grid.p, in_gdim[0],
+                                                                  in_gdim[1], in_gdim[2], rho.p, dc0.p, dc1.p,
+                                                                  filter_size, int(std::floor(filter_size)));
+  SGS_CUDA(cudaGetLastError());
+  SGS_CUDA(cudaMemcpyAsync(dc1_h, dc1.p, size_t(nin) * 64 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  g_d2h_bytes += size_t(nin) * 64 * sizeof(double);
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+// One optimality-criteria update (topo_opt/optimizer/optimality_criterion.cpp:19-145):
+// bisection on the Lagrange multiplier with the reference's bounds and stopping
+// rule, each trial one pass over the cells on the GPU (sums reduced in a fixed
+// order), then the densities of the final multiplier.  Returns the multiplier.
+double Solver::oc_update(double* rho_h, const double* dc0_h, const uint8_t* fixed_h, double volume_fraction,
+                         double step_limit, double minimum_density, double fixed_density, int smart_oc,
+                         int exclude_fixed, double* change) {
+  const long n = long(P.in_block.size()) * 64;
+  if (change) *change = 0;
+  if (n == 0) return 0;
+  DevBuf<double> rho, dc0, part_s, part_c, part3;
+  DevBuf<uint8_t> fx;
+  rho.upload(rho_h, size_t(n), stream);
+  dc0.upload(dc0_h, size_t(n), stream);
+  if (fixed_h) fx.upload(fixed_h, size_t(n), stream);
+  part_s.alloc(OC_BLOCKS);
+  part_c.alloc(OC_BLOCKS);
+  part3.alloc(3 * OC_BLOCKS);
+  oc_stats_kernel<<<OC_BLOCKS, OC_THREADS, 0, stream>>>(n, rho.p, dc0.p, fx.p, part3.p);
+  SGS_CUDA(cudaGetLastError());
+  std::vector<double> h3(3 * OC_BLOCKS), hs(OC_BLOCKS), hc(OC_BLOCKS);
+  SGS_CUDA(cudaMemcpyAsync(h3.data(), part3.p, h3.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  double inside = 0, nfix = 0, neg_dc_min = 1e30;
+  for (int k = 0; k < OC_BLOCKS; ++k) {
+    inside += h3[3 * k];
+    nfix += h3[3 * k + 1];
+    neg_dc_min = std::min(neg_dc_min, h3[3 * k + 2]);
+  }
+  const double shift = smart_oc ? std::min(0.0, neg_dc_min) : 0.0;
+  // the reference compares against volume_fraction (a float) times the cell count
+  const double target = double(float(volume_fraction) * float(inside - (exclude_fixed ? nfix : 0)));
+  auto trial = [&](double mid, double* out, double* chg) {
+    oc_trial_kernel<<<OC_BLOCKS, OC_THREADS, 0, stream>>>(n, rho.p, dc0.p, fx.p, mid, shift, step_limit,
+                                                          minimum_density, fixed_density, exclude_fixed, out,
+                                                          part_s.p, part_c.p);
+    SGS_CUDA(cudaGetLastError());
+    SGS_CUDA(cudaMemcpyAsync(hs.data(), part_s.p, OC_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    if (chg) SGS_CUDA(cudaMemcpyAsync(hc.data(), part_c.p, OC_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    double sum = 0;
+    for (double v : hs) sum += v;
+    if (chg) {
+      *chg = 0;
+      for (double v : hc) *chg = std::max(*chg, v);
+    }
+    return sum;
+  };
+  double mid = 0, lower = double(1e-20f), upper = 1e20;
+  const double factor = double(1.0f + 1e-7f);
+  while (lower * factor < upper) {
+    mid = 0.5 * (lower + upper);
+    const double sum = trial(mid, nullptr, nullptr);
+    if (!(sum == sum)) throw CudaError("OC update produced a non-finite volume", SGS_ERR_BREAKDOWN);
+    if (sum > target) lower = mid;
+    else upper = mid;
+  }
+  double chg = 0;
+  trial(mid, rho.p, &chg);
+  SGS_CUDA(cudaMemcpyAsync(rho_h, rho.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  g_d2h_bytes += size_t(n) * sizeof(double);
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  if (change) *change = chg;
+  return mid;
+}
+
 }  // namespace sgs
 
 // ===========================================================================
@@ -1501,6 +1601,33 @@ SGS_API double sgs_sensitivity(sgs_session* h, const double* density, double* dc
     h->error = e.what();
     return std::nan("");
   }
+}
+
+SGS_API int sgs_filter_sensitivity(sgs_session* h, const double* density, const double* dc0, double* dc1,
+                                   double filter_size) {
+  if (!h || !density || !dc0 || !dc1 || host_only(h) || !(filter_size >= 0)) return SGS_ERR_INPUT;
+  try {
+    h->solver->filter_sensitivity(density, dc0, dc1, filter_size);
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+SGS_API int sgs_oc_update(sgs_session* h, double* density, const double* dc0, const uint8_t* fixed,
+                          double volume_fraction, double step_limit, double minimum_density, double fixed_density,
+                          int smart_oc, int exclude_fixed, double* lagrange, double* max_change) {
+  if (!h || !density || !dc0 || host_only(h)) return SGS_ERR_INPUT;
+  try {
+    const double mid = h->solver->oc_update(density, dc0, fixed, volume_fraction, step_limit, minimum_density,
+                                            fixed_density, smart_oc, exclude_fixed, max_change);
+    if (lagrange) *lagrange = mid;
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -22,7 +22,8 @@ OP_KU, OP_RESIDUAL, OP_SMOOTH, OP_RESTRICT, OP_PROLONG, OP_STENCIL, OP_BOTTOM, O
 EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", "sgs_last_error", "sgs_solve",
                     "sgs_residual_history", "sgs_displacements", "sgs_sensitivity", "sgs_level_count",
                     "sgs_level_blocks", "sgs_level_flags", "sgs_boundary_blocks", "sgs_apply", "sgs_level_stencils",
-                    "sgs_codec_roundtrip", "sgs_time_op", "sgs_sensitivity_static", "sgs_set_density")
+                    "sgs_codec_roundtrip", "sgs_time_op", "sgs_sensitivity_static", "sgs_set_density",
+                    "sgs_filter_sensitivity", "sgs_oc_update")
 
 
 class SolverError(RuntimeError):
@@ -82,6 +83,11 @@ def load(build_if_missing: bool = False):
     L.sgs_sensitivity_static.argtypes = [P, P, P, P, P]
     L.sgs_sensitivity_static.restype = C.c_int
     L.sgs_set_density.argtypes = [P, P]
+    L.sgs_filter_sensitivity.argtypes = [P, P, P, P, C.c_double]
+    L.sgs_filter_sensitivity.restype = C.c_int
+    L.sgs_oc_update.argtypes = [P, P, P, P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.sgs_oc_update.restype = C.c_int
     _lib = L
     return L
 
@@ -207,6 +213,31 @@ class Session:
         if not np.isfinite(obj):
             raise SolverError(10, load().sgs_last_error(self.h).decode(errors="replace"))
         return obj, dc, se
+
+    def filter_sensitivity(self, density: np.ndarray, dc0: np.ndarray, filter_size: float = 1.5) -> np.ndarray:
+        """The driver's density-weighted sensitivity filter (Opt::smooth_dc,
+        topo_opt/spgrid_topo_opt.cpp:527-579) on the GPU; dc0 is the gradient
+        (the driver's sign, -dc of ``sensitivity``)."""
+        rho = np.ascontiguousarray(density, np.float64)
+        d0 = np.ascontiguousarray(dc0, np.float64)
+        out = np.zeros(rho.shape)
+        self._check(load().sgs_filter_sensitivity(self.h, _ptr(rho), _ptr(d0), _ptr(out), float(filter_size)))
+        return out
+
+    def oc_update(self, density: np.ndarray, dc0: np.ndarray, volume_fraction: float, step_limit: float = 0.2,
+                  minimum_density: float = 0.0, fixed: Optional[np.ndarray] = None, fixed_density: float = 1.0,
+                  smart_oc: bool = False, exclude_fixed: bool = True):
+        """One optimality-criteria update (topo_opt/optimizer/optimality_criterion.cpp:19-145)
+        on the GPU.  Returns (new density, Lagrange multiplier, largest change)."""
+        rho = np.array(density, np.float64, copy=True, order="C")
+        d0 = np.ascontiguousarray(dc0, np.float64)
+        fx = None if fixed is None else np.ascontiguousarray(fixed, np.uint8)
+        lag, chg = C.c_double(0), C.c_double(0)
+        self._check(load().sgs_oc_update(self.h, _ptr(rho), _ptr(d0), None if fx is None else _ptr(fx),
+                                         float(volume_fraction), float(step_limit), float(minimum_density),
+                                         float(fixed_density), int(smart_oc), int(exclude_fixed), C.byref(lag),
+                                         C.byref(chg)))
+        return rho, lag.value, chg.value
 
     def set_density(self, density: np.ndarray) -> None:
         """New densities for the same material pattern (operators are rebuilt)."""

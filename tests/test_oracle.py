@@ -68,3 +68,19 @@ def test_sensitivity_matches_finite_differences():
 def test_setup_errors():
     with pytest.raises(OracleError):
         Oracle(configs.to_inputs(configs.cantilever_box(8), mg_level=2))
+
+
+def test_topo_oracle_uniform_cases():
+    """Hand-checked cases of the optimizer-step restatement: a uniform field
+    filters to dc0 rho/(rho + 1e-3) away from the container's edge, and a uniform
+    gradient leaves a density at the volume fraction unchanged."""
+    from oracle import topo_oracle as torc
+    base = np.array([[x, y, z] for x in (0, 4, 8) for y in (0, 4, 8) for z in (0, 4, 8)], np.int32)
+    rho = np.full((len(base), 64), 0.4)
+    dc0 = np.full((len(base), 64), -2.0)
+    out = torc.filter_dc(base, [12, 12, 12], rho, dc0, 1.5)
+    centre = 13 * 64 + 1 * 16 + 1 * 4 + 1  # block (4,4,4), cell (1,1,1): all neighbours inside
+    assert out.reshape(-1)[centre] == pytest.approx(-2.0 * 0.4 / 0.401, rel=1e-14)
+    new, mid, change = torc.oc_update(rho, dc0, 0.4, step_limit=0.2)
+    assert np.allclose(new, 0.4, rtol=1e-6) and change < 1e-6
+    assert mid == pytest.approx(2.0, rel=1e-6)
