@@ -46,6 +46,25 @@ struct CudaError : std::runtime_error {
 // fem_solve report the difference across a call.
 static std::atomic<unsigned long long> g_h2d_bytes{0}, g_d2h_bytes{0};
 
+// Device buffers come from the device's default stream-ordered memory pool,
+// whose release threshold is raised once per device so that freed memory stays
+// with the process: a later session or fem_solve call of similar size then
+// allocates without going to the driver.  Allocation is ordered on the legacy
+// default stream and waited for, and release first waits for the device (as
+// cudaFree does), so a buffer is ready when alloc returns and idle when freed.
+static void keep_pool_memory() {
+  static bool done[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = ~uint64_t(0);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done[dev] = true;
+}
+
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
@@ -55,14 +74,21 @@ struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaDeviceSynchronize();
+      cudaFreeAsync(p, 0);
+    }
     p = nullptr;
     n = 0;
   }
   void alloc(size_t count) {
     release();
     n = count;
-    if (count) SGS_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    if (count) {
+      keep_pool_memory();
+      SGS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), 0));
+      SGS_CUDA(cudaStreamSynchronize(0));
+    }
   }
   void upload(const T* h, size_t count, cudaStream_t s) {
     alloc(count);
