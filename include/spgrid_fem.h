@@ -115,6 +115,42 @@ SGS_API int sgs_oc_update(sgs_session* s, double* density, const double* dc0, co
                           double volume_fraction, double step_limit, double minimum_density, double fixed_density,
                           int smart_oc, int exclude_fixed, double* lagrange, double* max_change);
 
+/* The optimizer loop kept on the GPU.  The reference's driver runs one
+ * Opt::iterate per step (topo_opt/spgrid_topo_opt.cpp:1289-1331): objective and
+ * sensitivity, smooth_dc, the OC update, then the next fem_solve with the new
+ * densities.  sgs_design_set uploads the design densities [nblocks][64] (and an
+ * optional fixed-cell mask, which may be NULL); each sgs_design_step solves with
+ * the current densities, computes the sensitivity, filters it, applies the OC
+ * update (container cells kept at density >= DBL_MIN, as the driver's packing
+ * does, spgrid_topo_opt.cpp:1122) and rebuilds the stiffness scales, coarse
+ * operators and bottom inverse on the device; sgs_design_get copies the
+ * densities back.  The material pattern of the session does not change. */
+typedef struct sgs_design_params {
+  double tolerance;        /* solve: relative L-inf residual */
+  double volume_fraction;  /* OC volume target fraction */
+  double step_limit;       /* OC move limit (0.2 in the driver) */
+  double filter_size;      /* smooth_dc radius (1.5 in the driver) */
+  double minimum_density;  /* OC lower bound */
+  double fixed_density;    /* density of fixed cells */
+  int32_t smart_oc;        /* shift by min(0, min -dc0) */
+  int32_t exclude_fixed;   /* leave fixed cells out of the volume */
+} sgs_design_params;
+
+typedef struct sgs_design_result {
+  double objective;             /* sum u_e^T K0 u_e (Emin + rho^p (1 - Emin)) before the update */
+  double change;                /* largest density change of the OC update */
+  double lagrange;              /* OC multiplier */
+  int32_t cg_iterations;
+  int32_t reserved;
+  double solve_device_seconds;
+  double solve_seconds;         /* host wall time of the solve */
+  double step_seconds;          /* sensitivity, filter, OC and operator rebuild */
+} sgs_design_result;
+
+SGS_API int sgs_design_set(sgs_session* s, const double* density, const uint8_t* fixed);
+SGS_API int sgs_design_step(sgs_session* s, const sgs_design_params* params, sgs_design_result* result);
+SGS_API int sgs_design_get(sgs_session* s, double* density);
+
 /* No counterpart in the reference.  Allocation-free variant of sgs_sensitivity
  * for callers that cannot allocate device memory while they run (frameworks
  * that own the allocator, code that must not call cudaMalloc/cudaFree once it

@@ -752,6 +752,16 @@ class Solver {
   void filter_sensitivity(const double* rho, const double* dc0, double* dc1, double filter_size);
   double oc_update(double* rho, const double* dc0, const uint8_t* fixed, double volume_fraction, double step_limit,
                    double minimum_density, double fixed_density, int smart_oc, int exclude_fixed, double* change);
+  // the same on device arrays (rho updated in place)
+  void filter_dev(const double* rho, const double* dc0, double* dc1, double filter_size, double scale);
+  double oc_dev(double* rho, const double* dc0, const uint8_t* fixed, double volume_fraction, double step_limit,
+                double minimum_density, double fixed_density, int smart_oc, int exclude_fixed, int keep_inside,
+                double* change);
+  // device-resident design: densities, sensitivities and fixed-cell mask kept on the GPU
+  DevBuf<double> design_rho, design_dc, design_dc1, design_scratch, design_part;
+  DevBuf<uint8_t> design_fixed;
+  void design_set(const double* rho, const uint8_t* fixed);
+  void design_step(const sgs_design_params& prm, sgs_design_result* out);
   // dense grid of the input 4x4x4 blocks (built on first use by the filter)
   DevBuf<int> in_grid, in_base_d;
   int in_gdim[3] = {0, 0, 0};
@@ -1289,7 +1299,7 @@ double Solver::sensitivity(const double* rho_host, double penalty, double emin, 
 
 // Sensitivity filter of the driver (topo_opt/spgrid_topo_opt.cpp:527-579) on the
 // input blocks; host arrays [input block][64].
-void Solver::filter_sensitivity(const double* rho_h, const double* dc0_h, double* dc1_h, double filter_size) {
+void Solver::filter_dev(const double* rho, const double* dc0, double* dc1, double filter_size, double scale) {
   const long nin = long(P.in_block.size());
   if (nin == 0) return;
   if (!in_grid.p) {
@@ -1301,14 +1311,20 @@ void Solver::filter_sensitivity(const double* rho_h, const double* dc0_h, double
     in_grid.upload(g, stream);
     in_base_d.upload(P.in_base, stream);
   }
+  filter_dc_kernel<<<blocks_for(nin * 64, 256), 256, 0, stream>>>(int(nin), in_base_d.p, in_grid.p, in_gdim[0],
+                                                                  in_gdim[1], in_gdim[2], rho, dc0, dc1, filter_size,
+                                                                  int(std::floor(filter_size)), scale);
+  SGS_CUDA(cudaGetLastError());
+}
+
+void Solver::filter_sensitivity(const double* rho_h, const double* dc0_h, double* dc1_h, double filter_size) {
+  const long nin = long(P.in_block.size());
+  if (nin == 0) return;
   DevBuf<double> rho, dc0, dc1;
   rho.upload(rho_h, size_t(nin) * 64, stream);
   dc0.upload(dc0_h, size_t(nin) * 64, stream);
   dc1.alloc(size_t(nin) * 64);
-  filter_dc_kernel<<<blocks_for(nin * 64, 256), 256, 0, stream>>>(int(nin), in_base_d.p, in_grid.p, in_gdim[0],
-                                                                  in_gdim[1], in_gdim[2], rho.p, dc0.p, dc1.p,
-                                                                  filter_size, int(std::floor(filter_size)));
-  SGS_CUDA(cudaGetLastError());
+  filter_dev(rho.p, dc0.p, dc1.p, filter_size, 1.0);
   SGS_CUDA(cudaMemcpyAsync(dc1_h, dc1.p, size_t(nin) * 64 * sizeof(double), cudaMemcpyDeviceToHost, stream));
   g_d2h_bytes += size_t(nin) * 64 * sizeof(double);
   SGS_CUDA(cudaStreamSynchronize(stream));
@@ -1318,21 +1334,17 @@ void Solver::filter_sensitivity(const double* rho_h, const double* dc0_h, double
 // bisection on the Lagrange multiplier with the reference's bounds and stopping
 // rule, each trial one pass over the cells on the GPU (sums reduced in a fixed
 // order), then the densities of the final multiplier.  Returns the multiplier.
-double Solver::oc_update(double* rho_h, const double* dc0_h, const uint8_t* fixed_h, double volume_fraction,
-                         double step_limit, double minimum_density, double fixed_density, int smart_oc,
-                         int exclude_fixed, double* change) {
+double Solver::oc_dev(double* rho, const double* dc0, const uint8_t* fx, double volume_fraction,
+                      double step_limit, double minimum_density, double fixed_density, int smart_oc,
+                      int exclude_fixed, int keep_inside, double* change) {
   const long n = long(P.in_block.size()) * 64;
   if (change) *change = 0;
   if (n == 0) return 0;
-  DevBuf<double> rho, dc0, part_s, part_c, part3;
-  DevBuf<uint8_t> fx;
-  rho.upload(rho_h, size_t(n), stream);
-  dc0.upload(dc0_h, size_t(n), stream);
-  if (fixed_h) fx.upload(fixed_h, size_t(n), stream);
+  DevBuf<double> part_s, part_c, part3;
   part_s.alloc(OC_BLOCKS);
   part_c.alloc(OC_BLOCKS);
   part3.alloc(3 * OC_BLOCKS);
-  oc_stats_kernel<<<OC_BLOCKS, OC_THREADS, 0, stream>>>(n, rho.p, dc0.p, fx.p, part3.p);
+  oc_stats_kernel<<<OC_BLOCKS, OC_THREADS, 0, stream>>>(n, rho, dc0, fx, part3.p);
   SGS_CUDA(cudaGetLastError());
   std::vector<double> h3(3 * OC_BLOCKS), hs(OC_BLOCKS), hc(OC_BLOCKS);
   SGS_CUDA(cudaMemcpyAsync(h3.data(), part3.p, h3.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -1347,9 +1359,9 @@ double Solver::oc_update(double* rho_h, const double* dc0_h, const uint8_t* fixe
   // the reference compares against volume_fraction (a float) times the cell count
   const double target = double(float(volume_fraction) * float(inside - (exclude_fixed ? nfix : 0)));
   auto trial = [&](double mid, double* out, double* chg) {
-    oc_trial_kernel<<<OC_BLOCKS, OC_THREADS, 0, stream>>>(n, rho.p, dc0.p, fx.p, mid, shift, step_limit,
-                                                          minimum_density, fixed_density, exclude_fixed, out,
-                                                          part_s.p, part_c.p);
+    oc_trial_kernel<<<OC_BLOCKS, OC_THREADS, 0, stream>>>(n, rho, dc0, fx, mid, shift, step_limit, minimum_density,
+                                                          fixed_density, exclude_fixed, out, part_s.p, part_c.p,
+                                                          keep_inside);
     SGS_CUDA(cudaGetLastError());
     SGS_CUDA(cudaMemcpyAsync(hs.data(), part_s.p, OC_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost, stream));
     if (chg) SGS_CUDA(cudaMemcpyAsync(hc.data(), part_c.p, OC_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -1372,12 +1384,87 @@ double Solver::oc_update(double* rho_h, const double* dc0_h, const uint8_t* fixe
     else upper = mid;
   }
   double chg = 0;
-  trial(mid, rho.p, &chg);
+  trial(mid, rho, &chg);
+  if (change) *change = chg;
+  return mid;
+}
+
+double Solver::oc_update(double* rho_h, const double* dc0_h, const uint8_t* fixed_h, double volume_fraction,
+                         double step_limit, double minimum_density, double fixed_density, int smart_oc,
+                         int exclude_fixed, double* change) {
+  const long n = long(P.in_block.size()) * 64;
+  if (change) *change = 0;
+  if (n == 0) return 0;
+  DevBuf<double> rho, dc0;
+  DevBuf<uint8_t> fx;
+  rho.upload(rho_h, size_t(n), stream);
+  dc0.upload(dc0_h, size_t(n), stream);
+  if (fixed_h) fx.upload(fixed_h, size_t(n), stream);
+  const double mid = oc_dev(rho.p, dc0.p, fx.p, volume_fraction, step_limit, minimum_density, fixed_density, smart_oc,
+                            exclude_fixed, 0, change);
   SGS_CUDA(cudaMemcpyAsync(rho_h, rho.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, stream));
   g_d2h_bytes += size_t(n) * sizeof(double);
   SGS_CUDA(cudaStreamSynchronize(stream));
-  if (change) *change = chg;
   return mid;
+}
+
+// Device-resident design (the optimizer loop without host round trips).
+void Solver::design_set(const double* rho_h, const uint8_t* fixed_h) {
+  const size_t n = P.in_block.size() * 64;
+  design_rho.upload(rho_h, n, stream);
+  if (fixed_h) design_fixed.upload(fixed_h, n, stream);
+  else design_fixed.release();
+  design_dc.alloc(n);
+  design_dc1.alloc(n);
+  design_scratch.alloc(n);
+  design_part.alloc(blocks_for(long(n), 256));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+// One iteration of the driver's loop (Opt::iterate, spgrid_topo_opt.cpp:1289-1331,
+// without page-map maintenance): solve, sensitivity, filter, OC update, and the
+// new stiffness scales with rebuilt coarse operators and bottom inverse.
+void Solver::design_step(const sgs_design_params& prm, sgs_design_result* out) {
+  const long nin = long(P.in_block.size());
+  if (!design_rho.p || nin == 0) throw CudaError("no design densities set", SGS_ERR_INPUT);
+  const auto t0 = std::chrono::steady_clock::now();
+  P.tolerance = prm.tolerance;
+  solve();
+  const auto t1 = std::chrono::steady_clock::now();
+  const unsigned nblk = blocks_for(nin * 64, 256);
+  sensitivity_kernel<<<nblk, 256, 0, stream>>>(int(nin), in_block.p, in_zoff.p, L64[0]->nbr.p, x.p, N0(),
+                                               design_rho.p, P.penalty, P.minimum_stiffness, design_dc.p,
+                                               design_scratch.p, design_part.p);
+  SGS_CUDA(cudaGetLastError());
+  std::vector<double> hp(nblk);
+  SGS_CUDA(cudaMemcpyAsync(hp.data(), design_part.p, nblk * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  filter_dev(design_rho.p, design_dc.p, design_dc1.p, prm.filter_size, -1.0);
+  double change = 0;
+  const double mid = oc_dev(design_rho.p, design_dc1.p, design_fixed.p, prm.volume_fraction, prm.step_limit,
+                            prm.minimum_density, prm.fixed_density, prm.smart_oc, prm.exclude_fixed, 1, &change);
+  simp_E_kernel<<<nblk, 256, 0, stream>>>(int(nin), in_block.p, in_zoff.p, design_rho.p, P.penalty,
+                                          P.minimum_stiffness, P.minimum_density, E64.p);
+  SGS_CUDA(cudaGetLastError());
+  if (mixed())
+    launch(convert_kernel<float, double>, blocks_for(long(P.E.size()), 256), 256, 0, E32.p, E64.p, long(P.E.size()));
+  if (iter_graph) {
+    SGS_CUDA(cudaGraphExecDestroy(iter_graph));
+    iter_graph = nullptr;
+  }
+  build_operators();
+  build_bottom();
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  double obj = 0;
+  for (double v : hp) obj += v;
+  if (out) {
+    out->objective = obj;
+    out->change = change;
+    out->lagrange = mid;
+    out->cg_iterations = iterations;
+    out->solve_device_seconds = solve_device_seconds;
+    out->solve_seconds = std::chrono::duration<double>(t1 - t0).count();
+    out->step_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+  }
 }
 
 }  // namespace sgs
@@ -1649,6 +1736,42 @@ SGS_API int sgs_oc_update(sgs_session* h, double* density, const double* dc0, co
     const double mid = h->solver->oc_update(density, dc0, fixed, volume_fraction, step_limit, minimum_density,
                                             fixed_density, smart_oc, exclude_fixed, max_change);
     if (lagrange) *lagrange = mid;
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+SGS_API int sgs_design_set(sgs_session* h, const double* density, const uint8_t* fixed) {
+  if (!h || !density || host_only(h)) return SGS_ERR_INPUT;
+  try {
+    h->solver->design_set(density, fixed);
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+SGS_API int sgs_design_step(sgs_session* h, const sgs_design_params* p, sgs_design_result* r) {
+  if (!h || !p || host_only(h)) return SGS_ERR_INPUT;
+  try {
+    h->solver->design_step(*p, r);
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+SGS_API int sgs_design_get(sgs_session* h, double* density) {
+  if (!h || !density || host_only(h) || !h->solver->design_rho.p) return SGS_ERR_INPUT;
+  try {
+    Solver& S = *h->solver;
+    SGS_CUDA(cudaMemcpyAsync(density, S.design_rho.p, S.design_rho.n * sizeof(double), cudaMemcpyDeviceToHost,
+                             S.stream));
+    SGS_CUDA(cudaStreamSynchronize(S.stream));
   } catch (const CudaError& e) {
     h->error = e.what();
     return e.code;

@@ -13,11 +13,12 @@ namespace sgs {
 
 // dc1 = sum_n w_n dc0_n rho_n / (sum_n w_n (rho + 1e-3)) over the container
 // cells n within the cube of half width floor(filter_size), w = max(0,
-// filter_size - |offset|).  Cells outside the container get 0 (the reference
-// leaves them undefined; nothing reads them).
+// filter_size - |offset|), dc0 being scale times the given field (scale -1
+// turns the compliance sensitivity dc into the driver's gradient).  Cells outside
+// the container get 0 (the reference leaves them undefined; nothing reads them).
 __global__ void filter_dc_kernel(int nin, const int* __restrict__ base, const int* __restrict__ grid, int gx, int gy,
                                  int gz, const double* __restrict__ rho, const double* __restrict__ dc0,
-                                 double* __restrict__ dc1, double fsize, int half) {
+                                 double* __restrict__ dc1, double fsize, int half, double scale) {
   const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= long(nin) * 64) return;
   const int b = int(t >> 6), e = int(t & 63);
@@ -41,7 +42,7 @@ __global__ void filter_dc_kernel(int nin, const int* __restrict__ base, const in
         const double rn = rho[c];
         if (!(rn > 0)) continue;
         const double w = fmax(0.0, fsize - sqrt(double(dx * dx + dy * dy + dz * dz)));
-        sum += w * dc0[c] * rn;
+        sum += w * (scale * dc0[c]) * rn;
         wsum += w;
       }
   dc1[t] = sum / (wsum * (r + 1e-3));
@@ -51,11 +52,13 @@ constexpr int OC_THREADS = 256, OC_BLOCKS = 592;
 
 // One trial of the OC bisection at multiplier mid: the new density of every
 // container cell, per-CTA partial sums of the counted densities and maxima of
-// the change; with rho_out the densities are also written.
-__global__ void oc_trial_kernel(long n, const double* __restrict__ rho, const double* __restrict__ dc0,
+// the change; with rho_out the densities are also written, at least DBL_MIN
+// when keep_inside (a container cell stays in the container, as the driver's
+// packing ensures, spgrid_topo_opt.cpp:1122).
+__global__ void oc_trial_kernel(long n, const double* rho, const double* __restrict__ dc0,
                                 const uint8_t* __restrict__ fixed, double mid, double shift, double step,
-                                double rho_min, double fixed_rho, int exclude_fixed, double* __restrict__ rho_out,
-                                double* __restrict__ part_sum, double* __restrict__ part_change) {
+                                double rho_min, double fixed_rho, int exclude_fixed, double* rho_out,
+                                double* __restrict__ part_sum, double* __restrict__ part_change, int keep_inside) {
   __shared__ double ss[OC_THREADS / 32], sc[OC_THREADS / 32];
   double sum = 0, chg = 0;
   for (long t = long(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += long(gridDim.x) * blockDim.x) {
@@ -67,8 +70,8 @@ __global__ void oc_trial_kernel(long n, const double* __restrict__ rho, const do
     const bool fx = fixed && fixed[t];
     if (fx) nd = fixed_rho;
     if (!(exclude_fixed && fx)) sum += nd;
-    if (rho_out) rho_out[t] = nd;
     chg = fmax(chg, fabs(nd - old));
+    if (rho_out) rho_out[t] = keep_inside ? fmax(nd, 2.2250738585072014e-308) : nd;
   }
   for (int o = 16; o; o >>= 1) {
     sum += __shfl_down_sync(0xffffffffu, sum, o);
@@ -123,6 +126,23 @@ __global__ void oc_stats_kernel(long n, const double* __restrict__ rho, const do
     part[3 * blockIdx.x + 1] = c;
     part[3 * blockIdx.x + 2] = m;
   }
+}
+
+// The SIMP map of the solver's input (fem_interface.h:343-353) from the design
+// densities into the level-0 stiffness scales: E = (1 - Emin) max(rho_min, d)^p
+// + Emin for d > 0 (d itself without penalty), 0 for the empty cells.
+__global__ void simp_E_kernel(int nin, const int* __restrict__ in_block, const int* __restrict__ in_zoff,
+                              const double* __restrict__ rho, double penalty, double emin, double rho_min,
+                              double* __restrict__ E) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nin) * 64) return;
+  const int b = int(t >> 6), e = int(t & 63);
+  const int blk = in_block[b];
+  if (blk < 0) return;
+  const double d = rho[t];
+  double val = 0;
+  if (d > 0) val = penalty != 0 ? (1 - emin) * pow(fmax(rho_min, d), penalty) + emin : d;
+  E[long(blk) * 128 + (e >> 4) * 32 + ((e >> 2) & 3) * 8 + (e & 3) + in_zoff[b]] = val;
 }
 
 }  // namespace sgs

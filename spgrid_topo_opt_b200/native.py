@@ -23,7 +23,20 @@ EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", 
                     "sgs_residual_history", "sgs_displacements", "sgs_sensitivity", "sgs_level_count",
                     "sgs_level_blocks", "sgs_level_flags", "sgs_boundary_blocks", "sgs_apply", "sgs_level_stencils",
                     "sgs_codec_roundtrip", "sgs_time_op", "sgs_sensitivity_static", "sgs_set_density",
-                    "sgs_filter_sensitivity", "sgs_oc_update")
+                    "sgs_filter_sensitivity", "sgs_oc_update", "sgs_design_set", "sgs_design_step",
+                    "sgs_design_get")
+
+
+class DesignParams(C.Structure):
+    _fields_ = [("tolerance", C.c_double), ("volume_fraction", C.c_double), ("step_limit", C.c_double),
+                ("filter_size", C.c_double), ("minimum_density", C.c_double), ("fixed_density", C.c_double),
+                ("smart_oc", C.c_int32), ("exclude_fixed", C.c_int32)]
+
+
+class DesignResult(C.Structure):
+    _fields_ = [("objective", C.c_double), ("change", C.c_double), ("lagrange", C.c_double),
+                ("cg_iterations", C.c_int32), ("reserved", C.c_int32), ("solve_device_seconds", C.c_double),
+                ("solve_seconds", C.c_double), ("step_seconds", C.c_double)]
 
 
 class SolverError(RuntimeError):
@@ -88,6 +101,12 @@ def load(build_if_missing: bool = False):
     L.sgs_oc_update.argtypes = [P, P, P, P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.sgs_oc_update.restype = C.c_int
+    L.sgs_design_set.argtypes = [P, P, P]
+    L.sgs_design_set.restype = C.c_int
+    L.sgs_design_step.argtypes = [P, C.POINTER(DesignParams), C.POINTER(DesignResult)]
+    L.sgs_design_step.restype = C.c_int
+    L.sgs_design_get.argtypes = [P, P]
+    L.sgs_design_get.restype = C.c_int
     _lib = L
     return L
 
@@ -238,6 +257,28 @@ class Session:
                                          float(fixed_density), int(smart_oc), int(exclude_fixed), C.byref(lag),
                                          C.byref(chg)))
         return rho, lag.value, chg.value
+
+    def design_set(self, density: np.ndarray, fixed: Optional[np.ndarray] = None) -> None:
+        """Upload the densities of a device-resident optimizer loop (sgs_design_set)."""
+        rho = np.ascontiguousarray(density, np.float64)
+        fx = None if fixed is None else np.ascontiguousarray(fixed, np.uint8)
+        self._design_keep = (rho, fx)
+        self._check(load().sgs_design_set(self.h, _ptr(rho), None if fx is None else _ptr(fx)))
+
+    def design_step(self, tolerance: float = 1e-6, volume_fraction: float = 0.1, step_limit: float = 0.2,
+                    filter_size: float = 1.5, minimum_density: float = 0.0, fixed_density: float = 1.0,
+                    smart_oc: bool = False, exclude_fixed: bool = True) -> dict:
+        """One optimizer iteration on the GPU (sgs_design_step)."""
+        p = DesignParams(tolerance, volume_fraction, step_limit, filter_size, minimum_density, fixed_density,
+                         int(smart_oc), int(exclude_fixed))
+        r = DesignResult()
+        self._check(load().sgs_design_step(self.h, C.byref(p), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in DesignResult._fields_ if k != "reserved"}
+
+    def design_get(self) -> np.ndarray:
+        out = np.zeros(self.inputs.density.data.shape)
+        self._check(load().sgs_design_get(self.h, _ptr(out)))
+        return out
 
     def set_density(self, density: np.ndarray) -> None:
         """New densities for the same material pattern (operators are rebuilt)."""

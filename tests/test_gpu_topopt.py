@@ -61,7 +61,7 @@ def test_simp_iterations_match_oracle(native_lib):
     inp = configs.to_inputs(configs.cantilever_box(16, density=0.5, bottom_size=4), tolerance=1e-12)
     # the session mirrors its densities into the inputs it was given: keep the oracle's apart
     opt = SIMP(copy.deepcopy(inp), precision=native.PRECISION_FP64, tolerance=1e-12, volume_fraction=0.4,
-               minimum_density=1e-3)
+               minimum_density=1e-3, device=False)
     rho = inp.density.data.copy()
     inside = rho > 0
     for it in range(3):
@@ -76,3 +76,19 @@ def test_simp_iterations_match_oracle(native_lib):
         assert r["objective"] == pytest.approx(obj, rel=1e-8), it
         assert np.abs(opt.density - rho).max() <= 1e-6, it
     opt.close()
+
+
+def test_device_loop_matches_host_loop(native_lib):
+    """sgs_design_step (densities kept on the GPU) against the same iterations
+    through the host-array entry points."""
+    inp = configs.to_inputs(configs.cantilever_box(16, density=0.5, bottom_size=4), tolerance=1e-12)
+    kw = dict(precision=native.PRECISION_FP64, tolerance=1e-12, volume_fraction=0.4, minimum_density=1e-3)
+    host = SIMP(copy.deepcopy(inp), device=False, **kw)
+    dev = SIMP(copy.deepcopy(inp), device=True, **kw)
+    for it in range(3):
+        a, b = host.iterate(), dev.iterate()
+        assert b["objective"] == pytest.approx(a["objective"], rel=1e-10), it
+        assert b["lagrange"] == pytest.approx(a["lagrange"], rel=1e-9), it
+        assert np.abs(dev.density - host.density).max() <= 1e-9, it
+    host.close()
+    dev.close()
