@@ -203,6 +203,65 @@ SGS_API int sgs_time_op(sgs_session* s, int op, int reps, double* ms);
  * Lets callers check byte compatibility without a GPU. */
 SGS_API int sgs_codec_roundtrip(const void* blob, int which, void** out);
 
+/* ---- narrow band: the optimizer driver's page maps ---------------------- */
+/* The driver keeps its design on a grid of 4x4x4 blocks with four page maps
+ * (topo_opt/spgrid_topo_opt.h:116-134): the container; the thin map, blocks that
+ * still hold material; the fat map, whose cells the filter and the OC update
+ * visit; the fatter map, the blocks packed into FEMInputs for fem_solve
+ * (spgrid_topo_opt.cpp:1068-1160).  A band holds the container on the GPU
+ * (blocks, per-cell flags and densities, FEMInputs density layout: cell
+ * e = i*16 + j*4 + k of block b at b*64 + e) and the three maps as one byte per
+ * block in the caller's block order.  Before the first update every map is the
+ * whole container (spgrid_topo_opt.cpp:391-394). */
+typedef struct sgs_band sgs_band;
+
+/* Cell flag bits: TopOptFlags inside_container, has_force, fixed_density
+ * (topo_opt/spgrid_topo_opt.h:30-42). */
+#define SGS_CELL_INSIDE 1
+#define SGS_CELL_FORCE 2
+#define SGS_CELL_FIXED 4
+
+typedef struct sgs_band_params {
+  double minimum_density;         /* Opt::minimum_density */
+  double active_threshold;        /* config "active_threshold" (driver default 1e-6) */
+  double fraction_to_keep;        /* config "fraction_to_keep" (1.0: no selection) */
+  int32_t fat_margin;             /* config "fat_margin" (default 1; 0..4 supported) */
+  int32_t connectivity_filtering; /* config "connectivity_filtering" (default 1) */
+} sgs_band_params;
+
+typedef struct sgs_band_stats {
+  int64_t container_blocks;
+  int64_t thin_before_pruning; /* thin blocks before fraction_to_keep and the connectivity filter */
+  int64_t thin_blocks, fat_blocks, fatter_blocks;
+  int64_t components;          /* 6-connected components of the thin blocks (0 when not filtered) */
+  int64_t active_voxels;       /* container cells of fatter blocks above active_threshold */
+  double device_seconds;       /* the update on the GPU (CUDA events) */
+} sgs_band_stats;
+
+/* Replaces the driver's container set-up of the four maps
+ * (spgrid_topo_opt.cpp:263-394): block_base[nblocks][3] are the container's
+ * 4x4x4 block bases (multiples of 4 inside resolution), cell_flags and density
+ * [nblocks][64].  Returns 0 and *out, or an error code with a message in err. */
+SGS_API int sgs_band_create(const int32_t* block_base, int64_t nblocks, const int32_t resolution[3],
+                            const uint8_t* cell_flags, const double* density, sgs_band** out, char* err,
+                            int errlen);
+SGS_API void sgs_band_destroy(sgs_band* b);
+SGS_API const char* sgs_band_last_error(sgs_band* b);
+SGS_API int sgs_band_set_density(sgs_band* b, const double* density);
+SGS_API int sgs_band_get_density(sgs_band* b, double* density);
+/* Replace the fat map the next update prunes from ([nblocks] bytes, 0/1). */
+SGS_API int sgs_band_set_fat(sgs_band* b, const uint8_t* fat);
+
+/* Replaces Opt::update_thin_page_map (spgrid_topo_opt.cpp:92-152), then, when
+ * connectivity_filtering, Opt::filter_isolated_blocks (:1404-1510), then
+ * Opt::update_fat_page_map (:154-241).  Where the reference stops (TC_ASSERT /
+ * TC_ERROR: no thin block, not exactly one component above 30% of the thin
+ * blocks, a fraction_to_keep selection beyond the fat list) this returns
+ * SGS_ERR_INPUT with the maps unchanged.  stats may be NULL. */
+SGS_API int sgs_band_update(sgs_band* b, const sgs_band_params* params, sgs_band_stats* stats);
+/* Copy the maps out, one byte per container block; any pointer may be NULL. */
+SGS_API int sgs_band_maps(sgs_band* b, uint8_t* thin, uint8_t* fat, uint8_t* fatter);
+
 #ifdef __cplusplus
 }
 #endif

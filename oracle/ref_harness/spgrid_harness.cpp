@@ -10,7 +10,12 @@
 //   * the element stiffness tables K_mu/K_la (solver/CPU_Kernels/Stiffness_Matrices.h)
 //     and Km_cell/Kl_cell (solver/MG/Linear_Elasticity_Stiffness_Matrix.h).
 //
+//   * the block order of the optimizer driver's grid (64-byte nodes, 4 KiB pages:
+//     4x4x4 blocks, topo_opt/spgrid_topo_opt.h:45-94), which its page maps
+//     (thin/fat/fatter) list their blocks in;
+//
 //   spgrid_harness order <size> <coords.txt>   block bases (x y z per line) -> page order
+//   spgrid_harness order4 <size> <coords.txt>  the same on the driver's 4x4x4 grid
 //   spgrid_harness offsets <coords.txt>         element offsets and level maps of nodes
 //   spgrid_harness tables <out.bin>             K_mu, K_la, Km_cell, Kl_cell as float64
 #include <array>
@@ -31,6 +36,12 @@ using Struct = Elasticity_Solver_Data<double, uint64_t>;
 using Alloc = SPGrid_Allocator<Struct, 3, 14>;
 using PageMap = SPGrid_Page_Map<14>;
 using Mask = Alloc::Array_mask<double>;
+struct DriverNode {
+  double field[8];
+};
+using DriverAlloc = SPGrid_Allocator<DriverNode, 3, 12>;
+using DriverPageMap = SPGrid_Page_Map<12>;
+using DriverMask = DriverAlloc::Array_mask<double>;
 
 static std::vector<std::array<int, 3>> read_coords(const char* fn) {
   std::vector<std::array<int, 3>> out;
@@ -52,6 +63,19 @@ int main(int argc, char** argv) {
     auto blocks = pm.Get_Blocks();
     for (unsigned b = 0; b < blocks.second; ++b) {
       auto c = Mask::LinearToCoord(blocks.first[b]);
+      std::printf("%d %d %d\n", c[0], c[1], c[2]);
+    }
+    return 0;
+  }
+  if (cmd == "order4" && argc >= 4) {
+    int size = std::atoi(argv[2]);
+    DriverAlloc alloc(size, size, size);
+    DriverPageMap pm(alloc);
+    for (auto& c : read_coords(argv[3])) pm.Set_Page(DriverMask::Linear_Offset(c[0], c[1], c[2]));
+    pm.Update_Block_Offsets();
+    auto blocks = pm.Get_Blocks();
+    for (unsigned b = 0; b < blocks.second; ++b) {
+      auto c = DriverMask::LinearToCoord(blocks.first[b]);
       std::printf("%d %d %d\n", c[0], c[1], c[2]);
     }
     return 0;

@@ -13,8 +13,8 @@ when its density is positive.
 Parity unpinned: the reference's driver needs Taichi, which is absent, so no
 reference output exists for these steps; they are restated from the source
 lines cited above and checked in tests/ against the GPU kernels and against
-hand-made cases.  Sums are accumulated in float64 here (the reference uses
-Taichi's ``real``).
+hand-made cases.  Everything is float64, like the driver's ``real`` (Taichi
+compiled in double precision, static_assert at spgrid_topo_opt.h:28-29).
 """
 from __future__ import annotations
 
@@ -50,7 +50,7 @@ def filter_dc(base, resolution, rho, dc0, filter_size: float = 1.5) -> np.ndarra
     half = int(math.floor(filter_size))
     pad = half + 1
     Rp = np.pad(R, pad)
-    DRp = np.pad(D * R, pad)
+    Dp = np.pad(D, pad)
     Ip = (Rp > 0).astype(np.float64)
     s = np.zeros_like(R)
     ws = np.zeros_like(R)
@@ -60,7 +60,7 @@ def filter_dc(base, resolution, rho, dc0, filter_size: float = 1.5) -> np.ndarra
             for dz in range(-half, half + 1):
                 w = max(0.0, filter_size - math.sqrt(dx * dx + dy * dy + dz * dz))
                 sl = (slice(pad + dx, pad + dx + X), slice(pad + dy, pad + dy + Y), slice(pad + dz, pad + dz + Z))
-                s += w * DRp[sl] * Ip[sl]
+                s += (w * Dp[sl]) * Rp[sl] * Ip[sl]   # (weight * dc0) * density, the reference's order
                 ws += w * Ip[sl]
     with np.errstate(divide="ignore", invalid="ignore"):
         out = np.where(R > 0, s / (ws * (R + 1e-3)), 0.0)
@@ -77,8 +77,8 @@ def oc_update(rho, dc0, volume_fraction: float, step_limit: float = 0.2, minimum
     neg_dc_min = float(np.min(-dc0[inside])) if (smart_oc and inside.any()) else 1e30
     shift = min(0.0, neg_dc_min)
     nfix = int(np.count_nonzero(fx & inside)) if exclude_fixed else 0
-    # volume_fraction is a float in the reference, multiplied by the cell count
-    target = float(np.float32(volume_fraction) * np.float32(int(np.count_nonzero(inside)) - nfix))
+    # the driver's real is float64 (static_assert, spgrid_topo_opt.h:28-29)
+    target = float(volume_fraction) * float(int(np.count_nonzero(inside)) - nfix)
 
     def trial(mid):
         old = rho[inside]
@@ -90,8 +90,8 @@ def oc_update(rho, dc0, volume_fraction: float, step_limit: float = 0.2, minimum
         counted = ~f if exclude_fixed else np.ones_like(f)
         return nd, float(np.sum(nd[counted]))
 
-    lower, upper, mid = float(np.float32(1e-20)), 1e20, 0.0
-    factor = float(np.float32(1.0) + np.float32(1e-7))
+    lower, upper, mid = 1e-20, 1e20, 0.0
+    factor = 1 + 1e-7
     while lower * factor < upper:
         mid = 0.5 * (lower + upper)
         _, s = trial(mid)
@@ -104,3 +104,135 @@ def oc_update(rho, dc0, volume_fraction: float, step_limit: float = 0.2, minimum
     out[inside] = nd
     change = float(np.max(np.abs(nd - rho[inside]))) if nd.size else 0.0
     return out, mid, change
+
+
+# ---------------------------------------------------------------------------
+# Narrow-band page maps of the driver (thin / fat / fatter)
+# ---------------------------------------------------------------------------
+CELL_INSIDE, CELL_FORCE, CELL_FIXED = 1, 2, 4   # TopOptFlags bits 0-2 (spgrid_topo_opt.h:30-42)
+
+
+class PageMapError(RuntimeError):
+    """A state the reference stops on (TC_ASSERT / TC_ERROR in the driver)."""
+
+
+def driver_page_keys(block_ijk) -> np.ndarray:
+    """Page index of the driver's 4x4x4 grid (64-byte nodes, 4 KiB pages): from the
+    SPGrid page masks (external/SPGrid/Core/SPGrid_Mask.h:38-47) with
+    block_bits = 6, bit 3m holds bit m of the block's z, 3m+1 of y, 3m+2 of x.
+    Sorting by it gives the order of the driver's page-map block lists."""
+    b = np.asarray(block_ijk, np.int64).reshape(-1, 3)
+    k = np.zeros(len(b), np.uint64)
+    for m in range(21):
+        k |= ((b[:, 2] >> m) & 1).astype(np.uint64) << np.uint64(3 * m)
+        k |= ((b[:, 1] >> m) & 1).astype(np.uint64) << np.uint64(3 * m + 1)
+        k |= ((b[:, 0] >> m) & 1).astype(np.uint64) << np.uint64(3 * m + 2)
+    return k
+
+
+def update_page_maps(base, density, flags, fat_prev, *, minimum_density: float = 0.0,
+                     active_threshold: float = 1e-6, fraction_to_keep: float = 1.0, fat_margin: int = 1,
+                     connectivity_filtering: bool = True):
+    """One page-map update of the driver: Opt::update_thin_page_map
+    (spgrid_topo_opt.cpp:92-152), Opt::filter_isolated_blocks (:1404-1510, when
+    ``connectivity_filtering``) and Opt::update_fat_page_map (:154-241).
+
+    base[n][3]: the container's 4x4x4 blocks (any order); density, flags[n][64]
+    per cell (i*16 + j*4 + k); fat_prev[n]: the fat map the thin map is pruned
+    from (the container itself before the first update, :391-394).  Returns
+    (thin, fat, fatter, stats) with the maps as bool[n] in the caller's order."""
+    base = np.asarray(base, np.int64).reshape(-1, 3)
+    n = len(base)
+    dens = np.asarray(density, np.float64).reshape(n, 64)
+    flg = np.asarray(flags, np.uint8).reshape(n, 64)
+    order = np.argsort(driver_page_keys(base // 4), kind="stable")   # list position -> block
+    where = {tuple(base[b]): b for b in range(n)}
+    fat_prev = np.asarray(fat_prev, bool)
+
+    # thin: blocks of the fat map whose largest density reaches the threshold or
+    # that carry a force (:100-116); BlockMeta starts at max 0, min 1, sum 0
+    fat_list = [b for b in order if fat_prev[b]]
+    sums = np.zeros(len(fat_list))
+    thin = np.zeros(n, bool)
+    for p, b in enumerate(fat_list):
+        dmax = max(0.0, float(dens[b].max()))
+        sums[p] = float(np.cumsum(dens[b])[-1])           # sequential, in region order
+        has_force = bool((flg[b] & CELL_FORCE).any())
+        thin[b] = dmax >= minimum_density + active_threshold or has_force
+    stats = {"thin_before_pruning": int(thin.sum())}
+
+    # fraction_to_keep (:121-151): note the reference reads block_meta (indexed by
+    # the fat list) at the position of each block in the thin list
+    if fraction_to_keep != 1.0:
+        keep = int(fraction_to_keep * n)
+        thin_list = [b for b in order if thin[b]]
+        if keep >= len(thin_list):
+            if keep < 1 or keep > len(fat_list):
+                raise PageMapError("fraction_to_keep selects outside the fat block list")
+            threshold = np.partition(sums, keep - 1)[keep - 1]
+            thin[:] = False
+            for p, b in enumerate(thin_list):
+                if sums[p] > threshold:
+                    thin[b] = True
+
+    # isolated-block filter: 6-connected components of the thin blocks (:1404-1510)
+    components = 0
+    if connectivity_filtering:
+        color = {}
+        sizes = []
+        for b in order:
+            if not thin[b] or b in color:
+                continue
+            queue = [b]
+            color[b] = len(sizes)
+            count = 1
+            head = 0
+            while head < len(queue):
+                u = queue[head]
+                head += 1
+                for d in ((4, 0, 0), (-4, 0, 0), (0, 4, 0), (0, -4, 0), (0, 0, 4), (0, 0, -4)):
+                    v = where.get((base[u][0] + d[0], base[u][1] + d[1], base[u][2] + d[2]))
+                    if v is not None and thin[v] and v not in color:
+                        color[v] = len(sizes)
+                        queue.append(v)
+                        count += 1
+            sizes.append(count)
+        components = len(sizes)
+        if components == 0:
+            raise PageMapError("no thin blocks left for the connectivity filter")
+        if components > 1:
+            total = sum(sizes)
+            big = [i for i, s in enumerate(sizes) if 1.0 * s / total > 0.3]
+            if len(big) != 1:
+                raise PageMapError(f"{len(big)} block components hold more than 30% of the thin blocks")
+            for b in range(n):
+                if thin[b] and color[b] != big[0]:
+                    thin[b] = False
+    stats["components"] = components
+
+    # fat: the pages of the diagonal neighbours at fat_margin of every cell above
+    # the threshold in a thin block, within the container (:166-186)
+    fat = np.zeros(n, bool)
+    offs = np.array([[a, b, c] for a in (-1, 1) for b in (-1, 1) for c in (-1, 1)]) * fat_margin
+    ijk = np.array([[e >> 4, (e >> 2) & 3, e & 3] for e in range(64)])
+    for b in np.nonzero(thin)[0]:
+        cells = ijk[dens[b] > active_threshold] + base[b]
+        pages = np.unique((((cells[:, None, :] + offs[None]) // 4) * 4).reshape(-1, 3), axis=0)
+        for pg in pages:
+            v = where.get(tuple(pg))
+            if v is not None:
+                fat[v] = True
+    # fatter: the fat blocks and their +1 neighbours in every combination (:188-200)
+    fatter = np.zeros(n, bool)
+    for b in np.nonzero(fat)[0]:
+        for a in (0, 4):
+            for bb in (0, 4):
+                for c in (0, 4):
+                    v = where.get((base[b][0] + a, base[b][1] + bb, base[b][2] + c))
+                    if v is not None:
+                        fatter[v] = True
+    inside = (flg & CELL_INSIDE) != 0
+    stats.update(container_blocks=n, thin_blocks=int(thin.sum()), fat_blocks=int(fat.sum()),
+                 fatter_blocks=int(fatter.sum()),
+                 active_voxels=int(np.count_nonzero((inside & (dens > active_threshold))[fatter])))
+    return thin, fat, fatter, stats

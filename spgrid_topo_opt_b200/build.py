@@ -15,8 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libspgrid_gpu_solver.so")
-SOURCES = ["solver.cu", "setup.cpp", "wire.cpp"]
-HEADERS = ["kernels.cuh", "setup_kernels.cuh", "topo_kernels.cuh", "setup.hpp", "wire.hpp"]
+SOURCES = ["solver.cu", "band.cu", "setup.cpp", "wire.cpp"]
+HEADERS = ["common.cuh", "band.hpp", "kernels.cuh", "setup_kernels.cuh", "topo_kernels.cuh", "setup.hpp", "wire.hpp"]
 
 
 def nvcc() -> str:

@@ -1,0 +1,545 @@
+// Narrow-band page maps on the GPU; see band.hpp.  Kernels work on the
+// container in the caller's block order: a warp per block for the per-cell
+// passes (two cells a lane, coalesced 256-byte rows), a thread per block for the
+// block passes, a lock-free union-find for the 6-connected components.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "band.hpp"
+
+namespace sgs {
+namespace {
+
+constexpr int BAND_WARPS = 8;  // warps per CTA of the warp-per-block kernels
+enum { CNT_THIN = 0, CNT_FAT, CNT_FATTER, CNT_ACTIVE, CNT_COMPONENTS, CNT_BIG, CNT_BIG_ROOT, CNT_ERROR, CNT_N };
+
+// Block of the container holding the cell block (bx, by, bz), or -1.
+__device__ __forceinline__ int lookup(const int* __restrict__ grid, int gx, int gy, int gz, int bx, int by, int bz) {
+  if (bx < 0 || by < 0 || bz < 0 || bx >= gx || by >= gy || bz >= gz) return -1;
+  return grid[(long(bx) * gy + by) * gz + bz];
+}
+
+// Page key of block (bx, by, bz) of its 4x4x4 grid: bit 3m is
+// bit m of bz, 3m+1 of by, 3m+2 of bx (SPGrid_Mask.h:38-47 with 64-byte
+// elements and 4 KiB pages).  Sorting by it gives the driver's list order.
+uint64_t driver_page_key(int bx, int by, int bz) {
+  uint64_t key = 0;
+  for (int m = 0; m < 21; ++m) {
+    key |= uint64_t((bz >> m) & 1) << (3 * m);
+    key |= uint64_t((by >> m) & 1) << (3 * m + 1);
+    key |= uint64_t((bx >> m) & 1) << (3 * m + 2);
+  }
+  return key;
+}
+
+// Thin map (update_thin_page_map, spgrid_topo_opt.cpp:100-116): a block of the
+// fat map stays when its largest density (BlockMeta starts at 0) reaches
+// minimum_density + active_threshold or one of its cells carries a force.  The
+// block's density sum is accumulated in region order (cell 0..63), one add at a
+// time as in the reference, for the fraction_to_keep selection.
+__global__ void band_thin_kernel(long n, const double* __restrict__ rho, const uint8_t* __restrict__ flags,
+                                 const uint8_t* __restrict__ fat_prev, double threshold, uint8_t* __restrict__ thin,
+                                 double* __restrict__ meta_sum, unsigned long long* __restrict__ cnt) {
+  __shared__ double cells[BAND_WARPS][64];
+  const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long b = long(blockIdx.x) * BAND_WARPS + wl;
+  if (b >= n) return;
+  if (!fat_prev[b]) {
+    if (lane == 0) thin[b] = 0;
+    return;
+  }
+  const double d0 = rho[b * 64 + lane], d1 = rho[b * 64 + 32 + lane];
+  const bool force = __any_sync(0xffffffffu, ((flags[b * 64 + lane] | flags[b * 64 + 32 + lane]) & SGS_CELL_FORCE) != 0);
+  // std::max(m, d) keeps m when d is NaN; so does fmax
+  double mx = fmax(0.0, fmax(d0, d1));
+  for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  cells[wl][lane] = d0;
+  cells[wl][lane + 32] = d1;
+  __syncwarp();
+  if (lane == 0) {
+    double s = 0;
+    for (int e = 0; e < 64; ++e) s += cells[wl][e];
+    meta_sum[b] = s;
+    const bool keep = mx >= threshold || force;
+    thin[b] = keep;
+    if (keep) atomicAdd(cnt + CNT_THIN, 1ull);
+  }
+}
+
+// fraction_to_keep: driver list position p -> the fat flag, density sum and
+// thin flag of the block at that position.
+__global__ void band_list_kernel(long n, const int* __restrict__ morton, const uint8_t* __restrict__ fat,
+                                 const uint8_t* __restrict__ thin, const double* __restrict__ meta_sum,
+                                 uint8_t* __restrict__ fat_m, uint8_t* __restrict__ thin_m, double* __restrict__ sum_m) {
+  const long p = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int b = morton[p];
+  fat_m[p] = fat[b];
+  thin_m[p] = thin[b];
+  sum_m[p] = meta_sum[b];
+}
+
+// The reference keeps the b-th block of the old thin list when block_meta[b] --
+// the meta of the b-th block of the fat list -- has a density sum above the
+// threshold (spgrid_topo_opt.cpp:140-147).
+__global__ void band_keep_kernel(long n_thin, const int* __restrict__ thin_list, const double* __restrict__ fat_sums,
+                                 const double* __restrict__ threshold, uint8_t* __restrict__ thin) {
+  const long p = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= n_thin) return;
+  if (fat_sums[p] > *threshold) thin[thin_list[p]] = 1;
+}
+
+// ---- 6-connected components of the thin blocks (filter_isolated_blocks) ----
+// Union-find with parent[x] <= x for every x: a root is hooked under a smaller
+// root by compare-and-swap, path halving writes ancestors only, so every chain
+// strictly decreases and each loop ends within n steps (the bound is checked).
+__device__ __forceinline__ int uf_find(int* parent, int x, long n, unsigned long long* err) {
+  for (long it = 0; it <= n; ++it) {
+    const int p = __ldcg(parent + x);
+    if (p == x) return x;
+    const int g = __ldcg(parent + p);
+    if (g == p) return p;
+    __stcg(parent + x, g);
+    x = g;
+  }
+  atomicExch(err, 1ull);
+  return x;
+}
+
+__global__ void band_cc_init_kernel(long n, const uint8_t* __restrict__ thin, int* __restrict__ parent,
+                                    int* __restrict__ size) {
+  const long b = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  parent[b] = thin[b] ? int(b) : -1;
+  size[b] = 0;
+}
+
+__global__ void band_cc_hook_kernel(long n, const int* __restrict__ base, const int* __restrict__ grid, int gx, int gy,
+                                    int gz, const uint8_t* __restrict__ thin, int* parent, unsigned long long* cnt) {
+  const long b = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= n || !thin[b]) return;
+  const int bx = base[3 * b] >> 2, by = base[3 * b + 1] >> 2, bz = base[3 * b + 2] >> 2;
+  const int nbx[3] = {bx + 1, bx, bx}, nby[3] = {by, by + 1, by}, nbz[3] = {bz, bz, bz + 1};
+  for (int v = 0; v < 3; ++v) {
+    const int c = lookup(grid, gx, gy, gz, nbx[v], nby[v], nbz[v]);
+    if (c < 0 || !thin[c]) continue;
+    int x = int(b), y = c;
+    for (long it = 0;; ++it) {
+      if (it > n) {
+        atomicExch(cnt + CNT_ERROR, 1ull);
+        break;
+      }
+      x = uf_find(parent, x, n, cnt + CNT_ERROR);
+      y = uf_find(parent, y, n, cnt + CNT_ERROR);
+      if (x == y) break;
+      if (x > y) {
+        const int t = x;
+        x = y;
+        y = t;
+      }
+      if (atomicCAS(parent + y, y, x) == y) break;  // else y gained a parent meanwhile: retry
+    }
+  }
+}
+
+__global__ void band_cc_flatten_kernel(long n, const uint8_t* __restrict__ thin, int* parent, int* __restrict__ size,
+                                       unsigned long long* cnt) {
+  const long b = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= n || !thin[b]) return;
+  const int r = uf_find(parent, int(b), n, cnt + CNT_ERROR);
+  atomicAdd(size + r, 1);
+}
+
+// Components (roots) and those holding more than 30% of the thin blocks: the
+// reference's fraction 1.0 * s / total in float64 compared with 0.3 (:1466-1480).
+__global__ void band_cc_roots_kernel(long n, const uint8_t* __restrict__ thin, const int* __restrict__ parent,
+                                     const int* __restrict__ size, unsigned long long* cnt) {
+  const long b = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= n || !thin[b] || __ldcg(parent + b) != int(b)) return;
+  atomicAdd(cnt + CNT_COMPONENTS, 1ull);
+  const double total = double(cnt[CNT_THIN]);
+  if (1.0 * size[b] / total > 0.3) {
+    atomicAdd(cnt + CNT_BIG, 1ull);
+    atomicExch(cnt + CNT_BIG_ROOT, (unsigned long long)b);
+  }
+}
+
+// No union runs any more: the walk to the root is read-only and ends within n steps.
+__global__ void band_cc_keep_kernel(long n, const int* __restrict__ parent, int root, uint8_t* __restrict__ thin) {
+  const long b = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= n || !thin[b]) return;
+  int r = int(b);
+  for (long it = 0; it <= n; ++it) {
+    const int p = parent[r];
+    if (p == r) break;
+    r = p;
+  }
+  if (r != root) thin[b] = 0;
+}
+
+// Fat map (update_fat_page_map, :166-186): every cell of a thin block whose
+// density exceeds active_threshold marks the pages of its 8 diagonal neighbours
+// at fat_margin that belong to the container.  With fat_margin <= 4 those pages
+// are among the block's 27 neighbours, so a warp ORs a 27-bit set over its 64
+// cells and 27 lanes write the marks.
+__global__ void band_fat_kernel(long n, const int* __restrict__ base, const int* __restrict__ grid, int gx, int gy,
+                                int gz, const uint8_t* __restrict__ thin, const double* __restrict__ rho,
+                                double active_threshold, int margin, uint8_t* __restrict__ fat) {
+  const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long b = long(blockIdx.x) * BAND_WARPS + wl;
+  if (b >= n || !thin[b]) return;
+  unsigned set = 0;
+  for (int h = 0; h < 2; ++h) {
+    const int e = lane + 32 * h;
+    if (!(rho[b * 64 + e] > active_threshold)) continue;
+    const int p[3] = {e >> 4, (e >> 2) & 3, e & 3};
+    for (int s = 0; s < 8; ++s) {
+      int bit = 0;
+      for (int v = 0; v < 3; ++v) {
+        const int q = p[v] + (((s >> (2 - v)) & 1) ? margin : -margin);
+        bit = bit * 3 + (q < 0 ? 0 : q > 3 ? 2 : 1);
+      }
+      set |= 1u << bit;
+    }
+  }
+  set = __reduce_or_sync(0xffffffffu, set);
+  if (lane < 27 && ((set >> lane) & 1)) {
+    const int c = lookup(grid, gx, gy, gz, (base[3 * b] >> 2) + lane / 9 - 1, (base[3 * b + 1] >> 2) + (lane / 3) % 3 - 1,
+                         (base[3 * b + 2] >> 2) + lane % 3 - 1);
+    if (c >= 0) fat[c] = 1;
+  }
+}
+
+// Fatter map (:188-200): a fat block and its +1 neighbours in every combination
+// of axes, within the container.
+__global__ void band_fatter_kernel(long n, const int* __restrict__ base, const int* __restrict__ grid, int gx, int gy,
+                                   int gz, const uint8_t* __restrict__ fat, uint8_t* __restrict__ fatter) {
+  const long b = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= n || !fat[b]) return;
+  const int bx = base[3 * b] >> 2, by = base[3 * b + 1] >> 2, bz = base[3 * b + 2] >> 2;
+  for (int s = 0; s < 8; ++s) {
+    const int c = lookup(grid, gx, gy, gz, bx + ((s >> 2) & 1), by + ((s >> 1) & 1), bz + (s & 1));
+    if (c >= 0) fatter[c] = 1;
+  }
+}
+
+// Map sizes and the active voxels of the fatter map (:215-235).
+__global__ void band_count_kernel(long n, const uint8_t* __restrict__ thin, const uint8_t* __restrict__ fat,
+                                  const uint8_t* __restrict__ fatter, const uint8_t* __restrict__ flags,
+                                  const double* __restrict__ rho, double active_threshold, unsigned long long* cnt) {
+  const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long b = long(blockIdx.x) * BAND_WARPS + wl;
+  if (b >= n) return;
+  if (lane == 0) {
+    if (thin[b]) atomicAdd(cnt + CNT_THIN, 1ull);
+    if (fat[b]) atomicAdd(cnt + CNT_FAT, 1ull);
+    if (fatter[b]) atomicAdd(cnt + CNT_FATTER, 1ull);
+  }
+  if (!fatter[b]) return;
+  int a = 0;
+  for (int h = 0; h < 2; ++h) {
+    const long c = b * 64 + lane + 32 * h;
+    a += (flags[c] & SGS_CELL_INSIDE) && rho[c] > active_threshold;
+  }
+  for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if (lane == 0 && a) atomicAdd(cnt + CNT_ACTIVE, (unsigned long long)a);
+}
+
+}  // namespace
+
+Band::Band(const int32_t* base_h, int64_t nblocks, const int32_t res[3], const uint8_t* flags_h,
+           const double* density_h) {
+  if (nblocks <= 0 || !base_h || !res || !flags_h || !density_h) throw CudaError("empty container", SGS_ERR_INPUT);
+  n = long(nblocks);
+  for (int v = 0; v < 3; ++v) {
+    if (res[v] <= 0) throw CudaError("resolution must be positive", SGS_ERR_INPUT);
+    gdim[v] = (res[v] + 3) / 4;
+  }
+  std::vector<int32_t> g(size_t(gdim[0]) * gdim[1] * gdim[2], -1);
+  std::vector<std::pair<uint64_t, int32_t>> keys(static_cast<size_t>(n));
+  for (long b = 0; b < n; ++b) {
+    int bi[3];
+    for (int v = 0; v < 3; ++v) {
+      const int c = base_h[3 * b + v];
+      if (c < 0 || c % 4 || c >= res[v]) throw CudaError("container block outside the grid or not 4-aligned", SGS_ERR_GRID);
+      bi[v] = c >> 2;
+    }
+    int32_t& slot = g[(size_t(bi[0]) * gdim[1] + bi[1]) * gdim[2] + bi[2]];
+    if (slot >= 0) throw CudaError("duplicate container block", SGS_ERR_GRID);
+    slot = int32_t(b);
+    keys[size_t(b)] = {driver_page_key(bi[0], bi[1], bi[2]), int32_t(b)};
+  }
+  std::sort(keys.begin(), keys.end());
+  std::vector<int32_t> order(static_cast<size_t>(n));
+  for (long p = 0; p < n; ++p) order[size_t(p)] = keys[size_t(p)].second;
+  SGS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  SGS_CUDA(cudaEventCreate(&ev[0]));
+  SGS_CUDA(cudaEventCreate(&ev[1]));
+  base.upload(base_h, size_t(n) * 3, stream);
+  grid.upload(g, stream);
+  morton.upload(order, stream);
+  flags.upload(flags_h, size_t(n) * 64, stream);
+  rho.upload(density_h, size_t(n) * 64, stream);
+  thin.alloc(size_t(n));
+  fat.alloc(size_t(n));
+  fatter.alloc(size_t(n));
+  for (auto* m : {&thin, &fat, &fatter}) SGS_CUDA(cudaMemsetAsync(m->p, 1, size_t(n), stream));
+  meta_sum.alloc(size_t(n));
+  parent.alloc(size_t(n));
+  comp_size.alloc(size_t(n));
+  counters.alloc(CNT_N);
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+Band::~Band() {
+  if (stream) cudaStreamSynchronize(stream);
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void Band::set_density(const double* h) {
+  SGS_CUDA(cudaMemcpyAsync(rho.p, h, size_t(n) * 64 * sizeof(double), cudaMemcpyHostToDevice, stream));
+  g_h2d_bytes += size_t(n) * 64 * sizeof(double);
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Band::get_density(double* h) {
+  SGS_CUDA(cudaMemcpyAsync(h, rho.p, size_t(n) * 64 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  g_d2h_bytes += size_t(n) * 64 * sizeof(double);
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Band::set_fat(const uint8_t* h) {
+  SGS_CUDA(cudaMemcpyAsync(fat.p, h, size_t(n), cudaMemcpyHostToDevice, stream));
+  g_h2d_bytes += size_t(n);
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Band::maps(uint8_t* t, uint8_t* f, uint8_t* ff) {
+  const uint8_t* src[3] = {thin.p, fat.p, fatter.p};
+  uint8_t* dst[3] = {t, f, ff};
+  for (int m = 0; m < 3; ++m)
+    if (dst[m]) {
+      SGS_CUDA(cudaMemcpyAsync(dst[m], src[m], size_t(n), cudaMemcpyDeviceToHost, stream));
+      g_d2h_bytes += size_t(n);
+    }
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+// fraction_to_keep (:121-151), with the reference's int(fraction * container
+// blocks) target and its nth_element threshold over the fat blocks' sums.
+void Band::keep_fraction(double fraction_to_keep, long n_thin) {
+  const long keep = long(int(fraction_to_keep * double(n)));
+  if (keep < n_thin) return;  // "constraint already satisfied"
+  DevBuf<uint8_t> fat_m, thin_m;
+  DevBuf<double> sum_m, fat_sums, sorted;
+  DevBuf<int32_t> thin_list;
+  DevBuf<int> nsel;
+  fat_m.alloc(size_t(n));
+  thin_m.alloc(size_t(n));
+  sum_m.alloc(size_t(n));
+  fat_sums.alloc(size_t(n));
+  sorted.alloc(size_t(n));
+  thin_list.alloc(size_t(n));
+  nsel.alloc(2);
+  band_list_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, morton.p, fat.p, thin.p, meta_sum.p, fat_m.p, thin_m.p,
+                                                            sum_m.p);
+  SGS_CUDA(cudaGetLastError());
+  size_t t1 = 0, t2 = 0, t3 = 0;
+  SGS_CUDA(cub::DeviceSelect::Flagged(nullptr, t1, sum_m.p, fat_m.p, fat_sums.p, nsel.p, int(n), stream));
+  SGS_CUDA(cub::DeviceSelect::Flagged(nullptr, t2, morton.p, thin_m.p, thin_list.p, nsel.p + 1, int(n), stream));
+  SGS_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, t3, fat_sums.p, sorted.p, int(n), 0, 64, stream));
+  DevBuf<uint8_t> tmp;
+  tmp.alloc(std::max(t1, std::max(t2, t3)));
+  size_t tb = tmp.n;
+  SGS_CUDA(cub::DeviceSelect::Flagged(tmp.p, tb, sum_m.p, fat_m.p, fat_sums.p, nsel.p, int(n), stream));
+  tb = tmp.n;
+  SGS_CUDA(cub::DeviceSelect::Flagged(tmp.p, tb, morton.p, thin_m.p, thin_list.p, nsel.p + 1, int(n), stream));
+  int h[2];
+  SGS_CUDA(cudaMemcpyAsync(h, nsel.p, sizeof(h), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  const long n_fat = h[0];
+  if (keep < 1 || keep > n_fat)
+    throw CudaError("fraction_to_keep selects " + std::to_string(keep) + " blocks of a fat list of " +
+                        std::to_string(n_fat),
+                    SGS_ERR_INPUT);
+  tb = tmp.n;
+  SGS_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, tb, fat_sums.p, sorted.p, int(n_fat), 0, 64, stream));
+  SGS_CUDA(cudaMemsetAsync(thin.p, 0, size_t(n), stream));
+  band_keep_kernel<<<blocks_for(n_thin, 256), 256, 0, stream>>>(n_thin, thin_list.p, fat_sums.p,
+                                                                 sorted.p + (keep - 1), thin.p);
+  SGS_CUDA(cudaGetLastError());
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Band::update(const sgs_band_params& prm, sgs_band_stats* st) {
+  if (prm.fat_margin < 0 || prm.fat_margin > 4) throw CudaError("fat_margin must be within 0..4", SGS_ERR_INPUT);
+  const int gx = gdim[0], gy = gdim[1], gz = gdim[2];
+  const unsigned wgrid = blocks_for(n, BAND_WARPS), tgrid = blocks_for(n, 256);
+  // work on copies so that an update the reference would stop on leaves the maps as they were
+  DevBuf<uint8_t> thin_new, fat_new, fatter_new;
+  thin_new.alloc(size_t(n));
+  fat_new.alloc(size_t(n));
+  fatter_new.alloc(size_t(n));
+  std::swap(thin.p, thin_new.p);  // thin_new holds the current thin map now
+  SGS_CUDA(cudaEventRecord(ev[0], stream));
+  SGS_CUDA(cudaMemsetAsync(counters.p, 0, CNT_N * sizeof(unsigned long long), stream));
+  band_thin_kernel<<<wgrid, 32 * BAND_WARPS, 0, stream>>>(n, rho.p, flags.p, fat.p,
+                                                         prm.minimum_density + prm.active_threshold, thin.p,
+                                                         meta_sum.p, counters.p);
+  SGS_CUDA(cudaGetLastError());
+  unsigned long long c[CNT_N];
+  auto read_counters = [&] {
+    SGS_CUDA(cudaMemcpyAsync(c, counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+  };
+  auto fail = [&](const std::string& m) {
+    std::swap(thin.p, thin_new.p);  // put the previous thin map back
+    throw CudaError(m, SGS_ERR_INPUT);
+  };
+  read_counters();
+  const long thin_before = long(c[CNT_THIN]);
+  long n_thin = thin_before;
+  if (prm.fraction_to_keep != 1.0) {
+    try {
+      keep_fraction(prm.fraction_to_keep, n_thin);
+    } catch (const CudaError& e) {
+      if (e.code != SGS_ERR_INPUT) throw;
+      fail(e.what());
+    }
+    SGS_CUDA(cudaMemsetAsync(counters.p, 0, sizeof(unsigned long long), stream));
+    band_count_kernel<<<wgrid, 32 * BAND_WARPS, 0, stream>>>(n, thin.p, fat.p, fatter.p, flags.p, rho.p, 0.0,
+                                                              counters.p);
+    SGS_CUDA(cudaGetLastError());
+    read_counters();
+    n_thin = long(c[CNT_THIN]);
+    SGS_CUDA(cudaMemsetAsync(counters.p, 0, CNT_N * sizeof(unsigned long long), stream));
+    SGS_CUDA(cudaMemcpyAsync(counters.p + CNT_THIN, c + CNT_THIN, sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                             stream));
+  }
+  long components = 0;
+  if (prm.connectivity_filtering) {
+    if (n_thin == 0) fail("no thin blocks left for the connectivity filter");
+    band_cc_init_kernel<<<tgrid, 256, 0, stream>>>(n, thin.p, parent.p, comp_size.p);
+    band_cc_hook_kernel<<<tgrid, 256, 0, stream>>>(n, base.p, grid.p, gx, gy, gz, thin.p, parent.p, counters.p);
+    band_cc_flatten_kernel<<<tgrid, 256, 0, stream>>>(n, thin.p, parent.p, comp_size.p, counters.p);
+    band_cc_roots_kernel<<<tgrid, 256, 0, stream>>>(n, thin.p, parent.p, comp_size.p, counters.p);
+    SGS_CUDA(cudaGetLastError());
+    read_counters();
+    if (c[CNT_ERROR]) throw CudaError("union-find exceeded its step bound", SGS_ERR_INTERNAL);
+    components = long(c[CNT_COMPONENTS]);
+    if (components > 1) {
+      if (c[CNT_BIG] != 1)
+        fail(std::to_string(c[CNT_BIG]) + " block components hold more than 30% of the thin blocks");
+      band_cc_keep_kernel<<<tgrid, 256, 0, stream>>>(n, parent.p, int(c[CNT_BIG_ROOT]), thin.p);
+      SGS_CUDA(cudaGetLastError());
+    }
+  }
+  SGS_CUDA(cudaMemsetAsync(fat_new.p, 0, size_t(n), stream));
+  SGS_CUDA(cudaMemsetAsync(fatter_new.p, 0, size_t(n), stream));
+  band_fat_kernel<<<wgrid, 32 * BAND_WARPS, 0, stream>>>(n, base.p, grid.p, gx, gy, gz, thin.p, rho.p,
+                                                        prm.active_threshold, prm.fat_margin, fat_new.p);
+  band_fatter_kernel<<<tgrid, 256, 0, stream>>>(n, base.p, grid.p, gx, gy, gz, fat_new.p, fatter_new.p);
+  SGS_CUDA(cudaMemsetAsync(counters.p, 0, CNT_N * sizeof(unsigned long long), stream));
+  band_count_kernel<<<wgrid, 32 * BAND_WARPS, 0, stream>>>(n, thin.p, fat_new.p, fatter_new.p, flags.p, rho.p,
+                                                            prm.active_threshold, counters.p);
+  SGS_CUDA(cudaGetLastError());
+  SGS_CUDA(cudaEventRecord(ev[1], stream));
+  read_counters();
+  std::swap(fat.p, fat_new.p);
+  std::swap(fatter.p, fatter_new.p);
+  float ms = 0;
+  SGS_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+  if (st) {
+    st->container_blocks = n;
+    st->thin_before_pruning = thin_before;
+    st->thin_blocks = long(c[CNT_THIN]);
+    st->fat_blocks = long(c[CNT_FAT]);
+    st->fatter_blocks = long(c[CNT_FATTER]);
+    st->components = components;
+    st->active_voxels = long(c[CNT_ACTIVE]);
+    st->device_seconds = ms * 1e-3;
+  }
+}
+
+}  // namespace sgs
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace sgs;
+
+struct sgs_band {
+  std::unique_ptr<Band> band;
+  std::string error;
+};
+
+template <typename F>
+static int band_call(sgs_band* h, F&& f) {
+  if (!h || !h->band) return SGS_ERR_INPUT;
+  try {
+    f(*h->band);
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    h->error = e.what();
+    return SGS_ERR_INTERNAL;
+  }
+  return 0;
+}
+
+SGS_API int sgs_band_create(const int32_t* block_base, int64_t nblocks, const int32_t resolution[3],
+                            const uint8_t* cell_flags, const double* density, sgs_band** out, char* err,
+                            int errlen) {
+  if (!out) return SGS_ERR_INPUT;
+  *out = nullptr;
+  std::unique_ptr<sgs_band> h(new sgs_band());
+  try {
+    h->band.reset(new Band(block_base, nblocks, resolution, cell_flags, density));
+  } catch (const CudaError& e) {
+    if (err && errlen > 0) std::snprintf(err, size_t(errlen), "%s", e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    if (err && errlen > 0) std::snprintf(err, size_t(errlen), "%s", e.what());
+    return SGS_ERR_INTERNAL;
+  }
+  *out = h.release();
+  return 0;
+}
+
+SGS_API void sgs_band_destroy(sgs_band* b) { delete b; }
+
+SGS_API const char* sgs_band_last_error(sgs_band* b) { return b ? b->error.c_str() : "null band"; }
+
+SGS_API int sgs_band_set_density(sgs_band* b, const double* density) {
+  if (!density) return SGS_ERR_INPUT;
+  return band_call(b, [&](Band& B) { B.set_density(density); });
+}
+
+SGS_API int sgs_band_get_density(sgs_band* b, double* density) {
+  if (!density) return SGS_ERR_INPUT;
+  return band_call(b, [&](Band& B) { B.get_density(density); });
+}
+
+SGS_API int sgs_band_set_fat(sgs_band* b, const uint8_t* fat) {
+  if (!fat) return SGS_ERR_INPUT;
+  return band_call(b, [&](Band& B) { B.set_fat(fat); });
+}
+
+SGS_API int sgs_band_update(sgs_band* b, const sgs_band_params* p, sgs_band_stats* stats) {
+  if (!p) return SGS_ERR_INPUT;
+  return band_call(b, [&](Band& B) { B.update(*p, stats); });
+}
+
+SGS_API int sgs_band_maps(sgs_band* b, uint8_t* thin, uint8_t* fat, uint8_t* fatter) {
+  return band_call(b, [&](Band& B) { B.maps(thin, fat, fatter); });
+}

@@ -19,6 +19,8 @@
 #include <vector>
 
 #include "../../include/spgrid_fem.h"
+#include "band.hpp"
+#include "common.cuh"
 #include "kernels.cuh"
 #include "setup.hpp"
 #include "setup_kernels.cuh"
@@ -27,81 +29,6 @@
 
 namespace sgs {
 
-// ---------------------------------------------------------------------------
-// small utilities
-// ---------------------------------------------------------------------------
-struct CudaError : std::runtime_error {
-  int code;
-  CudaError(const std::string& m, int c) : std::runtime_error(m), code(c) {}
-};
-
-#define SGS_CUDA(x)                                                                                     \
-  do {                                                                                                  \
-    cudaError_t e_ = (x);                                                                               \
-    if (e_ != cudaSuccess)                                                                              \
-      throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_), SGS_ERR_CUDA);                   \
-  } while (0)
-
-// Host<->device bytes moved by this library (uploads, read-backs); sessions and
-// fem_solve report the difference across a call.
-static std::atomic<unsigned long long> g_h2d_bytes{0}, g_d2h_bytes{0};
-
-// Device buffers come from the device's default stream-ordered memory pool,
-// whose release threshold is raised once per device so that freed memory stays
-// with the process: a later session or fem_solve call of similar size then
-// allocates without going to the driver.  Allocation is ordered on the legacy
-// default stream and waited for, and release first waits for the device (as
-// cudaFree does), so a buffer is ready when alloc returns and idle when freed.
-static void keep_pool_memory() {
-  static bool done[64] = {false};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev]) return;
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    uint64_t keep = ~uint64_t(0);
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  }
-  cudaGetLastError();
-  done[dev] = true;
-}
-
-template <typename T>
-struct DevBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  ~DevBuf() { release(); }
-  void release() {
-    if (p) {
-      cudaDeviceSynchronize();
-      cudaFreeAsync(p, 0);
-    }
-    p = nullptr;
-    n = 0;
-  }
-  void alloc(size_t count) {
-    release();
-    n = count;
-    if (count) {
-      keep_pool_memory();
-      SGS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), 0));
-      SGS_CUDA(cudaStreamSynchronize(0));
-    }
-  }
-  void upload(const T* h, size_t count, cudaStream_t s) {
-    alloc(count);
-    if (count) SGS_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
-    g_h2d_bytes += count * sizeof(T);
-  }
-  void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
-  void zero(cudaStream_t s) {
-    if (n) SGS_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
-  }
-};
-
-static inline unsigned blocks_for(long n, int t) { return unsigned((n + t - 1) / t); }
 
 // Element stiffness of the Q1 hex on the unit cube: K_mu = int(delta_ij grad Na.grad Nb
 // + d_j Na d_i Nb), K_la = int d_i Na d_j Nb; node index a = 4x + 2y + z.  These are
@@ -1356,8 +1283,9 @@ double Solver::oc_dev(double* rho, const double* dc0, const uint8_t* fx, double 
     neg_dc_min = std::min(neg_dc_min, h3[3 * k + 2]);
   }
   const double shift = smart_oc ? std::min(0.0, neg_dc_min) : 0.0;
-  // the reference compares against volume_fraction (a float) times the cell count
-  const double target = double(float(volume_fraction) * float(inside - (exclude_fixed ? nfix : 0)));
+  // Taichi's real is float64 in the driver (static_assert, spgrid_topo_opt.h:28-29):
+  // the target, the bracket and the stopping factor are all double
+  const double target = volume_fraction * (inside - (exclude_fixed ? nfix : 0));
   auto trial = [&](double mid, double* out, double* chg) {
     oc_trial_kernel<<<OC_BLOCKS, OC_THREADS, 0, stream>>>(n, rho, dc0, fx, mid, shift, step_limit, minimum_density,
                                                           fixed_density, exclude_fixed, out, part_s.p, part_c.p,
@@ -1374,8 +1302,8 @@ double Solver::oc_dev(double* rho, const double* dc0, const uint8_t* fx, double 
     }
     return sum;
   };
-  double mid = 0, lower = double(1e-20f), upper = 1e20;
-  const double factor = double(1.0f + 1e-7f);
+  double mid = 0, lower = 1e-20, upper = 1e20;
+  const double factor = 1 + 1e-7;
   while (lower * factor < upper) {
     mid = 0.5 * (lower + upper);
     const double sum = trial(mid, nullptr, nullptr);

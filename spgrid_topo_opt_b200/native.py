@@ -24,7 +24,11 @@ EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", 
                     "sgs_level_blocks", "sgs_level_flags", "sgs_boundary_blocks", "sgs_apply", "sgs_level_stencils",
                     "sgs_codec_roundtrip", "sgs_time_op", "sgs_sensitivity_static", "sgs_set_density",
                     "sgs_filter_sensitivity", "sgs_oc_update", "sgs_design_set", "sgs_design_step",
-                    "sgs_design_get")
+                    "sgs_design_get", "sgs_band_create", "sgs_band_destroy", "sgs_band_last_error",
+                    "sgs_band_set_density", "sgs_band_get_density", "sgs_band_set_fat", "sgs_band_update",
+                    "sgs_band_maps")
+
+CELL_INSIDE, CELL_FORCE, CELL_FIXED = 1, 2, 4   # SGS_CELL_* (driver TopOptFlags bits 0-2)
 
 
 class DesignParams(C.Structure):
@@ -37,6 +41,20 @@ class DesignResult(C.Structure):
     _fields_ = [("objective", C.c_double), ("change", C.c_double), ("lagrange", C.c_double),
                 ("cg_iterations", C.c_int32), ("reserved", C.c_int32), ("solve_device_seconds", C.c_double),
                 ("solve_seconds", C.c_double), ("step_seconds", C.c_double)]
+
+
+class BandParams(C.Structure):
+    _fields_ = [("minimum_density", C.c_double), ("active_threshold", C.c_double),
+                ("fraction_to_keep", C.c_double), ("fat_margin", C.c_int32), ("connectivity_filtering", C.c_int32)]
+
+
+class BandStats(C.Structure):
+    _fields_ = [("container_blocks", C.c_int64), ("thin_before_pruning", C.c_int64), ("thin_blocks", C.c_int64),
+                ("fat_blocks", C.c_int64), ("fatter_blocks", C.c_int64), ("components", C.c_int64),
+                ("active_voxels", C.c_int64), ("device_seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class SolverError(RuntimeError):
@@ -107,6 +125,19 @@ def load(build_if_missing: bool = False):
     L.sgs_design_step.restype = C.c_int
     L.sgs_design_get.argtypes = [P, P]
     L.sgs_design_get.restype = C.c_int
+    L.sgs_band_create.argtypes = [P, C.c_int64, P, P, P, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
+    L.sgs_band_create.restype = C.c_int
+    L.sgs_band_destroy.argtypes = [P]
+    L.sgs_band_destroy.restype = None
+    L.sgs_band_last_error.argtypes = [P]
+    L.sgs_band_last_error.restype = C.c_char_p
+    for name in ("sgs_band_set_density", "sgs_band_get_density", "sgs_band_set_fat"):
+        getattr(L, name).argtypes = [P, P]
+        getattr(L, name).restype = C.c_int
+    L.sgs_band_update.argtypes = [P, C.POINTER(BandParams), C.POINTER(BandStats)]
+    L.sgs_band_update.restype = C.c_int
+    L.sgs_band_maps.argtypes = [P, P, P, P]
+    L.sgs_band_maps.restype = C.c_int
     _lib = L
     return L
 
@@ -334,3 +365,63 @@ class Session:
         sp = np.zeros(n, np.uint32)
         self._check(load().sgs_level_stencils(self.h, level, _ptr(out), _ptr(sp)))
         return out, sp
+
+
+class Band:
+    """The optimizer driver's narrow band on the GPU: the container's 4x4x4
+    blocks with per-cell flags (CELL_*) and densities, and the thin / fat /
+    fatter page maps (include/spgrid_fem.h, sgs_band_*).  ``update`` runs the
+    driver's update_thin_page_map, filter_isolated_blocks and
+    update_fat_page_map (topo_opt/spgrid_topo_opt.cpp:92-241, 1404-1510)."""
+
+    def __init__(self, base: np.ndarray, resolution, flags: np.ndarray, density: np.ndarray):
+        L = load()
+        self.base = np.ascontiguousarray(base, np.int32).reshape(-1, 3)
+        self.n = self.base.shape[0]
+        self.flags = np.ascontiguousarray(flags, np.uint8).reshape(self.n, 64)
+        dens = np.ascontiguousarray(density, np.float64).reshape(self.n, 64)
+        res = np.ascontiguousarray(resolution, np.int32).reshape(3)
+        h = C.c_void_p(0)
+        err = C.create_string_buffer(512)
+        rc = L.sgs_band_create(_ptr(self.base), self.n, _ptr(res), _ptr(self.flags), _ptr(dens), C.byref(h), err, 512)
+        if rc != 0:
+            raise SolverError(rc, err.value.decode(errors="replace"))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().sgs_band_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise SolverError(rc, load().sgs_band_last_error(self.h).decode(errors="replace"))
+
+    def set_density(self, density: np.ndarray):
+        d = np.ascontiguousarray(density, np.float64).reshape(self.n, 64)
+        self._check(load().sgs_band_set_density(self.h, _ptr(d)))
+
+    def density(self) -> np.ndarray:
+        out = np.empty((self.n, 64))
+        self._check(load().sgs_band_get_density(self.h, _ptr(out)))
+        return out
+
+    def set_fat(self, fat: np.ndarray):
+        f = np.ascontiguousarray(np.asarray(fat) != 0, np.uint8)
+        self._check(load().sgs_band_set_fat(self.h, _ptr(f)))
+
+    def update(self, minimum_density: float = 0.0, active_threshold: float = 1e-6, fraction_to_keep: float = 1.0,
+               fat_margin: int = 1, connectivity_filtering: bool = True) -> dict:
+        p = BandParams(minimum_density, active_threshold, fraction_to_keep, fat_margin, int(connectivity_filtering))
+        st = BandStats()
+        self._check(load().sgs_band_update(self.h, C.byref(p), C.byref(st)))
+        return st.as_dict()
+
+    def maps(self):
+        """(thin, fat, fatter) as bool[nblocks] in the container's block order."""
+        t, f, ff = (np.zeros(self.n, np.uint8) for _ in range(3))
+        self._check(load().sgs_band_maps(self.h, _ptr(t), _ptr(f), _ptr(ff)))
+        return t != 0, f != 0, ff != 0

@@ -11,7 +11,9 @@ tree) and records their outputs here:
 * spgrid_order.npz: block bases and the page order the reference's page map
   iterates them in, for several grids;
 * spgrid_offsets.npz: element offsets and the (4,4,8)-origin level maps;
-* stiffness_tables.npy: K_mu, K_la, Km_cell, Kl_cell.
+* stiffness_tables.npy: K_mu, K_la, Km_cell, Kl_cell;
+* driver_order.npz: block bases and the order of the optimizer driver's 4x4x4
+  page map (the lists its thin/fat/fatter maps hold).
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -76,6 +78,21 @@ def main() -> None:
         run(spgrid, "tables", tf)
         tables = np.fromfile(tf, np.float64).reshape(4, 576)
         np.save(os.path.join(HERE, "stiffness_tables.npy"), tables)
+
+        # block order of the optimizer driver's 4x4x4 grid (its page-map lists)
+        rng4 = np.random.default_rng(20181202)
+        order4 = {}
+        for case, (size, n) in enumerate(((64, 60), (512, 3000))):
+            b = rng4.integers(2, size // 4 - 2, (n, 3))
+            bases = np.unique(b * 4, axis=0)
+            bases = bases[rng4.permutation(len(bases))].astype(np.int32)
+            cf = os.path.join(tmp, "c4.txt")
+            np.savetxt(cf, bases, fmt="%d")
+            out = np.loadtxt(run(spgrid, "order4", str(size), cf).splitlines(), dtype=np.int32).reshape(-1, 3)
+            order4[f"size{case}"] = np.array([size])
+            order4[f"bases{case}"] = bases
+            order4[f"ordered{case}"] = out
+        np.savez_compressed(os.path.join(HERE, "driver_order.npz"), **order4)
     print("golden fixtures written to", HERE)
 
 
