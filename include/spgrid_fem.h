@@ -262,6 +262,24 @@ SGS_API int sgs_band_update(sgs_band* b, const sgs_band_params* params, sgs_band
 /* Copy the maps out, one byte per container block; any pointer may be NULL. */
 SGS_API int sgs_band_maps(sgs_band* b, uint8_t* thin, uint8_t* fat, uint8_t* fatter);
 
+/* The driver's iteration on a band.  A session holds the fatter blocks as the
+ * driver packs them into FEMInputs (spgrid_topo_opt.cpp:1068-1160): its input
+ * block i is container block container_block[i], its cells hold max(density,
+ * DBL_MIN) in the container cells of fat blocks and 0 elsewhere.
+ * sgs_band_attach checks that and binds the two; build a new session (and
+ * attach it) whenever an update changes the fat map.
+ * sgs_band_step then runs Opt::iterate after its page-map update
+ * (spgrid_topo_opt.cpp:1301-1330): clear_gradients over the fat blocks, the
+ * solve, the compliance sensitivity of the fat container cells
+ * (minimal_compliance.cpp:74-146), smooth_dc over the fat blocks (:527-579,
+ * neighbours read from the whole container, stale values included), the OC
+ * update over the fat container cells with the volume target taken against all
+ * container cells (optimality_criterion.cpp:19-145; fixed cells from
+ * SGS_CELL_FIXED), and the session's new stiffness scales.  The densities stay
+ * on the band (sgs_band_get_density). */
+SGS_API int sgs_band_attach(sgs_band* b, sgs_session* s, const int64_t* container_block);
+SGS_API int sgs_band_step(sgs_band* b, sgs_session* s, const sgs_design_params* params, sgs_design_result* result);
+
 #ifdef __cplusplus
 }
 #endif

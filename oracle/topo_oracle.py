@@ -236,3 +236,77 @@ def update_page_maps(base, density, flags, fat_prev, *, minimum_density: float =
                  fatter_blocks=int(fatter.sum()),
                  active_voxels=int(np.count_nonzero((inside & (dens > active_threshold))[fatter])))
     return thin, fat, fatter, stats
+
+
+# ---------------------------------------------------------------------------
+# The optimizer step on a band (container state + fat map)
+# ---------------------------------------------------------------------------
+def band_filter(base, resolution, flags, fat, rho, dc0, filter_size: float = 1.5) -> np.ndarray:
+    """Opt::smooth_dc over the fat blocks (spgrid_topo_opt.cpp:527-579): every
+    neighbour inside the container counts with its stored dc0 and density, also
+    outside the fat map.  Returns dc0 after the swap: filtered on the container
+    cells of fat blocks, unchanged elsewhere (other cells of fat blocks get 0;
+    nothing reads them)."""
+    base = np.asarray(base, np.int64)
+    flg = np.asarray(flags, np.uint8).reshape(-1, 64)
+    inside = (flg & CELL_INSIDE) != 0
+    R = _dense(base, resolution, np.asarray(rho, np.float64))
+    D = _dense(base, resolution, np.asarray(dc0, np.float64))
+    INS = _dense(base, resolution, inside.astype(np.float64))
+    half = int(math.floor(filter_size))
+    pad = half + 1
+    Rp, Dp, Ip = np.pad(R, pad), np.pad(D, pad), np.pad(INS, pad)
+    s = np.zeros_like(R)
+    ws = np.zeros_like(R)
+    X, Y, Z = R.shape
+    for dx in range(-half, half + 1):
+        for dy in range(-half, half + 1):
+            for dz in range(-half, half + 1):
+                w = max(0.0, filter_size - math.sqrt(dx * dx + dy * dy + dz * dz))
+                sl = (slice(pad + dx, pad + dx + X), slice(pad + dy, pad + dy + Y), slice(pad + dz, pad + dz + Z))
+                s += (w * Dp[sl]) * Rp[sl] * Ip[sl]
+                ws += w * Ip[sl]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out = _gather(base, s / (ws * (R + 1e-3)))
+    res = np.array(dc0, np.float64, copy=True).reshape(-1, 64)
+    fat = np.asarray(fat, bool)
+    res[fat] = np.where(inside[fat], out[fat], 0.0)
+    return res
+
+
+def band_oc(flags, fat, rho, dc0, total_inside: int, volume_fraction: float, step_limit: float = 0.2,
+            minimum_density: float = 0.0, fixed_density: float = 1.0, smart_oc: bool = False,
+            exclude_fixed: bool = True):
+    """OptimalityCriterion::optimize over the container cells of the fat blocks
+    with the volume target against all container cells
+    (optimality_criterion.cpp:19-145).  Returns (new density, multiplier, change)."""
+    flg = np.asarray(flags, np.uint8).reshape(-1, 64)
+    rho = np.asarray(rho, np.float64).reshape(-1, 64)
+    dc0 = np.asarray(dc0, np.float64).reshape(-1, 64)
+    sel = np.asarray(fat, bool)[:, None] & ((flg & CELL_INSIDE) != 0)
+    fx = ((flg & CELL_FIXED) != 0)[sel]
+    neg_dc_min = float(np.min(-dc0[sel])) if (smart_oc and sel.any()) else 1e30
+    shift = min(0.0, neg_dc_min)
+    nfix = int(np.count_nonzero(fx)) if exclude_fixed else 0
+    target = float(volume_fraction) * float(total_inside - nfix)
+    old = rho[sel]
+
+    def trial(mid):
+        nd = old * np.sqrt(np.maximum(0.0, -dc0[sel] - shift) / mid)
+        nd = np.minimum(np.maximum(nd, old - step_limit), old + step_limit)
+        nd = np.minimum(np.maximum(nd, minimum_density), 1.0)
+        nd = np.where(fx, fixed_density, nd)
+        return nd, float(np.sum(nd[~fx] if exclude_fixed else nd))
+
+    lower, upper, mid = 1e-20, 1e20, 0.0
+    while lower * (1 + 1e-7) < upper:
+        mid = 0.5 * (lower + upper)
+        if trial(mid)[1] > target:
+            lower = mid
+        else:
+            upper = mid
+    nd, _ = trial(mid)
+    out = rho.copy()
+    out[sel] = nd
+    change = float(np.max(np.abs(nd - old))) if nd.size else 0.0
+    return out, mid, change

@@ -254,9 +254,9 @@ __global__ void band_count_kernel(long n, const uint8_t* __restrict__ thin, cons
 
 }  // namespace
 
-Band::Band(const int32_t* base_h, int64_t nblocks, const int32_t res[3], const uint8_t* flags_h,
+Band::Band(const int32_t* base_h_in, int64_t nblocks, const int32_t res[3], const uint8_t* flags_h,
            const double* density_h) {
-  if (nblocks <= 0 || !base_h || !res || !flags_h || !density_h) throw CudaError("empty container", SGS_ERR_INPUT);
+  if (nblocks <= 0 || !base_h_in || !res || !flags_h || !density_h) throw CudaError("empty container", SGS_ERR_INPUT);
   n = long(nblocks);
   for (int v = 0; v < 3; ++v) {
     if (res[v] <= 0) throw CudaError("resolution must be positive", SGS_ERR_INPUT);
@@ -267,7 +267,7 @@ Band::Band(const int32_t* base_h, int64_t nblocks, const int32_t res[3], const u
   for (long b = 0; b < n; ++b) {
     int bi[3];
     for (int v = 0; v < 3; ++v) {
-      const int c = base_h[3 * b + v];
+      const int c = base_h_in[3 * b + v];
       if (c < 0 || c % 4 || c >= res[v]) throw CudaError("container block outside the grid or not 4-aligned", SGS_ERR_GRID);
       bi[v] = c >> 2;
     }
@@ -279,10 +279,12 @@ Band::Band(const int32_t* base_h, int64_t nblocks, const int32_t res[3], const u
   std::sort(keys.begin(), keys.end());
   std::vector<int32_t> order(static_cast<size_t>(n));
   for (long p = 0; p < n; ++p) order[size_t(p)] = keys[size_t(p)].second;
+  base_h.assign(base_h_in, base_h_in + 3 * n);
+  for (long c = 0; c < n * 64; ++c) total_inside += (flags_h[c] & SGS_CELL_INSIDE) ? 1 : 0;
   SGS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   SGS_CUDA(cudaEventCreate(&ev[0]));
   SGS_CUDA(cudaEventCreate(&ev[1]));
-  base.upload(base_h, size_t(n) * 3, stream);
+  base.upload(base_h_in, size_t(n) * 3, stream);
   grid.upload(g, stream);
   morton.upload(order, stream);
   flags.upload(flags_h, size_t(n) * 64, stream);
@@ -476,11 +478,6 @@ void Band::update(const sgs_band_params& prm, sgs_band_stats* st) {
 // C ABI
 // ===========================================================================
 using namespace sgs;
-
-struct sgs_band {
-  std::unique_ptr<Band> band;
-  std::string error;
-};
 
 template <typename F>
 static int band_call(sgs_band* h, F&& f) {

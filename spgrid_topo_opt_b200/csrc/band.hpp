@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -49,8 +51,20 @@ class Band {
   DevBuf<unsigned long long> counters;
   cudaEvent_t ev[2] = {nullptr, nullptr};
 
+  // the driver's optimizer state on the container, for the band step
+  std::vector<int32_t> base_h;     // host copy of the block bases
+  long total_inside = 0;           // total_container_voxels
+  DevBuf<double> dc0, dc1;         // sensitivity channels; dc0 persists outside the fat map
+  DevBuf<int32_t> sess_map;        // attached session's input block -> container block
+  const void* attached = nullptr;  // the solver sess_map belongs to
+
  private:
   void keep_fraction(double fraction_to_keep, long n_thin);
 };
 
 }  // namespace sgs
+
+struct sgs_band {
+  std::unique_ptr<sgs::Band> band;
+  std::string error;
+};

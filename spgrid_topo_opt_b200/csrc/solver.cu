@@ -689,6 +689,12 @@ class Solver {
   DevBuf<uint8_t> design_fixed;
   void design_set(const double* rho, const uint8_t* fixed);
   void design_step(const sgs_design_params& prm, sgs_design_result* out);
+  // the same iteration on a narrow band whose fatter blocks this session holds
+  void band_attach(Band& B, const int64_t* container_block);
+  void band_step(Band& B, const sgs_design_params& prm, sgs_design_result* out);
+  // new stiffness scales from the design densities (session layout, rho_s):
+  // E, the coarse operators and the bottom inverse are rebuilt on the device
+  void design_refresh(const double* rho_s);
   // dense grid of the input 4x4x4 blocks (built on first use by the filter)
   DevBuf<int> in_grid, in_base_d;
   int in_gdim[3] = {0, 0, 0};
@@ -1370,8 +1376,24 @@ void Solver::design_step(const sgs_design_params& prm, sgs_design_result* out) {
   double change = 0;
   const double mid = oc_dev(design_rho.p, design_dc1.p, design_fixed.p, prm.volume_fraction, prm.step_limit,
                             prm.minimum_density, prm.fixed_density, prm.smart_oc, prm.exclude_fixed, 1, &change);
-  simp_E_kernel<<<nblk, 256, 0, stream>>>(int(nin), in_block.p, in_zoff.p, design_rho.p, P.penalty,
-                                          P.minimum_stiffness, P.minimum_density, E64.p);
+  design_refresh(design_rho.p);
+  double obj = 0;
+  for (double v : hp) obj += v;
+  if (out) {
+    out->objective = obj;
+    out->change = change;
+    out->lagrange = mid;
+    out->cg_iterations = iterations;
+    out->solve_device_seconds = solve_device_seconds;
+    out->solve_seconds = std::chrono::duration<double>(t1 - t0).count();
+    out->step_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+  }
+}
+
+void Solver::design_refresh(const double* rho_s) {
+  const long nin = long(P.in_block.size());
+  simp_E_kernel<<<blocks_for(nin * 64, 256), 256, 0, stream>>>(int(nin), in_block.p, in_zoff.p, rho_s, P.penalty,
+                                                               P.minimum_stiffness, P.minimum_density, E64.p);
   SGS_CUDA(cudaGetLastError());
   if (mixed())
     launch(convert_kernel<float, double>, blocks_for(long(P.E.size()), 256), 256, 0, E32.p, E64.p, long(P.E.size()));
@@ -1382,6 +1404,127 @@ void Solver::design_step(const sgs_design_params& prm, sgs_design_result* out) {
   build_operators();
   build_bottom();
   SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+// The session's input blocks must be the band's blocks container_block[i], in
+// order, and its material cells exactly the container cells of fat blocks (the
+// packing of spgrid_topo_opt.cpp:1068-1160).
+void Solver::band_attach(Band& B, const int64_t* container_block) {
+  const long nin = long(P.in_block.size());
+  std::vector<int32_t> map(static_cast<size_t>(nin));
+  std::vector<uint8_t> fat(static_cast<size_t>(B.n)), fl(static_cast<size_t>(B.n) * 64);
+  SGS_CUDA(cudaMemcpyAsync(fat.data(), B.fat.p, fat.size(), cudaMemcpyDeviceToHost, B.stream));
+  SGS_CUDA(cudaMemcpyAsync(fl.data(), B.flags.p, fl.size(), cudaMemcpyDeviceToHost, B.stream));
+  SGS_CUDA(cudaStreamSynchronize(B.stream));
+  for (long i = 0; i < nin; ++i) {
+    const int64_t c = container_block[i];
+    if (c < 0 || c >= B.n) throw CudaError("container block index out of range", SGS_ERR_INPUT);
+    for (int v = 0; v < 3; ++v)
+      if (B.base_h[size_t(3 * c + v)] != P.in_base[size_t(3 * i + v)])
+        throw CudaError("session block " + std::to_string(i) + " is not container block " + std::to_string(c),
+                        SGS_ERR_INPUT);
+    const int blk = P.in_block[size_t(i)];
+    for (int e = 0; e < 64; ++e) {
+      const bool material = fat[size_t(c)] && (fl[size_t(c) * 64 + e] & SGS_CELL_INSIDE);
+      const bool solid = blk >= 0 && P.E[size_t(blk) * 128 + (e >> 4) * 32 + ((e >> 2) & 3) * 8 + (e & 3) +
+                                         P.in_zoff[size_t(i)]] > 0;
+      if (material != solid)
+        throw CudaError("session material differs from the band's fat container cells", SGS_ERR_INPUT);
+    }
+    map[size_t(i)] = int32_t(c);
+  }
+  B.sess_map.upload(map, stream);
+  if (!B.dc0.p) {
+    B.dc0.alloc(size_t(B.n) * 64);
+    B.dc1.alloc(size_t(B.n) * 64);
+    B.dc0.zero(stream);
+    B.dc1.zero(stream);
+  }
+  design_scratch.alloc(size_t(nin) * 64);
+  design_dc.alloc(size_t(nin) * 64);
+  design_dc1.alloc(size_t(nin) * 64);  // element energies of the sensitivity pass
+  design_part.alloc(blocks_for(nin * 64, 256));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  B.attached = this;
+}
+
+// One iteration of the driver (Opt::iterate after its page-map update,
+// spgrid_topo_opt.cpp:1301-1330) with the design on the band: clear_gradients
+// over the fat blocks, solve, the compliance sensitivity of the fat container
+// cells, smooth_dc over the fat blocks, the OC update over the fat container
+// cells against total_container_voxels, and the new stiffness scales.
+void Solver::band_step(Band& B, const sgs_design_params& prm, sgs_design_result* out) {
+  if (B.attached != this) throw CudaError("the band is not attached to this session", SGS_ERR_INPUT);
+  const long nin = long(P.in_block.size()), ns = nin * 64, nc = B.n * 64;
+  const auto t0 = std::chrono::steady_clock::now();
+  // the band's updates ran on its own stream; the step runs on the solver's
+  SGS_CUDA(cudaStreamSynchronize(B.stream));
+  P.tolerance = prm.tolerance;
+  solve();
+  const auto t1 = std::chrono::steady_clock::now();
+  const unsigned gs = blocks_for(ns, 256), gc = blocks_for(nc, 256);
+  band_clear_kernel<<<gc, 256, 0, stream>>>(nc, B.fat.p, B.dc0.p);
+  band_gather_kernel<<<gs, 256, 0, stream>>>(ns, B.sess_map.p, B.fat.p, B.flags.p, B.rho.p, design_scratch.p);
+  sensitivity_kernel<<<gs, 256, 0, stream>>>(int(nin), in_block.p, in_zoff.p, L64[0]->nbr.p, x.p, N0(),
+                                             design_scratch.p, P.penalty, P.minimum_stiffness, design_dc.p,
+                                             design_dc1.p, design_part.p);
+  band_scatter_dc_kernel<<<gs, 256, 0, stream>>>(ns, B.sess_map.p, design_scratch.p, design_dc.p, B.dc0.p);
+  SGS_CUDA(cudaGetLastError());
+  std::vector<double> hp(gs);
+  SGS_CUDA(cudaMemcpyAsync(hp.data(), design_part.p, gs * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  band_filter_kernel<<<gc, 256, 0, stream>>>(nc, B.base.p, B.grid.p, B.gdim[0], B.gdim[1], B.gdim[2], B.fat.p,
+                                             B.flags.p, B.rho.p, B.dc0.p, B.dc1.p, prm.filter_size,
+                                             int(std::floor(prm.filter_size)));
+  band_copy_kernel<<<gc, 256, 0, stream>>>(nc, B.fat.p, B.dc1.p, B.dc0.p);
+  SGS_CUDA(cudaGetLastError());
+  // OC (optimality_criterion.cpp:19-145)
+  DevBuf<double> pa, pb;
+  pa.alloc(OC_BLOCKS);
+  pb.alloc(OC_BLOCKS);
+  std::vector<double> ha(OC_BLOCKS), hb(OC_BLOCKS);
+  auto read_parts = [&] {
+    SGS_CUDA(cudaMemcpyAsync(ha.data(), pa.p, OC_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaMemcpyAsync(hb.data(), pb.p, OC_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+  };
+  band_oc_stats_kernel<<<OC_BLOCKS, OC_THREADS, 0, stream>>>(nc, B.fat.p, B.flags.p, B.dc0.p, pa.p, pb.p);
+  SGS_CUDA(cudaGetLastError());
+  read_parts();
+  double nfix = 0, neg_dc_min = 1e30;
+  for (int k = 0; k < OC_BLOCKS; ++k) {
+    nfix += ha[size_t(k)];
+    neg_dc_min = std::min(neg_dc_min, hb[size_t(k)]);
+  }
+  const double shift = prm.smart_oc ? std::min(0.0, neg_dc_min) : 0.0;
+  const double target = prm.volume_fraction * double(B.total_inside - (prm.exclude_fixed ? long(nfix) : 0));
+  auto trial = [&](double mid, double* rho_out, double* chg) {
+    band_oc_trial_kernel<<<OC_BLOCKS, OC_THREADS, 0, stream>>>(nc, B.fat.p, B.flags.p, B.rho.p, B.dc0.p, mid, shift,
+                                                               prm.step_limit, prm.minimum_density, prm.fixed_density,
+                                                               prm.exclude_fixed, rho_out, pa.p, pb.p);
+    SGS_CUDA(cudaGetLastError());
+    read_parts();
+    double sum = 0;
+    for (double v : ha) sum += v;
+    if (chg) {
+      *chg = 0;
+      for (double v : hb) *chg = std::max(*chg, v);
+    }
+    return sum;
+  };
+  double mid = 0, lower = 1e-20, upper = 1e20;
+  const double factor = 1 + 1e-7;
+  while (lower * factor < upper) {
+    mid = 0.5 * (lower + upper);
+    const double sum = trial(mid, nullptr, nullptr);
+    if (!(sum == sum)) throw CudaError("OC update produced a non-finite volume", SGS_ERR_BREAKDOWN);
+    if (sum > target) lower = mid;
+    else upper = mid;
+  }
+  double change = 0;
+  trial(mid, B.rho.p, &change);
+  band_gather_kernel<<<gs, 256, 0, stream>>>(ns, B.sess_map.p, B.fat.p, B.flags.p, B.rho.p, design_scratch.p);
+  SGS_CUDA(cudaGetLastError());
+  design_refresh(design_scratch.p);
   double obj = 0;
   for (double v : hp) obj += v;
   if (out) {
@@ -1688,6 +1831,30 @@ SGS_API int sgs_design_step(sgs_session* h, const sgs_design_params* p, sgs_desi
     h->solver->design_step(*p, r);
   } catch (const CudaError& e) {
     h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+SGS_API int sgs_band_attach(sgs_band* b, sgs_session* h, const int64_t* container_block) {
+  if (!b || !b->band || !h || !container_block || host_only(h)) return SGS_ERR_INPUT;
+  try {
+    h->solver->band_attach(*b->band, container_block);
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    b->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+SGS_API int sgs_band_step(sgs_band* b, sgs_session* h, const sgs_design_params* p, sgs_design_result* r) {
+  if (!b || !b->band || !h || !p || host_only(h)) return SGS_ERR_INPUT;
+  try {
+    h->solver->band_step(*b->band, *p, r);
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    b->error = e.what();
     return e.code;
   }
   return 0;

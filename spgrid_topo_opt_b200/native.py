@@ -26,7 +26,7 @@ EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", 
                     "sgs_filter_sensitivity", "sgs_oc_update", "sgs_design_set", "sgs_design_step",
                     "sgs_design_get", "sgs_band_create", "sgs_band_destroy", "sgs_band_last_error",
                     "sgs_band_set_density", "sgs_band_get_density", "sgs_band_set_fat", "sgs_band_update",
-                    "sgs_band_maps")
+                    "sgs_band_maps", "sgs_band_attach", "sgs_band_step")
 
 CELL_INSIDE, CELL_FORCE, CELL_FIXED = 1, 2, 4   # SGS_CELL_* (driver TopOptFlags bits 0-2)
 
@@ -138,6 +138,10 @@ def load(build_if_missing: bool = False):
     L.sgs_band_update.restype = C.c_int
     L.sgs_band_maps.argtypes = [P, P, P, P]
     L.sgs_band_maps.restype = C.c_int
+    L.sgs_band_attach.argtypes = [P, P, P]
+    L.sgs_band_attach.restype = C.c_int
+    L.sgs_band_step.argtypes = [P, P, C.POINTER(DesignParams), C.POINTER(DesignResult)]
+    L.sgs_band_step.restype = C.c_int
     _lib = L
     return L
 
@@ -425,3 +429,19 @@ class Band:
         t, f, ff = (np.zeros(self.n, np.uint8) for _ in range(3))
         self._check(load().sgs_band_maps(self.h, _ptr(t), _ptr(f), _ptr(ff)))
         return t != 0, f != 0, ff != 0
+
+    def attach(self, session: "Session", container_block: np.ndarray):
+        """Bind a session built from this band's fatter blocks: its input block i
+        is container block ``container_block[i]`` (sgs_band_attach)."""
+        idx = np.ascontiguousarray(container_block, np.int64)
+        self._check(load().sgs_band_attach(self.h, session.h, _ptr(idx)))
+
+    def step(self, session: "Session", tolerance: float = 1e-6, volume_fraction: float = 0.1,
+             step_limit: float = 0.2, filter_size: float = 1.5, minimum_density: float = 0.0,
+             fixed_density: float = 1.0, smart_oc: bool = False, exclude_fixed: bool = True) -> dict:
+        """One driver iteration on the band (sgs_band_step)."""
+        p = DesignParams(tolerance, volume_fraction, step_limit, filter_size, minimum_density, fixed_density,
+                         int(smart_oc), int(exclude_fixed))
+        r = DesignResult()
+        self._check(load().sgs_band_step(self.h, session.h, C.byref(p), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in DesignResult._fields_ if k != "reserved"}

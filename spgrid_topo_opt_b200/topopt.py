@@ -1,7 +1,7 @@
 """SIMP topology optimization on the GPU solver.
 
-One iteration follows the reference driver's Opt::iterate
-(topo_opt/spgrid_topo_opt.cpp:1289-1331) without its page-map maintenance:
+``SIMP``: one iteration follows the reference driver's Opt::iterate
+(topo_opt/spgrid_topo_opt.cpp:1289-1331) on a fixed block set:
 solve (MGPCG), compliance sensitivity (minimal_compliance.cpp:86-146, gradient
 dc0 = -dc), density-weighted filter (Opt::smooth_dc, :527-579), optimality-
 criteria update (optimality_criterion.cpp:19-145), and the new densities fed
@@ -13,8 +13,11 @@ With ``device=True`` (the default) the whole iteration runs in the library
 stiffness scales are computed there; ``device=False`` goes through the host
 arrays of the individual entry points (the same arithmetic).
 
-Command line: ``python -m spgrid_topo_opt_b200.topopt --bridge 512 128 256 --iterations 20``
-prints one JSON line per iteration.
+``BandSIMP``: the same iteration with the driver's narrow band (page maps,
+repacking of the solver input; see the class).
+
+Command line: ``python -m spgrid_topo_opt_b200.topopt --bridge 512 128 256 --iterations 20
+[--narrow-band]`` prints one JSON line per iteration.
 """
 from __future__ import annotations
 
@@ -86,6 +89,112 @@ class SIMP:
         self.session.close()
 
 
+class BandSIMP:
+    """The driver's loop with its narrow band (Opt::iterate,
+    topo_opt/spgrid_topo_opt.cpp:1289-1331, page maps included): the design
+    lives on the container (the blocks of ``inputs.density``) in a GPU band;
+    from iteration ``grid_update_start`` on, every iteration first updates the
+    thin / fat / fatter maps (sgs_band_update) and, when the fat map changed,
+    repacks the solver input from the fatter blocks as the driver does
+    (spgrid_topo_opt.cpp:1068-1160) and builds a new session; then one
+    sgs_band_step runs solve, sensitivity, filter and OC on the GPU.
+
+    Container cells are those with positive density in ``inputs``; the cells
+    around each force node carry has_force (add_force, spgrid_topo_opt.h:577-592);
+    ``fixed`` marks fixed-density cells."""
+
+    def __init__(self, inputs, *, precision: int = native.PRECISION_MIXED, tolerance: float = 1e-6,
+                 volume_fraction: float = 0.1, step_limit: float = 0.2, filter_size: float = 1.5,
+                 minimum_density: float = 0.0, fixed: Optional[np.ndarray] = None, fixed_density: float = 1.0,
+                 smart_oc: bool = False, exclude_fixed: bool = True, grid_update_start: int = 5,
+                 active_threshold: float = 1e-6, fraction_to_keep: float = 1.0, fat_margin: int = 1,
+                 connectivity_filtering: bool = True):
+        self.template = inputs
+        self.precision = precision
+        base = np.asarray(inputs.density.base, np.int32)
+        dens = np.array(inputs.density.data, np.float64, copy=True)
+        self.inside = dens > 0
+        flags = np.where(self.inside, native.CELL_INSIDE, 0).astype(np.uint8)
+        # has_force on the container cells around every force node
+        gdim = (np.asarray(inputs.resolution) + 3) // 4 + 1
+        lut = np.full(tuple(gdim), -1, np.int64)
+        lut[base[:, 0] // 4, base[:, 1] // 4, base[:, 2] // 4] = np.arange(len(base))
+        fc = np.asarray(inputs.forces["coord"], np.int64).reshape(-1, 3)
+        if len(fc):
+            corners = np.array([[a, b, c] for a in (-1, 0) for b in (-1, 0) for c in (-1, 0)])
+            cells = (fc[:, None, :] + corners[None]).reshape(-1, 3)
+            cells = cells[((cells >= 0) & (cells // 4 < gdim)).all(axis=1)]
+            blk = lut[cells[:, 0] // 4, cells[:, 1] // 4, cells[:, 2] // 4]
+            cells, blk = cells[blk >= 0], blk[blk >= 0]
+            e = (cells[:, 0] % 4) * 16 + (cells[:, 1] % 4) * 4 + cells[:, 2] % 4
+            hit = (flags[blk, e] & native.CELL_INSIDE) != 0
+            flags[blk[hit], e[hit]] |= native.CELL_FORCE
+        if fixed is not None:
+            flags |= np.where(np.asarray(fixed).reshape(flags.shape) != 0, native.CELL_FIXED, 0).astype(np.uint8)
+        self.band = native.Band(base, inputs.resolution, flags, dens)
+        self.base = base
+        self.step_params = dict(tolerance=tolerance, volume_fraction=volume_fraction, step_limit=step_limit,
+                                filter_size=filter_size, minimum_density=minimum_density,
+                                fixed_density=fixed_density, smart_oc=smart_oc, exclude_fixed=exclude_fixed)
+        self.map_params = dict(minimum_density=minimum_density, active_threshold=active_threshold,
+                               fraction_to_keep=fraction_to_keep, fat_margin=fat_margin,
+                               connectivity_filtering=connectivity_filtering)
+        self.grid_update_start = grid_update_start
+        self.iteration = 0
+        self.session = None
+        self._fat = None
+        self._pack()
+
+    def _pack(self):
+        """New solver input from the fatter blocks (spgrid_topo_opt.cpp:1068-1160)."""
+        import copy as _copy
+        from .fem_interface import BlockedGrid
+        _, fat, fatter = self.band.maps()
+        idx = np.nonzero(fatter)[0]
+        dens = self.band.density()[idx]
+        material = fat[idx, None] & self.inside[idx]
+        inp = _copy.copy(self.template)
+        inp.density = BlockedGrid(resolution=list(self.template.density.resolution), base=self.base[idx].copy(),
+                                  data=np.where(material, np.maximum(dens, DBL_MIN), 0.0))
+        inp.preserve_output(len(idx))
+        if self.session is not None:
+            self.session.close()
+        self.session = native.Session(inp, precision=self.precision)
+        self.band.attach(self.session, idx)
+        self._fat = fat
+        self.session_blocks = len(idx)
+
+    @property
+    def density(self) -> np.ndarray:
+        return self.band.density()
+
+    def iterate(self) -> dict:
+        out = {}
+        if self.iteration >= self.grid_update_start:
+            t = time.perf_counter()
+            st = self.band.update(**self.map_params)
+            _, fat, _ = self.band.maps()
+            repacked = not np.array_equal(fat, self._fat)
+            if repacked:
+                self._pack()
+            out.update(thin=st["thin_blocks"], fat=st["fat_blocks"], fatter=st["fatter_blocks"],
+                       maps_device_s=round(st["device_seconds"], 5), repacked=repacked,
+                       maps_s=round(time.perf_counter() - t, 4))
+        r = self.band.step(self.session, **self.step_params)
+        self.iteration += 1
+        out.update(objective=r["objective"], change=r["change"], lagrange=r["lagrange"],
+                   cg_iterations=r["cg_iterations"], solve_device_s=round(r["solve_device_seconds"], 4),
+                   solve_s=round(r["solve_seconds"], 4), update_s=round(r["step_seconds"], 4),
+                   session_blocks=self.session_blocks)
+        return out
+
+    def close(self):
+        if self.session is not None:
+            self.session.close()
+            self.session = None
+        self.band.close()
+
+
 def main(argv=None) -> int:
     from . import configs
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
@@ -95,15 +204,23 @@ def main(argv=None) -> int:
     ap.add_argument("--step-limit", type=float, default=0.2)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--host-loop", action="store_true", help="run the step through the host-array entry points")
+    ap.add_argument("--narrow-band", action="store_true",
+                    help="keep the driver's page maps: prune, repack and re-solve on the fatter blocks")
+    ap.add_argument("--grid-update-start", type=int, default=5)
     args = ap.parse_args(argv)
     t = time.perf_counter()
     prob = configs.bridge(*args.bridge)
     inp = configs.to_inputs(prob)
     prec = native.PRECISION_MIXED if args.precision == "mixed" else native.PRECISION_FP64
-    opt = SIMP(inp, precision=prec, volume_fraction=args.volume_fraction, step_limit=args.step_limit,
-               device=not args.host_loop)
+    if args.narrow_band:
+        opt = BandSIMP(inp, precision=prec, volume_fraction=args.volume_fraction, step_limit=args.step_limit,
+                       grid_update_start=args.grid_update_start)
+    else:
+        opt = SIMP(inp, precision=prec, volume_fraction=args.volume_fraction, step_limit=args.step_limit,
+                   device=not args.host_loop)
     print(json.dumps({"workload": prob.name, "container_cells": int(np.count_nonzero(opt.inside)),
-                      "setup_s": round(time.perf_counter() - t, 2)}), flush=True)
+                      "narrow_band": bool(args.narrow_band), "setup_s": round(time.perf_counter() - t, 2)}),
+          flush=True)
     total = time.perf_counter()
     for it in range(args.iterations):
         r = opt.iterate()
