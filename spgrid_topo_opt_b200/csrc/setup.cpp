@@ -106,6 +106,7 @@ struct Builder {
     std::vector<int32_t> coords(L.coords.size());
     std::vector<uint32_t> flags(L.flags.size());
     std::vector<double> sc(scratch.size());
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < n_all; ++i) {
       int o = order[i];
       for (int v = 0; v < 3; ++v) coords[3 * i + v] = L.coords[3 * o + v];
@@ -118,8 +119,9 @@ struct Builder {
     L.coords.swap(coords);
     L.flags.swap(flags);
     scratch.swap(sc);
-    for (auto& g : L.bgrid)
-      if (g >= 0) g = remap[g];
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < long(L.bgrid.size()); ++c)
+      if (L.bgrid[size_t(c)] >= 0) L.bgrid[size_t(c)] = remap[size_t(L.bgrid[size_t(c)])];
     L.nb = int(act.size());
     return remap;
   }
@@ -294,6 +296,8 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   // block in parallel, which writes disjoint slots unless an input block is
   // repeated: then the cells go in input order, the last write winning.
   std::vector<int32_t> in_slot(nin);
+  b0.L.coords.reserve(3 * nin);  // at most one solver page per input block
+  b0.L.flags.reserve(nin * NODES_PER_BLOCK);
   bool repeated = false;
   {
     std::vector<uint8_t> halves;
@@ -311,10 +315,14 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   }
   // material slots ride along with the blocks through the renumbering
   b0.scratch.assign(b0.L.coords.size() / 3 * NODES_PER_BLOCK, 0.0);
-  auto cell_E = [&](size_t b, int e) {
-    const double d = in.density.data[b * 64 + e];
-    return d > 0 ? (penalty ? (1 - emin) * std::pow(std::max(rho_min, d), penalty) + emin : d) : 0.0;
-  };
+  // the SIMP map of every input cell, once (fem_interface.h:343-353)
+  std::vector<double> Ein(nin * 64);
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < long(nin) * 64; ++c) {
+    const double d = in.density.data[size_t(c)];
+    Ein[size_t(c)] = d > 0 ? (penalty ? (1 - emin) * std::pow(std::max(rho_min, d), penalty) + emin : d) : 0.0;
+  }
+  auto cell_E = [&](size_t b, int e) { return Ein[b * 64 + size_t(e)]; };
   // input cell e = i*16 + j*4 + k sits at slot offset i*32 + j*8 + k from the block's slot
   auto cell_slot = [](int e) { return (e >> 4) * 32 + ((e >> 2) & 3) * 8 + (e & 3); };
 #pragma omp parallel for schedule(static) if (!repeated)
@@ -326,9 +334,24 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   long first_bad = -1;
   {
     std::vector<long> bad(nin, -1);
+    // A corner leaves the block's page only across a +face of the page, so a
+    // block needs at most the 7 pages beyond its +faces: those are tested once
+    // per block, and only a block that misses one is searched cell by cell.
 #pragma omp parallel for schedule(static)
     for (long b = 0; b < long(nin); ++b) {
       const int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
+      const bool zlast = (z & 4) != 0;  // the upper 4x4x4 half of a 4x4x8 page
+      unsigned need = 0;
+      for (int e = 0; e < 64; ++e) {
+        if (!(cell_E(size_t(b), e) * P.mu0 > 0)) continue;
+        const int ex = (e >> 4) == 3, ey = ((e >> 2) & 3) == 3, ez = zlast && (e & 3) == 3;
+        for (int n = 1; n < 8; ++n)
+          if ((!(n & 4) || ex) && (!(n & 2) || ey) && (!(n & 1) || ez)) need |= 1u << n;
+      }
+      bool ok = true;
+      for (int n = 1; n < 8 && ok; ++n)
+        if (need >> n & 1) ok = b0.test_page(x + (n >> 2) * 4, y + ((n >> 1) & 1) * 4, z + (n & 1) * 4);
+      if (ok) continue;
       for (int e = 0; e < 64 && bad[size_t(b)] < 0; ++e) {
         if (!(cell_E(size_t(b), e) * P.mu0 > 0)) continue;
         const int cx = x + (e >> 4), cy = y + ((e >> 2) & 3), cz = z + (e & 3);
@@ -392,33 +415,55 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
     }
     Builder bc;
     bc.init(sz[0], sz[1], sz[2]);
+    // The cells of a fine block map into one coarse block: a 2x2x4 patch at
+    // ((bx+4)/2, (by+4)/2, (bz+8)/2).  Per fine block (in parallel) the OR of the
+    // cell flags landing on each patch cell and the set of coarse pages the
+    // cells' corners cx + n reach: a +1 offset leaves the patch's page only on
+    // an axis where the cell is on the page's last layer (bit dx*4 + dy*2 + dz of
+    // the page offset); n = 0 is excluded for Dirichlet cells.  The blocks are
+    // then created and marked in fine-block order, as a serial pass over the
+    // cells would.
+    struct Patch {
+      uint32_t flags[16];
+      uint8_t pages;
+      bool any;
+    };
+    std::vector<Patch> patch(static_cast<size_t>(F.nb));
+#pragma omp parallel for schedule(static)
     for (int b = 0; b < F.nb; ++b) {
+      Patch& pt = patch[size_t(b)];
+      std::fill(pt.flags, pt.flags + 16, 0u);
+      pt.pages = 0;
+      pt.any = false;
       const int bx = F.coords[3 * b], by = F.coords[3 * b + 1], bz = F.coords[3 * b + 2];
       for (int e = 0; e < NODES_PER_BLOCK; ++e) {
-        uint32_t ff = F.flags[size_t(b) * NODES_PER_BLOCK + e];
+        const uint32_t ff = F.flags[size_t(b) * NODES_PER_BLOCK + e];
         if (!(ff & (F_ACTIVE_CELL | F_DIRICHLET_CELL))) continue;
-        int x = bx + (e >> 5), y = by + ((e >> 3) & 3), z = bz + (e & 7);
-        int cx = (x + BLK_X) >> 1, cy = (y + BLK_Y) >> 1, cz = (z + BLK_Z) >> 1;
-        // the pages of the corners cx + n: a +1 offset leaves the cell's page
-        // only on an axis where the cell is on the page's last layer, so each
-        // distinct page is set once (n = 0 excluded for Dirichlet cells)
+        const int cx = (bx + (e >> 5) + BLK_X) >> 1, cy = (by + ((e >> 3) & 3) + BLK_Y) >> 1,
+                  cz = (bz + (e & 7) + BLK_Z) >> 1;
         const int kx = (cx & 3) == 3, ky = (cy & 3) == 3, kz = (cz & 7) == 7;
-        auto pages = [&](bool with_self) {
-          for (int dx = 0; dx <= kx; ++dx)
-            for (int dy = 0; dy <= ky; ++dy)
-              for (int dz = 0; dz <= kz; ++dz)
-                if (with_self || dx || dy || dz || !(kx && ky && kz)) bc.set_page(cx + dx, cy + dy, cz + dz);
-        };
-        if (ff & F_ACTIVE_CELL) {
-          if (uint32_t* f = bc.flag(cx, cy, cz)) *f |= F_ACTIVE_CELL;
-          pages(true);
-        }
-        for (int v = 0; v < 3; ++v)
-          if (ff & (F_DIRICHLET_CELL_X << v)) {
-            if (uint32_t* f = bc.flag(cx, cy, cz)) *f |= (F_DIRICHLET_CELL_X << v);
-            pages(false);
-          }
+        uint8_t reach = 0;
+        for (int dx = 0; dx <= kx; ++dx)
+          for (int dy = 0; dy <= ky; ++dy)
+            for (int dz = 0; dz <= kz; ++dz) reach |= uint8_t(1u << (dx * 4 + dy * 2 + dz));
+        const uint8_t no_self = (kx && ky && kz) ? uint8_t(reach & ~1u) : reach;
+        const int l = ((e >> 5) >> 1) * 8 + (((e >> 3) & 3) >> 1) * 4 + ((e & 7) >> 1);
+        pt.flags[l] |= ff & (F_ACTIVE_CELL | F_DIRICHLET_CELL);
+        pt.pages |= (ff & F_ACTIVE_CELL) ? reach : no_self;
+        pt.any = true;
       }
+    }
+    for (int b = 0; b < F.nb; ++b) {
+      const Patch& pt = patch[size_t(b)];
+      if (!pt.any) continue;
+      const int cx0 = (F.coords[3 * b] + BLK_X) >> 1, cy0 = (F.coords[3 * b + 1] + BLK_Y) >> 1,
+                cz0 = (F.coords[3 * b + 2] + BLK_Z) >> 1;
+      if (bc.L.touch(cx0, cy0, cz0) >= 0)
+        for (int l = 0; l < 16; ++l)
+          if (pt.flags[l]) *bc.flag(cx0 + (l >> 3), cy0 + ((l >> 2) & 1), cz0 + (l & 3)) |= pt.flags[l];
+      for (int d = 0; d < 8; ++d)
+        if (pt.pages >> d & 1)
+          bc.set_page(cx0 + ((d >> 2) & 1) * BLK_X, cy0 + ((d >> 1) & 1) * BLK_Y, cz0 + (d & 1) * BLK_Z);
     }
     bc.finalize();
     P.levels.push_back(std::move(bc.L));
