@@ -278,6 +278,12 @@ SGS_API int sgs_band_maps(sgs_band* b, uint8_t* thin, uint8_t* fat, uint8_t* fat
  * SGS_CELL_FIXED), and the session's new stiffness scales.  The densities stay
  * on the band (sgs_band_get_density). */
 SGS_API int sgs_band_attach(sgs_band* b, sgs_session* s, const int64_t* container_block);
+/* Pack and build that session from the band's current maps and densities and
+ * attach it, in one call: template_blob is an FEMInputs blob whose settings,
+ * forces and Dirichlet nodes are used as they are (its density grid is
+ * ignored; an empty one keeps the blob small).  precision as for sgs_create. */
+SGS_API int sgs_band_session(sgs_band* b, const void* template_blob, int precision, sgs_session** out, char* err,
+                             int errlen);
 SGS_API int sgs_band_step(sgs_band* b, sgs_session* s, const sgs_design_params* params, sgs_design_result* result);
 
 #ifdef __cplusplus

@@ -254,9 +254,9 @@ __global__ void band_count_kernel(long n, const uint8_t* __restrict__ thin, cons
 
 }  // namespace
 
-Band::Band(const int32_t* base_h_in, int64_t nblocks, const int32_t res[3], const uint8_t* flags_h,
+Band::Band(const int32_t* base_h_in, int64_t nblocks, const int32_t res[3], const uint8_t* flags_in,
            const double* density_h) {
-  if (nblocks <= 0 || !base_h_in || !res || !flags_h || !density_h) throw CudaError("empty container", SGS_ERR_INPUT);
+  if (nblocks <= 0 || !base_h_in || !res || !flags_in || !density_h) throw CudaError("empty container", SGS_ERR_INPUT);
   n = long(nblocks);
   for (int v = 0; v < 3; ++v) {
     if (res[v] <= 0) throw CudaError("resolution must be positive", SGS_ERR_INPUT);
@@ -280,14 +280,15 @@ Band::Band(const int32_t* base_h_in, int64_t nblocks, const int32_t res[3], cons
   std::vector<int32_t> order(static_cast<size_t>(n));
   for (long p = 0; p < n; ++p) order[size_t(p)] = keys[size_t(p)].second;
   base_h.assign(base_h_in, base_h_in + 3 * n);
-  for (long c = 0; c < n * 64; ++c) total_inside += (flags_h[c] & SGS_CELL_INSIDE) ? 1 : 0;
+  flags_h.assign(flags_in, flags_in + 64 * n);
+  for (long c = 0; c < n * 64; ++c) total_inside += (flags_in[c] & SGS_CELL_INSIDE) ? 1 : 0;
   SGS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   SGS_CUDA(cudaEventCreate(&ev[0]));
   SGS_CUDA(cudaEventCreate(&ev[1]));
   base.upload(base_h_in, size_t(n) * 3, stream);
   grid.upload(g, stream);
   morton.upload(order, stream);
-  flags.upload(flags_h, size_t(n) * 64, stream);
+  flags.upload(flags_in, size_t(n) * 64, stream);
   rho.upload(density_h, size_t(n) * 64, stream);
   thin.alloc(size_t(n));
   fat.alloc(size_t(n));

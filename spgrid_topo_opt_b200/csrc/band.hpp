@@ -53,6 +53,7 @@ class Band {
 
   // the driver's optimizer state on the container, for the band step
   std::vector<int32_t> base_h;     // host copy of the block bases
+  std::vector<uint8_t> flags_h;    // host copy of the cell flags
   long total_inside = 0;           // total_container_voxels
   DevBuf<double> dc0, dc1;         // sensitivity channels; dc0 persists outside the fat map
   DevBuf<int32_t> sess_map;        // attached session's input block -> container block

@@ -1848,6 +1848,70 @@ SGS_API int sgs_band_attach(sgs_band* b, sgs_session* h, const int64_t* containe
   return 0;
 }
 
+// The driver's packing of FEMInputs from its maps (spgrid_topo_opt.cpp:1068-1160):
+// the fatter blocks in container order, max(density, DBL_MIN) in the container
+// cells of fat blocks, 0 elsewhere; everything else from the template.
+SGS_API int sgs_band_session(sgs_band* b, const void* template_blob, int precision, sgs_session** out, char* err,
+                             int errlen) {
+  if (!b || !b->band || !template_blob || !out || precision == SGS_HOST_SETUP_ONLY) return SGS_ERR_INPUT;
+  *out = nullptr;
+  Band& B = *b->band;
+  std::string msg;
+  int code = 0;
+  try {
+    FEMInputs in = decode_inputs(template_blob);
+    std::vector<uint8_t> fat(static_cast<size_t>(B.n)), fatter(static_cast<size_t>(B.n));
+    std::vector<double> rho(static_cast<size_t>(B.n) * 64);
+    SGS_CUDA(cudaMemcpyAsync(fat.data(), B.fat.p, fat.size(), cudaMemcpyDeviceToHost, B.stream));
+    SGS_CUDA(cudaMemcpyAsync(fatter.data(), B.fatter.p, fatter.size(), cudaMemcpyDeviceToHost, B.stream));
+    SGS_CUDA(cudaMemcpyAsync(rho.data(), B.rho.p, rho.size() * sizeof(double), cudaMemcpyDeviceToHost, B.stream));
+    SGS_CUDA(cudaStreamSynchronize(B.stream));
+    g_d2h_bytes += 2 * fat.size() + rho.size() * sizeof(double);
+    std::vector<int64_t> idx;
+    for (long c = 0; c < B.n; ++c)
+      if (fatter[size_t(c)]) idx.push_back(c);
+    const size_t m = idx.size();
+    in.density.base.resize(3 * m);
+    in.density.data.resize(64 * m);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < long(m); ++i) {
+      const size_t c = size_t(idx[size_t(i)]);
+      for (int v = 0; v < 3; ++v) in.density.base[3 * size_t(i) + v] = B.base_h[3 * c + v];
+      for (int e = 0; e < 64; ++e) {
+        const bool material = fat[c] && (B.flags_h[c * 64 + e] & SGS_CELL_INSIDE);
+        in.density.data[64 * size_t(i) + e] = material ? std::max(rho[c * 64 + e], DBL_MIN_D) : 0.0;
+      }
+    }
+    // FEMInputs::preserve_output (fem_interface.h:445-454)
+    in.preserved_buffer_size = (uint64_t(1) << 20) + m * (3 * 4 + 64 * 4 * 8);
+    sgs_session* h = nullptr;
+    code = session_from_inputs(in, precision, &h, &msg);
+    if (code == 0) {
+      try {
+        h->solver->band_attach(B, idx.data());
+      } catch (const CudaError& e) {
+        delete h;
+        throw;
+      }
+      *out = h;
+    }
+  } catch (const CudaError& e) {
+    msg = e.what();
+    code = e.code;
+  } catch (const WireError& e) {
+    msg = e.what();
+    code = SGS_ERR_WIRE;
+  } catch (const std::exception& e) {
+    msg = e.what();
+    code = SGS_ERR_INTERNAL;
+  }
+  if (code) {
+    set_err(err, errlen, msg);
+    b->error = msg;
+  }
+  return code;
+}
+
 SGS_API int sgs_band_step(sgs_band* b, sgs_session* h, const sgs_design_params* p, sgs_design_result* r) {
   if (!b || !b->band || !h || !p || host_only(h)) return SGS_ERR_INPUT;
   try {

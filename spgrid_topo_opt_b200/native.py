@@ -26,7 +26,7 @@ EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", 
                     "sgs_filter_sensitivity", "sgs_oc_update", "sgs_design_set", "sgs_design_step",
                     "sgs_design_get", "sgs_band_create", "sgs_band_destroy", "sgs_band_last_error",
                     "sgs_band_set_density", "sgs_band_get_density", "sgs_band_set_fat", "sgs_band_update",
-                    "sgs_band_maps", "sgs_band_attach", "sgs_band_step")
+                    "sgs_band_maps", "sgs_band_attach", "sgs_band_session", "sgs_band_step")
 
 CELL_INSIDE, CELL_FORCE, CELL_FIXED = 1, 2, 4   # SGS_CELL_* (driver TopOptFlags bits 0-2)
 
@@ -140,6 +140,8 @@ def load(build_if_missing: bool = False):
     L.sgs_band_maps.restype = C.c_int
     L.sgs_band_attach.argtypes = [P, P, P]
     L.sgs_band_attach.restype = C.c_int
+    L.sgs_band_session.argtypes = [P, P, C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
+    L.sgs_band_session.restype = C.c_int
     L.sgs_band_step.argtypes = [P, P, C.POINTER(DesignParams), C.POINTER(DesignResult)]
     L.sgs_band_step.restype = C.c_int
     _lib = L
@@ -223,6 +225,16 @@ class Session:
         self.h = h
         self.precision = precision
         self.stats: Optional[dict] = None
+
+    @classmethod
+    def _adopt(cls, handle: C.c_void_p, precision: int) -> "Session":
+        """Wrap a session the library built (no FEMInputs on the Python side)."""
+        self = cls.__new__(cls)
+        self.h = handle
+        self.inputs = None
+        self.precision = precision
+        self.stats = None
+        return self
 
     def close(self):
         if getattr(self, "h", None):
@@ -445,3 +457,16 @@ class Band:
         r = DesignResult()
         self._check(load().sgs_band_step(self.h, session.h, C.byref(p), C.byref(r)))
         return {k: getattr(r, k) for k, _ in DesignResult._fields_ if k != "reserved"}
+
+    def session(self, template, precision: int = PRECISION_MIXED) -> "Session":
+        """A session packed from the band's fatter blocks and densities, already
+        attached (sgs_band_session); ``template`` gives the solver settings and
+        boundary conditions (FEMInputs or its blob; its density grid is ignored)."""
+        blob = template if isinstance(template, (bytes, bytearray)) else fi.serialize_inputs(template)
+        buf = C.create_string_buffer(bytes(blob), len(blob))
+        h = C.c_void_p(0)
+        err = C.create_string_buffer(512)
+        rc = load().sgs_band_session(self.h, C.cast(buf, C.c_void_p), precision, C.byref(h), err, 512)
+        if rc != 0:
+            raise SolverError(rc, err.value.decode(errors="replace"))
+        return Session._adopt(h, precision)

@@ -22,6 +22,7 @@ Command line: ``python -m spgrid_topo_opt_b200.topopt --bridge 512 128 256 --ite
 from __future__ import annotations
 
 import argparse
+import copy
 import json
 import sys
 import time
@@ -133,6 +134,12 @@ class BandSIMP:
             flags |= np.where(np.asarray(fixed).reshape(flags.shape) != 0, native.CELL_FIXED, 0).astype(np.uint8)
         self.band = native.Band(base, inputs.resolution, flags, dens)
         self.base = base
+        # settings and boundary conditions for every repack; the density grid comes from the band
+        from .fem_interface import BlockedGrid, serialize_inputs
+        tmpl = copy.copy(inputs)
+        tmpl.density = BlockedGrid(resolution=list(inputs.density.resolution), base=np.zeros((0, 3), np.int32),
+                                   data=np.zeros((0, 64)))
+        self._template_blob = serialize_inputs(tmpl)
         self.step_params = dict(tolerance=tolerance, volume_fraction=volume_fraction, step_limit=step_limit,
                                 filter_size=filter_size, minimum_density=minimum_density,
                                 fixed_density=fixed_density, smart_oc=smart_oc, exclude_fixed=exclude_fixed)
@@ -146,23 +153,14 @@ class BandSIMP:
         self._pack()
 
     def _pack(self):
-        """New solver input from the fatter blocks (spgrid_topo_opt.cpp:1068-1160)."""
-        import copy as _copy
-        from .fem_interface import BlockedGrid
+        """New solver input from the fatter blocks (spgrid_topo_opt.cpp:1068-1160),
+        packed and set up by the library (sgs_band_session)."""
         _, fat, fatter = self.band.maps()
-        idx = np.nonzero(fatter)[0]
-        dens = self.band.density()[idx]
-        material = fat[idx, None] & self.inside[idx]
-        inp = _copy.copy(self.template)
-        inp.density = BlockedGrid(resolution=list(self.template.density.resolution), base=self.base[idx].copy(),
-                                  data=np.where(material, np.maximum(dens, DBL_MIN), 0.0))
-        inp.preserve_output(len(idx))
         if self.session is not None:
             self.session.close()
-        self.session = native.Session(inp, precision=self.precision)
-        self.band.attach(self.session, idx)
+        self.session = self.band.session(self._template_blob, self.precision)
         self._fat = fat
-        self.session_blocks = len(idx)
+        self.session_blocks = int(fatter.sum())
 
     @property
     def density(self) -> np.ndarray:
