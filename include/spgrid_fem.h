@@ -236,6 +236,8 @@ typedef struct sgs_band_stats {
   int64_t components;          /* 6-connected components of the thin blocks (0 when not filtered) */
   int64_t active_voxels;       /* container cells of fatter blocks above active_threshold */
   double device_seconds;       /* the update on the GPU (CUDA events) */
+  int64_t fat_changed;         /* blocks that entered or left the fat map (0: a session packed
+                                  before the update still matches) */
 } sgs_band_stats;
 
 /* Replaces the driver's container set-up of the four maps

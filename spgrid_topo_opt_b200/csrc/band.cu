@@ -18,7 +18,9 @@ namespace sgs {
 namespace {
 
 constexpr int BAND_WARPS = 8;  // warps per CTA of the warp-per-block kernels
-enum { CNT_THIN = 0, CNT_FAT, CNT_FATTER, CNT_ACTIVE, CNT_COMPONENTS, CNT_BIG, CNT_BIG_ROOT, CNT_ERROR, CNT_N };
+enum {
+  CNT_THIN = 0, CNT_FAT, CNT_FATTER, CNT_ACTIVE, CNT_COMPONENTS, CNT_BIG, CNT_BIG_ROOT, CNT_ERROR, CNT_FAT_CHANGED, CNT_N
+};
 
 // Block of the container holding the cell block (bx, by, bz), or -1.
 __device__ __forceinline__ int lookup(const int* __restrict__ grid, int gx, int gy, int gz, int bx, int by, int bz) {
@@ -230,10 +232,12 @@ __global__ void band_fatter_kernel(long n, const int* __restrict__ base, const i
   }
 }
 
-// Map sizes and the active voxels of the fatter map (:215-235).
+// Map sizes, the blocks whose fat flag changed (fat_old may be null) and the
+// active voxels of the fatter map (:215-235).
 __global__ void band_count_kernel(long n, const uint8_t* __restrict__ thin, const uint8_t* __restrict__ fat,
-                                  const uint8_t* __restrict__ fatter, const uint8_t* __restrict__ flags,
-                                  const double* __restrict__ rho, double active_threshold, unsigned long long* cnt) {
+                                  const uint8_t* __restrict__ fatter, const uint8_t* __restrict__ fat_old,
+                                  const uint8_t* __restrict__ flags, const double* __restrict__ rho,
+                                  double active_threshold, unsigned long long* cnt) {
   const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long b = long(blockIdx.x) * BAND_WARPS + wl;
   if (b >= n) return;
@@ -241,6 +245,7 @@ __global__ void band_count_kernel(long n, const uint8_t* __restrict__ thin, cons
     if (thin[b]) atomicAdd(cnt + CNT_THIN, 1ull);
     if (fat[b]) atomicAdd(cnt + CNT_FAT, 1ull);
     if (fatter[b]) atomicAdd(cnt + CNT_FATTER, 1ull);
+    if (fat_old && (fat_old[b] != 0) != (fat[b] != 0)) atomicAdd(cnt + CNT_FAT_CHANGED, 1ull);
   }
   if (!fatter[b]) return;
   int a = 0;
@@ -419,8 +424,8 @@ void Band::update(const sgs_band_params& prm, sgs_band_stats* st) {
       fail(e.what());
     }
     SGS_CUDA(cudaMemsetAsync(counters.p, 0, sizeof(unsigned long long), stream));
-    band_count_kernel<<<wgrid, 32 * BAND_WARPS, 0, stream>>>(n, thin.p, fat.p, fatter.p, flags.p, rho.p, 0.0,
-                                                              counters.p);
+    band_count_kernel<<<wgrid, 32 * BAND_WARPS, 0, stream>>>(n, thin.p, fat.p, fatter.p, nullptr, flags.p, rho.p,
+                                                              0.0, counters.p);
     SGS_CUDA(cudaGetLastError());
     read_counters();
     n_thin = long(c[CNT_THIN]);
@@ -452,8 +457,8 @@ void Band::update(const sgs_band_params& prm, sgs_band_stats* st) {
                                                         prm.active_threshold, prm.fat_margin, fat_new.p);
   band_fatter_kernel<<<tgrid, 256, 0, stream>>>(n, base.p, grid.p, gx, gy, gz, fat_new.p, fatter_new.p);
   SGS_CUDA(cudaMemsetAsync(counters.p, 0, CNT_N * sizeof(unsigned long long), stream));
-  band_count_kernel<<<wgrid, 32 * BAND_WARPS, 0, stream>>>(n, thin.p, fat_new.p, fatter_new.p, flags.p, rho.p,
-                                                            prm.active_threshold, counters.p);
+  band_count_kernel<<<wgrid, 32 * BAND_WARPS, 0, stream>>>(n, thin.p, fat_new.p, fatter_new.p, fat.p, flags.p,
+                                                            rho.p, prm.active_threshold, counters.p);
   SGS_CUDA(cudaGetLastError());
   SGS_CUDA(cudaEventRecord(ev[1], stream));
   read_counters();
@@ -469,6 +474,7 @@ void Band::update(const sgs_band_params& prm, sgs_band_stats* st) {
     st->fatter_blocks = long(c[CNT_FATTER]);
     st->components = components;
     st->active_voxels = long(c[CNT_ACTIVE]);
+    st->fat_changed = long(c[CNT_FAT_CHANGED]);
     st->device_seconds = ms * 1e-3;
   }
 }

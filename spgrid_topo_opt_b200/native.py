@@ -51,7 +51,7 @@ class BandParams(C.Structure):
 class BandStats(C.Structure):
     _fields_ = [("container_blocks", C.c_int64), ("thin_before_pruning", C.c_int64), ("thin_blocks", C.c_int64),
                 ("fat_blocks", C.c_int64), ("fatter_blocks", C.c_int64), ("components", C.c_int64),
-                ("active_voxels", C.c_int64), ("device_seconds", C.c_double)]
+                ("active_voxels", C.c_int64), ("device_seconds", C.c_double), ("fat_changed", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

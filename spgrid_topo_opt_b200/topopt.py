@@ -149,17 +149,15 @@ class BandSIMP:
         self.grid_update_start = grid_update_start
         self.iteration = 0
         self.session = None
-        self._fat = None
         self._pack()
 
     def _pack(self):
         """New solver input from the fatter blocks (spgrid_topo_opt.cpp:1068-1160),
         packed and set up by the library (sgs_band_session)."""
-        _, fat, fatter = self.band.maps()
+        _, _, fatter = self.band.maps()
         if self.session is not None:
             self.session.close()
         self.session = self.band.session(self._template_blob, self.precision)
-        self._fat = fat
         self.session_blocks = int(fatter.sum())
 
     @property
@@ -171,8 +169,7 @@ class BandSIMP:
         if self.iteration >= self.grid_update_start:
             t = time.perf_counter()
             st = self.band.update(**self.map_params)
-            _, fat, _ = self.band.maps()
-            repacked = not np.array_equal(fat, self._fat)
+            repacked = st["fat_changed"] != 0
             if repacked:
                 self._pack()
             out.update(thin=st["thin_blocks"], fat=st["fat_blocks"], fatter=st["fatter_blocks"],

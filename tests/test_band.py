@@ -126,6 +126,7 @@ def test_band_updates_match_oracle(native_lib):
         st = band.update()
         ref = torc.update_page_maps(base, dens, flags, fat_prev)
         _compare(band, ref, st)
+        assert st["fat_changed"] == int(np.count_nonzero(ref[1] != fat_prev))
         fat_prev = ref[1]
         # the design moves: some blocks fade, others regain material
         fade = rng.random(len(base)) < 0.1
