@@ -288,6 +288,38 @@ SGS_API int sgs_band_session(sgs_band* b, const void* template_blob, int precisi
                              int errlen);
 SGS_API int sgs_band_step(sgs_band* b, sgs_session* s, const sgs_design_params* params, sgs_design_result* result);
 
+/* ---- headless density renderer ------------------------------------------ */
+/* The reference's visualiser (misc/volume_rendering_kernel.cu:340-437 with
+ * misc/volume_renderer.cpp:410-480) without window, OpenGL buffer or texture
+ * unit.  The cells with positive density span the volume (their bounding box,
+ * one voxel per cell: 0 for density 0, else uchar(d * 254) + 1); camera rays
+ * are traced per pixel and `frames` jittered frames are averaged.  mode 0:
+ * surface, the first voxel above `threshold` shaded by three ambient-occlusion
+ * rays under a two-colour sky; mode 1: volume, exp(-extinction *
+ * max(0.01 * sum of 1025 jittered samples - threshold, 0)).  Random numbers
+ * come from a counter-based hash of (pixel, frame, seed).  rgba[height][width]
+ * receives (a << 24 | b << 16 | g << 8 | r), row 0 at the bottom as in the
+ * reference's pixel buffer. */
+typedef struct sgs_render_params {
+  int32_t width, height;
+  int32_t mode;            /* 0 surface, 1 volume */
+  int32_t frames;          /* >= 1, the reference's progressive sample counter */
+  float threshold;         /* surface: solid above; volume: subtracted from the integral */
+  float extinction;        /* volume only */
+  float slice;             /* cut along z: 0.99999 shows the whole volume */
+  uint32_t seed;
+  float camera[12];        /* 3x4 rows: camera-to-world rotation | eye position (c_invViewMatrix) */
+  int32_t reverse_mapping; /* 1: densities are SIMP stiffness (penalty 0): d -> (d - 1e-6)^(1/3) (1 - 1e-6) */
+  int32_t reserved;
+} sgs_render_params;
+
+/* Host arrays in the FEMInputs density layout; volume_res (may be NULL)
+ * receives the volume's size. */
+SGS_API int sgs_render(const int32_t* block_base, int64_t nblocks, const double* density, const sgs_render_params* p,
+                       uint32_t* rgba, int32_t* volume_res);
+/* The same for a band's current densities, without a host round trip. */
+SGS_API int sgs_band_render(sgs_band* b, const sgs_render_params* p, uint32_t* rgba, int32_t* volume_res);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,7 +26,8 @@ EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", 
                     "sgs_filter_sensitivity", "sgs_oc_update", "sgs_design_set", "sgs_design_step",
                     "sgs_design_get", "sgs_band_create", "sgs_band_destroy", "sgs_band_last_error",
                     "sgs_band_set_density", "sgs_band_get_density", "sgs_band_set_fat", "sgs_band_update",
-                    "sgs_band_maps", "sgs_band_attach", "sgs_band_session", "sgs_band_step")
+                    "sgs_band_maps", "sgs_band_attach", "sgs_band_session", "sgs_band_step", "sgs_render",
+                    "sgs_band_render")
 
 CELL_INSIDE, CELL_FORCE, CELL_FIXED = 1, 2, 4   # SGS_CELL_* (driver TopOptFlags bits 0-2)
 
@@ -55,6 +56,62 @@ class BandStats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("mode", C.c_int32), ("frames", C.c_int32),
+                ("threshold", C.c_float), ("extinction", C.c_float), ("slice", C.c_float), ("seed", C.c_uint32),
+                ("camera", C.c_float * 12), ("reverse_mapping", C.c_int32), ("reserved", C.c_int32)]
+
+
+def render_params(width: int, height: int, camera, mode: int = 0, frames: int = 1, threshold: float = 0.5,
+                  extinction: float = 1.0, slice_: float = 0.99999, seed: int = 0,
+                  reverse_mapping: bool = False) -> RenderParams:
+    cam = np.ascontiguousarray(camera, np.float32).reshape(12)
+    return RenderParams(width, height, mode, frames, threshold, extinction, slice_, seed,
+                        (C.c_float * 12)(*cam.tolist()), int(reverse_mapping), 0)
+
+
+def render(base: np.ndarray, density: np.ndarray, width: int, height: int, camera, **kw):
+    """Render density blocks (FEMInputs layout) on the GPU (sgs_render): returns
+    (uint32 image [height][width], volume resolution)."""
+    b = np.ascontiguousarray(base, np.int32).reshape(-1, 3)
+    d = np.ascontiguousarray(density, np.float64).reshape(-1, 64)
+    p = render_params(width, height, camera, **kw)
+    out = np.zeros((height, width), np.uint32)
+    res = np.zeros(3, np.int32)
+    rc = load().sgs_render(_ptr(b), b.shape[0], _ptr(d), C.byref(p), _ptr(out), _ptr(res))
+    if rc != 0:
+        raise SolverError(rc, "sgs_render failed")
+    return out, res
+
+
+def view_matrix(rx_deg: float = 0.0, ry_deg: float = 0.0, rz_deg: float = 0.0, tx: float = 0.0, ty: float = 0.0,
+                tz: float = -4.0) -> np.ndarray:
+    """The reference viewer's camera (misc/volume_renderer.cpp:124-146: glRotatef
+    by -rx, -ry, -rz about x, y, z, then glTranslatef by -t, on the identity;
+    default translation (0, 0, -4), :56) as the 3x4 row matrix the renderer
+    takes."""
+    def rot(axis, deg):
+        a = np.deg2rad(deg)
+        c, s = np.cos(a), np.sin(a)
+        m = np.eye(4)
+        i, j = [(1, 2), (2, 0), (0, 1)][axis]
+        m[i, i], m[i, j], m[j, i], m[j, j] = c, -s, s, c
+        return m
+    t = np.eye(4)
+    t[:3, 3] = [-tx, -ty, -tz]
+    m = rot(0, -rx_deg) @ rot(1, -ry_deg) @ rot(2, -rz_deg) @ t
+    return m[:3, :4].astype(np.float32).reshape(12)
+
+
+def write_ppm(path: str, image: np.ndarray) -> None:
+    """Save a packed RGBA image (row 0 at the bottom) as a binary PPM."""
+    img = np.asarray(image, np.uint32)[::-1]
+    rgb = np.stack([img & 0xFF, (img >> 8) & 0xFF, (img >> 16) & 0xFF], -1).astype(np.uint8)
+    with open(path, "wb") as f:
+        f.write(b"P6 %d %d 255\n" % (rgb.shape[1], rgb.shape[0]))
+        f.write(rgb.tobytes())
 
 
 class SolverError(RuntimeError):
@@ -144,6 +201,10 @@ def load(build_if_missing: bool = False):
     L.sgs_band_session.restype = C.c_int
     L.sgs_band_step.argtypes = [P, P, C.POINTER(DesignParams), C.POINTER(DesignResult)]
     L.sgs_band_step.restype = C.c_int
+    L.sgs_render.argtypes = [P, C.c_int64, P, C.POINTER(RenderParams), P, P]
+    L.sgs_render.restype = C.c_int
+    L.sgs_band_render.argtypes = [P, C.POINTER(RenderParams), P, P]
+    L.sgs_band_render.restype = C.c_int
     _lib = L
     return L
 
@@ -470,3 +531,11 @@ class Band:
         if rc != 0:
             raise SolverError(rc, err.value.decode(errors="replace"))
         return Session._adopt(h, precision)
+
+    def render(self, width: int, height: int, camera, **kw):
+        """Render the band's current densities (sgs_band_render)."""
+        p = render_params(width, height, camera, **kw)
+        out = np.zeros((height, width), np.uint32)
+        res = np.zeros(3, np.int32)
+        self._check(load().sgs_band_render(self.h, C.byref(p), _ptr(out), _ptr(res)))
+        return out, res

@@ -202,6 +202,8 @@ def main(argv=None) -> int:
     ap.add_argument("--narrow-band", action="store_true",
                     help="keep the driver's page maps: prune, repack and re-solve on the fatter blocks")
     ap.add_argument("--grid-update-start", type=int, default=5)
+    ap.add_argument("--render", metavar="PPM", help="render the final design (surface mode) into a PPM image")
+    ap.add_argument("--render-size", type=int, nargs=2, default=[640, 360], metavar=("W", "H"))
     args = ap.parse_args(argv)
     t = time.perf_counter()
     prob = configs.bridge(*args.bridge)
@@ -224,6 +226,18 @@ def main(argv=None) -> int:
     rho = opt.density
     print(json.dumps({"iterations": args.iterations, "total_s": round(time.perf_counter() - total, 2),
                       "volume": float(rho[opt.inside].mean())}), flush=True)
+    if args.render:
+        t = time.perf_counter()
+        cam = native.view_matrix(20, -35, 0, 0, 0, -3.0)
+        kw = dict(mode=0, frames=16, threshold=0.5)
+        w, h = args.render_size
+        if isinstance(opt, BandSIMP):
+            img, res = opt.band.render(w, h, cam, **kw)
+        else:
+            img, res = native.render(inp.density.base, rho, w, h, cam, **kw)
+        native.write_ppm(args.render, img)
+        print(json.dumps({"render": args.render, "volume_res": res.tolist(),
+                          "render_s": round(time.perf_counter() - t, 3)}), flush=True)
     opt.close()
     return 0
 
