@@ -180,6 +180,17 @@ def flush_l2(buf):
         buf.fill_(1.0)
 
 
+def aggregate_replicas(per_step: float, dof: int, world: int, dist=None, device: str = "cuda"):
+    """Whole-job throughput of `world` independent replicas: the slowest rank's
+    seconds per step (max over ranks) and world x DOF / that time in MDOF/s."""
+    if dist is not None and world > 1:
+        import torch
+        tt = torch.tensor([per_step], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        per_step = float(tt.item())
+    return per_step, world * dof / per_step / 1e6
+
+
 def run_ours(args, rank, world):
     import torch
     from spgrid_topo_opt_b200 import fem_interface as fi
@@ -232,12 +243,7 @@ def run_ours(args, rank, world):
             dist.barrier()
     t_64, it_64, _, st_64 = timed_solves(fp64, max(2, args.steps // 2), 1)
     dof = st_mix["dof"]
-    per_step = float(np.mean(t_mix))
-    if dist:
-        tt = torch.tensor([per_step], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        per_step = float(tt.item())
-    value = world * dof / per_step / 1e6
+    per_step, value = aggregate_replicas(float(np.mean(t_mix)), dof, world, dist, "cuda")
 
     # dominant kernel: the level-0 smoothing sweep (8 colour launches); its
     # algorithmic bytes per node are u read+write (6w) + b (3w) + E (w) + flags (4 B)

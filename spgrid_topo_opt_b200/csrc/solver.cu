@@ -166,15 +166,29 @@ class Solver {
     precision = prec;
     SGS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     SGS_CUDA(cudaMallocHost(&h_scal, 16 * sizeof(double)));
-    auto t0 = std::chrono::steady_clock::now();
+    using clk = std::chrono::steady_clock;
+    auto t0 = clk::now();
+    auto mark = [&](double* slot) {
+      SGS_CUDA(cudaStreamSynchronize(stream));
+      const auto t = clk::now();
+      *slot = std::chrono::duration<double>(t - t0).count();
+      t0 = t;
+    };
+    const auto start = t0;
     upload_constants();
     build_levels();
+    mark(&setup_phase[0]);
     build_operators();
+    mark(&setup_phase[1]);
     build_bottom();
+    mark(&setup_phase[2]);
     alloc_cg();
-    SGS_CUDA(cudaStreamSynchronize(stream));
-    setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    mark(&setup_phase[3]);
+    setup_seconds = std::chrono::duration<double>(clk::now() - start).count();
   }
+  // device set-up phases: levels and lists, Galerkin operators, bottom inverse, CG vectors
+  double setup_phase[4] = {0, 0, 0, 0};
+  double host_setup_seconds = 0;
 
   void upload_constants() {
     double Kmu[8][8][3][3], Kla[8][8][3][3];
@@ -249,29 +263,51 @@ class Solver {
   // (active boundary-band) ones and clears the Dirichlet components of the
   // rest; those come last in a list, encoded as ~node.  Lists ascend, so a
   // warp's threads work on neighbouring nodes of few blocks.
+  // Built block-parallel: each block counts its entries of the 32 sub-lists
+  // (16 lists x {update, clear}), a prefix over blocks places them, and a
+  // second pass writes them, so every sub-list stays in ascending node order.
   static void colour_lists(const HostLevel& h, std::vector<int32_t>& out, int off[17]) {
-    std::vector<int32_t> upd[16], clr[16];
     std::vector<char> in_boundary(size_t(h.nb), 0);
     for (int b : h.boundary) in_boundary[size_t(b)] = 1;
-    const long N = long(h.nb) * NODES_PER_BLOCK;
-    for (long g = 0; g < N; ++g) {
+    const int nb = h.nb;
+    // sub-list of node g (or -1): 2k for updates of list k, 2k + 1 for clears
+    auto sub = [&](long g) {
       const uint32_t fl = h.flags[size_t(g)];
       const int e = int(g & 127);
       const int c = ((e >> 5) & 1) << 2 | ((e >> 3) & 1) << 1 | (e & 1);
       const bool act = fl & ACTIVE_NODE, dir = fl & (DIR_X | DIR_Y | DIR_Z);
-      if (act) upd[c].push_back(int32_t(g));
-      else if (dir) clr[c].push_back(~int32_t(g));
-      if (!in_boundary[size_t(g >> 7)]) continue;
-      if (act && (fl & BOUNDARY_NODE)) upd[8 + c].push_back(int32_t(g));
-      else if (dir) clr[8 + c].push_back(~int32_t(g));
-    }
-    out.clear();
+      int full = act ? 2 * c : (dir ? 2 * c + 1 : -1), band = -1;
+      if (in_boundary[size_t(g >> 7)]) band = (act && (fl & BOUNDARY_NODE)) ? 2 * (8 + c) : (dir ? 2 * (8 + c) + 1 : -1);
+      return std::make_pair(full, band);
+    };
+    std::vector<int32_t> cnt(size_t(nb) * 32, 0);
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < nb; ++b)
+      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+        const auto sl = sub(long(b) * NODES_PER_BLOCK + e);
+        if (sl.first >= 0) ++cnt[size_t(b) * 32 + size_t(sl.first)];
+        if (sl.second >= 0) ++cnt[size_t(b) * 32 + size_t(sl.second)];
+      }
+    // start of every (sub-list, block) slot: sub-lists in order, blocks within
+    long total = 0;
     off[0] = 0;
-    for (int k = 0; k < 16; ++k) {
-      out.insert(out.end(), upd[k].begin(), upd[k].end());
-      out.insert(out.end(), clr[k].begin(), clr[k].end());
-      off[k + 1] = int(out.size());
+    for (int l = 0; l < 32; ++l) {
+      for (int b = 0; b < nb; ++b) {
+        const int32_t c = cnt[size_t(b) * 32 + size_t(l)];
+        cnt[size_t(b) * 32 + size_t(l)] = int32_t(total);
+        total += c;
+      }
+      if (l & 1) off[l / 2 + 1] = int(total);
     }
+    out.assign(size_t(total), 0);
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < nb; ++b)
+      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+        const long g = long(b) * NODES_PER_BLOCK + e;
+        const auto sl = sub(g);
+        for (int l : {sl.first, sl.second})
+          if (l >= 0) out[size_t(cnt[size_t(b) * 32 + size_t(l)]++)] = (l & 1) ? ~int32_t(g) : int32_t(g);
+      }
   }
 
   // the packed level-0 iterate with its zero pad block, and the neighbour table naming it
@@ -289,8 +325,12 @@ class Solver {
     // the level-0 kernels index the [3][N] planes with 32-bit integers
     if (3 * long(P.levels[0].nb) * NODES_PER_BLOCK >= long(INT32_MAX))
       throw CudaError("the finest level has too many blocks for 32-bit node indices", SGS_ERR_INPUT);
-    active_nodes0 = 0;
-    for (long i = 0; i < N0(); ++i) active_nodes0 += (P.levels[0].flags[size_t(i)] & ACTIVE_NODE) ? 1 : 0;
+    long active = 0;
+    const long n0 = N0();
+    const uint32_t* fl0 = P.levels[0].flags.data();
+#pragma omp parallel for reduction(+ : active) schedule(static)
+    for (long i = 0; i < n0; ++i) active += (fl0[i] & ACTIVE_NODE) ? 1 : 0;
+    active_nodes0 = active;
     std::vector<int32_t> gsl;
     int off[17];
     colour_lists(P.levels[0], gsl, off);
@@ -1558,7 +1598,9 @@ static int session_from_inputs(const FEMInputs& in, int precision, sgs_session**
   std::unique_ptr<sgs_session> h(new sgs_session());
   h->solver.reset(new Solver());
   int code = 0;
+  const auto th = std::chrono::steady_clock::now();
   std::string m = build_problem(in, h->solver->P, &code);
+  h->solver->host_setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - th).count();
   if (!m.empty()) {
     *err = m;
     return code ? code : SGS_ERR_INPUT;
@@ -2098,6 +2140,11 @@ SGS_API void fem_solve(void* input, void* output) {
       outs.extra_doubles["initial_residual"] = st.initial_residual;
       outs.extra_doubles["final_residual"] = st.final_residual;
       outs.extra_doubles["setup_seconds"] = st.setup_seconds;
+      outs.extra_doubles["host_setup_seconds"] = h->solver->host_setup_seconds;
+      outs.extra_doubles["device_levels_seconds"] = h->solver->setup_phase[0];
+      outs.extra_doubles["device_operators_seconds"] = h->solver->setup_phase[1];
+      outs.extra_doubles["device_bottom_seconds"] = h->solver->setup_phase[2];
+      outs.extra_doubles["device_vectors_seconds"] = h->solver->setup_phase[3];
       outs.extra_doubles["solve_seconds"] = st.solve_seconds;
       if (rc) {
         outs.error_code = rc;
