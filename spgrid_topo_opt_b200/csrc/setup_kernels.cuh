@@ -307,6 +307,144 @@ __global__ void gj_store_pivot_kernel(double* M, long ld, int K, const double* _
 }
 
 // ---------------------------------------------------------------------------
+// Symmetric blocked Gauss-Jordan with 128-wide pivot panels.  The bottom matrix
+// is SPD, and after pivots 0..K-1 tile (I, J) equals the transpose of tile
+// (J, I), negated when exactly one of I, J has been pivoted.  So only the lower
+// tiles (I >= J) are updated; the panels a step needs are gathered from them:
+//   row panel  R_J = A_KJ  (J < K), A_KK, A_JK^T (J > K)
+//   col panel  C_I = A_IK  (I > K), A_KK, -A_KI^T (I < K)
+// then T = P^-1 R, lower tiles A_IJ -= C_I T_J, A_IK = -C_I P^-1 (I > K),
+// A_KJ = T_J (J < K), A_KK = P^-1.  After the last pivot the lower tiles hold
+// the lower half of M^-1 and are mirrored.  FP64 GEMM tiles of 128 x 128, a
+// thread computing 8 x 8 entries from k-chunks staged in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int SGJ = 128, SGJ_K = 16;
+
+__global__ void sgj_gather_kernel(const double* __restrict__ M, long ld, int K, double* __restrict__ R,
+                                  double* __restrict__ Cp, double* __restrict__ P) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(SGJ) * ld) return;
+  const long k0 = long(K) * SGJ;
+  {  // R[r][c], r < 128, c < ld
+    const long r = t / ld, c = t % ld, J = c / SGJ;
+    R[t] = (J <= K) ? M[(k0 + r) * ld + c] : M[c * ld + k0 + r];
+  }
+  {  // Cp[i][q], i < ld, q < 128
+    const long i = t / SGJ, q = t % SGJ, I = i / SGJ;
+    Cp[t] = (I >= K) ? M[i * ld + k0 + q] : -M[(k0 + q) * ld + i];
+  }
+  if (t < long(SGJ) * SGJ) P[t] = M[(k0 + t / SGJ) * ld + k0 + t % SGJ];
+}
+
+// One FP64 tensor-core MMA (m8n8k4): D = A B + D on an 8x8 tile, each lane
+// holding A[lane/4][lane%4], B[lane%4][lane/4] and D[lane/4][2*(lane%4) + {0,1}].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// C(tile) = alpha * A(tile rows, 0:k) * B(0:k, tile cols) + beta * C(tile) on
+// 128 x 128 tiles: eight warps of 32 x 64, k staged through shared memory in
+// chunks of 16 (register prefetch of the next chunk), FP64 MMAs.
+// lower: blockIdx.x enumerates the tiles I >= J of a square tile grid.
+constexpr int SGJ_AS = 20, SGJ_BS = 130;  // padded strides: conflict-free fragment loads
+__global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* __restrict__ A, long lda,
+                                                          const double* __restrict__ B, long ldb, double* C, long ldc,
+                                                          double alpha, double beta, int lower) {
+  __shared__ __align__(16) double As[SGJ * SGJ_AS];
+  __shared__ __align__(16) double Bs[SGJ_K * SGJ_BS];
+  long I, J;
+  if (lower) {
+    const long t = blockIdx.x;
+    long i = long((sqrt(8.0 * double(t) + 1.0) - 1.0) * 0.5);
+    while ((i + 1) * (i + 2) / 2 <= t) ++i;
+    while (i * (i + 1) / 2 > t) --i;
+    I = i;
+    J = t - i * (i + 1) / 2;
+  } else {
+    I = blockIdx.y;
+    J = blockIdx.x;
+  }
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 64;  // the warp's 32 x 64 sub-tile
+  const int fr = lane >> 2, fc = lane & 3;
+  const double* Ab = A + I * SGJ * lda;
+  const double* Bb = B + J * SGJ;
+  const int ar = tid >> 1, ak = (tid & 1) * 8;    // A chunk: row, first k
+  const int bk = tid >> 4, bc = (tid & 15) * 8;   // B chunk: k, first column
+  double2 pa[4], pb[4];
+  auto fetch = [&](int k0) {
+    const double2* a2 = reinterpret_cast<const double2*>(Ab + long(ar) * lda + k0 + ak);
+    const double2* b2 = reinterpret_cast<const double2*>(Bb + long(k0 + bk) * ldb + bc);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      pa[q] = a2[q];
+      pb[q] = b2[q];
+    }
+  };
+  double acc[4][8][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0;
+  fetch(0);
+  for (int k0 = 0; k0 < k; k0 += SGJ_K) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      *reinterpret_cast<double2*>(&As[ar * SGJ_AS + ak + 2 * q]) = pa[q];
+      *reinterpret_cast<double2*>(&Bs[bk * SGJ_BS + bc + 2 * q]) = pb[q];
+    }
+    __syncthreads();
+    if (k0 + SGJ_K < k) fetch(k0 + SGJ_K);
+#pragma unroll
+    for (int k4 = 0; k4 < SGJ_K; k4 += 4) {
+      double a[4], b[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[(wr + 8 * i + fr) * SGJ_AS + k4 + fc];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = Bs[(k4 + fc) * SGJ_BS + wc + 8 * j + fr];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double* row = C + (I * SGJ + wr + 8 * i + fr) * ldc + J * SGJ + wc + 2 * fc;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        double* p = row + 8 * j + h;
+        *p = (beta != 0 ? beta * *p : 0.0) + alpha * acc[i][j][h];
+      }
+  }
+}
+
+// mirror the lower triangle into the upper one
+__global__ void sgj_mirror_kernel(double* M, long ld) {
+  __shared__ double tile[32][33];
+  const int bx = blockIdx.x, by = blockIdx.y;  // source tile (row by, col bx), by > bx
+  if (by <= bx) {
+    if (by < bx) return;
+    // diagonal 32x32 tile: copy lower to upper in place
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+      const int j = threadIdx.x;
+      if (j > i) M[(long(by) * 32 + i) * ld + long(bx) * 32 + j] = M[(long(bx) * 32 + j) * ld + long(by) * 32 + i];
+    }
+    return;
+  }
+  for (int i = threadIdx.y; i < 32; i += blockDim.y)
+    tile[i][threadIdx.x] = M[(long(by) * 32 + i) * ld + long(bx) * 32 + threadIdx.x];
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y)
+    M[(long(bx) * 32 + i) * ld + long(by) * 32 + threadIdx.x] = tile[threadIdx.x][i];
+}
+
+// ---------------------------------------------------------------------------
 // Bottom solve (Exact_Solve, solver/MG/Multigrid_Hierarchy.h:346-372): nodes of
 // the level take b, DOF nodes then get the exact solution x = M^-1 b.
 // ---------------------------------------------------------------------------

@@ -434,7 +434,7 @@ class Solver {
       }
     bottom.ndof_nodes = int(dof_node.size());
     bottom.n = 3L * bottom.ndof_nodes;
-    bottom.ld = ((bottom.n + GJ - 1) / GJ) * GJ;
+    bottom.ld = ((bottom.n + SGJ - 1) / SGJ) * SGJ;
     const long max_dense = 24576;  // 4.8 GB of FP64
     if (bottom.n > max_dense) {
       char m[160];
@@ -460,22 +460,50 @@ class Solver {
     invert_dense(bottom.Minv.p, bottom.ld);
   }
 
+  // In-place inverse of the SPD bottom matrix (ld a multiple of SGJ): symmetric
+  // blocked Gauss-Jordan over 128-wide pivots (lower tiles only, see
+  // setup_kernels.cuh); each 128 x 128 pivot block is inverted by the 64-wide
+  // Gauss-Jordan kernels.
   void invert_dense(double* M, long ld) {
-    const int nt = int(ld / GJ);
-    DevBuf<double> pinv;
+    const int nt = int(ld / SGJ);
+    DevBuf<double> R, T, Cp, P, pinv;
+    R.alloc(size_t(SGJ) * ld);
+    T.alloc(size_t(SGJ) * ld);
+    Cp.alloc(size_t(SGJ) * ld);
+    P.alloc(size_t(SGJ) * SGJ);
     pinv.alloc(GJ * GJ);
     DevBuf<int> bad;
     bad.alloc(1);
     bad.zero(stream);
     const size_t tile_smem = 2 * GJ * 65 * sizeof(double);
     SGS_CUDA(cudaFuncSetAttribute(gj_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tile_smem)));
+    const long nel = long(SGJ) * ld;
+    const size_t row = size_t(ld) * sizeof(double);
     for (int K = 0; K < nt; ++K) {
-      gj_pivot_kernel<<<1, 256, GJ * 65 * sizeof(double), stream>>>(M, ld, K, pinv.p, bad.p);
-      gj_tile_kernel<<<nt, 256, tile_smem, stream>>>(M, ld, K, pinv.p, 0);
-      gj_tile_kernel<<<dim3(nt, nt), 256, tile_smem, stream>>>(M, ld, K, pinv.p, 1);
-      gj_tile_kernel<<<nt, 256, tile_smem, stream>>>(M, ld, K, pinv.p, 2);
-      gj_store_pivot_kernel<<<1, 256, 0, stream>>>(M, ld, K, pinv.p);
+      sgj_gather_kernel<<<blocks_for(nel, 256), 256, 0, stream>>>(M, ld, K, R.p, Cp.p, P.p);
+      for (int k = 0; k < SGJ / GJ; ++k) {  // P <- P^-1
+        gj_pivot_kernel<<<1, 256, GJ * 65 * sizeof(double), stream>>>(P.p, SGJ, k, pinv.p, bad.p);
+        gj_tile_kernel<<<SGJ / GJ, 256, tile_smem, stream>>>(P.p, SGJ, k, pinv.p, 0);
+        gj_tile_kernel<<<dim3(SGJ / GJ, SGJ / GJ), 256, tile_smem, stream>>>(P.p, SGJ, k, pinv.p, 1);
+        gj_tile_kernel<<<SGJ / GJ, 256, tile_smem, stream>>>(P.p, SGJ, k, pinv.p, 2);
+        gj_store_pivot_kernel<<<1, 256, 0, stream>>>(P.p, SGJ, k, pinv.p);
+      }
+      // T = P^-1 R; lower tiles M -= Cp T; A_IK = -Cp_I P^-1 below the pivot
+      sgj_gemm_kernel<<<dim3(nt, 1), 256, 0, stream>>>(SGJ, P.p, SGJ, R.p, ld, T.p, ld, 1.0, 0.0, 0);
+      sgj_gemm_kernel<<<unsigned(long(nt) * (nt + 1) / 2), 256, 0, stream>>>(SGJ, Cp.p, SGJ, T.p, ld, M, ld, -1.0,
+                                                                             1.0, 1);
+      if (K + 1 < nt)
+        sgj_gemm_kernel<<<dim3(1, nt - K - 1), 256, 0, stream>>>(SGJ, Cp.p + size_t(K + 1) * SGJ * SGJ, SGJ, P.p,
+                                                                 SGJ, M + size_t(K + 1) * SGJ * ld + size_t(K) * SGJ,
+                                                                 ld, -1.0, 0.0, 0);
+      // A_KJ = T_J left of the pivot, A_KK = P^-1
+      if (K > 0)
+        SGS_CUDA(cudaMemcpy2DAsync(M + size_t(K) * SGJ * ld, row, T.p, row, size_t(K) * SGJ * sizeof(double), SGJ,
+                                   cudaMemcpyDeviceToDevice, stream));
+      SGS_CUDA(cudaMemcpy2DAsync(M + size_t(K) * SGJ * ld + size_t(K) * SGJ, row, P.p, SGJ * sizeof(double),
+                                 SGJ * sizeof(double), SGJ, cudaMemcpyDeviceToDevice, stream));
     }
+    sgj_mirror_kernel<<<dim3(unsigned(ld / 32), unsigned(ld / 32)), dim3(32, 8), 0, stream>>>(M, ld);
     SGS_CUDA(cudaGetLastError());
     int hbad = 0;
     SGS_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
