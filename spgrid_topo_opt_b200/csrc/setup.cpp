@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <memory>
 #include <unordered_set>
 
 namespace sgs {
@@ -64,7 +65,6 @@ namespace {
 // active ones are renumbered into page order.
 struct Builder {
   HostLevel L;
-  std::vector<double> scratch;  // per-slot payload riding along with the blocks (E on level 0)
 
   void init(int sx, int sy, int sz) {
     L.size[0] = sx; L.size[1] = sy; L.size[2] = sz;
@@ -105,20 +105,15 @@ struct Builder {
     for (int i = 0; i < n_all; ++i) remap[order[i]] = i;
     std::vector<int32_t> coords(L.coords.size());
     std::vector<uint32_t> flags(L.flags.size());
-    std::vector<double> sc(scratch.size());
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n_all; ++i) {
       int o = order[i];
       for (int v = 0; v < 3; ++v) coords[3 * i + v] = L.coords[3 * o + v];
       std::copy(&L.flags[size_t(o) * NODES_PER_BLOCK], &L.flags[size_t(o) * NODES_PER_BLOCK] + NODES_PER_BLOCK,
                 &flags[size_t(i) * NODES_PER_BLOCK]);
-      if (!scratch.empty())
-        std::copy(&scratch[size_t(o) * NODES_PER_BLOCK], &scratch[size_t(o) * NODES_PER_BLOCK] + NODES_PER_BLOCK,
-                  &sc[size_t(i) * NODES_PER_BLOCK]);
     }
     L.coords.swap(coords);
     L.flags.swap(flags);
-    scratch.swap(sc);
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < long(L.bgrid.size()); ++c)
       if (L.bgrid[size_t(c)] >= 0) L.bgrid[size_t(c)] = remap[size_t(L.bgrid[size_t(c)])];
@@ -160,7 +155,7 @@ void flag_nodes(HostLevel& L) {
         L.touch(L.coords[3 * b] + (c >> 2) * BLK_X, L.coords[3 * b + 1] + ((c >> 1) & 1) * BLK_Y,
                 L.coords[3 * b + 2] + (c & 1) * BLK_Z);
   const int nall = int(L.coords.size() / 3);
-  std::vector<uint32_t> add(size_t(nall) * NODES_PER_BLOCK, 0u);
+  HostBuf<uint32_t> add(size_t(nall) * NODES_PER_BLOCK);  // every entry is written below
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nall; ++b) {
     int ring[27];
@@ -243,14 +238,33 @@ void flag_boundary(HostLevel& L, int band = 3) {
 }
 
 void finish_level(HostLevel& L) {
-  for (int v = 0; v < 3; ++v) L.dirichlet[v].clear();
+  // Dirichlet node lists in ascending node order: per-block counts, a prefix
+  // over the blocks, then a parallel fill
+  std::vector<int32_t> cnt(size_t(L.nb) * 3, 0);
+#pragma omp parallel for schedule(static)
   for (int b = 0; b < L.nb; ++b)
     for (int e = 0; e < NODES_PER_BLOCK; ++e) {
-      uint32_t f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
+      const uint32_t f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
+      for (int v = 0; v < 3; ++v) cnt[size_t(b) * 3 + v] += (f & (F_DIRICHLET_NODE_X << v)) ? 1 : 0;
+    }
+  for (int v = 0; v < 3; ++v) {
+    int32_t total = 0;
+    for (int b = 0; b < L.nb; ++b) {
+      const int32_t c = cnt[size_t(b) * 3 + v];
+      cnt[size_t(b) * 3 + v] = total;
+      total += c;
+    }
+    L.dirichlet[v].assign(size_t(total), 0);
+  }
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < L.nb; ++b)
+    for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+      const uint32_t f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
       for (int v = 0; v < 3; ++v)
-        if (f & (F_DIRICHLET_NODE_X << v)) L.dirichlet[v].push_back(b * NODES_PER_BLOCK + e);
+        if (f & (F_DIRICHLET_NODE_X << v)) L.dirichlet[v][size_t(cnt[size_t(b) * 3 + v]++)] = b * NODES_PER_BLOCK + e;
     }
   L.nbr.assign(size_t(L.nb) * 27, -1);
+#pragma omp parallel for schedule(static)
   for (int b = 0; b < L.nb; ++b) {
     const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
     for (int d = 0; d < 27; ++d)
@@ -313,10 +327,9 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
       halves[size_t(bk)] |= h;
     }
   }
-  // material slots ride along with the blocks through the renumbering
-  b0.scratch.assign(b0.L.coords.size() / 3 * NODES_PER_BLOCK, 0.0);
-  // the SIMP map of every input cell, once (fem_interface.h:343-353)
-  std::vector<double> Ein(nin * 64);
+  // the SIMP map of every input cell, once (fem_interface.h:343-353); the
+  // buffer is filled in parallel without a serial zero pass
+  std::unique_ptr<double[]> Ein(new double[nin * 64]);
 #pragma omp parallel for schedule(static)
   for (long c = 0; c < long(nin) * 64; ++c) {
     const double d = in.density.data[size_t(c)];
@@ -325,10 +338,6 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   auto cell_E = [&](size_t b, int e) { return Ein[b * 64 + size_t(e)]; };
   // input cell e = i*16 + j*4 + k sits at slot offset i*32 + j*8 + k from the block's slot
   auto cell_slot = [](int e) { return (e >> 4) * 32 + ((e >> 2) & 3) * 8 + (e & 3); };
-#pragma omp parallel for schedule(static) if (!repeated)
-  for (long b = 0; b < long(nin); ++b)
-    for (int e = 0; e < 64; ++e)
-      if (in.density.data[size_t(b) * 64 + e] > 0) b0.scratch[size_t(in_slot[size_t(b)] + cell_slot(e))] = cell_E(size_t(b), e);
   // Validate_With_Density (solver/CPU_Kernels/Validate_Blocks.h:311-335): every
   // material cell needs its +1 neighbour pages; the first failure in input order is reported.
   long first_bad = -1;
@@ -399,10 +408,25 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   }
   for (auto& d : in.dirichlet_nodes)
     if (d.axis < 0 || d.axis > 2) return fail(4, "Dirichlet axis out of range");
-  b0.finalize();
+  const std::vector<int32_t> remap0 = b0.finalize();
   P.levels.clear();
   P.levels.push_back(std::move(b0.L));
-  P.E.assign(b0.scratch.begin(), b0.scratch.begin() + size_t(P.levels[0].nb) * NODES_PER_BLOCK);
+  // the stiffness scale of every material cell at its slot in page order (the
+  // last input block wins where blocks repeat)
+  P.E.resize(size_t(P.levels[0].nb) * NODES_PER_BLOCK);
+  {
+    double* E = P.E.data();
+    const long nE = long(P.E.size());
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < nE; ++i) E[i] = 0.0;
+  }
+#pragma omp parallel for schedule(static) if (!repeated)
+  for (long b = 0; b < long(nin); ++b) {
+    const int32_t slot = in_slot[size_t(b)];
+    const size_t base = size_t(remap0[size_t(slot / NODES_PER_BLOCK)]) * NODES_PER_BLOCK + size_t(slot % NODES_PER_BLOCK);
+    for (int e = 0; e < 64; ++e)
+      if (in.density.data[size_t(b) * 64 + e] > 0) P.E[base + size_t(cell_slot(e))] = cell_E(size_t(b), e);
+  }
 
   // ---- coarse levels (Multigrid_Hierarchy.h:122-195)
   const int pad[3] = {2 * BLK_X, 2 * BLK_Y, 2 * BLK_Z};

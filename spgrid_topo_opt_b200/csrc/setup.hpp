@@ -11,6 +11,8 @@
 #include <array>
 #include <cstdint>
 #include <string>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "wire.hpp"
@@ -42,6 +44,30 @@ struct HostLevel {
   int touch(int x, int y, int z);                 // create a ghost block when needed
 };
 
+// A host vector whose resize leaves new elements uninitialised, so that a large
+// buffer can be zeroed and filled by parallel loops (first touch spread over
+// the threads) instead of one serial value-initialisation.
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = UninitAlloc<U>;
+  };
+  UninitAlloc() = default;
+  template <typename U>
+  UninitAlloc(const UninitAlloc<U>&) {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* p, Args&&... args) {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
+};
+template <typename T>
+using HostBuf = std::vector<T, UninitAlloc<T>>;
+
 struct Problem {
   // inputs
   int resolution[3] = {0, 0, 0};
@@ -55,7 +81,7 @@ struct Problem {
   int max_iterations = 500;
   // level data
   std::vector<HostLevel> levels;
-  std::vector<double> E;      // level-0 stiffness scale per cell slot (0 = empty)
+  HostBuf<double> E;          // level-0 stiffness scale per cell slot (0 = empty)
   // input blocks: level-0 block index and the z offset (0 or 4) inside it
   std::vector<int32_t> in_block, in_zoff;
   std::vector<int32_t> in_base;

@@ -353,7 +353,7 @@ class Solver {
         }
       }
     }
-    E64.upload(P.E, stream);
+    E64.upload(P.E.data(), P.E.size(), stream);
     if (mixed()) {
       E32.alloc(P.E.size());
       launch(convert_kernel<float, double>, blocks_for(long(P.E.size()), 256), 256, 0, E32.p, E64.p, long(P.E.size()));
@@ -771,7 +771,7 @@ class Solver {
   // the bottom inverse are rebuilt, the hierarchy and flags are kept.
   std::string update_density(const double* rho) {
     const size_t nin = P.in_block.size();
-    std::vector<double> E = P.E;
+    auto E = P.E;
     for (size_t b = 0; b < nin; ++b) {
       const int blk = P.in_block[b];
       if (blk < 0) continue;
