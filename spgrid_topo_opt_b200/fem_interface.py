@@ -316,9 +316,11 @@ def serialize_outputs(o: FEMOutputs) -> bytes:
 # Reader
 # --------------------------------------------------------------------------
 class _Reader:
-    def __init__(self, blob) -> None:
+    def __init__(self, blob, copy: bool = True) -> None:
         # any contiguous buffer (bytes, bytearray, a view of foreign memory) is
-        # read in place; arrays are copied out of it
+        # read in place; the grids are copied out of it unless copy is False,
+        # in which case they are views that keep the blob alive
+        self.copy = copy
         self.buf = memoryview(blob).cast("B")
         if len(self.buf) < 8:
             raise WireFormatError("blob shorter than its length header")
@@ -366,9 +368,13 @@ class _Reader:
         if n > (self.total - self.head) // rec.itemsize:
             raise WireFormatError("block count exceeds blob size")
         arr = np.frombuffer(self.take(n * rec.itemsize), rec, count=n)
-        data = arr["data"].copy()
+        data = arr["data"].copy() if self.copy else arr["data"]
         data = data.reshape(n, _BLOCK_VOLUME, 4) if vector else data.reshape(n, _BLOCK_VOLUME)
-        return BlockedGrid(resolution=res, base=arr["base"].copy(), data=data)
+        base = arr["base"].copy() if self.copy else arr["base"]
+        if not self.copy:
+            data.flags.writeable = False
+            base.flags.writeable = False
+        return BlockedGrid(resolution=res, base=base, data=data)
 
     def records(self, dtype: np.dtype) -> np.ndarray:
         n = self.u64()
@@ -420,8 +426,11 @@ def deserialize_inputs(blob) -> FEMInputs:
     return p
 
 
-def deserialize_outputs(blob) -> FEMOutputs:
-    r = _Reader(blob)
+def deserialize_outputs(blob, copy: bool = True) -> FEMOutputs:
+    """Decode a FEMOutputs blob.  With copy=False the displacement and residual
+    grids are read-only views into the blob (unaligned, record-strided), which
+    stays alive as long as they do."""
+    r = _Reader(blob, copy)
     o = FEMOutputs()
     _read_base(r, o)
     o.displacements = r.grid(vector=True)

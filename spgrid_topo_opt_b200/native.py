@@ -231,10 +231,32 @@ def fem_solve_blob(blob: bytes) -> bytes:
     return data
 
 
+class _LibraryBlob:
+    """An output blob allocated by the library, exposed through the buffer
+    protocol and released (fem_solve_free) when the last view of it is gone."""
+
+    def __init__(self, address: int, size: int):
+        self._address = address
+        self._array = (C.c_char * size).from_address(address)
+
+    def __buffer__(self, flags):
+        return memoryview(self._array)
+
+    def __release_buffer__(self, view):
+        view.release()
+
+    def __del__(self):
+        if getattr(self, "_address", None):
+            load().fem_solve_free(C.c_void_p(self._address))
+            self._address = None
+
+
 def fem_solve_outputs(blob: bytes):
     """``fem_solve`` on a serialized FEMInputs blob, returning the decoded
-    FEMOutputs.  The output blob is read in place before it is released, so the
-    displacement field is copied once (into the returned arrays)."""
+    FEMOutputs.  On Python 3.12+ the displacement field is a read-only view into
+    the library's output blob, which is released when the arrays are (no copy);
+    otherwise it is copied once out of the blob."""
+    import sys
     from . import fem_interface as fi
 
     L = load()
@@ -243,8 +265,10 @@ def fem_solve_outputs(blob: bytes):
     L.fem_solve(C.cast(C.c_char_p(blob), C.c_void_p), C.cast(C.pointer(out), C.c_void_p))
     if not out.value:
         raise SolverError(11, "fem_solve returned no output blob")
+    n = C.cast(out, C.POINTER(C.c_uint64))[0]
+    if sys.version_info >= (3, 12):
+        return fi.deserialize_outputs(_LibraryBlob(out.value, n), copy=False)
     try:
-        n = C.cast(out, C.POINTER(C.c_uint64))[0]
         return fi.deserialize_outputs((C.c_char * n).from_address(out.value))
     finally:
         L.fem_solve_free(out)
