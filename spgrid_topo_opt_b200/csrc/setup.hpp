@@ -44,29 +44,6 @@ struct HostLevel {
   int touch(int x, int y, int z);                 // create a ghost block when needed
 };
 
-// A host vector whose resize leaves new elements uninitialised, so that a large
-// buffer can be zeroed and filled by parallel loops (first touch spread over
-// the threads) instead of one serial value-initialisation.
-template <typename T>
-struct UninitAlloc : std::allocator<T> {
-  template <typename U>
-  struct rebind {
-    using other = UninitAlloc<U>;
-  };
-  UninitAlloc() = default;
-  template <typename U>
-  UninitAlloc(const UninitAlloc<U>&) {}
-  template <typename U>
-  void construct(U* p) noexcept {
-    ::new (static_cast<void*>(p)) U;
-  }
-  template <typename U, typename... Args>
-  void construct(U* p, Args&&... args) {
-    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
-  }
-};
-template <typename T>
-using HostBuf = std::vector<T, UninitAlloc<T>>;
 
 struct Problem {
   // inputs

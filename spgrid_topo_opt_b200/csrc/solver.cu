@@ -742,7 +742,8 @@ class Solver {
   void stage_residual();
   void record_iteration();
   void solve();
-  void pack_outputs(double* disp);
+  // displacements [nblocks][64][4] to host memory, records `pitch` bytes apart (0: packed)
+  void pack_outputs(void* disp, size_t pitch = 0);
   double sensitivity(const double* rho, double penalty, double emin, double* dc, double* se);
   void filter_sensitivity(const double* rho, const double* dc0, double* dc1, double filter_size);
   double oc_update(double* rho, const double* dc0, const uint8_t* fixed, double volume_fraction, double step_limit,
@@ -1267,12 +1268,15 @@ void Solver::solve() {
 
 // The output field, [input block][64 nodes][4] doubles, copied straight into
 // the caller's buffer.
-void Solver::pack_outputs(double* disp) {
+void Solver::pack_outputs(void* disp, size_t pitch) {
   const long nin = long(P.in_block.size());
   if (nin == 0) return;
   launch(pack_kernel, blocks_for(nin * 64, 256), 256, 0, int(nin), in_block.p, in_zoff.p, x.p, f.p, N0(), out_disp.p);
-  const size_t bytes = size_t(nin) * 256 * sizeof(double);
-  SGS_CUDA(cudaMemcpyAsync(disp, out_disp.p, bytes, cudaMemcpyDeviceToHost, stream));
+  const size_t row = 256 * sizeof(double), bytes = size_t(nin) * row;
+  if (pitch == 0 || pitch == row)
+    SGS_CUDA(cudaMemcpyAsync(disp, out_disp.p, bytes, cudaMemcpyDeviceToHost, stream));
+  else
+    SGS_CUDA(cudaMemcpy2DAsync(disp, pitch, out_disp.p, row, row, size_t(nin), cudaMemcpyDeviceToHost, stream));
   g_d2h_bytes += bytes;
   SGS_CUDA(cudaStreamSynchronize(stream));
 }
@@ -2178,27 +2182,40 @@ SGS_API void fem_solve(void* input, void* output) {
         outs.error_code = rc;
         outs.info = h->error;
       } else {
+        // The displacements go from the device straight into the output blob
+        // (a pitched copy into its records); the phase times that follow are
+        // patched into the encoded blob.
         const size_t nin = in.density.num_blocks();
         outs.displacements.base.assign(in.density.base.begin(), in.density.base.end());
-        outs.displacements.data.resize(nin * 256);
-        const auto t2 = clk::now();
-        rc = sgs_displacements(h, outs.displacements.data.data());
-        outs.extra_doubles["output_seconds"] = secs(t2, clk::now());
         outs.extra_doubles["h2d_bytes"] = double(g_h2d_bytes.load() - h2d0);
-        outs.extra_doubles["d2h_bytes"] = double(g_d2h_bytes.load() - d2h0);
+        outs.extra_doubles["d2h_bytes"] = double(g_d2h_bytes.load() - d2h0 + nin * 256 * sizeof(double));
         outs.extra_doubles["solve_device_seconds"] = st.solve_device_seconds;
+        outs.extra_doubles["output_seconds"] = 0;
+        outs.extra_doubles["teardown_seconds"] = 0;
         outs.extra_ints["kernel_launches"] = int(st.kernel_launches);
-        if (rc) {
+        outs.success = true;
+        char m[200];
+        std::snprintf(m, sizeof m, "converged in %d iterations, L-inf residual %.6g of %.6g", st.iterations,
+                      st.final_residual, st.initial_residual);
+        outs.info = m;
+        const auto t2 = clk::now();
+        char* blob = nullptr;
+        try {
+          Solver* S = h->solver.get();
+          blob = encode_outputs(outs, nullptr, [S](uint8_t* p, size_t pitch, size_t) { S->pack_outputs(p, pitch); });
+        } catch (const CudaError& e) {
           outs.displacements.base.clear();
-          outs.displacements.data.clear();
-          outs.error_code = rc;
-          outs.info = h->error;
-        } else {
-          outs.success = true;
-          char m[200];
-          std::snprintf(m, sizeof m, "converged in %d iterations, L-inf residual %.6g of %.6g", st.iterations,
-                        st.final_residual, st.initial_residual);
-          outs.info = m;
+          outs.success = false;
+          outs.error_code = e.code;
+          outs.info = e.what();
+        }
+        if (blob) {
+          patch_output_double(blob, outs, "output_seconds", secs(t2, clk::now()));
+          const auto t3 = clk::now();
+          guard.reset();
+          patch_output_double(blob, outs, "teardown_seconds", secs(t3, clk::now()));
+          *out_ptr = blob;
+          return;
         }
       }
       const auto t3 = clk::now();

@@ -30,19 +30,21 @@ class Writer {
       val(kv.second);
     }
   }
-  // records of {int base[3]; double data[64*width]}, copied block-parallel
-  void grid(const BlockedGrid& g, int width) {
+  // records of {int base[3]; double data[64*width]}, copied block-parallel;
+  // with `fill` the payloads come from it instead of g.data
+  void grid(const BlockedGrid& g, int width, const GridFill* fill = nullptr) {
     for (int v = 0; v < 3; ++v) pod<int32_t>(g.resolution[v]);
     const size_t n = g.num_blocks(), payload = sizeof(double) * 64 * size_t(width), rec = 12 + payload;
-    if (g.data.size() != n * 64 * size_t(width)) throw WireError("grid payload size mismatch");
+    if (!fill && g.data.size() != n * 64 * size_t(width)) throw WireError("grid payload size mismatch");
     count(n);
     if (dst_) {
       uint8_t* at = dst_ + pos_;
 #pragma omp parallel for schedule(static) if (n > 4096)
       for (long b = 0; b < long(n); ++b) {
         std::memcpy(at + size_t(b) * rec, &g.base[3 * size_t(b)], 12);
-        std::memcpy(at + size_t(b) * rec + 12, &g.data[size_t(b) * 64 * width], payload);
+        if (!fill) std::memcpy(at + size_t(b) * rec + 12, &g.data[size_t(b) * 64 * width], payload);
       }
+      if (fill && n) (*fill)(at + 12, rec, n);
     }
     pos_ += n * rec;
   }
@@ -265,9 +267,9 @@ std::vector<uint8_t> encode_inputs(const FEMInputs& p) {
   return out;
 }
 
-static void write_outputs(Writer& w, const FEMOutputs& o) {
+static void write_outputs(Writer& w, const FEMOutputs& o, const GridFill* fill = nullptr) {
   write_base(w, o);
-  w.grid(o.displacements, 4);
+  w.grid(o.displacements, 4, fill);
   w.grid(o.residual_field, 1);
   w.str(o.info);
   w.count(o.residuals.size());
@@ -283,6 +285,43 @@ char* encode_outputs(const FEMOutputs& o, size_t* length) {
   Writer w(reinterpret_cast<uint8_t*>(out));
   write_outputs(w, o);
   w.finish();
+  if (length) *length = sizer.size();
+  return out;
+}
+
+// Offset of the value of extra_doubles[key] in an encoded FEMOutputs blob: the
+// length header, the two version ints, extra_strings and extra_ints, then the
+// extra_doubles entries in key order (count, then length-prefixed key and value).
+static size_t output_double_offset(const FEMOutputs& o, const std::string& key) {
+  size_t pos = 8 + 4 + 4 + 8;
+  for (auto& kv : o.extra_strings) pos += 8 + kv.first.size() + 8 + kv.second.size();
+  pos += 8;
+  for (auto& kv : o.extra_ints) pos += 8 + kv.first.size() + 4;
+  pos += 8;
+  for (auto& kv : o.extra_doubles) {
+    pos += 8 + kv.first.size();
+    if (kv.first == key) return pos;
+    pos += 8;
+  }
+  throw WireError("no such output entry: " + key);
+}
+
+void patch_output_double(char* blob, const FEMOutputs& o, const std::string& key, double value) {
+  std::memcpy(blob + output_double_offset(o, key), &value, sizeof(double));
+}
+
+char* encode_outputs(const FEMOutputs& o, size_t* length, const GridFill& fill) {
+  Writer sizer;
+  write_outputs(sizer, o, &fill);
+  char* out = new char[sizer.size()];
+  try {
+    Writer w(reinterpret_cast<uint8_t*>(out));
+    write_outputs(w, o, &fill);
+    w.finish();
+  } catch (...) {
+    delete[] out;
+    throw;
+  }
   if (length) *length = sizer.size();
   return out;
 }

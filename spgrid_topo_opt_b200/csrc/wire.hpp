@@ -7,9 +7,12 @@
 // order.  The structs here keep the reference's field names.
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace sgs {
@@ -32,10 +35,34 @@ struct KrylovSolverParameters {
 
 // BlockedGrid with 4x4x4 blocks (fem_interface.h:109-160); payload per block is
 // `width` doubles per node, in-block index i*16 + j*4 + k.
+// A host vector whose resize leaves new elements uninitialised, so that a large
+// buffer can be zeroed and filled by parallel loops (first touch spread over
+// the threads) instead of one serial value-initialisation.
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = UninitAlloc<U>;
+  };
+  UninitAlloc() = default;
+  template <typename U>
+  UninitAlloc(const UninitAlloc<U>&) {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* p, Args&&... args) {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
+};
+template <typename T>
+using HostBuf = std::vector<T, UninitAlloc<T>>;
+
 struct BlockedGrid {
   int32_t resolution[3] = {0, 0, 0};
   std::vector<int32_t> base;   // [n*3]
-  std::vector<double> data;    // [n*64*width]
+  HostBuf<double> data;        // [n*64*width], filled in parallel by the codec
   size_t num_blocks() const { return base.size() / 3; }
 };
 
@@ -103,6 +130,13 @@ FEMInputs decode_inputs(const void* blob);
 // Encode outputs; the returned buffer is allocated with new char[] so that the
 // reference caller can release it with delete[] (fem_interface.h:438-441, 477).
 char* encode_outputs(const FEMOutputs& o, size_t* length);
+// The same, with the displacement payload written straight into the blob by
+// `fill` (o.displacements.base set, o.displacements.data empty):
+// fill(first record's payload, record pitch in bytes, record count).
+using GridFill = std::function<void(uint8_t*, size_t, size_t)>;
+char* encode_outputs(const FEMOutputs& o, size_t* length, const GridFill& fill);
+// Overwrite extra_doubles[key] (present in o when it was encoded) in the blob.
+void patch_output_double(char* blob, const FEMOutputs& o, const std::string& key, double value);
 // Encode inputs (used by tests and tools that drive the library from C++).
 std::vector<uint8_t> encode_inputs(const FEMInputs& p);
 FEMOutputs decode_outputs(const void* blob);
