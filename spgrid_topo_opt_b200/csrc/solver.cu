@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1268,17 +1269,50 @@ void Solver::solve() {
 
 // The output field, [input block][64 nodes][4] doubles, copied straight into
 // the caller's buffer.
+// Pinned staging for pitched read-backs, kept for the process: two halves of
+// 32 MiB, so that the copy of one chunk overlaps the host scatter of the last.
+static std::mutex g_staging_mutex;
+static char* g_staging = nullptr;
+constexpr size_t STAGING_HALF = size_t(32) << 20;
+
 void Solver::pack_outputs(void* disp, size_t pitch) {
   const long nin = long(P.in_block.size());
   if (nin == 0) return;
   launch(pack_kernel, blocks_for(nin * 64, 256), 256, 0, int(nin), in_block.p, in_zoff.p, x.p, f.p, N0(), out_disp.p);
   const size_t row = 256 * sizeof(double), bytes = size_t(nin) * row;
-  if (pitch == 0 || pitch == row)
-    SGS_CUDA(cudaMemcpyAsync(disp, out_disp.p, bytes, cudaMemcpyDeviceToHost, stream));
-  else
-    SGS_CUDA(cudaMemcpy2DAsync(disp, pitch, out_disp.p, row, row, size_t(nin), cudaMemcpyDeviceToHost, stream));
   g_d2h_bytes += bytes;
-  SGS_CUDA(cudaStreamSynchronize(stream));
+  if (pitch == 0 || pitch == row) {
+    SGS_CUDA(cudaMemcpyAsync(disp, out_disp.p, bytes, cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    return;
+  }
+  // records `pitch` bytes apart: chunks of rows through the pinned staging
+  // buffer, each scattered by the host threads while the next one is copied
+  std::lock_guard<std::mutex> lock(g_staging_mutex);
+  if (!g_staging) SGS_CUDA(cudaMallocHost(reinterpret_cast<void**>(&g_staging), 2 * STAGING_HALF));
+  const size_t rows_per = STAGING_HALF / row;
+  const size_t nchunks = (size_t(nin) + rows_per - 1) / rows_per;
+  cudaEvent_t done[2];
+  SGS_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+  SGS_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+  auto issue = [&](size_t c) {
+    const size_t r0 = c * rows_per, nr = std::min(rows_per, size_t(nin) - r0);
+    SGS_CUDA(cudaMemcpyAsync(g_staging + (c & 1) * STAGING_HALF, reinterpret_cast<const char*>(out_disp.p) + r0 * row,
+                             nr * row, cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaEventRecord(done[c & 1], stream));
+  };
+  issue(0);
+  for (size_t c = 0; c < nchunks; ++c) {
+    SGS_CUDA(cudaEventSynchronize(done[c & 1]));
+    if (c + 1 < nchunks) issue(c + 1);
+    const size_t r0 = c * rows_per, nr = std::min(rows_per, size_t(nin) - r0);
+    const char* src = g_staging + (c & 1) * STAGING_HALF;
+    char* dst = static_cast<char*>(disp) + r0 * pitch;
+#pragma omp parallel for schedule(static)
+    for (long r = 0; r < long(nr); ++r) std::memcpy(dst + size_t(r) * pitch, src + size_t(r) * row, row);
+  }
+  cudaEventDestroy(done[0]);
+  cudaEventDestroy(done[1]);
 }
 
 double Solver::sensitivity(const double* rho_host, double penalty, double emin, double* dc_host, double* se_host) {
