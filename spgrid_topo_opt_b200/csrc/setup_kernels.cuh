@@ -333,7 +333,7 @@ __global__ void sgj_gather_kernel(const double* __restrict__ M, long ld, int K, 
     const long i = t / SGJ, q = t % SGJ, I = i / SGJ;
     Cp[t] = (I >= K) ? M[i * ld + k0 + q] : -M[(k0 + q) * ld + i];
   }
-  if (t < long(SGJ) * SGJ) P[t] = M[(k0 + t / SGJ) * ld + k0 + t % SGJ];
+  if (P && t < long(SGJ) * SGJ) P[t] = M[(k0 + t / SGJ) * ld + k0 + t % SGJ];
 }
 
 // One FP64 tensor-core MMA (m8n8k4): D = A B + D on an 8x8 tile, each lane
@@ -347,21 +347,42 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 // C(tile) = alpha * A(tile rows, 0:k) * B(0:k, tile cols) + beta * C(tile) on
 // 128 x 128 tiles: eight warps of 32 x 64, k staged through shared memory in
 // chunks of 16 (register prefetch of the next chunk), FP64 MMAs.
-// lower: blockIdx.x enumerates the tiles I >= J of a square tile grid.
+// Tiles: SGJ_DENSE (blockIdx.y, blockIdx.x); SGJ_LOWER the tiles I >= J of a
+// square grid (blockIdx.x), leaving out row and column `skip` (none if < 0);
+// SGJ_CROSS the lower tiles of row and column `skip` (blockIdx.x = J for
+// J <= skip, else I).
 constexpr int SGJ_AS = 20, SGJ_BS = 130;  // padded strides: conflict-free fragment loads
+constexpr int SGJ_STAGE = SGJ * SGJ_AS + SGJ_K * SGJ_BS;  // doubles per pipeline stage
+constexpr size_t SGJ_SMEM = 2 * SGJ_STAGE * sizeof(double);
+enum { SGJ_DENSE = 0, SGJ_LOWER = 1, SGJ_CROSS = 2 };
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = unsigned(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// k staged through two shared-memory stages filled by cp.async: the copy of
+// chunk c + 1 runs while chunk c is multiplied.
 __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* __restrict__ A, long lda,
                                                           const double* __restrict__ B, long ldb, double* C, long ldc,
-                                                          double alpha, double beta, int lower) {
-  __shared__ __align__(16) double As[SGJ * SGJ_AS];
-  __shared__ __align__(16) double Bs[SGJ_K * SGJ_BS];
+                                                          double alpha, double beta, int mode, int skip) {
+  extern __shared__ __align__(16) double sg[];
   long I, J;
-  if (lower) {
+  if (mode == SGJ_LOWER) {
     const long t = blockIdx.x;
     long i = long((sqrt(8.0 * double(t) + 1.0) - 1.0) * 0.5);
     while ((i + 1) * (i + 2) / 2 <= t) ++i;
     while (i * (i + 1) / 2 > t) --i;
     I = i;
     J = t - i * (i + 1) / 2;
+    if (I == skip || J == skip) return;
+  } else if (mode == SGJ_CROSS) {
+    const long b = blockIdx.x;
+    I = b <= skip ? skip : b;
+    J = b <= skip ? b : skip;
   } else {
     I = blockIdx.y;
     J = blockIdx.x;
@@ -373,31 +394,35 @@ __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* _
   const double* Bb = B + J * SGJ;
   const int ar = tid >> 1, ak = (tid & 1) * 8;    // A chunk: row, first k
   const int bk = tid >> 4, bc = (tid & 15) * 8;   // B chunk: k, first column
-  double2 pa[4], pb[4];
-  auto fetch = [&](int k0) {
-    const double2* a2 = reinterpret_cast<const double2*>(Ab + long(ar) * lda + k0 + ak);
-    const double2* b2 = reinterpret_cast<const double2*>(Bb + long(k0 + bk) * ldb + bc);
+  auto stage = [&](int k0, int st) {
+    double* As = sg + st * SGJ_STAGE;
+    double* Bs = As + SGJ * SGJ_AS;
+    const double* a = Ab + long(ar) * lda + k0 + ak;
+    const double* b = Bb + long(k0 + bk) * ldb + bc;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      pa[q] = a2[q];
-      pb[q] = b2[q];
+      cp_async16(&As[ar * SGJ_AS + ak + 2 * q], a + 2 * q);
+      cp_async16(&Bs[bk * SGJ_BS + bc + 2 * q], b + 2 * q);
     }
+    cp_async_commit();
   };
   double acc[4][8][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0;
-  fetch(0);
-  for (int k0 = 0; k0 < k; k0 += SGJ_K) {
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      *reinterpret_cast<double2*>(&As[ar * SGJ_AS + ak + 2 * q]) = pa[q];
-      *reinterpret_cast<double2*>(&Bs[bk * SGJ_BS + bc + 2 * q]) = pb[q];
+  const int nchunks = k / SGJ_K;
+  stage(0, 0);
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) {
+      stage((c + 1) * SGJ_K, (c + 1) & 1);
+      cp_async_wait_prior();
+    } else {
+      cp_async_wait_all();
     }
     __syncthreads();
-    if (k0 + SGJ_K < k) fetch(k0 + SGJ_K);
+    const double* As = sg + (c & 1) * SGJ_STAGE;
+    const double* Bs = As + SGJ * SGJ_AS;
 #pragma unroll
     for (int k4 = 0; k4 < SGJ_K; k4 += 4) {
       double a[4], b[8];
@@ -410,6 +435,7 @@ __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* _
 #pragma unroll
         for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
+    __syncthreads();  // the stage is refilled two chunks later
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {

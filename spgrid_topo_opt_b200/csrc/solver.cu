@@ -464,46 +464,78 @@ class Solver {
   // In-place inverse of the SPD bottom matrix (ld a multiple of SGJ): symmetric
   // blocked Gauss-Jordan over 128-wide pivots (lower tiles only, see
   // setup_kernels.cuh); each 128 x 128 pivot block is inverted by the 64-wide
-  // Gauss-Jordan kernels.
+  // Gauss-Jordan kernels on a second stream, one step ahead: as soon as step K
+  // has updated the row and column of pivot K+1, that block is inverted while
+  // the rest of step K's update runs.
   void invert_dense(double* M, long ld) {
     const int nt = int(ld / SGJ);
-    DevBuf<double> R, T, Cp, P, pinv;
+    DevBuf<double> R, T, Cp, P[2], pinv;
     R.alloc(size_t(SGJ) * ld);
     T.alloc(size_t(SGJ) * ld);
     Cp.alloc(size_t(SGJ) * ld);
-    P.alloc(size_t(SGJ) * SGJ);
+    P[0].alloc(size_t(SGJ) * SGJ);
+    P[1].alloc(size_t(SGJ) * SGJ);
     pinv.alloc(GJ * GJ);
     DevBuf<int> bad;
     bad.alloc(1);
     bad.zero(stream);
     const size_t tile_smem = 2 * GJ * 65 * sizeof(double);
     SGS_CUDA(cudaFuncSetAttribute(gj_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tile_smem)));
+    SGS_CUDA(cudaFuncSetAttribute(sgj_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SGJ_SMEM)));
     const long nel = long(SGJ) * ld;
-    const size_t row = size_t(ld) * sizeof(double);
-    for (int K = 0; K < nt; ++K) {
-      sgj_gather_kernel<<<blocks_for(nel, 256), 256, 0, stream>>>(M, ld, K, R.p, Cp.p, P.p);
-      for (int k = 0; k < SGJ / GJ; ++k) {  // P <- P^-1
-        gj_pivot_kernel<<<1, 256, GJ * 65 * sizeof(double), stream>>>(P.p, SGJ, k, pinv.p, bad.p);
-        gj_tile_kernel<<<SGJ / GJ, 256, tile_smem, stream>>>(P.p, SGJ, k, pinv.p, 0);
-        gj_tile_kernel<<<dim3(SGJ / GJ, SGJ / GJ), 256, tile_smem, stream>>>(P.p, SGJ, k, pinv.p, 1);
-        gj_tile_kernel<<<SGJ / GJ, 256, tile_smem, stream>>>(P.p, SGJ, k, pinv.p, 2);
-        gj_store_pivot_kernel<<<1, 256, 0, stream>>>(P.p, SGJ, k, pinv.p);
+    const size_t row = size_t(ld) * sizeof(double), tile_row = SGJ * sizeof(double);
+    cudaStream_t aux;
+    SGS_CUDA(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    cudaEvent_t crossed, inverted;
+    SGS_CUDA(cudaEventCreateWithFlags(&crossed, cudaEventDisableTiming));
+    SGS_CUDA(cudaEventCreateWithFlags(&inverted, cudaEventDisableTiming));
+    // P <- (diagonal tile K)^-1 on stream st
+    auto invert_pivot = [&](int K, double* Pk, cudaStream_t st) {
+      SGS_CUDA(cudaMemcpy2DAsync(Pk, tile_row, M + size_t(K) * SGJ * ld + size_t(K) * SGJ, row, tile_row, SGJ,
+                                 cudaMemcpyDeviceToDevice, st));
+      for (int k = 0; k < SGJ / GJ; ++k) {
+        gj_pivot_kernel<<<1, 256, GJ * 65 * sizeof(double), st>>>(Pk, SGJ, k, pinv.p, bad.p);
+        gj_tile_kernel<<<SGJ / GJ, 256, tile_smem, st>>>(Pk, SGJ, k, pinv.p, 0);
+        gj_tile_kernel<<<dim3(SGJ / GJ, SGJ / GJ), 256, tile_smem, st>>>(Pk, SGJ, k, pinv.p, 1);
+        gj_tile_kernel<<<SGJ / GJ, 256, tile_smem, st>>>(Pk, SGJ, k, pinv.p, 2);
+        gj_store_pivot_kernel<<<1, 256, 0, st>>>(Pk, SGJ, k, pinv.p);
       }
-      // T = P^-1 R; lower tiles M -= Cp T; A_IK = -Cp_I P^-1 below the pivot
-      sgj_gemm_kernel<<<dim3(nt, 1), 256, 0, stream>>>(SGJ, P.p, SGJ, R.p, ld, T.p, ld, 1.0, 0.0, 0);
-      sgj_gemm_kernel<<<unsigned(long(nt) * (nt + 1) / 2), 256, 0, stream>>>(SGJ, Cp.p, SGJ, T.p, ld, M, ld, -1.0,
-                                                                             1.0, 1);
+    };
+    invert_pivot(0, P[0].p, stream);
+    for (int K = 0; K < nt; ++K) {
+      double* Pk = P[K & 1].p;
+      if (K > 0) SGS_CUDA(cudaStreamWaitEvent(stream, inverted, 0));
+      sgj_gather_kernel<<<blocks_for(nel, 256), 256, 0, stream>>>(M, ld, K, R.p, Cp.p, nullptr);
+      // T = P^-1 R
+      sgj_gemm_kernel<<<dim3(nt, 1), 256, SGJ_SMEM, stream>>>(SGJ, Pk, SGJ, R.p, ld, T.p, ld, 1.0, 0.0, SGJ_DENSE, -1);
+      const int next = K + 1 < nt ? K + 1 : -1;
+      if (next >= 0) {
+        // the row and column of the next pivot first, then its inverse on the side stream
+        sgj_gemm_kernel<<<nt, 256, SGJ_SMEM, stream>>>(SGJ, Cp.p, SGJ, T.p, ld, M, ld, -1.0, 1.0, SGJ_CROSS, next);
+        SGS_CUDA(cudaEventRecord(crossed, stream));
+        SGS_CUDA(cudaStreamWaitEvent(aux, crossed, 0));
+        invert_pivot(next, P[next & 1].p, aux);
+        SGS_CUDA(cudaEventRecord(inverted, aux));
+      }
+      // the other lower tiles: M -= Cp T
+      sgj_gemm_kernel<<<unsigned(long(nt) * (nt + 1) / 2), 256, SGJ_SMEM, stream>>>(SGJ, Cp.p, SGJ, T.p, ld, M, ld, -1.0,
+                                                                             1.0, SGJ_LOWER, next);
+      // A_IK = -Cp_I P^-1 below the pivot
       if (K + 1 < nt)
-        sgj_gemm_kernel<<<dim3(1, nt - K - 1), 256, 0, stream>>>(SGJ, Cp.p + size_t(K + 1) * SGJ * SGJ, SGJ, P.p,
-                                                                 SGJ, M + size_t(K + 1) * SGJ * ld + size_t(K) * SGJ,
-                                                                 ld, -1.0, 0.0, 0);
+        sgj_gemm_kernel<<<dim3(1, nt - K - 1), 256, SGJ_SMEM, stream>>>(SGJ, Cp.p + size_t(K + 1) * SGJ * SGJ, SGJ, Pk, SGJ,
+                                                                 M + size_t(K + 1) * SGJ * ld + size_t(K) * SGJ, ld,
+                                                                 -1.0, 0.0, SGJ_DENSE, -1);
       // A_KJ = T_J left of the pivot, A_KK = P^-1
       if (K > 0)
         SGS_CUDA(cudaMemcpy2DAsync(M + size_t(K) * SGJ * ld, row, T.p, row, size_t(K) * SGJ * sizeof(double), SGJ,
                                    cudaMemcpyDeviceToDevice, stream));
-      SGS_CUDA(cudaMemcpy2DAsync(M + size_t(K) * SGJ * ld + size_t(K) * SGJ, row, P.p, SGJ * sizeof(double),
-                                 SGJ * sizeof(double), SGJ, cudaMemcpyDeviceToDevice, stream));
+      SGS_CUDA(cudaMemcpy2DAsync(M + size_t(K) * SGJ * ld + size_t(K) * SGJ, row, Pk, tile_row, tile_row, SGJ,
+                                 cudaMemcpyDeviceToDevice, stream));
     }
+    SGS_CUDA(cudaStreamSynchronize(aux));
+    cudaEventDestroy(crossed);
+    cudaEventDestroy(inverted);
+    cudaStreamDestroy(aux);
     sgj_mirror_kernel<<<dim3(unsigned(ld / 32), unsigned(ld / 32)), dim3(32, 8), 0, stream>>>(M, ld);
     SGS_CUDA(cudaGetLastError());
     int hbad = 0;
