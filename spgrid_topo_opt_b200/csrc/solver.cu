@@ -238,7 +238,9 @@ class Solver {
     d.nbr.upload(h.nbr, stream);
     d.flags.upload(h.flags.data(), size_t(d.N), stream);
     std::vector<int32_t> g(h.bgrid.size());
-    for (size_t i = 0; i < g.size(); ++i) g[i] = (h.bgrid[i] >= 0 && h.bgrid[i] < h.nb) ? h.bgrid[i] : -1;
+    const long ng = long(g.size());
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < ng; ++i) g[size_t(i)] = (h.bgrid[size_t(i)] >= 0 && h.bgrid[size_t(i)] < h.nb) ? h.bgrid[size_t(i)] : -1;
     d.bgrid.upload(g, stream);
     d.grid = GridView{d.bgrid.p, h.grid[0], h.grid[1], h.grid[2]};
     d.boundary.upload(h.boundary, stream);
@@ -248,6 +250,36 @@ class Solver {
       for (auto& i : lst) i += v * int(d.N);  // index into the [3][N] planes
       d.dir[v].upload(lst, stream);
       d.ndir[v] = int(lst.size());
+    }
+    d.u.alloc(3 * d.N);
+    d.b.alloc(3 * d.N);
+    d.r.alloc(3 * d.N);
+    d.u.zero(stream);
+    d.b.zero(stream);
+    d.r.zero(stream);
+  }
+
+  // The single-precision copy of a level's index data comes from the
+  // double-precision level already on the device (device-to-device copies).
+  template <typename TD, typename TS>
+  void clone_level(Level<TD>& d, const Level<TS>& src) {
+    auto copy = [&](auto& dst, const auto& from) {
+      dst.alloc(from.n);
+      if (from.n)
+        SGS_CUDA(cudaMemcpyAsync(dst.p, from.p, from.n * sizeof(*from.p), cudaMemcpyDeviceToDevice, stream));
+    };
+    d.nb = src.nb;
+    d.N = src.N;
+    copy(d.coords, src.coords);
+    copy(d.nbr, src.nbr);
+    copy(d.flags, src.flags);
+    copy(d.bgrid, src.bgrid);
+    copy(d.boundary, src.boundary);
+    d.grid = GridView{d.bgrid.p, src.grid.gx, src.grid.gy, src.grid.gz};
+    d.nbound = src.nbound;
+    for (int v = 0; v < 3; ++v) {
+      copy(d.dir[v], src.dir[v]);
+      d.ndir[v] = src.ndir[v];
     }
     d.u.alloc(3 * d.N);
     d.b.alloc(3 * d.N);
@@ -346,9 +378,13 @@ class Solver {
       }
       if (mixed()) {
         L32.emplace_back(new Level<float>());
-        upload_level(*L32.back(), h);
+        clone_level(*L32.back(), *L64.back());
         if (first) {
-          L32.back()->gs_list.upload(gsl, stream);
+          auto& g32 = L32.back()->gs_list;
+          g32.alloc(L64.back()->gs_list.n);
+          if (g32.n)
+            SGS_CUDA(cudaMemcpyAsync(g32.p, L64.back()->gs_list.p, g32.n * sizeof(int), cudaMemcpyDeviceToDevice,
+                                     stream));
           std::copy(off, off + 17, L32.back()->gs_off);
           if (P.levels.size() > 1) alloc_packed(*L32.back(), h);
         }
