@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["shell", "band"], default="shell",
-                    help="shell: sphere shell (BASELINE config 1); band: narrow band of 8 spheres (config 4)")
+                    help="shell: 256^3 sphere shell; band: 1024^3 narrow band around 8 spheres")
     ap.add_argument("--n", type=int, default=None, help="grid size (default 256 shell, 1024 band)")
     ap.add_argument("--bottom-size", type=int, default=None)
     ap.add_argument("--cpu-sample-n", type=int, default=64, help="grid size of the CPU-baseline sample")

@@ -2,7 +2,7 @@
 
 The backward is the hand-written sensitivity kernel; it is checked against
 central finite differences of the compliance (step 1e-4, relative tolerance
-1e-4, as BASELINE config 2 asks) on seeded random cells, and against the
+1e-4) on seeded random cells, and against the
 oracle's restatement of the reference's sensitivity (minimal_compliance.cpp:86-146).
 """
 import numpy as np
