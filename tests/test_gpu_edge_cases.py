@@ -1,0 +1,92 @@
+"""Edge cases of the drop-in solve, against the oracle where it has an answer:
+no load, prescribed (non-zero) Dirichlet values, input blocks in any order
+and repeated, a single level (the exact bottom solve on level 0), and the
+iteration cap.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from spgrid_topo_opt_b200 import configs, native
+from spgrid_topo_opt_b200.fem_interface import BlockedGrid
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def test_zero_load_converges_at_once(native_lib):
+    inp = configs.to_inputs(configs.cantilever_box(16, bottom_size=4))
+    inp.forces = inp.forces[:0]
+    out = native.fem_solve(inp)
+    r = orc.Oracle(inp, mode=orc.MODE_REF).solve()
+    assert out.success and r["status"] == 0
+    assert out.extra_ints["iterations"] == r["iterations"] == 0
+    assert np.all(out.displacements.data[..., :3] == 0)
+    assert list(out.residuals) == [0.0]
+
+
+def test_prescribed_displacement(native_lib):
+    """Non-zero Dirichlet values go through the lift (SPGrid_CPU_Solver.cpp:281-341):
+    without forces the body translates rigidly by the prescribed value."""
+    inp = configs.to_inputs(configs.cantilever_box(16, bottom_size=4))
+    inp.forces = inp.forces[:0]
+    d = inp.dirichlet_nodes
+    d["value"][d["axis"] == 0] = 1e-3
+    r = orc.Oracle(inp, mode=orc.MODE_FP64, tolerance=1e-10).solve()
+    with native.Session(inp, precision=native.PRECISION_FP64) as s:
+        s.solve(tolerance=1e-10)
+        u = s.displacements()
+    assert _rel(u[..., :3], r["displacements"][..., :3]) < 1e-7
+    solid = np.asarray(inp.density.data) > 0
+    ux = u[..., 0][solid]
+    assert np.abs(ux - 1e-3).max() < 1e-9
+    assert np.abs(u[..., 1:3][solid]).max() < 1e-9
+
+
+def test_block_order_and_repeated_blocks(native_lib):
+    inp = configs.to_inputs(configs.cantilever_box(16, density=(0.2, 1.0), bottom_size=4))
+    base, data = np.asarray(inp.density.base), np.asarray(inp.density.data)
+    out0 = native.fem_solve(inp)
+    perm = np.random.default_rng(3).permutation(len(base))
+    shuffled = copy.copy(inp)
+    shuffled.density = BlockedGrid(resolution=list(inp.density.resolution), base=base[perm].copy(),
+                                   data=data[perm].copy())
+    out1 = native.fem_solve(shuffled)
+    assert out1.success and out1.extra_ints["iterations"] == out0.extra_ints["iterations"]
+    assert np.array_equal(out1.displacements.base, base[perm])
+    assert np.array_equal(out1.displacements.data, out0.displacements.data[perm])
+    # a repeated block (the later copy wins, here with the same values) changes nothing
+    rep = copy.copy(inp)
+    rep.density = BlockedGrid(resolution=list(inp.density.resolution), base=np.concatenate([base, base[:1]]),
+                              data=np.concatenate([data, data[:1]]))
+    rep.preserve_output(len(base) + 1)
+    out2 = native.fem_solve(rep)
+    assert out2.success
+    assert np.array_equal(out2.displacements.data[:-1], out0.displacements.data)
+    assert np.array_equal(out2.displacements.data[-1], out0.displacements.data[0])
+
+
+def test_single_level_is_an_exact_solve(native_lib):
+    prob = configs.cantilever_box(8, density=(0.2, 1.0), bottom_size=64)
+    inp = configs.to_inputs(prob, mg_level=1)
+    r = orc.Oracle(inp, mode=orc.MODE_FP64, tolerance=1e-12).solve()
+    with native.Session(inp, precision=native.PRECISION_FP64) as s:
+        st = s.solve(tolerance=1e-12)
+        u = s.displacements()
+    assert st["levels"] == 1
+    assert st["iterations"] <= 2 and r["iterations"] <= 2
+    assert _rel(u[..., :3], r["displacements"][..., :3]) < 1e-9
+
+
+def test_iteration_cap(native_lib):
+    inp = configs.to_inputs(configs.cantilever_box(16, bottom_size=4))
+    inp.krylov.max_iterations = 3
+    inp.extra_ints["sgs_honor_max_iterations"] = 1
+    out = native.fem_solve(inp)
+    assert out.extra_ints["iterations"] == 3
+    assert len(out.residuals) == 4
