@@ -2310,6 +2310,11 @@ SGS_API void fem_solve(void* input, void* output) {
           outs.success = false;
           outs.error_code = e.code;
           outs.info = e.what();
+        } catch (const std::exception& e) {
+          outs.displacements.base.clear();
+          outs.success = false;
+          outs.error_code = SGS_ERR_INTERNAL;
+          outs.info = e.what();
         }
         if (blob) {
           patch_output_double(blob, outs, "output_seconds", secs(t2, clk::now()));
@@ -2330,6 +2335,11 @@ SGS_API void fem_solve(void* input, void* output) {
   } catch (const std::exception& e) {
     outs.error_code = SGS_ERR_INTERNAL;
     outs.info = e.what();
+  }
+  // a failure after the displacement grid was named leaves it without payload
+  if (outs.displacements.data.size() != outs.displacements.num_blocks() * 256) {
+    outs.displacements.base.clear();
+    outs.displacements.data.clear();
   }
   try {
     *out_ptr = encode_outputs(outs, nullptr);
