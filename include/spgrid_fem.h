@@ -43,7 +43,15 @@ extern "C" {
  *   "sgs_precision"  0 = reference arithmetic (float-rounded CG updates and
  *                        V-cycle casts, the default), 1 = FP64, 2 = FP32 V-cycle
  *                        with FP64 outer PCG;
- *   "sgs_honor_max_iterations"  1 = stop at krylov.max_iterations instead of 500. */
+ *   "sgs_honor_max_iterations"  1 = stop at krylov.max_iterations instead of 500.
+ * Warm starting as the reference's (SPGrid_CPU_Solver.cpp:56-73, 240-321,
+ * 389-408): with extra_ints "keep_state" = 1 the output's extra_ints
+ * "state_ptr_lower"/"state_ptr_higher" name a solver state (the last solution
+ * per level-0 page and the first call's zero-guess residual); passed back in
+ * the next input, the previous solution is the initial guess when
+ * "forced_reuse" is set or it beats the zero guess, and the stopping rule stays
+ * relative to the stored residual.  A call without keep_state releases the
+ * state it was given. */
 SGS_API void fem_solve(void* input, void* output);
 
 /* Release an output blob from fem_solve (callers that cannot call delete[]). */

@@ -17,6 +17,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/spgrid_fem.h"
@@ -117,6 +118,13 @@ class Solver {
   // stats
   int iterations = 0;
   double initial_residual = 0, final_residual = 0, setup_seconds = 0, solve_seconds = 0;
+  // warm start (SPGrid_CPU_Solver.cpp:240-321): a previous solution gathered
+  // into the level-0 layout, the residual the stopping rule is relative to
+  // (the zero-guess residual of the call that created the kept state), and
+  // whether the previous solution was reused
+  DevBuf<double> warm_u;
+  double warm_reference = 0, warm_residual = 0;
+  bool forced_reuse = false, warm_reused = false;
   std::vector<double> history;
   std::string error;
   int error_code = 0;
@@ -1253,27 +1261,50 @@ void Solver::solve() {
     SGS_CUDA(cudaEventCreate(&ev_end));
   }
   SGS_CUDA(cudaEventRecord(ev_start, stream));
-  // u = g on the listed Dirichlet nodes (SPGrid_CPU_Solver.cpp:241-285)
-  x.zero(stream);
-  if (!P.lift_node.empty())
-    launch(scatter_lift_kernel, blocks_for(long(P.lift_node.size()), 128), 128, 0, 
-        x.p, lift_node.p, lift_axis.p, lift_val.p, int(P.lift_node.size()), N);
+  // u = g on the listed Dirichlet nodes (SPGrid_CPU_Solver.cpp:241-285),
+  // over the previous solution when warm starting
+  auto lift = [&] {
+    if (!P.lift_node.empty())
+      launch(scatter_lift_kernel, blocks_for(long(P.lift_node.size()), 128), 128, 0, x.p, lift_node.p, lift_axis.p,
+             lift_val.p, int(P.lift_node.size()), N);
+  };
   // s = forces; Project; Project_Nullspace; f = s - K u; Project (:287-301)
-  s.zero(stream);
-  if (!P.force_node.empty())
-    launch(scatter_force_kernel, blocks_for(long(P.force_node.size()), 128), 128, 0, 
-        s.p, force_node.p, force_val.p, int(P.force_node.size()), N);
-  project<double>(l0, s.p);
-  project_null<double>(l0, s.p);
-  level0<double, OP_RES>(x.p, s.p, f.p);
-  project<double>(l0, f.p);
+  auto residual = [&] {
+    s.zero(stream);
+    if (!P.force_node.empty())
+      launch(scatter_force_kernel, blocks_for(long(P.force_node.size()), 128), 128, 0, s.p, force_node.p,
+             force_val.p, int(P.force_node.size()), N);
+    project<double>(l0, s.p);
+    project_null<double>(l0, s.p);
+    level0<double, OP_RES>(x.p, s.p, f.p);
+    project<double>(l0, f.p);
+  };
+  const bool warm = warm_u.p != nullptr;
+  warm_reused = false;
+  if (warm) {
+    // keep the previous u only if forced or if it beats the zero guess (:247-277)
+    SGS_CUDA(cudaMemcpyAsync(x.p, warm_u.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    lift();
+    residual();
+    linf(f.p, nullptr);
+    SGS_CUDA(cudaMemcpyAsync(h_scal, scal.p, 16 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    warm_residual = h_scal[3];
+    warm_reused = forced_reuse || warm_reference > warm_residual;
+  }
+  if (!warm_reused) {
+    x.zero(stream);
+    lift();
+  }
+  residual();
   SGS_CUDA(cudaMemcpyAsync(ubk.p, x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
   q.zero(stream);
   s.zero(stream);
   linf(f.p, nullptr);
   SGS_CUDA(cudaMemcpyAsync(h_scal, scal.p, 16 * sizeof(double), cudaMemcpyDeviceToHost, stream));
   SGS_CUDA(cudaStreamSynchronize(stream));
-  initial_residual = h_scal[3];
+  // the stopping rule is relative to the first call's zero-guess residual
+  initial_residual = warm ? warm_reference : h_scal[3];
   const double tol = P.tolerance * initial_residual;
   auto t0 = std::chrono::steady_clock::now();
   x.zero(stream);
@@ -1710,6 +1741,90 @@ void Solver::band_step(Band& B, const sgs_design_params& prm, sgs_design_result*
     out->solve_seconds = std::chrono::duration<double>(t1 - t0).count();
     out->step_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
   }
+}
+
+// ---------------------------------------------------------------------------
+// The solver state kept between fem_solve calls with keep_state
+// (SPGrid_CPU_Solver.cpp:17-26, 56-73, 389-408): the zero-guess residual of the
+// call that created it and the last solution on every level-0 page solved on
+// (the reference keeps both in its SPGrid allocation), to warm-start later calls.
+// ---------------------------------------------------------------------------
+struct KeptState {
+  static constexpr uint64_t MAGIC = 0x5347535354415445ull;
+  uint64_t magic = MAGIC;
+  double initial_residual_linf = 0;
+  std::unordered_map<uint64_t, int32_t> slot;  // page -> slot of the store
+  DevBuf<double> store;                         // [slot][3][128]
+  long nslots = 0;
+};
+
+static uint64_t page_id(int x, int y, int z) {
+  return (uint64_t(uint32_t(x >> 2)) << 42) | (uint64_t(uint32_t(y >> 2)) << 21) | uint64_t(uint32_t(z >> 3));
+}
+
+// x[v][b*128 + e] <- store[slot[b]][v][e] (0 where the page has no slot)
+__global__ void warm_gather_kernel(long nb, const int* __restrict__ slot, const double* __restrict__ store,
+                                   double* __restrict__ x, long N) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nb * 128) return;
+  const long b = t >> 7;
+  const int e = int(t & 127), sl = slot[b];
+  for (int v = 0; v < 3; ++v) x[v * N + t] = sl >= 0 ? store[(long(sl) * 3 + v) * 128 + e] : 0.0;
+}
+
+__global__ void warm_scatter_kernel(long nb, const int* __restrict__ slot, const double* __restrict__ x, long N,
+                                    double* __restrict__ store) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nb * 128) return;
+  const long b = t >> 7;
+  const int e = int(t & 127), sl = slot[b];
+  for (int v = 0; v < 3; ++v) store[(long(sl) * 3 + v) * 128 + e] = x[v * N + t];
+}
+
+// The previous solution on this call's pages becomes the warm-start candidate.
+static void warm_start_from(Solver& S, const KeptState& K) {
+  const HostLevel& h = S.P.levels[0];
+  std::vector<int32_t> sl(static_cast<size_t>(h.nb));
+  for (int b = 0; b < h.nb; ++b) {
+    auto it = K.slot.find(page_id(h.coords[3 * b], h.coords[3 * b + 1], h.coords[3 * b + 2]));
+    sl[size_t(b)] = it == K.slot.end() ? -1 : it->second;
+  }
+  DevBuf<int32_t> d;
+  d.upload(sl, S.stream);
+  S.warm_u.alloc(size_t(3) * S.N0());
+  const long nb = h.nb;
+  if (nb)
+    warm_gather_kernel<<<blocks_for(nb * 128, 256), 256, 0, S.stream>>>(nb, d.p, K.store.p, S.warm_u.p, S.N0());
+  SGS_CUDA(cudaGetLastError());
+  SGS_CUDA(cudaStreamSynchronize(S.stream));
+  S.warm_reference = K.initial_residual_linf;
+}
+
+// The solution of this call into the kept state (new pages get new slots).
+static void keep_solution(Solver& S, KeptState& K) {
+  const HostLevel& h = S.P.levels[0];
+  std::vector<int32_t> sl(static_cast<size_t>(h.nb));
+  for (int b = 0; b < h.nb; ++b) {
+    const uint64_t id = page_id(h.coords[3 * b], h.coords[3 * b + 1], h.coords[3 * b + 2]);
+    auto it = K.slot.find(id);
+    if (it == K.slot.end()) it = K.slot.emplace(id, int32_t(K.nslots++)).first;
+    sl[size_t(b)] = it->second;
+  }
+  const size_t need = size_t(K.nslots) * 3 * 128;
+  if (K.store.n < need) {  // grow, keeping the stored pages
+    DevBuf<double> grown;
+    grown.alloc(std::max(need, 2 * K.store.n));
+    if (K.store.n)
+      SGS_CUDA(cudaMemcpyAsync(grown.p, K.store.p, K.store.n * sizeof(double), cudaMemcpyDeviceToDevice, S.stream));
+    std::swap(grown.p, K.store.p);
+    std::swap(grown.n, K.store.n);
+  }
+  DevBuf<int32_t> d;
+  d.upload(sl, S.stream);
+  const long nb = h.nb;
+  if (nb) warm_scatter_kernel<<<blocks_for(nb * 128, 256), 256, 0, S.stream>>>(nb, d.p, S.x.p, S.N0(), K.store.p);
+  SGS_CUDA(cudaGetLastError());
+  SGS_CUDA(cudaStreamSynchronize(S.stream));
 }
 
 }  // namespace sgs
@@ -2267,8 +2382,39 @@ SGS_API void fem_solve(void* input, void* output) {
       outs.info = err.empty() ? "invalid sgs_precision" : err;
     } else {
       std::unique_ptr<sgs_session> guard(h);
+      // a kept state passed back by the caller (fem_interface.h:200-214): warm start
+      KeptState* state = nullptr;
+      if (in.extra_ints.count("state_ptr_lower")) {
+        const uint64_t addr = (uint64_t(uint32_t(in.get_int("state_ptr_higher", 0))) << 32) |
+                              uint64_t(uint32_t(in.get_int("state_ptr_lower", 0)));
+        state = reinterpret_cast<KeptState*>(addr);
+        if (state && state->magic != KeptState::MAGIC)
+          throw CudaError("the solver state pointer does not name a state of this library", SGS_ERR_INPUT);
+      }
+      const bool keep = in.get_int("keep_state", 0) != 0;
+      if (state) {
+        warm_start_from(*h->solver, *state);
+        h->solver->forced_reuse = in.get_int("forced_reuse", 0) != 0;
+      }
       sgs_stats st{};
       rc = sgs_solve(h, 0, 0, &st);
+      if (state) {
+        outs.extra_ints["warm_start_reused"] = h->solver->warm_reused ? 1 : 0;
+        outs.extra_doubles["warm_start_residual"] = h->solver->warm_residual;
+      }
+      // keep (or create) the state, or release a state passed in (:389-408)
+      if (keep) {
+        if (!state) {
+          state = new KeptState();
+          state->initial_residual_linf = h->solver->initial_residual;
+        }
+        if (rc == 0) keep_solution(*h->solver, *state);
+        const uint64_t addr = reinterpret_cast<uint64_t>(state);
+        outs.extra_ints["state_ptr_lower"] = int32_t(uint32_t(addr & 0xffffffffu));
+        outs.extra_ints["state_ptr_higher"] = int32_t(uint32_t(addr >> 32));
+      } else if (state) {
+        delete state;
+      }
       outs.residuals = h->solver->history;
       outs.extra_ints["iterations"] = st.iterations;
       outs.extra_doubles["initial_residual"] = st.initial_residual;
@@ -2332,6 +2478,9 @@ SGS_API void fem_solve(void* input, void* output) {
   } catch (const WireError& e) {
     outs.error_code = SGS_ERR_WIRE;
     outs.info = std::string("malformed input blob: ") + e.what();
+  } catch (const CudaError& e) {
+    outs.error_code = e.code;
+    outs.info = e.what();
   } catch (const std::exception& e) {
     outs.error_code = SGS_ERR_INTERNAL;
     outs.info = e.what();

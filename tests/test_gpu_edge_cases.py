@@ -90,3 +90,53 @@ def test_iteration_cap(native_lib):
     out = native.fem_solve(inp)
     assert out.extra_ints["iterations"] == 3
     assert len(out.residuals) == 4
+
+
+def _with_state(inp, out, keep=1, forced=1):
+    nxt = copy.deepcopy(inp)
+    nxt.extra_ints["keep_state"] = keep
+    nxt.extra_ints["forced_reuse"] = forced
+    nxt.extra_ints["state_ptr_lower"] = out.extra_ints["state_ptr_lower"]
+    nxt.extra_ints["state_ptr_higher"] = out.extra_ints["state_ptr_higher"]
+    return nxt
+
+
+def test_keep_state_warm_start(native_lib):
+    """keep_state returns a solver state through extra_ints (fem_interface.h:200-214);
+    passed back, it warm-starts the next solve from the last solution, with the
+    stopping rule still relative to the first call's zero-guess residual
+    (SPGrid_CPU_Solver.cpp:240-321, 389-408)."""
+    inp = configs.to_inputs(configs.cantilever_box(16, density=(0.2, 1.0), bottom_size=4))
+    inp.extra_ints["keep_state"] = 1
+    out1 = native.fem_solve(inp)
+    assert out1.success and "state_ptr_lower" in out1.extra_ints and out1.extra_ints["iterations"] > 0
+    # the same problem again: the converged solution is reused, no iteration is needed
+    out2 = native.fem_solve(_with_state(inp, out1))
+    assert out2.success and out2.extra_ints["warm_start_reused"] == 1
+    assert out2.extra_ints["iterations"] == 0
+    assert np.array_equal(out2.displacements.data[..., :3], out1.displacements.data[..., :3])
+    assert out2.extra_doubles["initial_residual"] == out1.extra_doubles["initial_residual"]
+    # a slightly stiffer design: the warm start needs fewer iterations than a cold solve
+    stiffer = _with_state(inp, out2)
+    stiffer.density = BlockedGrid(resolution=list(inp.density.resolution), base=np.asarray(inp.density.base),
+                                  data=np.minimum(np.asarray(inp.density.data) * 1.05, 1.0))
+    out3 = native.fem_solve(stiffer)
+    cold = copy.deepcopy(stiffer)
+    for k in ("keep_state", "state_ptr_lower", "state_ptr_higher"):
+        cold.extra_ints.pop(k)
+    out_cold = native.fem_solve(cold)
+    assert out3.success and out3.extra_ints["iterations"] < out_cold.extra_ints["iterations"]
+    assert _rel(out3.displacements.data[..., :3], out_cold.displacements.data[..., :3]) < 1e-3
+    # without keep_state the state passed in is released and none is returned
+    out4 = native.fem_solve(_with_state(inp, out3, keep=0))
+    assert out4.success and "state_ptr_lower" not in out4.extra_ints
+
+
+def test_foreign_state_pointer_is_rejected(native_lib):
+    inp = configs.to_inputs(configs.cantilever_box(16, bottom_size=4))
+    junk = np.zeros(8, np.uint64)
+    addr = junk.ctypes.data
+    inp.extra_ints["state_ptr_lower"] = int(np.uint32(addr & 0xFFFFFFFF).view(np.int32))
+    inp.extra_ints["state_ptr_higher"] = int(np.uint32(addr >> 32).view(np.int32))
+    out = native.fem_solve(inp)
+    assert not out.success and out.error_code == 1
