@@ -318,7 +318,8 @@ typedef struct sgs_render_params {
   uint32_t seed;
   float camera[12];        /* 3x4 rows: camera-to-world rotation | eye position (c_invViewMatrix) */
   int32_t reverse_mapping; /* 1: densities are SIMP stiffness (penalty 0): d -> (d - 1e-6)^(1/3) (1 - 1e-6) */
-  int32_t reserved;
+  int32_t mirror;          /* bits 0-2: show the volume mirrored across its +x, +y, +z face (the viewer's
+                              mirroring, volume_rendering_kernel.cu:133-143, volume_renderer.cpp set_mirroring) */
 } sgs_render_params;
 
 /* Host arrays in the FEMInputs density layout; volume_res (may be NULL)

@@ -73,20 +73,23 @@ def build_volume(base, density, reverse_mapping: bool = False):
 
 
 class Volume:
-    def __init__(self, vox, res, slice_=0.99999):
+    def __init__(self, vox, res, slice_=0.99999, mirror=""):
         self.vox = vox
         self.res = np.asarray(res)
         rmax = F(int(self.res.max()))
-        self.box_size = np.array([F(int(r)) / rmax for r in self.res], F)
-        self.box_res = np.array([F(int(r)) for r in self.res], F)
+        self.scale = np.array([F(2) if a in mirror else F(1) for a in "xyz"], F)
+        self.box_size = np.array([F(int(r)) / rmax * s for r, s in zip(self.res, self.scale)], F)
+        self.box_res = np.array([F(int(r)) * s for r, s in zip(self.res, self.scale)], F)
+        self.tex_res = np.array([F(int(r)) for r in self.res], F)   # the texture keeps the volume's size
         self.slice = F(slice_)
 
     def point_sample(self, p):
-        p = p * F(0.5) + F(0.5)
+        # wrap_coord (:133-143): box_scale 2 on mirrored axes reflects past the far face
+        p = (p * F(0.5) + F(0.5)) * self.scale
         p = np.where(p > 1, F(2) - p, p)
         p = p * F(2) + F(-1.0)
         t = p * F(0.5) + F(0.5)
-        i = np.floor(t * self.box_res).astype(np.int64)
+        i = np.floor(t * self.tex_res).astype(np.int64)
         i = np.clip(i, 0, self.res - 1)
         return self.vox[i[:, 2], i[:, 1], i[:, 0]].astype(F) / F(255.0)
 
@@ -184,10 +187,10 @@ def pack_rgba(r, g, b, a):
 
 
 def render(base, density, width, height, camera, mode=0, frames=1, threshold=0.5, extinction=1.0,
-           slice_=0.99999, seed=0, reverse_mapping=False):
+           slice_=0.99999, seed=0, reverse_mapping=False, mirror=""):
     """The image as uint32 [height][width] (a<<24 | b<<16 | g<<8 | r), row 0 at the bottom."""
     vox, res = build_volume(base, density, reverse_mapping)
-    V = Volume(vox, res, slice_)
+    V = Volume(vox, res, slice_, mirror)
     npix = width * height
     buf = np.zeros((npix, 3), F)
     out = None

@@ -18,7 +18,9 @@
 // CPU restatement draws the same numbers; the primary direction is normalised
 // by a division by its length (the reference multiplies by an approximate
 // reciprocal square root); a point sample reads voxel clamp(floor(t * res)) of
-// the texture coordinate t.  This file is compiled without fused multiply-adds.
+// the texture coordinate t.  Mirroring (the viewer's box_scale) doubles the box
+// on the chosen axes and reflects coordinates past the volume's far face.
+// This file is compiled without fused multiply-adds.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,8 +44,9 @@ struct Camera {
 struct VolumeView {
   const uint8_t* vox;  // x fastest: x + y*W + z*W*H
   int res[3];
-  float3 box_size;  // half extents: res / max(res)
-  float3 box_res;
+  float3 scale;     // 2 on mirrored axes, else 1 (box_scale)
+  float3 box_size;  // half extents: res / max(res), times scale
+  float3 box_res;   // res times scale
   float slice;
 };
 
@@ -77,7 +80,7 @@ __device__ inline bool inside_unit_cube(float3 p) {
 // values read as v / 255; the coordinate p in [-1, 1] goes through the
 // reference's wrap_coord (mirroring off) first (:133-158).
 __device__ inline float point_sample(const VolumeView& V, float3 p) {
-  p = addc(scale(p, 0.5f), 0.5f);
+  p = mul(addc(scale(p, 0.5f), 0.5f), V.scale);
   if (p.x > 1) p.x = 2 - p.x;
   if (p.y > 1) p.y = 2 - p.y;
   if (p.z > 1) p.z = 2 - p.z;
@@ -312,8 +315,11 @@ void render_device(const int* base_d, const double* rho_d, long nblocks, const s
   V.vox = vox.p;
   const int rmax = std::max(res[0], std::max(res[1], res[2]));
   for (int a = 0; a < 3; ++a) V.res[a] = res[a];
-  V.box_size = make_float3(float(res[0]) / float(rmax), float(res[1]) / float(rmax), float(res[2]) / float(rmax));
-  V.box_res = make_float3(float(res[0]), float(res[1]), float(res[2]));
+  const float sc[3] = {(p.mirror & 1) ? 2.0f : 1.0f, (p.mirror & 2) ? 2.0f : 1.0f, (p.mirror & 4) ? 2.0f : 1.0f};
+  V.scale = make_float3(sc[0], sc[1], sc[2]);
+  V.box_size = make_float3(float(res[0]) / float(rmax) * sc[0], float(res[1]) / float(rmax) * sc[1],
+                           float(res[2]) / float(rmax) * sc[2]);
+  V.box_res = make_float3(float(res[0]) * sc[0], float(res[1]) * sc[1], float(res[2]) * sc[2]);
   V.slice = p.slice;
   Camera C;
   for (int k = 0; k < 12; ++k) C.m[k] = p.camera[k];

@@ -61,15 +61,17 @@ class BandStats(C.Structure):
 class RenderParams(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("mode", C.c_int32), ("frames", C.c_int32),
                 ("threshold", C.c_float), ("extinction", C.c_float), ("slice", C.c_float), ("seed", C.c_uint32),
-                ("camera", C.c_float * 12), ("reverse_mapping", C.c_int32), ("reserved", C.c_int32)]
+                ("camera", C.c_float * 12), ("reverse_mapping", C.c_int32), ("mirror", C.c_int32)]
 
 
 def render_params(width: int, height: int, camera, mode: int = 0, frames: int = 1, threshold: float = 0.5,
                   extinction: float = 1.0, slice_: float = 0.99999, seed: int = 0,
-                  reverse_mapping: bool = False) -> RenderParams:
+                  reverse_mapping: bool = False, mirror: str = "") -> RenderParams:
+    """mirror: any of "x", "y", "z" -- the volume shown mirrored across that far face."""
     cam = np.ascontiguousarray(camera, np.float32).reshape(12)
+    bits = sum(1 << "xyz".index(a) for a in set(mirror))
     return RenderParams(width, height, mode, frames, threshold, extinction, slice_, seed,
-                        (C.c_float * 12)(*cam.tolist()), int(reverse_mapping), 0)
+                        (C.c_float * 12)(*cam.tolist()), int(reverse_mapping), bits)
 
 
 def render(base: np.ndarray, density: np.ndarray, width: int, height: int, camera, **kw):

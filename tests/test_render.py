@@ -48,11 +48,11 @@ def _agree(got, ref, exact=0.995, near=0.999):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", [0, 1])
-def test_render_matches_oracle(native_lib, mode):
+@pytest.mark.parametrize("mode,mirror", [(0, ""), (1, ""), (0, "xz")])
+def test_render_matches_oracle(native_lib, mode, mirror):
     inp = void_box()
     cam = native.view_matrix(-20, 30, 0, 0, 0, -5)
-    kw = dict(mode=mode, frames=3, threshold=0.3 if mode == 0 else 0.05, extinction=3.0, seed=7)
+    kw = dict(mode=mode, frames=3, threshold=0.3 if mode == 0 else 0.05, extinction=3.0, seed=7, mirror=mirror)
     got, res = native.render(inp.density.base, inp.density.data, 96, 64, cam, **kw)
     ref, rres = ro.render(inp.density.base, inp.density.data, 96, 64, cam, **kw)
     assert res.tolist() == list(rres)
@@ -70,3 +70,13 @@ def test_band_render_matches_host_render(native_lib):
     b, _ = native.render(base, dens, 64, 64, cam, mode=0, frames=2, threshold=0.3)
     assert np.array_equal(a, b)
     band.close()
+
+
+def test_mirroring_reflects_past_the_far_face():
+    vox = np.arange(16, dtype=np.uint8).reshape(2, 2, 4)     # [z][y][x], res (4, 2, 2)
+    V = ro.Volume(vox, (4, 2, 2), mirror="x")
+    ipos = np.array([[5, 1, 0], [2, 1, 0], [7, 0, 1], [0, 0, 1]], np.float32)
+    s = V.sample_voxel(ipos)
+    assert s[0] == s[1] and s[2] == s[3]                    # x = 5 <-> 2, x = 7 <-> 0 in the doubled box
+    assert s[1] == np.float32(vox[0, 1, 2]) / np.float32(255) and s[3] == np.float32(vox[1, 0, 0]) / np.float32(255)
+    assert V.box_res.tolist() == [8, 2, 2]
