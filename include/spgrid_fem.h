@@ -271,6 +271,31 @@ SGS_API int sgs_band_set_fat(sgs_band* b, const uint8_t* fat);
 SGS_API int sgs_band_update(sgs_band* b, const sgs_band_params* params, sgs_band_stats* stats);
 /* Copy the maps out, one byte per container block; any pointer may be NULL. */
 SGS_API int sgs_band_maps(sgs_band* b, uint8_t* thin, uint8_t* fat, uint8_t* fatter);
+/* Copy the cell flags out ([nblocks][64]); the voxel filter and the kill change them. */
+SGS_API int sgs_band_get_flags(sgs_band* b, uint8_t* cell_flags);
+
+typedef struct sgs_band_voxel_stats {
+  int64_t voxels;         /* container cells of the thin blocks (the search's total) */
+  int64_t components;     /* their 6-connected components */
+  int64_t kept, removed;  /* cells of the component kept / cells taken out of the container */
+  double device_seconds;
+} sgs_band_voxel_stats;
+
+/* Replaces Opt::filter_isolated_voxels (spgrid_topo_opt.cpp:1512-1633), the
+ * driver's "voxel_connectivity_filtering" action (:625-627): the 6-connected
+ * components of the container cells of the thin blocks; with more than one,
+ * the single component above 30% of those cells stays and every other cell
+ * leaves the container with density 0.  The container voxel count behind the
+ * volume target stays as it was, as in the reference.  No container cell in a
+ * thin block, or not exactly one component above 30%, returns SGS_ERR_INPUT
+ * with nothing changed.  stats may be NULL. */
+SGS_API int sgs_band_filter_voxels(sgs_band* b, sgs_band_voxel_stats* stats);
+/* The first loop of Opt::threshold_and_kill (spgrid_topo_opt.cpp:1333-1344):
+ * every container cell with density below threshold leaves the container (its
+ * density stays).  The reference's action then runs the voxel filter and a
+ * page-map update without the block filter (:1341-1343); chain
+ * sgs_band_filter_voxels and sgs_band_update for that.  killed may be NULL. */
+SGS_API int sgs_band_kill_below(sgs_band* b, double threshold, int64_t* killed);
 
 /* The driver's iteration on a band.  A session holds the fatter blocks as the
  * driver packs them into FEMInputs (spgrid_topo_opt.cpp:1068-1160): its input

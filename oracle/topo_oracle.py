@@ -5,6 +5,9 @@ reference's driver -- test infrastructure (the oracle), not part of the product.
   (topo_opt/spgrid_topo_opt.cpp:527-579).
 * oc_update: the optimality-criteria update OptimalityCriterion::optimize
   (topo_opt/optimizer/optimality_criterion.cpp:19-145).
+* update_page_maps / filter_isolated_voxels / kill_below: the driver's
+  narrow-band page maps and its voxel-level clean-up
+  (topo_opt/spgrid_topo_opt.cpp:92-241, 1333-1344, 1404-1633).
 
 Both act on the FEMInputs density layout: input 4x4x4 blocks (base coordinates
 ``base[nblocks][3]``), cell e = i*16 + j*4 + k.  A cell is inside the container
@@ -310,3 +313,76 @@ def band_oc(flags, fat, rho, dc0, total_inside: int, volume_fraction: float, ste
     out[sel] = nd
     change = float(np.max(np.abs(nd - old))) if nd.size else 0.0
     return out, mid, change
+
+
+# ---------------------------------------------------------------------------
+# Voxel-level connectivity filter and threshold-and-kill
+# ---------------------------------------------------------------------------
+def filter_isolated_voxels(base, density, flags, thin):
+    """Opt::filter_isolated_voxels (spgrid_topo_opt.cpp:1512-1633): breadth-first
+    search over the container cells of the thin blocks with 6-connectivity, in
+    the order of the thin list and of the cells in a block.  With one component
+    nothing changes; otherwise exactly one component must hold more than 30% of
+    those cells, and every other cell loses its container flag and its density.
+    The container voxel count the optimizer's volume target uses is not changed.
+    Returns (flags, density, stats) as new arrays."""
+    base = np.asarray(base, np.int64).reshape(-1, 3)
+    n = len(base)
+    dens = np.array(density, np.float64, copy=True).reshape(n, 64)
+    flg = np.array(flags, np.uint8, copy=True).reshape(n, 64)
+    thin = np.asarray(thin, bool)
+    part = thin[:, None] & ((flg & CELL_INSIDE) != 0)          # the cells the search can reach
+    ijk = np.array([[e >> 4, (e >> 2) & 3, e & 3] for e in range(64)])
+    lo = base.min(axis=0) - 1
+    ext = base.max(axis=0) - lo + 5
+    index = np.full(tuple(ext), -1, np.int64)                   # cell coordinate -> b * 64 + e
+    for b in range(n):
+        x, y, z = base[b] - lo
+        index[x:x + 4, y:y + 4, z:z + 4] = np.where(part[b], b * 64 + np.arange(64), -1).reshape(4, 4, 4)
+    color = np.full(n * 64, -1, np.int64)
+    sizes = []
+    order = np.argsort(driver_page_keys(base // 4), kind="stable")
+    steps = ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1))
+    for b in order:
+        if not thin[b]:
+            continue
+        for e in range(64):
+            c0 = b * 64 + e
+            if not part[b, e] or color[c0] >= 0:
+                continue
+            color[c0] = len(sizes)
+            queue, head = [c0], 0
+            while head < len(queue):
+                u = queue[head]
+                head += 1
+                p = base[u // 64] - lo + ijk[u % 64]
+                for d in steps:
+                    v = index[p[0] + d[0], p[1] + d[1], p[2] + d[2]]
+                    if v >= 0 and color[v] < 0:
+                        color[v] = len(sizes)
+                        queue.append(v)
+            sizes.append(len(queue))
+    total = int(sum(sizes))
+    stats = {"voxels": total, "components": len(sizes), "kept": total, "removed": 0}
+    if not sizes:
+        raise PageMapError("no container voxels in the thin blocks")
+    if len(sizes) == 1:
+        return flg, dens, stats
+    big = [i for i, s in enumerate(sizes) if 1.0 * s / total > 0.3]
+    if len(big) != 1:
+        raise PageMapError(f"{len(big)} voxel components hold more than 30% of the voxels")
+    drop = (part.reshape(-1) & (color != big[0])).reshape(n, 64)
+    flg[drop] &= np.uint8(~CELL_INSIDE & 0xFF)
+    dens[drop] = 0.0
+    stats.update(kept=int(sizes[big[0]]), removed=int(np.count_nonzero(drop)))
+    return flg, dens, stats
+
+
+def kill_below(density, flags, threshold: float):
+    """The first loop of Opt::threshold_and_kill (spgrid_topo_opt.cpp:1333-1344):
+    every container cell whose density is below the threshold leaves the
+    container (its density stays).  Returns (flags, cells killed)."""
+    flg = np.array(flags, np.uint8, copy=True)
+    kill = ((flg & CELL_INSIDE) != 0) & (np.asarray(density, np.float64).reshape(flg.shape) < threshold)
+    flg[kill] &= np.uint8(~CELL_INSIDE & 0xFF)
+    return flg, int(np.count_nonzero(kill))

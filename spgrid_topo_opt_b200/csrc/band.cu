@@ -19,7 +19,8 @@ namespace {
 
 constexpr int BAND_WARPS = 8;  // warps per CTA of the warp-per-block kernels
 enum {
-  CNT_THIN = 0, CNT_FAT, CNT_FATTER, CNT_ACTIVE, CNT_COMPONENTS, CNT_BIG, CNT_BIG_ROOT, CNT_ERROR, CNT_FAT_CHANGED, CNT_N
+  CNT_THIN = 0, CNT_FAT, CNT_FATTER, CNT_ACTIVE, CNT_COMPONENTS, CNT_BIG, CNT_BIG_ROOT, CNT_ERROR, CNT_FAT_CHANGED,
+  CNT_VOXELS, CNT_REMOVED, CNT_N
 };
 
 // Block of the container holding the cell block (bx, by, bz), or -1.
@@ -115,6 +116,24 @@ __device__ __forceinline__ int uf_find(int* parent, int x, long n, unsigned long
   return x;
 }
 
+__device__ __forceinline__ void uf_union(int* parent, int x, int y, long n, unsigned long long* err) {
+  for (long it = 0;; ++it) {
+    if (it > n) {
+      atomicExch(err, 1ull);
+      return;
+    }
+    x = uf_find(parent, x, n, err);
+    y = uf_find(parent, y, n, err);
+    if (x == y) return;
+    if (x > y) {
+      const int t = x;
+      x = y;
+      y = t;
+    }
+    if (atomicCAS(parent + y, y, x) == y) return;  // else y gained a parent meanwhile: retry
+  }
+}
+
 __global__ void band_cc_init_kernel(long n, const uint8_t* __restrict__ thin, int* __restrict__ parent,
                                     int* __restrict__ size) {
   const long b = long(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -131,23 +150,7 @@ __global__ void band_cc_hook_kernel(long n, const int* __restrict__ base, const 
   const int nbx[3] = {bx + 1, bx, bx}, nby[3] = {by, by + 1, by}, nbz[3] = {bz, bz, bz + 1};
   for (int v = 0; v < 3; ++v) {
     const int c = lookup(grid, gx, gy, gz, nbx[v], nby[v], nbz[v]);
-    if (c < 0 || !thin[c]) continue;
-    int x = int(b), y = c;
-    for (long it = 0;; ++it) {
-      if (it > n) {
-        atomicExch(cnt + CNT_ERROR, 1ull);
-        break;
-      }
-      x = uf_find(parent, x, n, cnt + CNT_ERROR);
-      y = uf_find(parent, y, n, cnt + CNT_ERROR);
-      if (x == y) break;
-      if (x > y) {
-        const int t = x;
-        x = y;
-        y = t;
-      }
-      if (atomicCAS(parent + y, y, x) == y) break;  // else y gained a parent meanwhile: retry
-    }
+    if (c >= 0 && thin[c]) uf_union(parent, int(b), c, n, cnt + CNT_ERROR);
   }
 }
 
@@ -184,6 +187,101 @@ __global__ void band_cc_keep_kernel(long n, const int* __restrict__ parent, int 
     r = p;
   }
   if (r != root) thin[b] = 0;
+}
+
+// ---- 6-connected components of the container cells (filter_isolated_voxels) ----
+// The same union-find over cells c = b * 64 + e of the thin blocks; a cell's +x,
+// +y, +z neighbours lie in its own block or at the opposite face of the
+// neighbouring block.
+__device__ __forceinline__ bool vox_member(const uint8_t* __restrict__ thin, const uint8_t* __restrict__ flags,
+                                           long c) {
+  return thin[c >> 6] && (flags[c] & SGS_CELL_INSIDE);
+}
+
+// adds the warp's count of true predicates to *counter (every lane of the warp calls it)
+__device__ __forceinline__ void warp_count(bool pred, unsigned long long* counter) {
+  const unsigned m = __ballot_sync(0xffffffffu, pred);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(counter, (unsigned long long)__popc(m));
+}
+
+__global__ void vox_init_kernel(long N, const uint8_t* __restrict__ thin, const uint8_t* __restrict__ flags,
+                                int* __restrict__ parent, int* __restrict__ size, unsigned long long* cnt) {
+  const long c = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  const bool m = c < N && vox_member(thin, flags, c);
+  if (c < N) {
+    parent[c] = m ? int(c) : -1;
+    size[c] = 0;
+  }
+  warp_count(m, cnt + CNT_VOXELS);
+}
+
+__global__ void vox_hook_kernel(long N, const int* __restrict__ base, const int* __restrict__ grid, int gx, int gy,
+                                int gz, const uint8_t* __restrict__ thin, const uint8_t* __restrict__ flags,
+                                int* parent, unsigned long long* cnt) {
+  const long c = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= N || !vox_member(thin, flags, c)) return;
+  const long b = c >> 6;
+  const int e = int(c & 63);
+  const int q[3] = {e >> 4, (e >> 2) & 3, e & 3}, stride[3] = {16, 4, 1};
+  for (int v = 0; v < 3; ++v) {
+    long d = c + stride[v];
+    if (q[v] == 3) {
+      const int nb = lookup(grid, gx, gy, gz, (base[3 * b] >> 2) + (v == 0), (base[3 * b + 1] >> 2) + (v == 1),
+                            (base[3 * b + 2] >> 2) + (v == 2));
+      if (nb < 0) continue;
+      d = long(nb) * 64 + e - 3 * stride[v];
+    }
+    if (vox_member(thin, flags, d)) uf_union(parent, int(c), int(d), N, cnt + CNT_ERROR);
+  }
+}
+
+__global__ void vox_flatten_kernel(long N, const uint8_t* __restrict__ thin, const uint8_t* __restrict__ flags,
+                                   int* parent, int* __restrict__ size, unsigned long long* cnt) {
+  const long c = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= N || !vox_member(thin, flags, c)) return;
+  atomicAdd(size + uf_find(parent, int(c), N, cnt + CNT_ERROR), 1);
+}
+
+// Components and those above 30% of the cells searched (:1580-1606).
+__global__ void vox_roots_kernel(long N, const int* __restrict__ parent, const int* __restrict__ size,
+                                 unsigned long long* cnt) {
+  const long c = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= N || __ldcg(parent + c) != int(c)) return;
+  atomicAdd(cnt + CNT_COMPONENTS, 1ull);
+  if (1.0 * size[c] / double(cnt[CNT_VOXELS]) > 0.3) {
+    atomicAdd(cnt + CNT_BIG, 1ull);
+    atomicExch(cnt + CNT_BIG_ROOT, (unsigned long long)c);
+  }
+}
+
+// Cells outside the kept component leave the container with density 0 (:1611-1626).
+__global__ void vox_keep_kernel(long N, const uint8_t* __restrict__ thin, const int* __restrict__ parent, int root,
+                                uint8_t* __restrict__ flags, double* __restrict__ rho, unsigned long long* cnt) {
+  const long c = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  bool drop = false;
+  if (c < N && vox_member(thin, flags, c)) {
+    int r = int(c);
+    for (long it = 0; it <= N; ++it) {
+      const int p = parent[r];
+      if (p == r) break;
+      r = p;
+    }
+    drop = r != root;
+    if (drop) {
+      flags[c] = uint8_t(flags[c] & ~SGS_CELL_INSIDE);
+      rho[c] = 0.0;
+    }
+  }
+  warp_count(drop, cnt + CNT_REMOVED);
+}
+
+// threshold_and_kill (:1333-1340): container cells below the threshold leave it.
+__global__ void vox_kill_kernel(long N, const double* __restrict__ rho, double threshold, uint8_t* __restrict__ flags,
+                                unsigned long long* cnt) {
+  const long c = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  const bool kill = c < N && (flags[c] & SGS_CELL_INSIDE) && rho[c] < threshold;
+  if (kill) flags[c] = uint8_t(flags[c] & ~SGS_CELL_INSIDE);
+  warp_count(kill, cnt + CNT_REMOVED);
 }
 
 // Fat map (update_fat_page_map, :166-186): every cell of a thin block whose
@@ -340,6 +438,72 @@ void Band::maps(uint8_t* t, uint8_t* f, uint8_t* ff) {
       g_d2h_bytes += size_t(n);
     }
   SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Band::get_flags(uint8_t* h) {
+  SGS_CUDA(cudaMemcpyAsync(h, flags.p, size_t(n) * 64, cudaMemcpyDeviceToHost, stream));
+  g_d2h_bytes += size_t(n) * 64;
+  SGS_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Band::pull_flags() { get_flags(flags_h.data()); }
+
+void Band::filter_voxels(sgs_band_voxel_stats* st) {
+  const long N = n * 64;
+  if (N > long(INT32_MAX)) throw CudaError("container too large for the voxel filter", SGS_ERR_INPUT);
+  DevBuf<int32_t> vparent, vsize;
+  vparent.alloc(size_t(N));
+  vsize.alloc(size_t(N));
+  const unsigned cgrid = blocks_for(N, 256);
+  SGS_CUDA(cudaEventRecord(ev[0], stream));
+  SGS_CUDA(cudaMemsetAsync(counters.p, 0, CNT_N * sizeof(unsigned long long), stream));
+  vox_init_kernel<<<cgrid, 256, 0, stream>>>(N, thin.p, flags.p, vparent.p, vsize.p, counters.p);
+  vox_hook_kernel<<<cgrid, 256, 0, stream>>>(N, base.p, grid.p, gdim[0], gdim[1], gdim[2], thin.p, flags.p, vparent.p,
+                                              counters.p);
+  vox_flatten_kernel<<<cgrid, 256, 0, stream>>>(N, thin.p, flags.p, vparent.p, vsize.p, counters.p);
+  vox_roots_kernel<<<cgrid, 256, 0, stream>>>(N, vparent.p, vsize.p, counters.p);
+  SGS_CUDA(cudaGetLastError());
+  unsigned long long c[CNT_N];
+  SGS_CUDA(cudaMemcpyAsync(c, counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  if (c[CNT_ERROR]) throw CudaError("union-find exceeded its step bound", SGS_ERR_INTERNAL);
+  if (c[CNT_VOXELS] == 0) throw CudaError("no container voxels in the thin blocks", SGS_ERR_INPUT);
+  const long components = long(c[CNT_COMPONENTS]);
+  long removed = 0;
+  if (components > 1) {
+    if (c[CNT_BIG] != 1)
+      throw CudaError(std::to_string(c[CNT_BIG]) + " voxel components hold more than 30% of the voxels",
+                      SGS_ERR_INPUT);
+    vox_keep_kernel<<<cgrid, 256, 0, stream>>>(N, thin.p, vparent.p, int(c[CNT_BIG_ROOT]), flags.p, rho.p,
+                                               counters.p);
+    SGS_CUDA(cudaGetLastError());
+    SGS_CUDA(cudaMemcpyAsync(c + CNT_REMOVED, counters.p + CNT_REMOVED, sizeof(c[0]), cudaMemcpyDeviceToHost, stream));
+    removed = long(c[CNT_REMOVED]);
+  }
+  SGS_CUDA(cudaEventRecord(ev[1], stream));
+  if (removed) pull_flags();
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  float ms = 0;
+  SGS_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+  if (st) {
+    st->voxels = long(c[CNT_VOXELS]);
+    st->components = components;
+    st->kept = st->voxels - removed;
+    st->removed = removed;
+    st->device_seconds = ms * 1e-3;
+  }
+}
+
+long Band::kill_below(double threshold) {
+  const long N = n * 64;
+  SGS_CUDA(cudaMemsetAsync(counters.p + CNT_REMOVED, 0, sizeof(unsigned long long), stream));
+  vox_kill_kernel<<<blocks_for(N, 256), 256, 0, stream>>>(N, rho.p, threshold, flags.p, counters.p);
+  SGS_CUDA(cudaGetLastError());
+  unsigned long long killed = 0;
+  SGS_CUDA(cudaMemcpyAsync(&killed, counters.p + CNT_REMOVED, sizeof(killed), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  if (killed) pull_flags();
+  return long(killed);
 }
 
 // fraction_to_keep (:121-151), with the reference's int(fraction * container
@@ -546,4 +710,20 @@ SGS_API int sgs_band_update(sgs_band* b, const sgs_band_params* p, sgs_band_stat
 
 SGS_API int sgs_band_maps(sgs_band* b, uint8_t* thin, uint8_t* fat, uint8_t* fatter) {
   return band_call(b, [&](Band& B) { B.maps(thin, fat, fatter); });
+}
+
+SGS_API int sgs_band_get_flags(sgs_band* b, uint8_t* cell_flags) {
+  if (!cell_flags) return SGS_ERR_INPUT;
+  return band_call(b, [&](Band& B) { B.get_flags(cell_flags); });
+}
+
+SGS_API int sgs_band_filter_voxels(sgs_band* b, sgs_band_voxel_stats* stats) {
+  return band_call(b, [&](Band& B) { B.filter_voxels(stats); });
+}
+
+SGS_API int sgs_band_kill_below(sgs_band* b, double threshold, int64_t* killed) {
+  return band_call(b, [&](Band& B) {
+    const long k = B.kill_below(threshold);
+    if (killed) *killed = k;
+  });
 }

@@ -6,11 +6,12 @@
 // updates) and the fatter map (the blocks handed to fem_solve).  One update runs
 // Opt::update_thin_page_map (topo_opt/spgrid_topo_opt.cpp:92-152),
 // Opt::filter_isolated_blocks (:1404-1510) and Opt::update_fat_page_map
-// (:154-241).  Band holds the container on the device (block bases, a dense
-// block lookup, per-cell flags and densities) and the three maps as byte masks
-// in the caller's block order; only the driver's list order (its Morton page
-// order, needed where the reference indexes one list by another's positions) is
-// kept as a permutation.
+// (:154-241); the voxel-level Opt::filter_isolated_voxels (:1512-1633) and the
+// kill of Opt::threshold_and_kill (:1333-1344) change the cell flags.  Band
+// holds the container on the device (block bases, a dense block lookup, per-cell
+// flags and densities) and the three maps as byte masks in the caller's block
+// order; only the driver's list order (its Morton page order, needed where the
+// reference indexes one list by another's positions) is kept as a permutation.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -36,6 +37,9 @@ class Band {
   void set_fat(const uint8_t* fat);          // host, [nblocks]
   void update(const sgs_band_params& p, sgs_band_stats* stats);
   void maps(uint8_t* thin, uint8_t* fat, uint8_t* fatter);
+  void get_flags(uint8_t* flags);
+  void filter_voxels(sgs_band_voxel_stats* stats);
+  long kill_below(double threshold);
 
   long n = 0;                 // container blocks
   int gdim[3] = {0, 0, 0};    // dense block lookup extent (blocks per axis)
@@ -61,6 +65,7 @@ class Band {
 
  private:
   void keep_fraction(double fraction_to_keep, long n_thin);
+  void pull_flags();  // device flags -> flags_h after a change on the device
 };
 
 }  // namespace sgs

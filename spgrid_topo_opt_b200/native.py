@@ -27,7 +27,7 @@ EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", 
                     "sgs_design_get", "sgs_band_create", "sgs_band_destroy", "sgs_band_last_error",
                     "sgs_band_set_density", "sgs_band_get_density", "sgs_band_set_fat", "sgs_band_update",
                     "sgs_band_maps", "sgs_band_attach", "sgs_band_session", "sgs_band_step", "sgs_render",
-                    "sgs_band_render")
+                    "sgs_band_render", "sgs_band_get_flags", "sgs_band_filter_voxels", "sgs_band_kill_below")
 
 CELL_INSIDE, CELL_FORCE, CELL_FIXED = 1, 2, 4   # SGS_CELL_* (driver TopOptFlags bits 0-2)
 
@@ -53,6 +53,14 @@ class BandStats(C.Structure):
     _fields_ = [("container_blocks", C.c_int64), ("thin_before_pruning", C.c_int64), ("thin_blocks", C.c_int64),
                 ("fat_blocks", C.c_int64), ("fatter_blocks", C.c_int64), ("components", C.c_int64),
                 ("active_voxels", C.c_int64), ("device_seconds", C.c_double), ("fat_changed", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class VoxelStats(C.Structure):
+    _fields_ = [("voxels", C.c_int64), ("components", C.c_int64), ("kept", C.c_int64), ("removed", C.c_int64),
+                ("device_seconds", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -197,6 +205,12 @@ def load(build_if_missing: bool = False):
     L.sgs_band_update.restype = C.c_int
     L.sgs_band_maps.argtypes = [P, P, P, P]
     L.sgs_band_maps.restype = C.c_int
+    L.sgs_band_get_flags.argtypes = [P, P]
+    L.sgs_band_get_flags.restype = C.c_int
+    L.sgs_band_filter_voxels.argtypes = [P, C.POINTER(VoxelStats)]
+    L.sgs_band_filter_voxels.restype = C.c_int
+    L.sgs_band_kill_below.argtypes = [P, C.c_double, C.POINTER(C.c_int64)]
+    L.sgs_band_kill_below.restype = C.c_int
     L.sgs_band_attach.argtypes = [P, P, P]
     L.sgs_band_attach.restype = C.c_int
     L.sgs_band_session.argtypes = [P, P, C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
@@ -475,7 +489,9 @@ class Band:
     blocks with per-cell flags (CELL_*) and densities, and the thin / fat /
     fatter page maps (include/spgrid_fem.h, sgs_band_*).  ``update`` runs the
     driver's update_thin_page_map, filter_isolated_blocks and
-    update_fat_page_map (topo_opt/spgrid_topo_opt.cpp:92-241, 1404-1510)."""
+    update_fat_page_map (topo_opt/spgrid_topo_opt.cpp:92-241, 1404-1510);
+    ``filter_voxels`` and ``threshold_and_kill`` its voxel-level clean-up
+    (:1333-1344, 1512-1633).  ``flags`` is the host copy of the cell flags."""
 
     def __init__(self, base: np.ndarray, resolution, flags: np.ndarray, density: np.ndarray):
         L = load()
@@ -528,6 +544,37 @@ class Band:
         t, f, ff = (np.zeros(self.n, np.uint8) for _ in range(3))
         self._check(load().sgs_band_maps(self.h, _ptr(t), _ptr(f), _ptr(ff)))
         return t != 0, f != 0, ff != 0
+
+    def cell_flags(self) -> np.ndarray:
+        out = np.empty((self.n, 64), np.uint8)
+        self._check(load().sgs_band_get_flags(self.h, _ptr(out)))
+        return out
+
+    def filter_voxels(self) -> dict:
+        """The driver's voxel_connectivity_filtering action, Opt::filter_isolated_voxels
+        (topo_opt/spgrid_topo_opt.cpp:1512-1633): container cells of the thin
+        blocks outside the one component above 30% leave the container with
+        density 0 (sgs_band_filter_voxels)."""
+        st = VoxelStats()
+        self._check(load().sgs_band_filter_voxels(self.h, C.byref(st)))
+        if st.removed:
+            self.flags = self.cell_flags()
+        return st.as_dict()
+
+    def threshold_and_kill(self, threshold: float, **update) -> dict:
+        """Opt::threshold_and_kill (topo_opt/spgrid_topo_opt.cpp:1333-1344):
+        container cells below ``threshold`` leave the container, then the voxel
+        filter and a page-map update without the block filter.  ``update`` takes
+        the page-map settings of ``update``.  Returns the killed count and both
+        stats.  As in the reference, the kill stays applied when the filter
+        stops on an error."""
+        k = C.c_int64(0)
+        self._check(load().sgs_band_kill_below(self.h, float(threshold), C.byref(k)))
+        if k.value:
+            self.flags = self.cell_flags()
+        vox = self.filter_voxels()
+        maps = self.update(**dict(update, connectivity_filtering=False))
+        return {"killed": int(k.value), "voxels": vox, "maps": maps}
 
     def attach(self, session: "Session", container_block: np.ndarray):
         """Bind a session built from this band's fatter blocks: its input block i

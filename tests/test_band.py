@@ -190,3 +190,142 @@ def test_band_errors_leave_maps_unchanged(native_lib):
     band.close()
     with pytest.raises(native.SolverError):
         native.Band(base + 1, res, flags, dens)
+
+
+# ---------------------------------------------------------------- voxel filter (CPU, oracle)
+def _row(cells_per_block):
+    """Three blocks in a row along x; cells_per_block[b] lists the inside cells of block b."""
+    base = np.array([[8, 8, 8], [12, 8, 8], [16, 8, 8]], np.int32)
+    flags = np.zeros((3, 64), np.uint8)
+    for b, cells in enumerate(cells_per_block):
+        flags[b, cells] = torc.CELL_INSIDE
+    dens = np.where(flags != 0, 0.5, 0.0)
+    return base, flags, dens
+
+
+def test_oracle_voxel_filter_removes_a_small_island():
+    # block 0 full; block 2 holds one cell that touches nothing
+    base, flags, dens = _row([list(range(64)), [], [21]])
+    f, d, st = torc.filter_isolated_voxels(base, dens, flags, np.ones(3, bool))
+    assert st == {"voxels": 65, "components": 2, "kept": 64, "removed": 1}
+    assert f[2, 21] == 0 and d[2, 21] == 0.0
+    assert np.array_equal(f[:2], flags[:2]) and np.array_equal(d[:2], dens[:2])
+
+
+def test_oracle_voxel_filter_crosses_block_faces_but_not_edges():
+    # cell (3, 1, 1) of block 0 and (0, 1, 1) of block 1 share a face: one component
+    e_hi, e_lo = 3 * 16 + 1 * 4 + 1, 0 * 16 + 1 * 4 + 1
+    base, flags, dens = _row([list(range(64)), [e_lo], []])
+    _, _, st = torc.filter_isolated_voxels(base, dens, flags, np.ones(3, bool))
+    assert st["components"] == 1 and st["removed"] == 0
+    # (0, 2, 2) touches (3, 1, 1) only along an edge: a second component, removed
+    base, flags, dens = _row([list(range(64)), [0 * 16 + 2 * 4 + 2], []])
+    flags[0, 3 * 16 + 2 * 4 + 2] = 0
+    flags[0, 3 * 16 + 1 * 4 + 2] = 0
+    flags[0, 3 * 16 + 2 * 4 + 1] = 0
+    f, _, st = torc.filter_isolated_voxels(base, dens, flags, np.ones(3, bool))
+    assert st["components"] == 2 and st["removed"] == 1 and f[1].sum() == 0
+
+
+def test_oracle_voxel_filter_only_searches_thin_blocks():
+    base, flags, dens = _row([list(range(64)), [], [21]])
+    f, d, st = torc.filter_isolated_voxels(base, dens, flags, np.array([True, True, False]))
+    assert st["components"] == 1 and st["voxels"] == 64
+    assert np.array_equal(f, flags) and np.array_equal(d, dens)
+
+
+def test_oracle_voxel_filter_stops_where_the_reference_stops():
+    base, flags, dens = _row([list(range(32)), [], list(range(32))])     # two halves of 50%
+    with pytest.raises(torc.PageMapError):
+        torc.filter_isolated_voxels(base, dens, flags, np.ones(3, bool))
+    # four pieces of 25%: none above 30%
+    base, flags, dens = _row([[0, 63], [], [0, 63]])
+    with pytest.raises(torc.PageMapError):
+        torc.filter_isolated_voxels(base, dens, flags, np.ones(3, bool))
+    base, flags, dens = _row([[], [], []])
+    with pytest.raises(torc.PageMapError):
+        torc.filter_isolated_voxels(base, dens, flags, np.ones(3, bool))
+
+
+def test_oracle_kill_below_keeps_density_and_nan():
+    flags = np.full((1, 64), torc.CELL_INSIDE | torc.CELL_FORCE, np.uint8)
+    flags[0, 7] = 0
+    dens = np.full((1, 64), 0.9)
+    dens[0, :4] = 0.1
+    dens[0, 4] = np.nan
+    dens[0, 7] = 0.0
+    f, k = torc.kill_below(dens, flags, 0.5)
+    assert k == 4
+    assert f[0, :4].tolist() == [torc.CELL_FORCE] * 4 and f[0, 4] == flags[0, 4] and f[0, 7] == 0
+
+
+# ---------------------------------------------------------------- voxel filter (GPU)
+def _voxel_islands(flags, base):
+    """Clear the 26 neighbours of one inside cell per chosen block so that it is
+    an island (cells of other blocks are not touched, so some may stay connected
+    across a face)."""
+    out = flags.copy()
+    rng = np.random.default_rng(11)
+    for b in rng.choice(len(base), size=max(1, len(base) // 20), replace=False):
+        e = 1 * 16 + 1 * 4 + 1 + 21 * int(rng.integers(0, 2))      # (1,1,1) or (2,2,2): interior cells
+        i, j, k = e >> 4, (e >> 2) & 3, e & 3
+        for di in (-1, 0, 1):
+            for dj in (-1, 0, 1):
+                for dk in (-1, 0, 1):
+                    out[b, (i + di) * 16 + (j + dj) * 4 + (k + dk)] &= np.uint8(~torc.CELL_INSIDE & 0xFF)
+        out[b, e] |= torc.CELL_INSIDE
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("after_update", [False, True])
+def test_band_voxel_filter_matches_oracle(native_lib, after_update):
+    from spgrid_topo_opt_b200 import native
+    base, res, flags, dens = container(seed=7)
+    flags = _voxel_islands(flags, base)
+    band = native.Band(base, res, flags, dens)
+    thin = np.ones(len(base), bool)
+    if after_update:
+        band.update()
+        thin = band.maps()[0]
+    st = band.filter_voxels()
+    f, d, rst = torc.filter_isolated_voxels(base, dens, flags, thin)
+    assert {k: st[k] for k in rst} == rst
+    assert rst["removed"] > 0 and rst["components"] > 2
+    assert np.array_equal(band.cell_flags(), f) and np.array_equal(band.flags, f)
+    assert np.array_equal(band.density(), d)
+    # a second pass finds a single component and changes nothing
+    st2 = band.filter_voxels()
+    assert st2["components"] == 1 and st2["removed"] == 0 and st2["voxels"] == rst["kept"]
+    band.close()
+
+
+@pytest.mark.gpu
+def test_band_voxel_filter_errors_change_nothing(native_lib):
+    from spgrid_topo_opt_b200 import native
+    base, flags, dens = _row([list(range(32)), [], list(range(32))])
+    band = native.Band(base, np.array([40, 24, 24], np.int32), flags, dens)
+    with pytest.raises(native.SolverError) as e:
+        band.filter_voxels()
+    assert e.value.code == 1
+    assert np.array_equal(band.cell_flags(), flags) and np.array_equal(band.density(), dens)
+    band.close()
+
+
+@pytest.mark.gpu
+def test_band_threshold_and_kill_matches_oracle(native_lib):
+    from spgrid_topo_opt_b200 import native
+    base, res, flags, dens = container(seed=8, pruned=0.1)
+    band = native.Band(base, res, flags, dens)
+    band.update()
+    _, fat0, *_ = torc.update_page_maps(base, dens, flags, np.ones(len(base), bool))
+    thin0 = band.maps()[0]
+    out = band.threshold_and_kill(0.3)
+    f1, killed = torc.kill_below(dens, flags, 0.3)
+    f2, d2, vst = torc.filter_isolated_voxels(base, dens, f1, thin0)
+    ref = torc.update_page_maps(base, d2, f2, fat0, connectivity_filtering=False)
+    assert out["killed"] == killed > 0
+    assert {k: out["voxels"][k] for k in vst} == vst and vst["removed"] > 0
+    assert np.array_equal(band.cell_flags(), f2) and np.array_equal(band.density(), d2)
+    _compare(band, ref, out["maps"])
+    band.close()
