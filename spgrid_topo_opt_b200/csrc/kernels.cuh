@@ -109,8 +109,16 @@ __device__ __forceinline__ void pdl_wait() {
 // ---------------------------------------------------------------------------
 enum { OP_KU = 0, OP_RES = 1, OP_KUP = 2 };  // OP_KUP: K u with Project, and the CTA's partial u.(Ku)
 
-// halo geometry: nodes [-1,4]x[-1,4]x[-1,8] (6x6x10), cells [-1,3]x[-1,3]x[-1,7] (5x5x9)
+// halo geometry: nodes [-1,4]x[-1,4]x[-1,8] (6x6x10), cells [-1,3]x[-1,3]x[-1,7] (5x5x9).
+// In shared memory a y-row of the halo starts every HSY = 24 entries: a warp
+// reads 4 consecutive rows of 8 consecutive z at once, and with the row starts
+// at 0, 24, 48, 72 (mod 32 banks: 0, 24, 16, 8) those 32 words fall in distinct
+// banks (FP32), or in distinct bank pairs per half-warp (FP64).  Rows of 10
+// entries would put rows y and y+3 on the same banks.
 constexpr int HU = 360, HE = 225;
+constexpr int HSY = 24;
+constexpr int HSX = 5 * HSY + 10, HN = 6 * HSX;   // node halo: x-plane stride, entries
+constexpr int ESX = 4 * HSY + 9, HEN = 5 * ESX;   // cell halo
 
 template <typename T, int OP>
 __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ block_list, int nblocks,
@@ -119,8 +127,8 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
                                                         long N, T dx, const uint32_t* __restrict__ flags,
                                                         double* __restrict__ part) {
   pdl_wait();
-  __shared__ T su[3][HU];
-  __shared__ T sE[HE];
+  __shared__ T su[3][HN];
+  __shared__ T sE[HEN];
   __shared__ int snb[27];
   const int bi = block_list ? block_list[blockIdx.x] : blockIdx.x;
   if (bi >= 0 && threadIdx.x < 27) snb[threadIdx.x] = nbr[long(bi) * 27 + threadIdx.x];
@@ -138,16 +146,17 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
       bb = u[idx + N];
       c = u[idx + 2 * N];
     }
-    su[0][h] = a;
-    su[1][h] = bb;
-    su[2][h] = c;
+    const int s = sx * HSX + sy * HSY + sz;
+    su[0][s] = a;
+    su[1][s] = bb;
+    su[2][s] = c;
   }
   for (int h = threadIdx.x; h < HE; h += 128) {
     const int sx = h / 45, sy = (h / 9) % 5, sz = h % 9;
     const int lx = sx - 1, ly = sy - 1, lz = sz - 1;
     const int dxb = lx < 0 ? 0 : 1, dyb = ly < 0 ? 0 : 1, dzb = lz < 0 ? 0 : 1;
     const int nb = snb[dxb * 9 + dyb * 3 + dzb];
-    sE[h] = nb >= 0 ? E[long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7)] : T(0);
+    sE[sx * ESX + sy * HSY + sz] = nb >= 0 ? E[long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7)] : T(0);
   }
   __syncthreads();
   const int e = threadIdx.x;
@@ -158,13 +167,13 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
   for (int I = 0; I < 8; ++I) {
     const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
     const int cx = x - Ix, cy = y - Iy, cz = z - Iz;  // cell, in [-1,3]x[-1,3]x[-1,7]
-    const T Ec = sE[((cx + 1) * 5 + (cy + 1)) * 9 + (cz + 1)];
+    const T Ec = sE[(cx + 1) * ESX + (cy + 1) * HSY + (cz + 1)];
     if (Ec == T(0)) continue;
     T g0 = 0, g1 = 0, g2 = 0;
 #pragma unroll
     for (int J = 0; J < 8; ++J) {
       const int nx = cx + (J >> 2) + 1, ny = cy + ((J >> 1) & 1) + 1, nz = cz + (J & 1) + 1;
-      const int h = (nx * 6 + ny) * 10 + nz;
+      const int h = nx * HSX + ny * HSY + nz;
       const T ux = su[0][h], uy = su[1][h], uz = su[2][h];
       const int k = (I * 8 + J) * 9;
       g0 += kc<T>(k + 0) * ux + kc<T>(k + 1) * uy + kc<T>(k + 2) * uz;
@@ -195,7 +204,7 @@ __global__ void __launch_bounds__(128) level0_op_kernel(const int* __restrict__ 
     out[gidx] = f0;
     out[gidx + N] = f1;
     out[gidx + 2 * N] = f2;
-    const int hc = ((x + 1) * 6 + (y + 1)) * 10 + (z + 1);
+    const int hc = (x + 1) * HSX + (y + 1) * HSY + (z + 1);
     double d = double(su[0][hc]) * double(f0) + double(su[1][hc]) * double(f1) + double(su[2][hc]) * double(f2);
 #pragma unroll
     for (int o = 16; o; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
@@ -474,8 +483,8 @@ __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int
                                                           const typename Pack4<T>::type* __restrict__ u4,
                                                           const T* __restrict__ b, T* __restrict__ out, long N, T dx) {
   pdl_wait();
-  __shared__ T su[3][HU];
-  __shared__ T sE[HU];
+  __shared__ T su[3][HN];
+  __shared__ T sE[HN];
   __shared__ int snb[27];
   const int bi = blockIdx.x;
   KcReg<T> K;
@@ -488,10 +497,11 @@ __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int
     const int dxb = lx < 0 ? 0 : (lx > 3 ? 2 : 1), dyb = ly < 0 ? 0 : (ly > 3 ? 2 : 1), dzb = lz < 0 ? 0 : (lz > 7 ? 2 : 1);
     const int nb = snb[dxb * 9 + dyb * 3 + dzb];  // the zero pad block where there is none
     const auto v = u4[long(nb) * 128 + ((lx & 3) << 5) + ((ly & 3) << 3) + (lz & 7)];
-    su[0][h] = v.x;
-    su[1][h] = v.y;
-    su[2][h] = v.z;
-    sE[h] = v.w;
+    const int s = sx * HSX + sy * HSY + sz;
+    su[0][s] = v.x;
+    su[1][s] = v.y;
+    su[2][s] = v.z;
+    sE[s] = v.w;
   }
   __syncthreads();
   const int e = threadIdx.x;
@@ -502,13 +512,13 @@ __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int
   for (int I = 0; I < 8; ++I) {
     const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
     const int cx = x - Ix, cy = y - Iy, cz = z - Iz;  // cell = its min-corner node, in the halo
-    const T Ec = sE[((cx + 1) * 6 + (cy + 1)) * 10 + (cz + 1)];
+    const T Ec = sE[(cx + 1) * HSX + (cy + 1) * HSY + (cz + 1)];
     if (Ec == T(0)) continue;
     T g0 = 0, g1 = 0, g2 = 0;
 #pragma unroll
     for (int J = 0; J < 8; ++J) {
       const int nx = cx + (J >> 2) + 1, ny = cy + ((J >> 1) & 1) + 1, nz = cz + (J & 1) + 1;
-      const int h = (nx * 6 + ny) * 10 + nz;
+      const int h = nx * HSX + ny * HSY + nz;
       const T ux = su[0][h], uy = su[1][h], uz = su[2][h];
       g0 += K(I, J, 0, 0) * ux + K(I, J, 0, 1) * uy + K(I, J, 0, 2) * uz;
       g1 += K(I, J, 1, 0) * ux + K(I, J, 1, 1) * uy + K(I, J, 1, 2) * uz;

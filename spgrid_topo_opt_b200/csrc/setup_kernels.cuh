@@ -336,12 +336,15 @@ __global__ void sgj_gather_kernel(const double* __restrict__ M, long ld, int K, 
   if (P && t < long(SGJ) * SGJ) P[t] = M[(k0 + t / SGJ) * ld + k0 + t % SGJ];
 }
 
-// One FP64 tensor-core MMA (m8n8k4): D = A B + D on an 8x8 tile, each lane
-// holding A[lane/4][lane%4], B[lane%4][lane/4] and D[lane/4][2*(lane%4) + {0,1}].
-__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+// One FP64 tensor-core MMA (m16n8k8): D = A B + D on a 16 x 8 tile.  With
+// g = lane / 4 and t = lane % 4, a lane holds A[g][t], A[g+8][t], A[g][t+4],
+// A[g+8][t+4]; B[t][g], B[t+4][g]; D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1].
+__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 // C(tile) = alpha * A(tile rows, 0:k) * B(0:k, tile cols) + beta * C(tile) on
@@ -351,7 +354,7 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 // square grid (blockIdx.x), leaving out row and column `skip` (none if < 0);
 // SGJ_CROSS the lower tiles of row and column `skip` (blockIdx.x = J for
 // J <= skip, else I).
-constexpr int SGJ_AS = 20, SGJ_BS = 130;  // padded strides: conflict-free fragment loads
+constexpr int SGJ_AS = 20, SGJ_BS = 132;  // padded strides (4 mod 16 doubles): conflict-free fragment loads
 constexpr int SGJ_STAGE = SGJ * SGJ_AS + SGJ_K * SGJ_BS;  // doubles per pipeline stage
 constexpr size_t SGJ_SMEM = 2 * SGJ_STAGE * sizeof(double);
 enum { SGJ_DENSE = 0, SGJ_LOWER = 1, SGJ_CROSS = 2 };
@@ -406,11 +409,11 @@ __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* _
     }
     cp_async_commit();
   };
-  double acc[4][8][2];
+  double acc[2][8][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0;
+    for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0;
   const int nchunks = k / SGJ_K;
   stage(0, 0);
   for (int c = 0; c < nchunks; ++c) {
@@ -424,30 +427,41 @@ __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* _
     const double* As = sg + (c & 1) * SGJ_STAGE;
     const double* Bs = As + SGJ * SGJ_AS;
 #pragma unroll
-    for (int k4 = 0; k4 < SGJ_K; k4 += 4) {
-      double a[4], b[8];
+    for (int k8 = 0; k8 < SGJ_K; k8 += 8) {
+      double a[2][4], b[8][2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[(wr + 8 * i + fr) * SGJ_AS + k4 + fc];
+      for (int i = 0; i < 2; ++i) {
+        const double* r = As + (wr + 16 * i + fr) * SGJ_AS + k8 + fc;
+        a[i][0] = r[0];
+        a[i][1] = r[8 * SGJ_AS];
+        a[i][2] = r[4];
+        a[i][3] = r[8 * SGJ_AS + 4];
+      }
 #pragma unroll
-      for (int j = 0; j < 8; ++j) b[j] = Bs[(k4 + fc) * SGJ_BS + wc + 8 * j + fr];
+      for (int j = 0; j < 8; ++j) {
+        b[j][0] = Bs[(k8 + fc) * SGJ_BS + wc + 8 * j + fr];
+        b[j][1] = Bs[(k8 + fc + 4) * SGJ_BS + wc + 8 * j + fr];
+      }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        for (int j = 0; j < 8; ++j) dmma_16x8x8(acc[i][j], a[i], b[j]);
     }
     __syncthreads();  // the stage is refilled two chunks later
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    double* row = C + (I * SGJ + wr + 8 * i + fr) * ldc + J * SGJ + wc + 2 * fc;
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
+    for (int hr = 0; hr < 2; ++hr) {
+      double* row = C + (I * SGJ + wr + 16 * i + 8 * hr + fr) * ldc + J * SGJ + wc + 2 * fc;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        double* p = row + 8 * j + h;
-        *p = (beta != 0 ? beta * *p : 0.0) + alpha * acc[i][j][h];
-      }
-  }
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          double* p = row + 8 * j + h;
+          *p = (beta != 0 ? beta * *p : 0.0) + alpha * acc[i][j][2 * hr + h];
+        }
+    }
 }
 
 // mirror the lower triangle into the upper one
