@@ -254,7 +254,7 @@ def run_ours(args, rank, world):
     peak, peak_kind = measured_peaks()
     sweep_bytes = nodes * (10 * 4 + 4)
     achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9
-    ku_bytes = nodes * 7 * 4
+    ku_bytes = nodes * 7 * 8   # the FP64 PCG matvec: s read, q written (3 x 8 B each), E (8 B)
     # DRAM bytes of one full sweep (dram__bytes_read.sum + dram__bytes_write.sum over its 8
     # colour-pass launches) from the ncu launch list of this workload, where one was taken
     traffic = SWEEP_DRAM_BYTES.get(config_dict(args, inp, {})["workload"])

@@ -202,8 +202,9 @@ SGS_API int sgs_apply(sgs_session* s, int op, int level, int arg, const double* 
 SGS_API int sgs_level_stencils(sgs_session* s, int level, double* out, uint32_t* spokes);
 
 /* Average device time (ms, CUDA events) of `reps` back-to-back runs of a level-0
- * operator on the session's resident data: 0 K*u, 1 residual, 2 one smoothing
- * sweep (8 colours), 3 one preconditioner application (V-cycle). */
+ * operator on the session's resident data: 0 the PCG matvec q = K s (FP64, with
+ * Project and the s.q partials), 1 residual, 2 one smoothing sweep (8 colours),
+ * 3 one preconditioner application (V-cycle). */
 SGS_API int sgs_time_op(sgs_session* s, int op, int reps, double* ms);
 
 /* Decode a blob and encode it again with this library's codec (which = 0 for

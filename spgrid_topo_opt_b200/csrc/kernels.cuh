@@ -477,6 +477,109 @@ __global__ void __launch_bounds__(128, MINB) gs0_list4_kernel(const int* __restr
   u4[g] = Pack4<T>::make(v0, v1, v2, Ec[0]);  // corner I = 0: the node's own cell
 }
 
+// gs0_list4_kernel for the short passes of the boundary band (about 10^3
+// nodes): those are bound by one thread's chain of dependent loads, so eight
+// threads share a node, thread I taking the cell of which the node is corner I.
+// The Q1 element is symmetric under reflections, K(I, J) = S K(0, I^J) S with S
+// = diag(-1 on the axes where I has its bit) (checked on the host at set-up);
+// looping over J' = I^J keeps the coefficients K(0, J') compile-time register
+// selections while the corner J a thread reads varies with I.  Per thread: 8
+// gathers and 72 FMA; the cells' E g and diagonal blocks are summed over the
+// eight threads with shuffles and thread 0 updates the node.  Same products as
+// gs0_list4_kernel, summed in another order.
+template <typename T>
+__global__ void __launch_bounds__(128) gs0_cell4_kernel(const int* __restrict__ list, int n,
+                                                        const int* __restrict__ nbrz,
+                                                        typename Pack4<T>::type* u4, const T* __restrict__ b,
+                                                        const uint32_t* __restrict__ flags, int N, T dx) {
+  using V = typename Pack4<T>::type;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = t >> 3, I = t & 7;  // groups of 8 threads never straddle a warp
+  if (k >= n) {
+    pdl_wait();
+    return;
+  }
+  const int raw = list[k];
+  const int g = raw >= 0 ? raw : ~raw;
+  const uint32_t fl = flags[g];
+  const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
+  // per axis: block selector and slot for offset 0 and for the offset 1 - 2 I_a
+  // towards the cell's other corners
+  const int bi = g >> 7, e = g & 127;
+  const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
+  const int Ix = I >> 2, Iy = (I >> 1) & 1, Iz = I & 1;
+  const int x1 = x + 1 - 2 * Ix, y1 = y + 1 - 2 * Iy, z1 = z + 1 - 2 * Iz;
+  const int sx[2] = {9, (x1 < 0 ? 0 : (x1 > 3 ? 2 : 1)) * 9}, lx[2] = {(x & 3) << 5, (x1 & 3) << 5};
+  const int sy[2] = {3, (y1 < 0 ? 0 : (y1 > 3 ? 2 : 1)) * 3}, ly[2] = {(y & 3) << 3, (y1 & 3) << 3};
+  const int sz[2] = {1, z1 < 0 ? 0 : (z1 > 7 ? 2 : 1)}, lz[2] = {z & 7, z1 & 7};
+  const int* nb = nbrz + long(bi) * 27;
+  int idx[8];
+#pragma unroll
+  for (int Jp = 0; Jp < 8; ++Jp) {
+    const int a = Jp >> 2, c = (Jp >> 1) & 1, d = Jp & 1;
+    idx[Jp] = (__ldg(nb + sx[a] + sy[c] + sz[d]) << 7) + lx[a] + ly[c] + lz[d];
+  }
+  KcReg<T> K;
+  K.load();
+  pdl_wait();
+  if (raw < 0) {
+    if (I == 0) {
+      V v = u4[g];
+      if (fx) v.x = T(0);
+      if (fy) v.y = T(0);
+      if (fz) v.z = T(0);
+      u4[g] = v;
+    }
+    return;
+  }
+  const T s0 = Ix ? T(-1) : T(1), s1 = Iy ? T(-1) : T(1), s2 = Iz ? T(-1) : T(1);
+  T gv[3] = {0, 0, 0}, Ec = 0, uc[3] = {0, 0, 0};
+#pragma unroll
+  for (int Jp = 0; Jp < 8; ++Jp) {
+    const V v = u4[idx[Jp]];
+    if (Jp == 0) {  // J = I: the node itself
+      uc[0] = v.x;
+      uc[1] = v.y;
+      uc[2] = v.z;
+    }
+    if (Jp == I) Ec = v.w;  // J = 0: the cell's min corner carries its E
+    const T w0 = s0 * v.x, w1 = s1 * v.y, w2 = s2 * v.z;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      gv[r] = fma(K(0, Jp, r, 0), w0, fma(K(0, Jp, r, 1), w1, fma(K(0, Jp, r, 2), w2, gv[r])));
+  }
+  // this cell's share of the node's row and of its diagonal block
+  T red[9] = {Ec * s0 * gv[0], Ec * s1 * gv[1], Ec * s2 * gv[2],
+              Ec * K(0, 0, 0, 0), Ec * K(0, 0, 1, 1), Ec * K(0, 0, 2, 2),
+              Ec * (s0 * s1) * K(0, 0, 0, 1), Ec * (s0 * s2) * K(0, 0, 0, 2), Ec * (s1 * s2) * K(0, 0, 1, 2)};
+  // the eight threads of a node take the same branches: shuffle within the group only
+  const unsigned group = 0xffu << (threadIdx.x & 24);
+#pragma unroll
+  for (int o = 4; o; o >>= 1)
+#pragma unroll
+    for (int q = 0; q < 9; ++q) red[q] += __shfl_xor_sync(group, red[q], o);
+  if (I != 0) return;
+  const T r0 = b[g] - red[0] * dx, r1 = b[g + N] - red[1] * dx, r2 = b[g + 2 * N] - red[2] * dx;
+  T d0 = red[3] * dx, d1 = red[4] * dx, d2 = red[5] * dx, d3 = red[6] * dx, d4 = red[7] * dx, d5 = red[8] * dx;
+  if (fx) { d0 = 1; d3 = 0; d4 = 0; }
+  if (fy) { d1 = 1; d3 = 0; d5 = 0; }
+  if (fz) { d2 = 1; d4 = 0; d5 = 0; }
+  const T m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
+  const T m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
+  const T inv = T(1) / (d0 * m11 + d3 * m12 + d4 * m13);
+  T a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
+  if (fx) { a0 = 0; a3 = 0; a4 = 0; }
+  if (fy) { a1 = 0; a3 = 0; a5 = 0; }
+  if (fz) { a2 = 0; a4 = 0; a5 = 0; }
+  T v0 = uc[0] + r0 * a0 + r1 * a3 + r2 * a4;
+  T v1 = uc[1] + r0 * a3 + r1 * a1 + r2 * a5;
+  T v2 = uc[2] + r0 * a4 + r1 * a5 + r2 * a2;
+  if (fx) v0 = 0;
+  if (fy) v1 = 0;
+  if (fz) v2 = 0;
+  u4[g] = Pack4<T>::make(v0, v1, v2, Ec);  // thread 0: the node's own cell
+}
+
 // level0_op_kernel<T, OP_RES> on the packed iterate: r = b - dx K u
 template <typename T>
 __global__ void __launch_bounds__(128) level0_res4_kernel(int nblocks, const int* __restrict__ nbrz,

@@ -514,6 +514,36 @@ __global__ void gemv_kernel(const double* __restrict__ M, long ld, long n, const
   if (lane == 0) y[row] = s;
 }
 
+// y = M x with an FP32 copy of M (ld a multiple of 128, rows 16-byte aligned),
+// 32 rows per CTA of 1024 threads, one warp per row.  x is staged once per CTA
+// in shared memory as FP32 (exact: in mixed precision it is gathered from an
+// FP32 right-hand side), so the loop streams only M.
+constexpr int GEMV32_ROWS = 32;
+__global__ void __launch_bounds__(1024) gemv32_kernel(const float* __restrict__ M, long ld, long n,
+                                                      const double* __restrict__ x, double* __restrict__ y) {
+  extern __shared__ float4 xs4[];
+  float* xs = reinterpret_cast<float*>(xs4);
+  pdl_wait();
+  for (long c = threadIdx.x; c < n; c += blockDim.x) xs[c] = float(x[c]);
+  __syncthreads();
+  const long row = long(blockIdx.x) * GEMV32_ROWS + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const float4* m = reinterpret_cast<const float4*>(M + row * ld);
+  float s0 = 0.f, s1 = 0.f;
+  for (long c = lane; c < n / 4; c += 32) {
+    const float4 a = __ldcs(m + c);  // read once per application: do not keep it in L2
+    const float4 v = xs4[c];
+    s0 = fmaf(a.x, v.x, s0);
+    s1 = fmaf(a.y, v.y, s1);
+    s0 = fmaf(a.z, v.z, s0);
+    s1 = fmaf(a.w, v.w, s1);
+  }
+  double s = double(s0) + double(s1);
+  for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) y[row] = s;
+}
+
 template <typename T>
 __global__ void bottom_scatter_kernel(int ndof, const int* __restrict__ dof_node, const double* __restrict__ xs,
                                       T* __restrict__ u, long N) {

@@ -87,6 +87,7 @@ struct Bottom {
   long n = 0, ld = 0;
   DevBuf<int> dof_node, node_dof;
   DevBuf<double> Minv, xb, xs;
+  DevBuf<float> Minv32;  // mixed precision: the FP32 V-cycle applies an FP32 copy of Minv
 };
 
 enum Precision { PREC_REFERENCE = 0, PREC_FP64 = 1, PREC_MIXED = 2 };
@@ -231,6 +232,10 @@ class Solver {
                 (neg ? -kv[c] : kv[c]) != kc32[(I * 8 + J) * 9 + v * 3 + w] ||
                 (neg ? -kv64[c] : kv64[c]) != kc64[(I * 8 + J) * 9 + v * 3 + w])
               throw CudaError("element table classes are inconsistent", SGS_ERR_INTERNAL);
+            // the reflection symmetry gs0_cell4_kernel relies on: K(I, J) = S K(0, I^J) S
+            const double sg = ((I >> (2 - v)) & 1 ? -1.0 : 1.0) * ((I >> (2 - w)) & 1 ? -1.0 : 1.0);
+            if (Kmu[I][J][v][w] != sg * Kmu[0][I ^ J][v][w] || Kla[I][J][v][w] != sg * Kla[0][I ^ J][v][w])
+              throw CudaError("element table lacks the reflection symmetry", SGS_ERR_INTERNAL);
           }
     SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kv32, kv, sizeof(kv), 0, cudaMemcpyHostToDevice, stream));
     SGS_CUDA(cudaMemcpyToSymbolAsync(c_Kv64, kv64, sizeof(kv64), 0, cudaMemcpyHostToDevice, stream));
@@ -503,6 +508,17 @@ class Solver {
       identity_pad_kernel<<<blocks_for(bottom.ld - bottom.n, 64), 64, 0, stream>>>(bottom.Minv.p, bottom.ld, bottom.n);
     SGS_CUDA(cudaGetLastError());
     invert_dense(bottom.Minv.p, bottom.ld);
+    if (mixed()) {
+      SGS_CUDA(cudaFuncSetAttribute(gemv32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(bottom.ld * sizeof(float))));
+      bottom.Minv32.alloc(bottom.Minv.n);
+      convert_kernel<float, double><<<blocks_for(long(bottom.Minv.n), 256), 256, 0, stream>>>(
+          bottom.Minv32.p, bottom.Minv.p, long(bottom.Minv.n));
+      SGS_CUDA(cudaGetLastError());
+      // Minv stays allocated until the session ends: released here, its block
+      // would be split by later allocations of the set-up, and the next
+      // session's inverse would then grow the memory pool through the driver
+    }
   }
 
   // In-place inverse of the SPD bottom matrix (ld a multiple of SGJ): symmetric
@@ -669,6 +685,12 @@ class Solver {
         const int c = (boundary ? 8 : 0) + (forward ? k : 7 - k);
         const int lo = d.gs_off[c], cnt = d.gs_off[c + 1] - lo;
         if (cnt == 0) continue;
+        if (!u && boundary) {  // boundary band: few nodes, eight threads per node
+          launch(gs0_cell4_kernel<T>, blocks_for(long(cnt) * 8, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbrz.p, d.u4.p,
+                 b, d.flags.p, int(d.N), T(P.dx));
+          ++launch_counter;
+          continue;
+        }
         if (!u) {  // the packed iterate of the V-cycle
           if constexpr (sizeof(T) == 4)
             launch(gs0_list4_kernel<T, 6>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbrz.p, d.u4.p, b,
@@ -746,8 +768,12 @@ class Solver {
     if (bottom.ndof_nodes > 0) {
       launch(bottom_gather_kernel<T>, blocks_for(bottom.ndof_nodes, 128), 128, 0, bottom.ndof_nodes, bottom.dof_node.p,
                                                                                      d.b.p, d.N, bottom.xb.p);
-      launch(gemv_kernel, blocks_for(bottom.ld * 32, 256), 256, 0, bottom.Minv.p, bottom.ld, bottom.ld, bottom.xb.p,
-                                                                      bottom.xs.p);
+      if (bottom.Minv32.p)
+        launch(gemv32_kernel, blocks_for(bottom.ld, GEMV32_ROWS), 1024, size_t(bottom.ld) * sizeof(float),
+               bottom.Minv32.p, bottom.ld, bottom.ld, bottom.xb.p, bottom.xs.p);
+      else
+        launch(gemv_kernel, blocks_for(bottom.ld * 32, 256), 256, 0, bottom.Minv.p, bottom.ld, bottom.ld, bottom.xb.p,
+               bottom.xs.p);
       launch(bottom_scatter_kernel<T>, blocks_for(bottom.ndof_nodes, 128), 128, 0, bottom.ndof_nodes,
                                                                                       bottom.dof_node.p, bottom.xs.p,
                                                                                       d.u.p, d.N);
@@ -1962,7 +1988,7 @@ static double time_op(Solver& S, int op, int reps) {
   const bool packed = S.packed0();
   auto run = [&]() {
     if (op == 0) {
-      S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);
+      S.level0<double, OP_KUP>(S.s.p, nullptr, S.q.p);  // the PCG matvec, FP64 in every mode
     } else if (op == 1) {
       if (packed) {
         S.launch(level0_res4_kernel<T>, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, d.b.p, d.r.p, d.N, T(S.P.dx));
@@ -2502,7 +2528,8 @@ SGS_API void fem_solve_free(void* blob) { delete[] static_cast<char*>(blob); }
 SGS_API int sgs_time_op(sgs_session* h, int op, int reps, double* ms) {
   if (!h || !ms || host_only(h) || reps <= 0 || op < 0 || op > 3) return SGS_ERR_INPUT;
   try {
-    *ms = h->solver->mixed() && op != 3 ? time_op<float>(*h->solver, op, reps) : time_op<double>(*h->solver, op, reps);
+    *ms = h->solver->mixed() && op != 0 && op != 3 ? time_op<float>(*h->solver, op, reps)
+                                                   : time_op<double>(*h->solver, op, reps);
   } catch (const CudaError& e) {
     h->error = e.what();
     return e.code;

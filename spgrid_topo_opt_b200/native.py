@@ -437,8 +437,8 @@ class Session:
         self.inputs.density.data = rho.copy()
 
     def time_op(self, op: int, reps: int = 20) -> float:
-        """Average device milliseconds of a level-0 operator (0 K*u, 1 residual,
-        2 smoothing sweep, 3 V-cycle) on the resident data."""
+        """Average device milliseconds of a level-0 operator (0 the FP64 PCG
+        matvec K*s, 1 residual, 2 smoothing sweep, 3 V-cycle) on the resident data."""
         ms = C.c_double(0)
         self._check(load().sgs_time_op(self.h, op, reps, C.byref(ms)))
         return ms.value
