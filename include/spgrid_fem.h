@@ -297,6 +297,15 @@ SGS_API int sgs_band_filter_voxels(sgs_band* b, sgs_band_voxel_stats* stats);
  * page-map update without the block filter (:1341-1343); chain
  * sgs_band_filter_voxels and sgs_band_update for that.  killed may be NULL. */
 SGS_API int sgs_band_kill_below(sgs_band* b, double threshold, int64_t* killed);
+/* Replaces Opt::threshold_density (spgrid_topo_opt.cpp:1780-1797) and, with a
+ * threshold >= 0, Opt::threshold_density_trail(threshold, true) (:1756-1778):
+ * every cell of the fat blocks whose density is >= the threshold, or that has a
+ * fixed density, becomes 1, every other cell of those blocks 0.  A negative
+ * threshold asks for the reference's bisection on [0, 1] (until lo + 1e-8 >= hi)
+ * against volume_fraction x the container voxel count; the threshold used and
+ * the solid voxel count come back (either pointer may be NULL). */
+SGS_API int sgs_band_threshold_density(sgs_band* b, double volume_fraction, double threshold,
+                                       double* threshold_used, int64_t* solid_voxels);
 
 /* The driver's iteration on a band.  A session holds the fatter blocks as the
  * driver packs them into FEMInputs (spgrid_topo_opt.cpp:1068-1160): its input

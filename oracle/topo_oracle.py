@@ -386,3 +386,35 @@ def kill_below(density, flags, threshold: float):
     kill = ((flg & CELL_INSIDE) != 0) & (np.asarray(density, np.float64).reshape(flg.shape) < threshold)
     flg[kill] &= np.uint8(~CELL_INSIDE & 0xFF)
     return flg, int(np.count_nonzero(kill))
+
+
+def threshold_density(flags, fat, rho, total_inside: int, volume_fraction: float, threshold=None):
+    """Opt::threshold_density (spgrid_topo_opt.cpp:1780-1797) over
+    threshold_density_trail (:1756-1778): all 64 cells of every fat block count
+    as solid when their density is >= t or they have a fixed density; the
+    bisection on [0, 1] runs until lo + 1e-8 >= hi, keeping lo while the solid
+    count exceeds volume_fraction x total_inside, and the design is thresholded
+    at lo (1 solid, 0 otherwise; cells outside fat blocks keep their density).
+    A given threshold is applied directly.  Returns (density, threshold, solid count)."""
+    flg = np.asarray(flags, np.uint8).reshape(-1, 64)
+    rho = np.asarray(rho, np.float64).reshape(-1, 64)
+    fat = np.asarray(fat, bool)
+    fixed = (flg[fat] & CELL_FIXED) != 0
+    d = rho[fat]
+
+    def count(t):
+        return int(np.count_nonzero((d >= t) | fixed))
+
+    if threshold is None:
+        target = volume_fraction * float(total_inside)
+        lo, hi = 0.0, 1.0
+        while lo + 1e-8 < hi:
+            mid = (lo + hi) * 0.5
+            if float(count(mid)) > target:
+                lo = mid
+            else:
+                hi = mid
+        threshold = lo
+    out = rho.copy()
+    out[fat] = np.where((d >= threshold) | fixed, 1.0, 0.0)
+    return out, threshold, count(threshold)

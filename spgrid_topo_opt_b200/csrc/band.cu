@@ -20,7 +20,7 @@ namespace {
 constexpr int BAND_WARPS = 8;  // warps per CTA of the warp-per-block kernels
 enum {
   CNT_THIN = 0, CNT_FAT, CNT_FATTER, CNT_ACTIVE, CNT_COMPONENTS, CNT_BIG, CNT_BIG_ROOT, CNT_ERROR, CNT_FAT_CHANGED,
-  CNT_VOXELS, CNT_REMOVED, CNT_N
+  CNT_VOXELS, CNT_REMOVED, CNT_SOLID, CNT_N
 };
 
 // Block of the container holding the cell block (bx, by, bz), or -1.
@@ -284,6 +284,25 @@ __global__ void vox_kill_kernel(long N, const double* __restrict__ rho, double t
   warp_count(kill, cnt + CNT_REMOVED);
 }
 
+// threshold_density_trail (:1756-1778): the cells of fat blocks (all 64, as the
+// reference walks whole blocks) with density >= t or a fixed density count as
+// solid; with apply their density becomes 1, else 0.
+__global__ void band_threshold_kernel(long n, const uint8_t* __restrict__ fat, const uint8_t* __restrict__ flags,
+                                      double* __restrict__ rho, double t, int apply, unsigned long long* cnt) {
+  const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long b = long(blockIdx.x) * BAND_WARPS + wl;
+  if (b >= n || !fat[b]) return;
+  int solid = 0;
+  for (int h = 0; h < 2; ++h) {
+    const long c = b * 64 + lane + 32 * h;
+    const bool s = rho[c] >= t || (flags[c] & SGS_CELL_FIXED);
+    solid += s;
+    if (apply) rho[c] = s ? 1.0 : 0.0;
+  }
+  for (int o = 16; o; o >>= 1) solid += __shfl_xor_sync(0xffffffffu, solid, o);
+  if (lane == 0 && solid) atomicAdd(cnt + CNT_SOLID, (unsigned long long)solid);
+}
+
 // Fat map (update_fat_page_map, :166-186): every cell of a thin block whose
 // density exceeds active_threshold marks the pages of its 8 diagonal neighbours
 // at fat_margin that belong to the container.  With fat_margin <= 4 those pages
@@ -492,6 +511,38 @@ void Band::filter_voxels(sgs_band_voxel_stats* st) {
     st->removed = removed;
     st->device_seconds = ms * 1e-3;
   }
+}
+
+long Band::threshold_trail(double t, bool apply) {
+  SGS_CUDA(cudaMemsetAsync(counters.p + CNT_SOLID, 0, sizeof(unsigned long long), stream));
+  band_threshold_kernel<<<blocks_for(n, BAND_WARPS), 32 * BAND_WARPS, 0, stream>>>(n, fat.p, flags.p, rho.p, t,
+                                                                                 apply ? 1 : 0, counters.p);
+  SGS_CUDA(cudaGetLastError());
+  unsigned long long c = 0;
+  SGS_CUDA(cudaMemcpyAsync(&c, counters.p + CNT_SOLID, sizeof(c), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  return long(c);
+}
+
+// threshold_density (:1780-1797): bisection on [0, 1] until lo + 1e-8 >= hi for
+// the threshold whose solid count meets volume_fraction x total_container_voxels,
+// then the design is thresholded at lo.  A threshold given (>= 0) is applied as is.
+long Band::threshold_density(double volume_fraction, double threshold, double* used) {
+  double t = threshold;
+  if (!(threshold >= 0)) {
+    const double target = volume_fraction * double(total_inside);
+    double lo = 0, hi = 1;
+    while (lo + 1e-8 < hi) {
+      const double mid = (lo + hi) * 0.5;
+      if (double(threshold_trail(mid, false)) > target)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    t = lo;
+  }
+  if (used) *used = t;
+  return threshold_trail(t, true);
 }
 
 long Band::kill_below(double threshold) {
@@ -725,5 +776,13 @@ SGS_API int sgs_band_kill_below(sgs_band* b, double threshold, int64_t* killed) 
   return band_call(b, [&](Band& B) {
     const long k = B.kill_below(threshold);
     if (killed) *killed = k;
+  });
+}
+
+SGS_API int sgs_band_threshold_density(sgs_band* b, double volume_fraction, double threshold, double* threshold_used,
+                                       int64_t* solid_voxels) {
+  return band_call(b, [&](Band& B) {
+    const long v = B.threshold_density(volume_fraction, threshold, threshold_used);
+    if (solid_voxels) *solid_voxels = v;
   });
 }

@@ -40,6 +40,7 @@ class Band {
   void get_flags(uint8_t* flags);
   void filter_voxels(sgs_band_voxel_stats* stats);
   long kill_below(double threshold);
+  long threshold_density(double volume_fraction, double threshold, double* used);
 
   long n = 0;                 // container blocks
   int gdim[3] = {0, 0, 0};    // dense block lookup extent (blocks per axis)
@@ -66,6 +67,7 @@ class Band {
  private:
   void keep_fraction(double fraction_to_keep, long n_thin);
   void pull_flags();  // device flags -> flags_h after a change on the device
+  long threshold_trail(double t, bool apply);
 };
 
 }  // namespace sgs

@@ -27,7 +27,8 @@ EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", 
                     "sgs_design_get", "sgs_band_create", "sgs_band_destroy", "sgs_band_last_error",
                     "sgs_band_set_density", "sgs_band_get_density", "sgs_band_set_fat", "sgs_band_update",
                     "sgs_band_maps", "sgs_band_attach", "sgs_band_session", "sgs_band_step", "sgs_render",
-                    "sgs_band_render", "sgs_band_get_flags", "sgs_band_filter_voxels", "sgs_band_kill_below")
+                    "sgs_band_render", "sgs_band_get_flags", "sgs_band_filter_voxels", "sgs_band_kill_below",
+                    "sgs_band_threshold_density")
 
 CELL_INSIDE, CELL_FORCE, CELL_FIXED = 1, 2, 4   # SGS_CELL_* (driver TopOptFlags bits 0-2)
 
@@ -211,6 +212,8 @@ def load(build_if_missing: bool = False):
     L.sgs_band_filter_voxels.restype = C.c_int
     L.sgs_band_kill_below.argtypes = [P, C.c_double, C.POINTER(C.c_int64)]
     L.sgs_band_kill_below.restype = C.c_int
+    L.sgs_band_threshold_density.argtypes = [P, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    L.sgs_band_threshold_density.restype = C.c_int
     L.sgs_band_attach.argtypes = [P, P, P]
     L.sgs_band_attach.restype = C.c_int
     L.sgs_band_session.argtypes = [P, P, C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
@@ -506,6 +509,7 @@ class Band:
         if rc != 0:
             raise SolverError(rc, err.value.decode(errors="replace"))
         self.h = h
+        self._initial_inside = (self.flags & CELL_INSIDE) != 0   # total_container_voxels counts these
 
     def close(self):
         if getattr(self, "h", None):
@@ -575,6 +579,45 @@ class Band:
         vox = self.filter_voxels()
         maps = self.update(**dict(update, connectivity_filtering=False))
         return {"killed": int(k.value), "voxels": vox, "maps": maps}
+
+    def threshold_density(self, volume_fraction: float = 0.1, threshold: Optional[float] = None):
+        """Opt::threshold_density (topo_opt/spgrid_topo_opt.cpp:1756-1797): the
+        cells of the fat blocks become 1 (density >= threshold, or fixed) or 0.
+        Without ``threshold`` the reference's bisection finds the one that meets
+        volume_fraction x the container voxels.  Returns (threshold, solid voxels)."""
+        t = C.c_double(0)
+        v = C.c_int64(0)
+        self._check(load().sgs_band_threshold_density(self.h, float(volume_fraction),
+                                                      -1.0 if threshold is None else float(threshold),
+                                                      C.byref(t), C.byref(v)))
+        return t.value, int(v.value)
+
+    def packed_density(self) -> np.ndarray:
+        """The densities of the session sgs_band_session packs from the maps
+        (spgrid_topo_opt.cpp:1068-1160): the fatter blocks in container order,
+        max(density, DBL_MIN) in the container cells of fat blocks, 0 elsewhere."""
+        _, fat, fatter = self.maps()
+        idx = np.nonzero(fatter)[0]
+        rho = self.density()[idx]
+        material = fat[idx][:, None] & ((self.flags[idx] & CELL_INSIDE) != 0)
+        return np.where(material, np.maximum(rho, np.finfo(np.float64).tiny), 0.0)
+
+    def threshold_and_compute_objective(self, template, volume_fraction: float = 0.1,
+                                        threshold: Optional[float] = None, precision: int = PRECISION_MIXED,
+                                        tolerance: float = 0.0) -> dict:
+        """The driver's threshold_and_compute_objective action
+        (topo_opt/spgrid_topo_opt.cpp:839-864): threshold the design (bisection
+        when no threshold is given, the volume then reported as volume_fraction x
+        the container voxels; with a threshold, its solid count), solve the
+        packed design and evaluate the compliance objective."""
+        t, solid = self.threshold_density(volume_fraction, threshold)
+        vol = float(solid) if threshold is not None else float(volume_fraction * int(
+            np.count_nonzero(self._initial_inside)))
+        with self.session(template, precision) as s:
+            st = s.solve(tolerance)
+            obj, _, _ = s.sensitivity(self.packed_density())
+        return {"objective": obj, "volume": vol, "threshold": t, "solid_voxels": solid,
+                "cg_iterations": st["iterations"]}
 
     def attach(self, session: "Session", container_block: np.ndarray):
         """Bind a session built from this band's fatter blocks: its input block i

@@ -329,3 +329,41 @@ def test_band_threshold_and_kill_matches_oracle(native_lib):
     assert np.array_equal(band.cell_flags(), f2) and np.array_equal(band.density(), d2)
     _compare(band, ref, out["maps"])
     band.close()
+
+
+# ---------------------------------------------------------------- threshold_density
+def test_oracle_threshold_bisection_meets_the_target():
+    rng = np.random.default_rng(2)
+    rho = rng.random((40, 64))
+    flags = np.full((40, 64), torc.CELL_INSIDE, np.uint8)
+    flags[0, :8] |= torc.CELL_FIXED
+    rho[0, :8] = 0.0                                   # fixed cells count as solid whatever their density
+    rho[1, 0] = np.nan                                 # NaN is never >= t: void
+    fat = np.ones(40, bool)
+    fat[39] = False                                    # outside the fat map: untouched
+    out, t, solid = torc.threshold_density(flags, fat, rho, 40 * 64, 0.25)
+    target = 0.25 * 40 * 64
+    d = rho[fat]
+    fx = (flags[fat] & torc.CELL_FIXED) != 0
+    assert np.count_nonzero((d >= t) | fx) == solid > target >= np.count_nonzero((d >= t + 1e-8) | fx)
+    assert np.all(out[fat][fx] == 1.0) and out[1, 0] == 0.0 and np.array_equal(out[39], rho[39])
+    assert set(np.unique(out[fat])) <= {0.0, 1.0}
+    out2, t2, solid2 = torc.threshold_density(flags, fat, rho, 40 * 64, 0.25, threshold=0.5)
+    assert t2 == 0.5 and solid2 == np.count_nonzero((d >= 0.5) | fx)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("threshold", [None, 0.4])
+def test_band_threshold_density_matches_oracle(native_lib, threshold):
+    from spgrid_topo_opt_b200 import native
+    base, res, flags, dens = container(seed=9)
+    flags[:5, :3] |= torc.CELL_FIXED
+    band = native.Band(base, res, flags, dens)
+    band.update()
+    fat = band.maps()[1]
+    t, solid = band.threshold_density(0.3, threshold)
+    total = int(np.count_nonzero(flags & torc.CELL_INSIDE))
+    ref, rt, rsolid = torc.threshold_density(flags, fat, dens, total, 0.3, threshold)
+    assert t == rt and solid == rsolid
+    assert np.array_equal(band.density(), ref)
+    band.close()

@@ -83,3 +83,39 @@ def test_band_loop_without_updates_matches_device_loop(native_lib):
         assert np.abs(band.density - dev.density).max() <= 1e-9, it
     band.close()
     dev.close()
+
+
+def test_threshold_and_compute_objective(native_lib):
+    """The driver's threshold_and_compute_objective (spgrid_topo_opt.cpp:839-864)
+    after two band iterations: the design thresholded by the bisection, the
+    packed input solved, and the compliance against the oracle's FP64 solve of
+    the same packed input."""
+    inp = void_cantilever()
+    opt = BandSIMP(copy.deepcopy(inp), precision=native.PRECISION_FP64, grid_update_start=0, tolerance=1e-12,
+                   volume_fraction=0.4, minimum_density=1e-3)
+    for _ in range(2):
+        opt.iterate()
+    opt.session.close()
+    opt.session = None
+    band = opt.band
+    flags = band.flags
+    base = np.asarray(inp.density.base)
+    _, fat, fatter = band.maps()
+    rho = band.density()
+    total = int(np.count_nonzero(flags & torc.CELL_INSIDE))
+    ref, t, solid = torc.threshold_density(flags, fat, rho, total, 0.4)
+    r = band.threshold_and_compute_objective(opt._template_blob, volume_fraction=0.4,
+                                             precision=native.PRECISION_FP64, tolerance=1e-12)
+    assert r["threshold"] == t and r["solid_voxels"] == solid and r["volume"] == 0.4 * total
+    assert np.array_equal(band.density(), ref)
+    idx = np.nonzero(fatter)[0]
+    inside = (flags & torc.CELL_INSIDE) != 0
+    packed = copy.copy(inp)
+    packed.density = BlockedGrid(resolution=list(inp.density.resolution), base=base[idx].copy(),
+                                 data=np.where(fat[idx, None] & inside[idx], np.maximum(ref[idx], DBL_MIN), 0.0))
+    assert np.array_equal(band.packed_density(), packed.density.data)
+    o = orc.Oracle(packed, mode=orc.MODE_FP64, tolerance=1e-12)
+    o.solve()
+    obj, _, _ = o.sensitivity()
+    assert r["objective"] == pytest.approx(obj, rel=1e-6)
+    opt.close()
