@@ -392,6 +392,11 @@ __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* _
   }
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 64;  // the warp's 32 x 64 sub-tile
+  if (beta != 0) {  // the epilogue reads this C tile: bring it into L2 while the products run
+    const double* half_row = C + (I * SGJ + (tid >> 1)) * ldc + J * SGJ + (tid & 1) * 64;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(half_row + 16 * q));
+  }
   const int fr = lane >> 2, fc = lane & 3;
   const double* Ab = A + I * SGJ * lda;
   const double* Bb = B + J * SGJ;
