@@ -348,12 +348,13 @@ __device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4]
 }
 
 // C(tile) = alpha * A(tile rows, 0:k) * B(0:k, tile cols) + beta * C(tile) on
-// 128 x 128 tiles: eight warps of 32 x 64, k staged through shared memory in
-// chunks of 16 (register prefetch of the next chunk), FP64 MMAs.
+// 128 x 128 tiles: sixteen warps of 32 x 32 (four per SM sub-partition, to hide
+// the MMA latency), k staged through shared memory in chunks of 16, FP64 MMAs.
 // Tiles: SGJ_DENSE (blockIdx.y, blockIdx.x); SGJ_LOWER the tiles I >= J of a
 // square grid (blockIdx.x), leaving out row and column `skip` (none if < 0);
 // SGJ_CROSS the lower tiles of row and column `skip` (blockIdx.x = J for
 // J <= skip, else I).
+constexpr int SGJ_THREADS = 512;          // sixteen warps of 32 x 32 per 128 x 128 tile
 constexpr int SGJ_AS = 20, SGJ_BS = 132;  // padded strides (4 mod 16 doubles): conflict-free fragment loads
 constexpr int SGJ_STAGE = SGJ * SGJ_AS + SGJ_K * SGJ_BS;  // doubles per pipeline stage
 constexpr size_t SGJ_SMEM = 2 * SGJ_STAGE * sizeof(double);
@@ -369,7 +370,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // k staged through two shared-memory stages filled by cp.async: the copy of
 // chunk c + 1 runs while chunk c is multiplied.
-__global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* __restrict__ A, long lda,
+__global__ void __launch_bounds__(SGJ_THREADS, 1) sgj_gemm_kernel(int k, const double* __restrict__ A, long lda,
                                                           const double* __restrict__ B, long ldb, double* C, long ldc,
                                                           double alpha, double beta, int mode, int skip) {
   extern __shared__ __align__(16) double sg[];
@@ -391,34 +392,34 @@ __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* _
     J = blockIdx.x;
   }
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 64;  // the warp's 32 x 64 sub-tile
+  const int wr = (warp >> 2) * 32, wc = (warp & 3) * 32;  // the warp's 32 x 32 sub-tile
   if (beta != 0) {  // the epilogue reads this C tile: bring it into L2 while the products run
-    const double* half_row = C + (I * SGJ + (tid >> 1)) * ldc + J * SGJ + (tid & 1) * 64;
+    const double* quarter_row = C + (I * SGJ + (tid >> 2)) * ldc + J * SGJ + (tid & 3) * 32;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(half_row + 16 * q));
+    for (int q = 0; q < 2; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(quarter_row + 16 * q));
   }
   const int fr = lane >> 2, fc = lane & 3;
   const double* Ab = A + I * SGJ * lda;
   const double* Bb = B + J * SGJ;
-  const int ar = tid >> 1, ak = (tid & 1) * 8;    // A chunk: row, first k
-  const int bk = tid >> 4, bc = (tid & 15) * 8;   // B chunk: k, first column
+  const int ar = tid >> 2, ak = (tid & 3) * 4;    // A chunk: row, first k
+  const int bk = tid >> 5, bc = (tid & 31) * 4;   // B chunk: k, first column
   auto stage = [&](int k0, int st) {
     double* As = sg + st * SGJ_STAGE;
     double* Bs = As + SGJ * SGJ_AS;
     const double* a = Ab + long(ar) * lda + k0 + ak;
     const double* b = Bb + long(k0 + bk) * ldb + bc;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < 2; ++q) {
       cp_async16(&As[ar * SGJ_AS + ak + 2 * q], a + 2 * q);
       cp_async16(&Bs[bk * SGJ_BS + bc + 2 * q], b + 2 * q);
     }
     cp_async_commit();
   };
-  double acc[2][8][4];
+  double acc[2][4][4];
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0;
   const int nchunks = k / SGJ_K;
   stage(0, 0);
   for (int c = 0; c < nchunks; ++c) {
@@ -433,7 +434,7 @@ __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* _
     const double* Bs = As + SGJ * SGJ_AS;
 #pragma unroll
     for (int k8 = 0; k8 < SGJ_K; k8 += 8) {
-      double a[2][4], b[8][2];
+      double a[2][4], b[4][2];
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         const double* r = As + (wr + 16 * i + fr) * SGJ_AS + k8 + fc;
@@ -443,14 +444,14 @@ __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* _
         a[i][3] = r[8 * SGJ_AS + 4];
       }
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
+      for (int j = 0; j < 4; ++j) {
         b[j][0] = Bs[(k8 + fc) * SGJ_BS + wc + 8 * j + fr];
         b[j][1] = Bs[(k8 + fc + 4) * SGJ_BS + wc + 8 * j + fr];
       }
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) dmma_16x8x8(acc[i][j], a[i], b[j]);
+        for (int j = 0; j < 4; ++j) dmma_16x8x8(acc[i][j], a[i], b[j]);
     }
     __syncthreads();  // the stage is refilled two chunks later
   }
@@ -460,7 +461,7 @@ __global__ void __launch_bounds__(256, 1) sgj_gemm_kernel(int k, const double* _
     for (int hr = 0; hr < 2; ++hr) {
       double* row = C + (I * SGJ + wr + 16 * i + 8 * hr + fr) * ldc + J * SGJ + wc + 2 * fc;
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
+      for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           double* p = row + 8 * j + h;

@@ -544,8 +544,12 @@ class Solver {
     SGS_CUDA(cudaFuncSetAttribute(sgj_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SGJ_SMEM)));
     const long nel = long(SGJ) * ld;
     const size_t row = size_t(ld) * sizeof(double), tile_row = SGJ * sizeof(double);
+    // the look-ahead pivot inversion runs beside the update, whose CTAs fill the
+    // SMs: its stream has the highest priority so that it takes the first free SM
     cudaStream_t aux;
-    SGS_CUDA(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    int prio_low = 0, prio_high = 0;
+    SGS_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    SGS_CUDA(cudaStreamCreateWithPriority(&aux, cudaStreamNonBlocking, prio_high));
     cudaEvent_t crossed, inverted;
     SGS_CUDA(cudaEventCreateWithFlags(&crossed, cudaEventDisableTiming));
     SGS_CUDA(cudaEventCreateWithFlags(&inverted, cudaEventDisableTiming));
@@ -567,22 +571,22 @@ class Solver {
       if (K > 0) SGS_CUDA(cudaStreamWaitEvent(stream, inverted, 0));
       sgj_gather_kernel<<<blocks_for(nel, 256), 256, 0, stream>>>(M, ld, K, R.p, Cp.p, nullptr);
       // T = P^-1 R
-      sgj_gemm_kernel<<<dim3(nt, 1), 256, SGJ_SMEM, stream>>>(SGJ, Pk, SGJ, R.p, ld, T.p, ld, 1.0, 0.0, SGJ_DENSE, -1);
+      sgj_gemm_kernel<<<dim3(nt, 1), SGJ_THREADS, SGJ_SMEM, stream>>>(SGJ, Pk, SGJ, R.p, ld, T.p, ld, 1.0, 0.0, SGJ_DENSE, -1);
       const int next = K + 1 < nt ? K + 1 : -1;
       if (next >= 0) {
         // the row and column of the next pivot first, then its inverse on the side stream
-        sgj_gemm_kernel<<<nt, 256, SGJ_SMEM, stream>>>(SGJ, Cp.p, SGJ, T.p, ld, M, ld, -1.0, 1.0, SGJ_CROSS, next);
+        sgj_gemm_kernel<<<nt, SGJ_THREADS, SGJ_SMEM, stream>>>(SGJ, Cp.p, SGJ, T.p, ld, M, ld, -1.0, 1.0, SGJ_CROSS, next);
         SGS_CUDA(cudaEventRecord(crossed, stream));
         SGS_CUDA(cudaStreamWaitEvent(aux, crossed, 0));
         invert_pivot(next, P[next & 1].p, aux);
         SGS_CUDA(cudaEventRecord(inverted, aux));
       }
       // the other lower tiles: M -= Cp T
-      sgj_gemm_kernel<<<unsigned(long(nt) * (nt + 1) / 2), 256, SGJ_SMEM, stream>>>(SGJ, Cp.p, SGJ, T.p, ld, M, ld, -1.0,
+      sgj_gemm_kernel<<<unsigned(long(nt) * (nt + 1) / 2), SGJ_THREADS, SGJ_SMEM, stream>>>(SGJ, Cp.p, SGJ, T.p, ld, M, ld, -1.0,
                                                                              1.0, SGJ_LOWER, next);
       // A_IK = -Cp_I P^-1 below the pivot
       if (K + 1 < nt)
-        sgj_gemm_kernel<<<dim3(1, nt - K - 1), 256, SGJ_SMEM, stream>>>(SGJ, Cp.p + size_t(K + 1) * SGJ * SGJ, SGJ, Pk, SGJ,
+        sgj_gemm_kernel<<<dim3(1, nt - K - 1), SGJ_THREADS, SGJ_SMEM, stream>>>(SGJ, Cp.p + size_t(K + 1) * SGJ * SGJ, SGJ, Pk, SGJ,
                                                                  M + size_t(K + 1) * SGJ * ld + size_t(K) * SGJ, ld,
                                                                  -1.0, 0.0, SGJ_DENSE, -1);
       // A_KJ = T_J left of the pivot, A_KK = P^-1
