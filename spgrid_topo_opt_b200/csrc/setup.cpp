@@ -44,7 +44,7 @@ int HostLevel::active_block_at(int x, int y, int z) const {
   return (b >= 0 && b < nb) ? b : -1;
 }
 
-int HostLevel::touch(int x, int y, int z) {
+int HostLevel::touch(int x, int y, int z, bool with_flags) {
   long c = cell(x, y, z);
   if (c < 0) return -1;
   int b = bgrid[c];
@@ -54,7 +54,7 @@ int HostLevel::touch(int x, int y, int z) {
     coords.push_back(x & ~3);
     coords.push_back(y & ~3);
     coords.push_back(z & ~7);
-    flags.resize(flags.size() + NODES_PER_BLOCK, 0u);
+    if (with_flags) flags.resize(flags.size() + NODES_PER_BLOCK, 0u);
   }
   return b;
 }
@@ -72,12 +72,20 @@ struct Builder {
     L.bgrid.assign(size_t(L.grid[0]) * L.grid[1] * L.grid[2], -1);
     L.active_page.assign(L.bgrid.size(), 0);
   }
-  int set_page(int x, int y, int z) {
+  int set_page(int x, int y, int z, bool with_flags = true) {
     long c = L.cell(x, y, z);
     if (c < 0) return -1;
-    int b = L.touch(x, y, z);
+    int b = L.touch(x, y, z, with_flags);
     L.active_page[c] = 1;
     return b;
+  }
+  // flags of the blocks created by set_page(..., false), zeroed in parallel
+  void add_flags() {
+    const size_t have = L.flags.size(), want = L.coords.size() / 3 * NODES_PER_BLOCK;
+    L.flags.resize(want);  // uninitialised
+    uint32_t* f = L.flags.data();
+#pragma omp parallel for schedule(static)
+    for (long i = long(have); i < long(want); ++i) f[i] = 0u;
   }
   bool test_page(int x, int y, int z) const {
     long c = L.cell(x, y, z);
@@ -104,7 +112,7 @@ struct Builder {
     std::vector<int32_t> remap(n_all);
     for (int i = 0; i < n_all; ++i) remap[order[i]] = i;
     std::vector<int32_t> coords(L.coords.size());
-    std::vector<uint32_t> flags(L.flags.size());
+    HostBuf<uint32_t> flags(L.flags.size());  // every entry is written below
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n_all; ++i) {
       int o = order[i];
@@ -158,18 +166,30 @@ void flag_nodes(HostLevel& L) {
   HostBuf<uint32_t> add(size_t(nall) * NODES_PER_BLOCK);  // every entry is written below
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nall; ++b) {
-    int ring[27];
-    block_ring(L, b, ring);
+    // the blocks at offsets -(c>>2, (c>>1)&1, c&1) that hold a node's cells; only
+    // cells of active blocks spread their flags
+    int src[8];
+    const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
+    for (int c = 0; c < 8; ++c) {
+      const int nb = c ? L.block_at(bx - (c >> 2) * BLK_X, by - ((c >> 1) & 1) * BLK_Y, bz - (c & 1) * BLK_Z) : b;
+      src[c] = (nb >= 0 && nb < L.nb) ? nb : -1;
+    }
+    const uint32_t* own = src[0] >= 0 ? &L.flags[size_t(src[0]) * NODES_PER_BLOCK] : nullptr;
+    uint32_t* out = &add[size_t(b) * NODES_PER_BLOCK];
     for (int e = 0; e < NODES_PER_BLOCK; ++e) {
       const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
       uint32_t acc = 0;
-      for (int c = 0; c < 8; ++c) {
-        const int cx = x - (c >> 2), cy = y - ((c >> 1) & 1), cz = z - (c & 1);
-        const int nb = ring[(cx < 0 ? 0 : 1) * 9 + (cy < 0 ? 0 : 1) * 3 + (cz < 0 ? 0 : 1)];
-        if (nb < 0 || nb >= L.nb) continue;  // only cells of active blocks spread their flags
-        acc |= (L.flags[size_t(nb) * NODES_PER_BLOCK + node_slot(cx, cy, cz)] & CELL) >> 4;
+      if (x && y && z) {  // all 8 cells in this block, at slot offsets 0, 1, 8, 9, 32, 33, 40, 41 below
+        if (own)
+          acc = own[e] | own[e - 1] | own[e - 8] | own[e - 9] | own[e - 32] | own[e - 33] | own[e - 40] | own[e - 41];
+      } else {
+        for (int c = 0; c < 8; ++c) {
+          const int cx = x - (c >> 2), cy = y - ((c >> 1) & 1), cz = z - (c & 1);
+          const int nb = src[(cx < 0 ? 4 : 0) | (cy < 0 ? 2 : 0) | (cz < 0 ? 1 : 0)];
+          if (nb >= 0) acc |= L.flags[size_t(nb) * NODES_PER_BLOCK + node_slot(cx, cy, cz)];
+        }
       }
-      add[size_t(b) * NODES_PER_BLOCK + e] = acc;
+      out[e] = (acc & CELL) >> 4;
     }
   }
 #pragma omp parallel for schedule(static)
@@ -190,7 +210,7 @@ void flag_boundary(HostLevel& L, int band = 3) {
     const int nb = ring[(x < 0 ? 0 : (x > 3 ? 2 : 1)) * 9 + (y < 0 ? 0 : (y > 3 ? 2 : 1)) * 3 + (z < 0 ? 0 : (z > 7 ? 2 : 1))];
     return nb < 0 ? 0u : L.flags[size_t(nb) * NODES_PER_BLOCK + node_slot(x, y, z)];
   };
-  std::vector<uint8_t> seeded(static_cast<size_t>(nall), 0);
+  std::vector<uint8_t> seeded(static_cast<size_t>(nall), 0), is_cand(static_cast<size_t>(L.nb), 0);
   std::vector<int> cand;
   for (int pass = 0; pass < band; ++pass) {
 #pragma omp parallel for schedule(static)
@@ -199,15 +219,18 @@ void flag_boundary(HostLevel& L, int band = 3) {
       for (int e = 0; e < NODES_PER_BLOCK && !s; ++e) s = (L.flags[size_t(b) * NODES_PER_BLOCK + e] & SEED) != 0;
       seeded[size_t(b)] = s;
     }
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < L.nb; ++b) {
+      uint8_t near = 0;
+      for (int d = 0; d < 27 && !near; ++d) {
+        const int nb = rings[size_t(b)][d];
+        near = nb >= 0 && seeded[size_t(nb)];
+      }
+      is_cand[size_t(b)] = near;
+    }
     cand.clear();
     for (int b = 0; b < L.nb; ++b)
-      for (int d = 0; d < 27; ++d) {
-        const int nb = rings[size_t(b)][d];
-        if (nb >= 0 && seeded[size_t(nb)]) {
-          cand.push_back(b);
-          break;
-        }
-      }
+      if (is_cand[size_t(b)]) cand.push_back(b);
 #pragma omp parallel for schedule(dynamic, 16)
     for (long k = 0; k < long(cand.size()); ++k) {
       const int b = cand[size_t(k)];
@@ -311,14 +334,13 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   // repeated: then the cells go in input order, the last write winning.
   std::vector<int32_t> in_slot(nin);
   b0.L.coords.reserve(3 * nin);  // at most one solver page per input block
-  b0.L.flags.reserve(nin * NODES_PER_BLOCK);
   bool repeated = false;
   {
     std::vector<uint8_t> halves;
     for (size_t b = 0; b < nin; ++b) {
       int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
       if ((x & 3) || (y & 3) || (z & 3)) return fail(4, "density block base is not a multiple of 4");
-      const int bk = b0.set_page(x, y, z);
+      const int bk = b0.set_page(x, y, z, false);
       if (bk < 0) return fail(4, "density block outside the grid");
       in_slot[b] = bk * NODES_PER_BLOCK + node_slot(x, y, z);
       if (halves.size() <= size_t(bk)) halves.resize(size_t(bk) + 1, 0);
@@ -326,6 +348,7 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
       repeated |= (halves[size_t(bk)] & h) != 0;
       halves[size_t(bk)] |= h;
     }
+    b0.add_flags();
   }
   // the SIMP map of every input cell, once (fem_interface.h:343-353); the
   // buffer is filled in parallel without a serial zero pass

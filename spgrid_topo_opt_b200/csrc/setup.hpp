@@ -32,7 +32,7 @@ struct HostLevel {
   std::vector<int32_t> bgrid;         // block grid -> block index (active or ghost), -1 if untouched
   int nb = 0;                         // active blocks (first nb entries of coords/flags)
   std::vector<int32_t> coords;        // block base coordinates, [nb_all*3]
-  std::vector<uint32_t> flags;        // [nb_all*128]
+  HostBuf<uint32_t> flags;            // [nb_all*128]
   std::vector<uint8_t> active_page;   // per block-grid cell
   std::vector<int32_t> nbr;           // [nb*27] neighbour block (active only) or -1
   std::vector<int32_t> boundary;      // active blocks with a boundary-band node
@@ -41,7 +41,7 @@ struct HostLevel {
   long cell(int x, int y, int z) const;
   int block_at(int x, int y, int z) const;       // active or ghost, -1 if none
   int active_block_at(int x, int y, int z) const;  // active only
-  int touch(int x, int y, int z);                 // create a ghost block when needed
+  int touch(int x, int y, int z, bool with_flags = true);  // create a ghost block when needed
 };
 
 
