@@ -696,8 +696,10 @@ class Solver {
           continue;
         }
         if (!u) {  // the packed iterate of the V-cycle
+          // single precision: 64 registers, 8 CTAs per SM (faster than 6 or 10
+          // despite a few spilled bytes); double: 128, 4 per SM
           if constexpr (sizeof(T) == 4)
-            launch(gs0_list4_kernel<T, 6>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbrz.p, d.u4.p, b,
+            launch(gs0_list4_kernel<T, 8>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbrz.p, d.u4.p, b,
                    d.flags.p, int(d.N), T(P.dx));
           else
             launch(gs0_list4_kernel<T, 4>, blocks_for(cnt, 128), 128, 0, d.gs_list.p + lo, cnt, d.nbrz.p, d.u4.p, b,
