@@ -212,13 +212,15 @@ void flag_boundary(HostLevel& L, int band = 3) {
   };
   std::vector<uint8_t> seeded(static_cast<size_t>(nall), 0), is_cand(static_cast<size_t>(L.nb), 0);
   std::vector<int> cand;
-  for (int pass = 0; pass < band; ++pass) {
+  // blocks holding a Dirichlet or band node; after the first pass only the
+  // candidates of the last pass can have gained band nodes
 #pragma omp parallel for schedule(static)
-    for (int b = 0; b < nall; ++b) {
-      uint8_t s = 0;
-      for (int e = 0; e < NODES_PER_BLOCK && !s; ++e) s = (L.flags[size_t(b) * NODES_PER_BLOCK + e] & SEED) != 0;
-      seeded[size_t(b)] = s;
-    }
+  for (int b = 0; b < nall; ++b) {
+    uint8_t s = 0;
+    for (int e = 0; e < NODES_PER_BLOCK && !s; ++e) s = (L.flags[size_t(b) * NODES_PER_BLOCK + e] & SEED) != 0;
+    seeded[size_t(b)] = s;
+  }
+  for (int pass = 0; pass < band; ++pass) {
 #pragma omp parallel for schedule(static)
     for (int b = 0; b < L.nb; ++b) {
       uint8_t near = 0;
@@ -248,7 +250,10 @@ void flag_boundary(HostLevel& L, int band = 3) {
     for (long k = 0; k < long(cand.size()); ++k)
       for (int e = 0; e < NODES_PER_BLOCK; ++e) {
         uint32_t& f = L.flags[size_t(cand[size_t(k)]) * NODES_PER_BLOCK + e];
-        if (f & F_BOUNDARY_TEMP) f = (f & ~F_BOUNDARY_TEMP) | F_BOUNDARY_NODE;
+        if (f & F_BOUNDARY_TEMP) {
+          f = (f & ~F_BOUNDARY_TEMP) | F_BOUNDARY_NODE;
+          seeded[size_t(cand[size_t(k)])] = 1;
+        }
       }
   }
   L.boundary.clear();
