@@ -1,13 +1,18 @@
 #!/usr/bin/env python
 """Benchmark: MGPCG time-to-solution and MDOF/s to a relative L-inf residual of
 1e-6 on one B200, mixed precision (FP32 V-cycle, FP64 outer PCG) against the
-same GPU's plain FP64 MGPCG, on the narrow-band sphere-shell workload (256^3
-grid, shell radii 0.4-0.5, seeded smoothed-noise density).
+same GPU's plain FP64 MGPCG.  Default workload: the 1024^3 narrow band (a
+12-voxel shell around the union of 8 seeded random spheres, seeded uniform
+density in [1e-3, 1], Dirichlet on the lowest band cell layer, 16 seeded unit
+point loads).  ``--workload shell`` runs the 256^3 sphere shell instead.
 
 One step = one complete PCG solve (first residual to convergence) of the
 resident problem; set-up (flags, Galerkin operators, bottom inverse) is done
 once before the timed region and reported separately.  MDOF/s = 3 * nodes of
-the active level-0 blocks / solve time / 1e6.
+the active level-0 blocks / solve time / 1e6.  After the timed solves the FP64
+session solves again to a relative residual of 1e-12; the displacements and
+the compliance f.u of both arms are reported with their relative errors
+against that FP64 solution.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -33,8 +38,9 @@ sys.path.insert(0, ROOT)
 METRIC = "MGPCG time & MDOF/s to rel.res 1e-6: mixed-prec vs FP64, same B200"
 ACTIVE_NODE = 0x10  # node flag of an active node (solver/Flags.h); DOF = 3 x active nodes
 TOL = 1e-6
-# ncu-measured DRAM traffic of one level-0 sweep per workload
-# (profiles/gs0_list4_kernel_sphere_shell256.md)
+TIGHT_TOL = 1e-12  # the FP64 solution the errors are measured against
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one level-0 FP32
+# sweep (its 8 colour launches) per workload, from ncu captures of this kernel
 SWEEP_DRAM_BYTES = {"sphere_shell256": 1.125e9}
 L2_BYTES = 126 * 1024 * 1024
 
@@ -45,11 +51,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["shell", "band"], default="shell",
-                    help="shell: 256^3 sphere shell; band: 1024^3 narrow band around 8 spheres")
-    ap.add_argument("--n", type=int, default=None, help="grid size (default 256 shell, 1024 band)")
+    ap.add_argument("--workload", choices=["shell", "band"], default="band",
+                    help="band: 1024^3 narrow band around 8 spheres; shell: 256^3 sphere shell")
+    ap.add_argument("--n", type=int, default=None, help="grid size (default 1024 band, 256 shell)")
     ap.add_argument("--bottom-size", type=int, default=None)
-    ap.add_argument("--cpu-sample-n", type=int, default=64, help="grid size of the CPU-baseline sample")
+    ap.add_argument("--cpu-sample-n", type=int, default=None,
+                    help="grid size of the CPU-baseline sample (default 128 band, 64 shell)")
+    ap.add_argument("--no-tight", action="store_true", help="skip the tight FP64 solve the errors are measured against")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-iterations", type=int, default=0,
@@ -60,6 +68,8 @@ def parse():
     args = ap.parse_args()
     if args.n is None:
         args.n = 256 if args.workload == "shell" else 1024
+    if args.cpu_sample_n is None:
+        args.cpu_sample_n = 64 if args.workload == "shell" else 128
     if args.bottom_size is None:
         # mg_bottom_size 16, the value of the reference's dense-box configuration
         args.bottom_size = 16
@@ -75,22 +85,22 @@ def workload(n: int, bottom: int, kind: str = "shell"):
     return prob, inp
 
 
-def config_dict(args, inp, extra=None):
+def config_dict(args, inp, extra=None, n=None):
+    """The workload's description; n names a smaller grid of the same generator
+    (the CPU samples)."""
+    n = args.n if n is None else n
+    common = {"mg_level": int(inp.mg_level), "mg_bottom_size": int(args.bottom_size),
+              "smoothing": [int(inp.pre_and_post_smoothing_iter), int(inp.extra_ints["boundary_smoothing"])],
+              "tolerance": TOL, "stopping_rule": "L-inf residual <= tol * zero-guess L-inf residual",
+              "input_blocks_4x4x4": int(inp.density.base.shape[0]),
+              "l2": "flushed (256 MiB write) before every timed solve"}
     if args.workload == "band":
-        d = {"workload": f"spheres_band{args.n}", "grid": [args.n] * 3,
+        d = {"workload": f"spheres_band{n}", "grid": [n] * 3,
              "band": "12-voxel shell around the union of 8 seeded spheres (radii 0.1-0.3), seed 7",
-             "density": "uniform [1e-3, 1], seeded", "mg_level": int(inp.mg_level),
-             "smoothing": [int(inp.pre_and_post_smoothing_iter), int(inp.extra_ints["boundary_smoothing"])],
-             "tolerance": TOL, "stopping_rule": "L-inf residual <= tol * zero-guess L-inf residual",
-             "input_blocks_4x4x4": int(inp.density.base.shape[0]), "l2": "flushed (256 MiB write) before every timed solve"}
-        if extra:
-            d.update(extra)
-        return d
-    d = {"workload": f"sphere_shell{args.n}", "grid": [args.n] * 3, "shell_radii": [0.4, 0.5],
-         "density": "clamp(0.5+0.3*smoothed uniform noise, 1e-3, 1), seed 1234", "mg_level": int(inp.mg_level),
-         "smoothing": [int(inp.pre_and_post_smoothing_iter), int(inp.extra_ints["boundary_smoothing"])],
-         "tolerance": TOL, "stopping_rule": "L-inf residual <= tol * zero-guess L-inf residual",
-         "input_blocks_4x4x4": int(inp.density.base.shape[0]), "l2": "flushed (256 MiB write) before every timed solve"}
+             "density": "uniform [1e-3, 1], seeded", **common}
+    else:
+        d = {"workload": f"sphere_shell{n}", "grid": [n] * 3, "shell_radii": [0.4, 0.5],
+             "density": "clamp(0.5+0.3*smoothed uniform noise, 1e-3, 1), seed 1234", **common}
     if extra:
         d.update(extra)
     return d
@@ -158,21 +168,28 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def cpu_sample(args):
+    """A bounded CPU sample of the workload: the same generator at the smaller
+    grid args.cpu_sample_n, with the same mg_bottom_size, solved completely."""
+    return workload(args.cpu_sample_n, args.bottom_size, args.workload)[1]
+
+
 def cpu_baseline(args):
-    """The oracle port (CPU restatement of the reference solver, FP64) timed on a
-    bounded sample of the same workload: a complete solve of the same shell
-    generator at a smaller grid, all host threads."""
+    """The oracle port (CPU restatement of the reference solver, FP64 with the
+    reference's float rounding) timed on one complete solve of the bounded
+    sample, all host threads."""
     from oracle.oracle import Oracle, MODE_REF
-    prob, inp = workload(args.cpu_sample_n, 4, args.workload)
+    inp = cpu_sample(args)
     cores = os.cpu_count() or 1
     o = Oracle(inp, mode=MODE_REF, tolerance=TOL, threads=cores)
     t0 = time.perf_counter()
     r = o.solve()
     t = time.perf_counter() - t0
     dof = 3 * int(np.count_nonzero(o.flags(0) & ACTIVE_NODE))
+    name = config_dict(args, inp, n=args.cpu_sample_n)["workload"]
     return {"value": dof / t / 1e6, "unit": "MDOF/s", "cores": cores, "kind": "port",
-            "sample": f"complete REF-mode solve of sphere_shell{args.cpu_sample_n} ({dof} DOF, {r['iterations']} "
-                      f"iterations, {t:.2f} s, tol {TOL})"}
+            "sample": f"one complete REF-mode solve of {name} ({dof} DOF, {r['iterations']} iterations, "
+                      f"{t:.2f} s, tol {TOL}, mg_bottom_size {args.bottom_size})"}
 
 
 def flush_l2(buf):
@@ -245,25 +262,54 @@ def run_ours(args, rank, world):
     dof = st_mix["dof"]
     per_step, value = aggregate_replicas(float(np.mean(t_mix)), dof, world, dist, "cuda")
 
+    # accuracy of both arms against a tight FP64 solve of the same problem on the
+    # same GPU: displacements (L-inf relative) and the compliance f.u
+    u_mix, u_64 = mixed.displacements()[..., :3], fp64.displacements()[..., :3]
+    accuracy = None
+    if not args.no_tight:
+        st_t = fp64.solve(tolerance=TIGHT_TOL)
+        u_ref = fp64.displacements()[..., :3]
+        f_at, f_val = force_layout(inp)
+        c_ref, c_mix, c_64 = (compliance(u, f_at, f_val) for u in (u_ref, u_mix, u_64))
+        nrm = float(np.abs(u_ref).max())
+        accuracy = {"against": f"FP64 MGPCG on the same GPU to relative L-inf residual {TIGHT_TOL:g} "
+                               f"({st_t['iterations']} iterations)",
+                    "rel_err_u_mixed": float(np.abs(u_mix - u_ref).max() / nrm),
+                    "rel_err_u_fp64": float(np.abs(u_64 - u_ref).max() / nrm),
+                    "rel_err_u_mixed_vs_fp64": float(np.abs(u_mix - u_64).max() / float(np.abs(u_64).max())),
+                    "compliance": c_ref,
+                    "rel_err_compliance_mixed": abs(c_mix - c_ref) / abs(c_ref),
+                    "rel_err_compliance_fp64": abs(c_64 - c_ref) / abs(c_ref)}
+
     # dominant kernel: the level-0 smoothing sweep (8 colour launches); its
     # algorithmic bytes per node are u read+write (6w) + b (3w) + E (w) + flags (4 B)
     sweep_ms = mixed.time_op(2, reps=20)
-    ku_ms = mixed.time_op(0, reps=20)
+    ku32_ms = mixed.time_op(4, reps=20)
+    res32_ms = mixed.time_op(1, reps=20)
+    ku64_ms = mixed.time_op(0, reps=20)
     vcyc_ms = mixed.time_op(3, reps=5)
     nodes = dof // 3
     peak, peak_kind = measured_peaks()
     sweep_bytes = nodes * (10 * 4 + 4)
     achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9
-    ku_bytes = nodes * 7 * 8   # the FP64 PCG matvec: s read, q written (3 x 8 B each), E (8 B)
-    # DRAM bytes of one full sweep (dram__bytes_read.sum + dram__bytes_write.sum over its 8
-    # colour-pass launches) from the ncu launch list of this workload, where one was taken
-    traffic = SWEEP_DRAM_BYTES.get(config_dict(args, inp, {})["workload"])
+    # K u: u read and f written (3w each) + the cell's stiffness scale E (w)
+    ku32_bytes, ku64_bytes, res32_bytes = nodes * 7 * 4, nodes * 7 * 8, nodes * 10 * 4
+    gbs = lambda b, ms: b / (ms * 1e-3) / 1e9
+    traffic = SWEEP_DRAM_BYTES.get(config_dict(args, inp)["workload"])
     roofline = {"bound": "hbm", "kernel": "level0 Gauss-Seidel sweep (8 colour launches of gs0_list4_kernel, FP32)",
                 "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch_set": sweep_bytes, "sweep_ms": round(sweep_ms, 4),
-                "ku_ms": round(ku_ms, 4), "ku_achieved_gbs": round(ku_bytes / (ku_ms * 1e-3) / 1e9, 1),
-                "vcycle_ms": round(vcyc_ms, 4)}
+                "vcycle_ms": round(vcyc_ms, 4),
+                "ku_fp32": {"kernel": "level0_op_kernel<float, K u>", "ms": round(ku32_ms, 4),
+                            "algorithmic_bytes": ku32_bytes, "achieved": round(gbs(ku32_bytes, ku32_ms), 1),
+                            "frac": round(gbs(ku32_bytes, ku32_ms) / peak, 4)},
+                "residual_fp32": {"kernel": "level0_res4_kernel<float> (V-cycle residual)", "ms": round(res32_ms, 4),
+                                  "algorithmic_bytes": res32_bytes, "achieved": round(gbs(res32_bytes, res32_ms), 1),
+                                  "frac": round(gbs(res32_bytes, res32_ms) / peak, 4)},
+                "ku_fp64": {"kernel": "level0_op_kernel<double, PCG matvec>", "ms": round(ku64_ms, 4),
+                            "algorithmic_bytes": ku64_bytes, "achieved": round(gbs(ku64_bytes, ku64_ms), 1),
+                            "frac": round(gbs(ku64_bytes, ku64_ms) / peak, 4)}}
 
     # end to end through the drop-in C ABI: serialize on the host, fem_solve (set-up,
     # H2D, solve, D2H), deserialize; mixed precision selected through extra_ints
@@ -296,6 +342,7 @@ def run_ours(args, rank, world):
                      "value": round(dof / float(np.mean(t_64)) / 1e6, 3), "unit": "MDOF/s",
                      "iterations": int(np.median(it_64))},
             "mixed_over_fp64_speedup": round(float(np.mean(t_64)) / per_step, 3),
+            "accuracy": accuracy,
             "setup_seconds": round(st_mix["setup_seconds"], 3),
             "roofline": roofline,
             "cpu_baseline": cpu,
@@ -314,18 +361,39 @@ def run_ours(args, rank, world):
     return result
 
 
+def force_layout(inp):
+    """For each force of the input: the (input block, node) slot of its node in
+    the displacement output [nblocks][64] (in-block index i*16 + j*4 + k), or -1
+    when no input block holds it; and the force vectors."""
+    base = np.asarray(inp.density.base)
+    index = {tuple(b): i for i, b in enumerate(base.tolist())}
+    slots = []
+    for c in np.asarray(inp.forces["coord"]).tolist():
+        b = index.get((c[0] & ~3, c[1] & ~3, c[2] & ~3), -1)
+        slots.append(-1 if b < 0 else b * 64 + (c[0] & 3) * 16 + (c[1] & 3) * 4 + (c[2] & 3))
+    return np.array(slots), np.asarray(inp.forces["f"], dtype=np.float64)
+
+
+def compliance(u, slots, f):
+    """f.u over the forces whose node lies in an input block."""
+    flat = u.reshape(-1, 3)
+    ok = slots >= 0
+    return float((flat[slots[ok]] * f[ok]).sum())
+
+
 def run_reference(args, rank, world):
     """The reference arm: the reference solver cannot be built here (ICC-only C++ and
     MKL PARDISO), so its CPU restatement (the oracle, reference-rounding mode) is
-    timed on the host cores on a bounded sample of the same workload."""
+    timed on the host cores, each step one complete solve of a bounded sample of
+    the workload (the same generator on a smaller grid)."""
     if rank != 0:
         return None
     from oracle.oracle import Oracle, MODE_REF
-    prob, inp = workload(args.cpu_sample_n, 4, args.workload)
+    inp = cpu_sample(args)
     cores = os.cpu_count() or 1
     o = Oracle(inp, mode=MODE_REF, tolerance=TOL, threads=cores)
     dof = 3 * int(np.count_nonzero(o.flags(0) & ACTIVE_NODE))
-    for _ in range(max(0, min(args.warmup, 1))):
+    for _ in range(args.warmup):
         o.solve()
     times, iters = [], []
     for _ in range(args.steps):
@@ -335,15 +403,15 @@ def run_reference(args, rank, world):
         iters.append(r["iterations"])
     t = float(np.mean(times))
     value = dof / t / 1e6
-    sample = (f"complete REF-mode solve of sphere_shell{args.cpu_sample_n} ({dof} DOF, {int(np.median(iters))} "
-              f"iterations) per step; the reference needs ICC and MKL PARDISO and is not built, its CPU "
-              f"restatement (oracle/spgrid_oracle.cpp) is timed instead")
+    cfg = config_dict(args, inp, n=args.cpu_sample_n)
+    sample = (f"one complete REF-mode solve of {cfg['workload']} ({dof} DOF, {int(np.median(iters))} iterations) "
+              f"per step, a bounded sample of {config_dict(args, inp)['workload']}; the reference needs ICC and MKL "
+              f"PARDISO and is not built, its CPU restatement (oracle/spgrid_oracle.cpp) is timed instead")
+    cfg["sample_of"] = config_dict(args, inp)["workload"]
     return {"metric": METRIC, "value": round(value, 4), "unit": "MDOF/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 (float-rounded CG updates, as the reference)", "data": "synthetic (seeded)",
-            "config": config_dict(args, inp, {"workload": f"sphere_shell{args.cpu_sample_n} (bounded CPU sample of "
-                                                          f"sphere_shell{args.n})"}),
-            "impl": "reference",
+            "config": cfg, "impl": "reference",
             "cpu_baseline": {"value": round(value, 4), "unit": "MDOF/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(value, 4), "unit": "MDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

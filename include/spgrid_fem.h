@@ -162,17 +162,21 @@ SGS_API int sgs_design_get(sgs_session* s, double* density);
 /* No counterpart in the reference.  Allocation-free variant of sgs_sensitivity
  * for callers that cannot allocate device memory while they run (frameworks
  * that own the allocator, code that must not call cudaMalloc/cudaFree once it
- * has started).  All arrays are caller-owned DEVICE buffers on the session's
- * device: density_dev[nblocks][64] in, dc_dev and element_energy_dev
- * [nblocks][64] out, objective_dev one double out.  The only scratch, the
- * per-CTA partial sums of the objective, lives in a static device array of
+ * has started).  Like sgs_sensitivity it reads the displacements of the
+ * session's last sgs_solve: call it after a solve (before one it reads zeros,
+ * after a change of density it reads the previous solution).  All arrays are
+ * caller-owned DEVICE buffers on the session's device, and that device must be
+ * current (another current device returns SGS_ERR_INPUT):
+ * density_dev[nblocks][64] in, dc_dev and element_energy_dev [nblocks][64] out,
+ * objective_dev one double out.  The only scratch, the per-CTA partial sums of
+ * the objective, lives in a static device array of
  * SGS_SENSITIVITY_STATIC_MAX_PARTIALS doubles that every GPU loading the
  * library holds until exit; problems with more than that many 256-cell CTAs
- * (nblocks * 64 > MAX * 256) are rejected with SGS_ERR_INPUT.  The first call
- * on a device looks the array's device address up, so make that first call
- * before any stream capture.  Every call reuses the same array: calls that
- * overlap on the GPU (other host threads, other sessions on the device) race.
- * Synchronous; returns 0 or an error code (message in sgs_last_error). */
+ * (nblocks * 64 > MAX * 256) are rejected with SGS_ERR_INPUT.  The session's
+ * set-up (sgs_create) looks the array's device address up on its device, so
+ * this call itself makes no lookup.  Every call reuses the same array: calls
+ * that overlap on the GPU (other host threads, other sessions on the device)
+ * race.  Synchronous; returns 0 or an error code (message in sgs_last_error). */
 #define SGS_SENSITIVITY_STATIC_MAX_PARTIALS 16384
 SGS_API int sgs_sensitivity_static(sgs_session* s, const double* density_dev, double* dc_dev,
                                    double* element_energy_dev, double* objective_dev);
@@ -204,7 +208,8 @@ SGS_API int sgs_level_stencils(sgs_session* s, int level, double* out, uint32_t*
 /* Average device time (ms, CUDA events) of `reps` back-to-back runs of a level-0
  * operator on the session's resident data: 0 the PCG matvec q = K s (FP64, with
  * Project and the s.q partials), 1 residual, 2 one smoothing sweep (8 colours),
- * 3 one preconditioner application (V-cycle). */
+ * 3 one preconditioner application (V-cycle), 4 K u on the planar fields.  Ops
+ * 1, 2 and 4 run in the V-cycle's precision (FP32 in mixed sessions). */
 SGS_API int sgs_time_op(sgs_session* s, int op, int reps, double* ms);
 
 /* Decode a blob and encode it again with this library's codec (which = 0 for

@@ -92,6 +92,11 @@ struct Bottom {
 
 enum Precision { PREC_REFERENCE = 0, PREC_FP64 = 1, PREC_MIXED = 2 };
 
+// Scratch of the allocation-free sensitivity entry point (sgs_sensitivity_static):
+// per-CTA partial sums of the objective in a static device array that every GPU
+// loading the library holds until the process exits.
+static __device__ __align__(256) double g_sensitivity_partials[SGS_SENSITIVITY_STATIC_MAX_PARTIALS];
+
 // ---------------------------------------------------------------------------
 // The solver: device hierarchy + PCG
 // ---------------------------------------------------------------------------
@@ -99,6 +104,8 @@ class Solver {
  public:
   Problem P;
   int precision = PREC_REFERENCE;
+  int device = -1;                    // CUDA device of the session (current at set-up)
+  double* static_partials = nullptr;  // device address of g_sensitivity_partials on that device
   cudaStream_t stream = nullptr;
   // level data (double for reference/fp64, float for the mixed V-cycle)
   std::vector<std::unique_ptr<Level<double>>> L64;
@@ -174,7 +181,17 @@ class Solver {
 
   void init(int prec) {
     precision = prec;
+    // the device the session lives on (current at set-up); entry points that
+    // take caller-owned device buffers check that it is current again
+    SGS_CUDA(cudaGetDevice(&device));
     SGS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    // the host-side name of a __device__ array is not its device address:
+    // resolve it here, once per session, with the session's device current
+    {
+      void* p = nullptr;
+      SGS_CUDA(cudaGetSymbolAddress(&p, g_sensitivity_partials));
+      static_partials = static_cast<double*>(p);
+    }
     SGS_CUDA(cudaMallocHost(&h_scal, 16 * sizeof(double)));
     using clk = std::chrono::steady_clock;
     auto t0 = clk::now();
@@ -2005,6 +2022,8 @@ static double time_op(Solver& S, int op, int reps) {
       S.sweep<T>(0, packed ? nullptr : d.u.p, d.b.p, true, false);
     } else if (op == 3) {
       S.precondition();
+    } else if (op == 4) {
+      S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);  // K u in the V-cycle's precision
     }
   };
   run();
@@ -2270,8 +2289,8 @@ SGS_API int sgs_design_get(sgs_session* h, double* density) {
 // array of SGS_SENSITIVITY_STATIC_MAX_PARTIALS doubles (128 KiB, held by every
 // GPU that loads the library until the process exits).
 // ---------------------------------------------------------------------------
-static __device__ __align__(256) double g_sensitivity_partials[SGS_SENSITIVITY_STATIC_MAX_PARTIALS];
-static double* g_sensitivity_partials_addr[128] = {nullptr};  // device address per device ordinal
+// The array itself is declared before the Solver class, whose set-up resolves
+// its device address on the session's device.
 
 // Sum the partials in index order, the order sgs_sensitivity uses on the host.
 __global__ void sum_in_order_kernel(const double* __restrict__ part, int n, double* __restrict__ out) {
@@ -2296,16 +2315,17 @@ SGS_API int sgs_sensitivity_static(sgs_session* h, const double* density_dev, do
     return SGS_ERR_INPUT;
   }
   try {
-    int dev = 0;
+    // the buffers, the stream and the scratch address all belong to the session's device
+    int dev = -1;
     SGS_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 128) throw CudaError("device ordinal out of range", SGS_ERR_CUDA);
-    if (!g_sensitivity_partials_addr[dev]) {
-      // the symbol's host-side name is not a device address: resolve it once per device
-      void* p = nullptr;
-      SGS_CUDA(cudaGetSymbolAddress(&p, g_sensitivity_partials));
-      g_sensitivity_partials_addr[dev] = static_cast<double*>(p);
+    if (dev != S.device) {
+      char m[160];
+      std::snprintf(m, sizeof m, "sgs_sensitivity_static called with device %d current; the session lives on device %d",
+                    dev, S.device);
+      h->error = m;
+      return SGS_ERR_INPUT;
     }
-    double* part = g_sensitivity_partials_addr[dev];
+    double* part = S.static_partials;
     if (nin == 0) {
       SGS_CUDA(cudaMemsetAsync(objective_dev, 0, sizeof(double), S.stream));
     } else {
@@ -2532,7 +2552,7 @@ SGS_API void fem_solve(void* input, void* output) {
 SGS_API void fem_solve_free(void* blob) { delete[] static_cast<char*>(blob); }
 
 SGS_API int sgs_time_op(sgs_session* h, int op, int reps, double* ms) {
-  if (!h || !ms || host_only(h) || reps <= 0 || op < 0 || op > 3) return SGS_ERR_INPUT;
+  if (!h || !ms || host_only(h) || reps <= 0 || op < 0 || op > 4) return SGS_ERR_INPUT;
   try {
     *ms = h->solver->mixed() && op != 0 && op != 3 ? time_op<float>(*h->solver, op, reps)
                                                    : time_op<double>(*h->solver, op, reps);

@@ -140,3 +140,49 @@ def test_foreign_state_pointer_is_rejected(native_lib):
     inp.extra_ints["state_ptr_higher"] = int(np.uint32(addr >> 32).view(np.int32))
     out = native.fem_solve(inp)
     assert not out.success and out.error_code == 1
+
+
+def _two_bodies(gap_cells: int = 4):
+    """A 24x16x16 cantilever fixed at x = 0 and, beyond a gap of empty cells, a
+    loose 8x8x8 box carrying a load: the second body has no support."""
+    n = (24 + gap_cells + 8, 16, 16)
+    rho = np.zeros(n)
+    rho[:24] = 0.5
+    rho[24 + gap_cells:, 4:12, 4:12] = 0.5
+    cells = np.argwhere(np.ones((1, 16, 16), bool)).astype(np.int32)
+    f = np.zeros(2, configs.FORCE_DTYPE)
+    f["coord"][0] = (24, 8, 8)
+    f["f"][0] = (0.0, -1.0, 0.0)
+    f["coord"][1] = (n[0], 8, 8)
+    f["f"][1] = (0.0, -1.0, 0.0)
+    return configs.Problem("two_bodies", n, rho, cells, f, 1.0 / n[0], configs.mg_level_for(n[0], 8))
+
+
+def test_indefinite_operator_reports_breakdown(native_lib):
+    """Material whose SIMP stiffness is negative (a negative minimum_stiffness:
+    E = (1 - Emin) rho^p + Emin < 0 for rho^p < -Emin / (1 - Emin)) makes the
+    operator indefinite.  The reference's CG throws on s.q <= 0
+    (CONJUGATE_GRADIENT.cpp:49-52) and its PARDISO factorization fails on the
+    bottom; here the call returns success = 0 with SGS_ERR_BREAKDOWN, whichever
+    check sees it first, and the context stays usable."""
+    prob = _two_bodies()
+    prob.density[:24] = np.where(np.arange(24)[:, None, None] >= 12, 0.2, 0.9)
+    inp = configs.to_inputs(prob, minimum_stiffness=-0.5)
+    out = native.fem_solve(inp)
+    assert not out.success and out.error_code == 8, (out.error_code, out.info)
+    # the device is still usable afterwards
+    ok = native.fem_solve(configs.to_inputs(configs.cantilever_box(16, bottom_size=4)))
+    assert ok.success
+
+
+def test_unsupported_island_reports_breakdown(native_lib):
+    """A loaded body with no Dirichlet support makes the operator singular (its
+    rigid motions cost no energy).  The reference's PARDISO stops on the zero
+    pivots of the bottom factorization (Elasticity_Matrix.cpp:213-231); here the
+    bottom inverse or the CG checks report SGS_ERR_BREAKDOWN, in every precision
+    mode."""
+    inp = configs.to_inputs(_two_bodies())
+    for prec in (native.PRECISION_REFERENCE, native.PRECISION_FP64, native.PRECISION_MIXED):
+        inp.extra_ints["sgs_precision"] = prec
+        out = native.fem_solve(inp)
+        assert not out.success and out.error_code == 8, (prec, out.error_code, out.info, out.extra_ints)

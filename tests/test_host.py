@@ -81,3 +81,42 @@ def test_host_hierarchy_matches_oracle(native_lib, problem):
         assert np.array_equal(ses.blocks(lev), ref.blocks(lev)), lev
         assert np.array_equal(ses.flags(lev), ref.flags(lev)), lev
         assert np.array_equal(ses.boundary_blocks(lev), ref.boundary_blocks(lev)), lev
+
+
+# ---- host-injected failures (the reference's abort/throw sites, SURVEY of
+# CG_SYSTEM.cpp:59-74 and CONJUGATE_GRADIENT.cpp:49-52): each one is caught on
+# the host before any device work and comes back as success = 0 with a code
+@pytest.mark.parametrize("bad", [np.nan, np.inf])
+def test_fem_solve_rejects_non_finite_force(native_lib, bad):
+    inp = configs.to_inputs(configs.cantilever_box(8))
+    inp.forces["f"][0, 1] = bad
+    out = _fem_outputs(fi.serialize_inputs(inp))
+    assert not out.success and out.error_code == 4 and "non-finite force" in out.info
+
+
+def test_fem_solve_rejects_non_finite_dirichlet_value(native_lib):
+    inp = configs.to_inputs(configs.cantilever_box(8))
+    inp.dirichlet_nodes["value"][3] = np.nan
+    out = _fem_outputs(fi.serialize_inputs(inp))
+    assert not out.success and out.error_code == 4 and "non-finite Dirichlet" in out.info
+
+
+def test_negative_and_nan_density_cells_are_empty(native_lib):
+    """The reference stores material only where density > 0
+    (SPGrid_CPU_Solver.cpp:123-129): a negative or NaN density leaves the cell
+    empty, exactly as 0 does, so the hierarchy and its flags are those of the
+    zero-density input."""
+    prob = configs.cantilever_box(16, density=(0.2, 1.0), bottom_size=4)
+    zero = prob.density.copy()
+    zero[10:14, 4:9, 2:6] = 0.0
+    ref = native.Session(configs.to_inputs(configs.Problem(**{**prob.__dict__, "density": zero})),
+                         precision=native.HOST_SETUP_ONLY)
+    for fill in (-0.5, np.nan):
+        rho = prob.density.copy()
+        rho[10:14, 4:9, 2:6] = fill
+        ses = native.Session(configs.to_inputs(configs.Problem(**{**prob.__dict__, "density": rho})),
+                             precision=native.HOST_SETUP_ONLY)
+        assert ses.levels == ref.levels
+        for lev in range(ref.levels):
+            assert np.array_equal(ses.blocks(lev), ref.blocks(lev)), (fill, lev)
+            assert np.array_equal(ses.flags(lev), ref.flags(lev)), (fill, lev)

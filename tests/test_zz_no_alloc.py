@@ -5,8 +5,9 @@ every buffer, and the entry point's only scratch is a static device array.  The
 test drives it through the C ABI with device buffers it allocated itself and
 checks two calls in a row against sgs_sensitivity, the entry point that
 allocates its own buffers, within the 1e-12 relative tolerance the parity tests
-use for the same quantity computed twice on the GPU.  It also checks that a
-problem larger than the static array is refused.  Collected last so a
+use for the same quantity computed twice on the GPU, and that further calls
+take no device memory.  It also checks that a problem larger than the static
+array is refused, and a call made with another device current.  Collected last so a
 stop-at-first-failure run has already run every other test when it gets here.
 """
 import ctypes as C
@@ -37,9 +38,13 @@ def test_static_sensitivity_matches_allocating_entry_point(native_lib):
         se = torch.full_like(rho, np.nan)
         obj = torch.full((1,), np.nan, dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
+
+        def call_static():
+            return lib.sgs_sensitivity_static(s.h, C.c_void_p(rho.data_ptr()), C.c_void_p(dc.data_ptr()),
+                                              C.c_void_p(se.data_ptr()), C.c_void_p(obj.data_ptr()))
+
         for call in range(2):
-            rc = lib.sgs_sensitivity_static(s.h, C.c_void_p(rho.data_ptr()), C.c_void_p(dc.data_ptr()),
-                                            C.c_void_p(se.data_ptr()), C.c_void_p(obj.data_ptr()))
+            rc = call_static()
             assert rc == 0, lib.sgs_last_error(s.h)
             assert _rel(dc.cpu().numpy(), dc_ref) < 1e-12, call
             assert _rel(se.cpu().numpy(), se_ref) < 1e-12, call
@@ -47,6 +52,35 @@ def test_static_sensitivity_matches_allocating_entry_point(native_lib):
             dc.fill_(np.nan)
             se.fill_(np.nan)
             obj.fill_(np.nan)
+        # the point of the entry point: further calls take no device memory, neither
+        # from the driver (free memory unchanged) nor from torch's caching pool
+        torch.cuda.synchronize()
+        free_before, _ = torch.cuda.mem_get_info()
+        reserved_before = torch.cuda.memory_reserved()
+        for _ in range(3):
+            assert call_static() == 0, lib.sgs_last_error(s.h)
+        torch.cuda.synchronize()
+        free_after, _ = torch.cuda.mem_get_info()
+        assert free_after == free_before
+        assert torch.cuda.memory_reserved() == reserved_before
+
+
+@pytest.mark.skipif("__import__('torch').cuda.device_count() < 2", reason="needs two visible GPUs")
+def test_static_sensitivity_rejects_another_current_device(native_lib):
+    import torch
+
+    torch.cuda.set_device(0)
+    inp = configs.to_inputs(configs.cantilever_box(8, bottom_size=8))
+    lib = native.load()
+    with native.Session(inp, precision=native.PRECISION_FP64) as s:
+        s.solve(tolerance=1e-8)
+        n = inp.density.data.size
+        with torch.cuda.device(1):
+            bufs = [torch.zeros(n, dtype=torch.float64, device="cuda:1") for _ in range(3)]
+            obj = torch.zeros(1, dtype=torch.float64, device="cuda:1")
+            rc = lib.sgs_sensitivity_static(s.h, *[C.c_void_p(b.data_ptr()) for b in bufs],
+                                            C.c_void_p(obj.data_ptr()))
+        assert rc == 1 and b"device 1 current" in lib.sgs_last_error(s.h)
 
 
 def test_static_sensitivity_rejects_problems_above_the_limit(native_lib):
