@@ -2493,10 +2493,18 @@ SGS_API void fem_solve(void* input, void* output) {
         outs.extra_doubles["output_seconds"] = 0;
         outs.extra_doubles["teardown_seconds"] = 0;
         outs.extra_ints["kernel_launches"] = int(st.kernel_launches);
+        // as the reference, a solve that reaches the iteration cap still
+        // returns its displacements with success set (SPGrid_CPU_Solver.cpp:326-341);
+        // "converged" and the message say whether the stopping rule was met
+        const bool converged = st.final_residual <= h->solver->P.tolerance * st.initial_residual;
+        outs.extra_ints["converged"] = converged ? 1 : 0;
         outs.success = true;
         char m[200];
-        std::snprintf(m, sizeof m, "converged in %d iterations, L-inf residual %.6g of %.6g", st.iterations,
-                      st.final_residual, st.initial_residual);
+        std::snprintf(m, sizeof m,
+                      converged ? "converged in %d iterations, L-inf residual %.6g of %.6g"
+                                : "stopped at the iteration cap after %d iterations without converging, L-inf residual "
+                                  "%.6g of %.6g",
+                      st.iterations, st.final_residual, st.initial_residual);
         outs.info = m;
         const auto t2 = clk::now();
         char* blob = nullptr;
