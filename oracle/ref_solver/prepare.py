@@ -6,7 +6,8 @@ explicit specialisations without ``template<>``, its dependent member templates
 without the ``template`` disambiguator, a local variable that shadows a
 template parameter, and a never-instantiated function that names an undeclared
 ``omega``.  This script copies those sources, unchanged apart from the
-mechanical patch below, into a build folder that is not committed
+mechanical patch below (plus a compile-time switch for the float rounding and
+full-precision residual prints, both for the tests), into a build folder that is not committed
 (``oracle/_ref/src``); ``oracle/Makefile`` then compiles them with
 ``oracle/ref_solver/ref_support.cpp`` (an exact SPD solve behind the
 ``pardiso_64`` calling convention, replacing MKL PARDISO) into
@@ -44,6 +45,16 @@ PATCH = [
     ("solver/CG/CG_VECTOR.cpp", r"\bd\(offset\)", "d_arr(offset)", 4),
     # Correction::Run (never instantiated) uses an omega it does not declare
     ("solver/CPU_Kernels/Correction.h", r"(const T Struct_Type::\* const d_fields\[6\])\)", r"\1, T omega = T(1))", 1),
+    # test toggle: SGS_REF_FLOAT_ROUNDING (compiler definition, true as shipped)
+    # switches the float rounding of the CG updates (SPGrid_CPU_Solver.cpp:164-168)
+    # and of the V-cycle's Cast_To_Float (Multigrid_Hierarchy.h:439-451), so that
+    # a plain FP64 build of the same code exists for tight parity checks
+    ("solver/SPGrid_CPU_Solver.cpp", r"\b(\w)\.using_float = true;", r"\1.using_float = SGS_REF_FLOAT_ROUNDING;", 5),
+    ("solver/MG/Multigrid_Hierarchy.h", r"float tmp = d\(offset\);\s*d\(offset\) = tmp;",
+     "if (SGS_REF_FLOAT_ROUNDING) { float tmp = d(offset); d(offset) = tmp; }", 1),
+    # residual prints with all digits (the harness reads the residual history from them)
+    ("solver/SPGrid_CPU_Solver.cpp", r'extern "C" void fem_solve\(void \*input, void \*output\) \{',
+     r"\g<0> std::cout.precision(17);", 1),
 ]
 
 

@@ -1,0 +1,59 @@
+"""Regenerate ref_solves.npz: solves of the cases in solve_cases.py by the
+reference's own fem_solve, built with GCC from the reference sources
+(oracle/Makefile, target ``refsolver``; oracle/ref_solver/ref_run.py calls it).
+
+Per case and build ("shipped", "fp64") the file holds the iteration count, the
+residual history (L-inf before each iteration), the digest of the input blob,
+and the displacements: the whole field [blocks][64][3] for the small cases,
+otherwise a seeded sample of node slots with per-component sums and maxima of
+the whole field.
+
+Run from the repository root:  python tests/golden/make_solve_golden.py
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+from solve_cases import CASES, SAMPLES, digest, inputs  # noqa: E402
+
+
+def main() -> None:
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "refsolver"], check=True)
+    from oracle.ref_solver import ref_run
+    out = {}
+    for name, (_, tol_shipped, tol_fp64, whole) in CASES.items():
+        for flavour, tol in (("shipped", tol_shipped), ("fp64", tol_fp64)):
+            inp = inputs(name, tol)
+            res, iterations, history = ref_run.solve(inp, flavour)
+            assert res.success, (name, flavour, res.info)
+            u = np.asarray(res.displacements.data)[..., :3]
+            key = f"{name}/{flavour}"
+            out[key + "/digest"] = np.array(digest(inp))
+            out[key + "/iterations"] = np.array(iterations)
+            out[key + "/history"] = np.array(history)
+            if whole:
+                out[key + "/u"] = u
+            else:
+                rng = np.random.default_rng(1234)
+                flat = u.reshape(-1, 3)
+                slots = np.sort(rng.choice(len(flat), size=min(SAMPLES, len(flat)), replace=False))
+                out[key + "/slots"] = slots
+                out[key + "/u_sample"] = flat[slots]
+                out[key + "/u_sum"] = flat.sum(0)
+                out[key + "/u_absmax"] = np.abs(flat).max(0)
+            print(f"{key}: {iterations} iterations, |u|max {np.abs(u).max():.6g}")
+    np.savez_compressed(os.path.join(HERE, "ref_solves.npz"), **out)
+    print("written", os.path.join(HERE, "ref_solves.npz"))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,32 @@
+"""The solve cases whose reference outputs are committed in ref_solves.npz.
+
+Each case is a seeded synthetic input built by spgrid_topo_opt_b200.configs
+(the tests rebuild it and check its serialized bytes against the stored
+digest), solved by the reference's own fem_solve in two builds: as shipped
+("shipped": float-rounded CG updates and V-cycle casts) and with that rounding
+switched off ("fp64").  Config 0 of the benchmark suite is the 64^3 cantilever
+with density 0.1, mg_bottom_size 16 and tolerance 1e-4.
+"""
+from __future__ import annotations
+
+import hashlib
+
+from spgrid_topo_opt_b200 import configs, fem_interface as fi
+
+# name: (builder, tolerance of the shipped solve, tolerance of the fp64 solve, full field stored)
+CASES = {
+    "cantilever16": (lambda: configs.cantilever_box(16, density=(0.2, 1.0), bottom_size=4), 1e-10, 1e-10, True),
+    "shell24": (lambda: configs.sphere_shell(24, bottom_size=4), 1e-10, 1e-10, True),
+    "config0_box32": (lambda: configs.cantilever_box(32, density=0.1, bottom_size=16), 1e-4, 1e-10, False),
+    "config0_box64": (lambda: configs.cantilever_box(64, density=0.1, bottom_size=16), 1e-4, 1e-10, False),
+    "shell64": (lambda: configs.sphere_shell(64, bottom_size=16), 1e-6, 1e-10, False),
+}
+SAMPLES = 4096  # nodes sampled (seeded) from the displacement field where it is not stored whole
+
+
+def inputs(name: str, tolerance: float):
+    return configs.to_inputs(CASES[name][0](), tolerance=tolerance)
+
+
+def digest(inp) -> str:
+    return hashlib.sha256(fi.serialize_inputs(inp)).hexdigest()
