@@ -43,7 +43,15 @@ extern "C" {
  *   "sgs_precision"  0 = reference arithmetic (float-rounded CG updates and
  *                        V-cycle casts, the default), 1 = FP64, 2 = FP32 V-cycle
  *                        with FP64 outer PCG;
- *   "sgs_honor_max_iterations"  1 = stop at krylov.max_iterations instead of 500.
+ *   "sgs_honor_max_iterations"  1 = stop at krylov.max_iterations instead of 500;
+ *   "sgs_dense_bottom_max"  largest bottom (unknowns) inverted densely (default
+ *                        24576).  A larger bottom -- the reference driver's
+ *                        default mg_bottom_size 64 gives 10^5-10^6 unknowns,
+ *                        which the reference factors with PARDISO -- is solved
+ *                        exactly (to round-off) by CG preconditioned with
+ *                        V-cycles over further levels coarsened below it.
+ * A solve that reaches the iteration cap returns success = 1 as the
+ * reference's does, with extra_ints "converged" = 0. 
  * Warm starting as the reference's (SPGrid_CPU_Solver.cpp:56-73, 240-321,
  * 389-408): with extra_ints "keep_state" = 1 the output's extra_ints
  * "state_ptr_lower"/"state_ptr_higher" name a solver state (the last solution
@@ -187,6 +195,34 @@ SGS_API int sgs_sensitivity_static(sgs_session* s, const double* density_dev, do
  * SGS_ERR_INPUT when a cell's material status would change. */
 SGS_API int sgs_set_density(sgs_session* s, const double* density);
 
+/* ---- device-resident calls (the PyTorch layer) --------------------------- */
+/* No counterpart in the reference (its driver owns host arrays only).  These
+ * keep the differentiable compliance on the GPU: densities in, compliance and
+ * gradient out, all as DEVICE buffers on the session's device, which must be
+ * current.  caller_stream (a cudaStream_t, may be NULL for a device-wide
+ * synchronization) is the stream that produced the inputs; the session's
+ * stream waits for it, and each call returns when its results are complete.
+ * Return 0 or an error code (message in sgs_last_error). */
+
+/* Entries of the level-0 solution in the layout the gradient reads: 3 * nodes. */
+SGS_API int64_t sgs_solution_size(sgs_session* s);
+/* sgs_set_density from device memory ([nblocks][64], input block order): the
+ * stiffness scales, Galerkin operators and bottom are rebuilt on the device;
+ * SGS_ERR_INPUT when a cell's material status would change or a stiffness is
+ * not finite (the session is then unchanged). */
+SGS_API int sgs_set_density_device(sgs_session* s, const double* density_dev, void* caller_stream);
+/* Copy the last solve's displacements (level-0 layout, sgs_solution_size entries). */
+SGS_API int sgs_solution_device(sgs_session* s, double* u_dev, void* caller_stream);
+/* out_dev[0] = f.u of the last solve: each loaded node once, with the force
+ * the solve assembled for it (the last entry of a node, SPGrid_CPU_Solver.cpp:290-296). */
+SGS_API int sgs_compliance_device(sgs_session* s, double* out_dev, void* caller_stream);
+/* grad[nblocks][64] = factor * (*scale_dev) * p rho^(p-1) (1 - Emin) u_e^T K0 u_e
+ * (topo_opt/objective/minimal_compliance.cpp:86-146), 0 for cells with rho <= 0;
+ * u_dev is a saved solution (sgs_solution_device) or NULL for the last solve;
+ * scale_dev may be NULL (1). */
+SGS_API int sgs_sensitivity_device(sgs_session* s, const double* u_dev, const double* density_dev, double factor,
+                                   const double* scale_dev, double* grad_dev, void* caller_stream);
+
 /* ---- inspection and unit operators (tests) ------------------------------ */
 SGS_API int sgs_level_count(sgs_session* s);
 /* Active blocks of a level in SPGrid page order; coords may be null. */
@@ -198,7 +234,8 @@ SGS_API int sgs_boundary_blocks(sgs_session* s, int level, int32_t* ordinals);
  *  0 level-0 K*u            1 level-0 residual b - K u
  *  2 one smoothing sweep    (arg bit0 forward, bit1 boundary band only)
  *  3 restriction level -> level+1     4 prolongation level+1 -> level (accumulate)
- *  5 stencil multiply       6 bottom solve (last level)   7 one V-cycle on level 0 */
+ *  5 stencil multiply       6 bottom solve (the V-cycle's last level, mg_level - 1)
+ *  7 one V-cycle on level 0 */
 SGS_API int sgs_apply(sgs_session* s, int op, int level, int arg, const double* in, const double* in2, double* out);
 
 /* Galerkin stencils of a level as [nblocks*128][243] (row node, comp v; column

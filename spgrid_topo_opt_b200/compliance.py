@@ -15,8 +15,12 @@ free nodes with homogeneous Dirichlet conditions, and for densities above
 ``minimum_density`` (where the SIMP map is differentiable).
 
 ``rho`` has the shape of the input density blocks, [nblocks, 64] (in-block index
-i*16 + j*4 + k).  The problem stays resident on the GPU between calls; only the
-densities change (the set of material cells, rho > 0, must not).
+i*16 + j*4 + k), on the GPU or the host.  The problem stays resident on the GPU
+between calls; only the densities change (the set of material cells, rho > 0,
+must not).  Everything runs on the device: the densities go to the solver
+device to device, f.u is summed there, and the backward's sensitivity kernel
+writes the gradient tensor directly; under ``torch.no_grad()`` (or for a rho
+that does not require a gradient) no solution copy is kept.
 """
 from __future__ import annotations
 
@@ -45,22 +49,36 @@ def force_work(inputs: fi.FEMInputs, disp: np.ndarray) -> float:
 
 
 class _ComplianceFn(torch.autograd.Function):
+    """Forward: densities to the session (device to device), solve, f.u on the
+    device.  When a gradient will be needed the forward keeps a device copy of
+    the solution; the backward launches the sensitivity kernel on it, scaled by
+    -dx and the incoming gradient (a device scalar), straight into the gradient
+    tensor.  No array crosses to the host in either pass."""
+
     @staticmethod
-    def forward(ctx, rho: torch.Tensor, model: "Compliance"):
-        r = rho.detach().to("cpu", torch.float64).numpy().reshape(-1, 64)
-        model.session.set_density(r)
+    def forward(ctx, rho: torch.Tensor, model: "Compliance", keep: bool):
+        dev = torch.device("cuda", torch.cuda.current_device())
+        r = rho.detach().to(dev, torch.float64).reshape(-1, 64).contiguous()
+        model.session.set_density_device(r)
         model.last_stats = model.session.solve(tolerance=model.tolerance)
-        disp = model.session.displacements()
-        _, dc, _ = model.session.sensitivity(r)
-        model.displacements = disp
+        c = torch.empty(1, dtype=torch.float64, device=dev)
+        model.session.compliance_device(c)
+        if keep:
+            u = torch.empty(model.session.solution_size(), dtype=torch.float64, device=dev)
+            model.session.solution_device(u)
+            ctx.save_for_backward(r, u)
         ctx.dx = float(model.inputs.dx)
-        ctx.save_for_backward(torch.as_tensor(dc.reshape(rho.shape), dtype=rho.dtype, device=rho.device))
-        return torch.tensor(force_work(model.inputs, disp), dtype=rho.dtype, device=rho.device)
+        ctx.model = model
+        ctx.shape, ctx.dtype, ctx.device = rho.shape, rho.dtype, rho.device
+        return c.reshape(()).to(rho.device, rho.dtype)
 
     @staticmethod
     def backward(ctx, grad_out: torch.Tensor):
-        (dc,) = ctx.saved_tensors
-        return -ctx.dx * dc * grad_out, None
+        r, u = ctx.saved_tensors
+        g = grad_out.detach().to(r.device, torch.float64).reshape(1).contiguous()
+        grad = torch.empty_like(r)
+        ctx.model.session.sensitivity_device(u, r, -ctx.dx, g, grad)
+        return grad.reshape(ctx.shape).to(ctx.device, ctx.dtype), None, None
 
 
 class Compliance:
@@ -70,11 +88,15 @@ class Compliance:
         self.inputs = copy.deepcopy(inputs)
         self.tolerance = tolerance
         self.session = native.Session(self.inputs, precision=precision)
-        self.displacements = None
         self.last_stats = None
 
     def __call__(self, rho: torch.Tensor) -> torch.Tensor:
-        return _ComplianceFn.apply(rho, self)
+        keep = torch.is_grad_enabled() and rho.requires_grad
+        return _ComplianceFn.apply(rho, self, keep)
+
+    def displacements(self) -> np.ndarray:
+        """The last solve's displacements per input block, [nblocks, 64, 4] (host copy)."""
+        return self.session.displacements()
 
     def close(self):
         self.session.close()

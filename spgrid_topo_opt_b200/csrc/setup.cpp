@@ -320,6 +320,7 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   P.lambda0 = in.global_lambda;
   P.disable_mg = in.mg_level <= 0;
   P.mg_levels = in.mg_level <= 0 ? 1 : in.mg_level;
+  P.dense_bottom_max = in.get_int("sgs_dense_bottom_max", 24576);
   P.smoothing = in.pre_and_post_smoothing_iter;
   P.boundary_smoothing = in.get_int("boundary_smoothing", 5);
   P.tolerance = in.krylov.tolerance;
@@ -458,8 +459,7 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
 
   // ---- coarse levels (Multigrid_Hierarchy.h:122-195)
   const int pad[3] = {2 * BLK_X, 2 * BLK_Y, 2 * BLK_Z};
-  for (int lev = 1; lev < P.mg_levels; ++lev) {
-    HostLevel& F = P.levels[lev - 1];
+  auto coarsen = [&](const HostLevel& F) {
     int sz[3];
     for (int v = 0; v < 3; ++v) {
       int fine = F.size[v] + 1 - pad[v];
@@ -518,11 +518,29 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
           bc.set_page(cx0 + ((d >> 2) & 1) * BLK_X, cy0 + ((d >> 1) & 1) * BLK_Y, cz0 + (d & 1) * BLK_Z);
     }
     bc.finalize();
-    P.levels.push_back(std::move(bc.L));
-  }
+    return std::move(bc.L);
+  };
+  for (int lev = 1; lev < P.mg_levels; ++lev) P.levels.push_back(coarsen(P.levels[lev - 1]));
   for (auto& L : P.levels) flag_nodes(L);
   for (auto& L : P.levels) flag_boundary(L);
   for (auto& L : P.levels) finish_level(L);
+  // levels below a bottom too large for the dense inverse: the bottom is then
+  // solved by CG with V-cycles over them (same coarsening rule, Galerkin
+  // operators down to depth 6)
+  if (!P.disable_mg) {
+    auto active_nodes = [](const HostLevel& L) {
+      long n = 0;
+      for (long i = 0; i < long(L.nb) * NODES_PER_BLOCK; ++i) n += (L.flags[size_t(i)] & F_ACTIVE_NODE) ? 1 : 0;
+      return n;
+    };
+    while (P.levels.size() < 7 && 3 * active_nodes(P.levels.back()) > P.dense_bottom_max) {
+      HostLevel L = coarsen(P.levels.back());
+      flag_nodes(L);
+      flag_boundary(L);
+      finish_level(L);
+      P.levels.push_back(std::move(L));
+    }
+  }
 
   // ---- padding check (Multigrid_Hierarchy.h:145-157)
   {

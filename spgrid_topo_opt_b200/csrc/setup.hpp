@@ -50,8 +50,12 @@ struct Problem {
   int resolution[3] = {0, 0, 0};
   double dx = 1, mu0 = 0, lambda0 = 0;
   double penalty = 0, minimum_stiffness = 0, minimum_density = 0;  // SIMP parameters (fem_interface.h:318-353)
-  int mg_levels = 3;          // levels after the mg_level=0 rewrite
+  int mg_levels = 3;          // levels of the V-cycle after the mg_level=0 rewrite
   bool disable_mg = false;
+  // A bottom level (levels[mg_levels - 1]) with more unknowns than this is
+  // solved by CG preconditioned with V-cycles over further levels, which then
+  // follow it in `levels` (at most 7 levels in all); smaller ones are inverted.
+  long dense_bottom_max = 24576;
   int explicit_level = 2;
   int smoothing = 1, boundary_smoothing = 5;
   double tolerance = 1e-4;

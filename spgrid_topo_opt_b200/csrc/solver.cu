@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -92,6 +93,31 @@ struct Bottom {
 
 enum Precision { PREC_REFERENCE = 0, PREC_FP64 = 1, PREC_MIXED = 2 };
 
+// Unknowns of a bottom level are the nodes with an active spoke (the rows of
+// Build_CSR_Matrix, Elasticity_Matrix.cpp:16-164): out = in there, 0 elsewhere
+// (in-place allowed).
+__global__ void inner_mask_kernel(double* out, const double* in, const uint32_t* __restrict__ spokes, long N) {
+  pdl_wait();
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const bool on = spokes[i] & 0x07ffffffu;
+#pragma unroll
+  for (int v = 0; v < 3; ++v) out[i + v * N] = on ? in[i + v * N] : 0.0;
+}
+
+// The inner solve's result on the unknowns, b elsewhere (PARDISO_Solve writes
+// back only the rows it solved, Elasticity_Matrix.cpp:238-269).
+template <typename T>
+__global__ void inner_select_kernel(T* __restrict__ out, const double* __restrict__ x, const double* __restrict__ b,
+                                    const uint32_t* __restrict__ spokes, long N) {
+  pdl_wait();
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const bool on = spokes[i] & 0x07ffffffu;
+#pragma unroll
+  for (int v = 0; v < 3; ++v) out[i + v * N] = T(on ? x[i + v * N] : b[i + v * N]);
+}
+
 // Scratch of the allocation-free sensitivity entry point (sgs_sensitivity_static):
 // per-CTA partial sums of the objective in a static device array that every GPU
 // loading the library holds until the process exits.
@@ -117,6 +143,8 @@ class Solver {
   DevBuf<double> x, f, s, q, ubk, scratch;
   DevBuf<int> lift_node, lift_axis, force_node;
   DevBuf<double> lift_val, force_val;
+  DevBuf<int> load_node;     // loaded nodes, once each (the compliance f.u)
+  DevBuf<double> load_val;
   DevBuf<double> red;      // reduction partials
   DevBuf<double> scal;     // device scalars: 0 rho, 1 rho_old, 2 sq, 3 norm, 4 beta, 5 alpha, 6 -alpha, 7 breakdown
   double* h_scal = nullptr;  // pinned mirror
@@ -175,9 +203,13 @@ class Solver {
   bool mixed() const { return precision == PREC_MIXED; }
   // the mixed and FP64 V-cycles keep their level-0 iterate packed (see
   // reset_u4_kernel); the reference-rounding mode rounds planar fields
-  bool packed0() const { return (mixed() || precision == PREC_FP64) && nlev() > 1; }
+  bool packed0() const { return (mixed() || precision == PREC_FP64) && nout() > 1; }
   bool round_ref() const { return precision == PREC_REFERENCE; }
+  // levels on the device: the V-cycle's (the reference's mg_level) followed by
+  // the levels of the inner solve of a large bottom, if any
   int nlev() const { return int(P.levels.size()); }
+  int nout() const { return std::min(P.mg_levels, nlev()); }
+  bool inner() const { return !P.disable_mg && nlev() > nout(); }
 
   void init(int prec) {
     precision = prec;
@@ -433,7 +465,10 @@ class Solver {
   void build_operators() {
     if (P.disable_mg) return;
     const int n = nlev();
-    const int first = (n == 1) ? 0 : P.explicit_level;
+    // levels >= explicit_level, or every level when the V-cycle has one level
+    // (its bottom is level 0, factored from the depth-0 stencil as in
+    // Multigrid_Hierarchy.h:215-226); the inner-solve levels are all >= them
+    const int first = (nout() == 1) ? 0 : P.explicit_level;
     for (int lev = first; lev < n; ++lev) {
       Level<double>& d = *L64[lev];
       if (lev > 6) throw CudaError("multigrid depth above 6 is not supported", SGS_ERR_INPUT);
@@ -505,7 +540,9 @@ class Solver {
     const long max_dense = 24576;  // 4.8 GB of FP64
     if (bottom.n > max_dense) {
       char m[160];
-      std::snprintf(m, sizeof m, "bottom level has %ld unknowns; the dense bottom solve supports at most %ld (raise mg_level)",
+      std::snprintf(m, sizeof m,
+                    "the deepest level has %ld unknowns; the dense bottom solve supports at most %ld (the hierarchy "
+                    "cannot be deeper than 7 levels)",
                     bottom.n, max_dense);
       throw CudaError(m, SGS_ERR_INPUT);
     }
@@ -636,6 +673,27 @@ class Solver {
     lift_val.upload(P.lift_val, stream);
     force_node.upload(P.force_node, stream);
     force_val.upload(P.force_val, stream);
+    {
+      // the loads as the solve assembles them: one value per node, the last entry wins
+      std::unordered_map<int32_t, size_t> at;
+      std::vector<int32_t> nodes;
+      std::vector<double> vals;
+      for (size_t k = 0; k < P.force_node.size(); ++k) {
+        auto it = at.find(P.force_node[k]);
+        size_t slot;
+        if (it == at.end()) {
+          slot = nodes.size();
+          at.emplace(P.force_node[k], slot);
+          nodes.push_back(P.force_node[k]);
+          vals.resize(vals.size() + 3);
+        } else {
+          slot = it->second;
+        }
+        for (int v = 0; v < 3; ++v) vals[3 * slot + size_t(v)] = P.force_val[3 * k + size_t(v)];
+      }
+      load_node.upload(nodes, stream);
+      load_val.upload(vals, stream);
+    }
     red.alloc(size_t(std::max<long>(1024, P.levels[0].nb)));  // reduction partials (one per level-0 block at most)
     scal.alloc(16);
     scal.zero(stream);
@@ -696,12 +754,12 @@ class Solver {
 
   // one full smoothing sweep (8 colours) of level l on u given b
   template <typename T>
-  void sweep(int l, T* u, const T* b, bool forward, bool boundary) {
+  void sweep(int l, T* u, const T* b, bool forward, bool boundary, bool matrix_free = true) {
     Level<T>& d = lev<T>(l);
     const int* list = boundary ? d.boundary.p : nullptr;
     const int count = boundary ? d.nbound : d.nb;
     if (count == 0) return;
-    if (l == 0) {
+    if (l == 0 && matrix_free) {
       for (int k = 0; k < 8; ++k) {
         const int c = (boundary ? 8 : 0) + (forward ? k : 7 - k);
         const int lo = d.gs_off[c], cnt = d.gs_off[c + 1] - lo;
@@ -768,7 +826,7 @@ class Solver {
   }
 
   template <typename T>
-  void prolongate_to(int lf, T* fine_u) {
+  void prolongate_to(int lf, T* fine_u, int round = -1) {
     Level<T>& fl = lev<T>(lf);
     Level<T>& c = lev<T>(lf + 1);
     if (fl.N == 0) return;
@@ -779,19 +837,31 @@ class Solver {
       return;
     }
     launch(prolongate_kernel<T>, blocks_for(fl.N, 128), 128, 0, fl.nb, fl.coords.p, fl.flags.p, c.grid, c.u.p, c.N,
-                                                                   fine_u, fl.N, round_ref() ? 1 : 0);
+                                                                   fine_u, fl.N, round < 0 ? (round_ref() ? 1 : 0) : round);
     ++launch_counter;
   }
 
+  // the V-cycle's bottom: the dense inverse, or the inner solve of a large bottom
   template <typename T>
   void bottom_solve(int l) {
+    if (inner() && l == nout() - 1) {
+      inner_solve<T>(l);
+      if (round_ref()) round3(lev<T>(l), lev<T>(l).u.p);
+      return;
+    }
+    bottom_dense<T>(l, round_ref());
+  }
+
+  // u = M^-1 b on the deepest level (nodes without unknowns keep b)
+  template <typename T>
+  void bottom_dense(int l, bool round) {
     Level<T>& d = lev<T>(l);
     // nodes without unknowns keep b (the reference copies b in and out)
     SGS_CUDA(cudaMemcpyAsync(d.u.p, d.b.p, 3 * d.N * sizeof(T), cudaMemcpyDeviceToDevice, stream));
     if (bottom.ndof_nodes > 0) {
       launch(bottom_gather_kernel<T>, blocks_for(bottom.ndof_nodes, 128), 128, 0, bottom.ndof_nodes, bottom.dof_node.p,
                                                                                      d.b.p, d.N, bottom.xb.p);
-      if (bottom.Minv32.p)
+      if (sizeof(T) == 4 && bottom.Minv32.p)  // the FP32 V-cycle applies the FP32 copy
         launch(gemv32_kernel, blocks_for(bottom.ld, GEMV32_ROWS), 1024, size_t(bottom.ld) * sizeof(float),
                bottom.Minv32.p, bottom.ld, bottom.ld, bottom.xb.p, bottom.xs.p);
       else
@@ -802,13 +872,79 @@ class Solver {
                                                                                       d.u.p, d.N);
       launch_counter += 3;
     }
-    if (round_ref()) round3(d, d.u.p);
+    if (round) round3(d, d.u.p);
   }
+
+  // ---- exact solve of a bottom level too large for the dense inverse.  The
+  // reference factors the bottom's Galerkin operator with PARDISO
+  // (Elasticity_Matrix.cpp:169-269); here it is solved in FP64 by CG on the
+  // unknowns of the dense path (nodes with an active spoke), preconditioned by
+  // V-cycles over the levels that follow it (Gauss-Seidel on every level with
+  // the stencil operators, the dense inverse at the deepest), until the
+  // residual's 2-norm is below 1e-13 of the right-hand side's or stops
+  // decreasing.  Nodes without unknowns keep b, as with PARDISO_Solve.
+  struct InnerSolve {
+    DevBuf<double> b, x, r, p, z, q, scal;
+    int last_iterations = 0;
+  } ib;
+
+  void inner_alloc(int l) {
+    const long n3 = 3 * L64[l]->N;
+    for (DevBuf<double>* v : {&ib.b, &ib.x, &ib.r, &ib.p, &ib.z, &ib.q})
+      if (long(v->n) != n3) v->alloc(size_t(n3));
+    if (!ib.scal.p) ib.scal.alloc(16);
+  }
+
+  // V-cycle of the inner solve on levels top..nlev()-1 in FP64, no rounding:
+  // right-hand side in L64[top]->b, result in L64[top]->u
+  void inner_vcycle(int top) {
+    const int n = nlev();
+    Level<double>& t = *L64[top];
+    SGS_CUDA(cudaMemsetAsync(t.u.p, 0, 3 * t.N * sizeof(double), stream));
+    for (int l = top; l < n - 1; ++l) {
+      Level<double>& d = *L64[l];
+      inner_sweeps(l, true);
+      Level<double>& c = *L64[l + 1];
+      SGS_CUDA(cudaMemsetAsync(c.u.p, 0, 3 * c.N * sizeof(double), stream));
+      SGS_CUDA(cudaMemsetAsync(c.b.p, 0, 3 * c.N * sizeof(double), stream));
+      stencil<double, SOP_RES>(l, nullptr, d.nb, d.u.p, nullptr, d.b.p, d.r.p, 0, 0, 0);
+      restrict_to<double>(l + 1, d.r.p);
+    }
+    bottom_dense<double>(n - 1, false);
+    for (int l = n - 2; l >= top; --l) {
+      prolongate_to<double>(l, L64[l]->u.p, 0);
+      inner_sweeps(l, false);
+    }
+  }
+
+  void inner_sweeps(int l, bool forward) {
+    Level<double>& d = *L64[l];
+    for (int t = 0; t < P.boundary_smoothing; ++t) sweep<double>(l, d.u.p, d.b.p, forward, true, false);
+    for (int t = 0; t < std::max(1, P.smoothing); ++t) sweep<double>(l, d.u.p, d.b.p, forward, false, false);
+    for (int t = 0; t < P.boundary_smoothing; ++t) sweep<double>(l, d.u.p, d.b.p, forward, true, false);
+  }
+
+  template <typename T>
+  void inner_solve(int l) {
+    Level<T>& d = lev<T>(l);
+    Level<double>& D = *L64[l];
+    const long N = D.N, n3 = 3 * N;
+    inner_alloc(l);
+    if constexpr (sizeof(T) == 4)
+      launch(convert_kernel<double, float>, blocks_for(n3, 256), 256, 0, ib.b.p, d.b.p, n3);
+    else
+      SGS_CUDA(cudaMemcpyAsync(ib.b.p, d.b.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    inner_pcg(l);
+    launch(inner_select_kernel<T>, blocks_for(N, 256), 256, 0, d.u.p, ib.x.p, ib.b.p, D.spokes.p, N);
+    launch_counter += 2;
+  }
+
+  void inner_pcg(int l);
 
   // V-cycle (Run_VCycle): level-0 right-hand side b0, correction written to u0.
   template <typename T>
   void vcycle(const T* b0, T* u0) {
-    const int n = nlev();
+    const int n = nout();
     const int ex = P.explicit_level;
     const bool rr = round_ref();
     Level<T>& l0 = lev<T>(0);
@@ -1227,6 +1363,76 @@ __global__ void sensitivity_kernel(int nin, const int* __restrict__ in_block, co
   if (threadIdx.x == 0) obj_part[blockIdx.x] = sm[0];
 }
 
+// Gradient of the compliance per input-block cell for the PyTorch layer:
+// grad = factor * (*scale) * p rho^(p-1) (1-Emin) u_e^T K0 u_e (0 for empty cells),
+// u in the level-0 layout [3][N] (a saved solution).
+__global__ void sensitivity_grad_kernel(int nin, const int* __restrict__ in_block, const int* __restrict__ in_zoff,
+                                        const int* __restrict__ nbr, const double* __restrict__ u, long N,
+                                        const double* __restrict__ rho, double penalty, double emin, double factor,
+                                        const double* __restrict__ scale, double* __restrict__ grad) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nin) * 64) return;
+  const int b = int(t >> 6), e = int(t & 63);
+  const int blk = in_block[b];
+  const double r = rho[t];
+  if (blk < 0 || !(r > 0)) {
+    grad[t] = 0;
+    return;
+  }
+  const int x = e >> 4, y = (e >> 2) & 3, z = (e & 3) + in_zoff[b];
+  double ue[8][3];
+  for (int a = 0; a < 8; ++a) {
+    const int nx = x + (a >> 2), ny = y + ((a >> 1) & 1), nz = z + (a & 1);
+    const int d = (nx > 3 ? 2 : 1) * 9 + (ny > 3 ? 2 : 1) * 3 + (nz > 7 ? 2 : 1);
+    const int nb = nbr[long(blk) * 27 + d];
+    for (int v = 0; v < 3; ++v)
+      ue[a][v] = nb < 0 ? 0.0 : u[long(nb) * 128 + ((nx & 3) << 5) + ((ny & 3) << 3) + (nz & 7) + v * N];
+  }
+  double s = 0;
+  for (int a = 0; a < 8; ++a)
+    for (int bb = 0; bb < 8; ++bb) {
+      const int k = (a * 8 + bb) * 9;
+      for (int i = 0; i < 3; ++i)
+        s += ue[a][i] * (c_Kc64[k + i * 3] * ue[bb][0] + c_Kc64[k + i * 3 + 1] * ue[bb][1] + c_Kc64[k + i * 3 + 2] * ue[bb][2]);
+    }
+  grad[t] = factor * (scale ? *scale : 1.0) * s * pow(r, penalty - 1.0) * penalty * (1 - emin);
+}
+
+// f.u over the loaded nodes (one value per node, the last force entry of a node,
+// as the solve assembles them), summed in a fixed order by one CTA.
+__global__ void compliance_kernel(const int* __restrict__ node, const double* __restrict__ val, int n,
+                                  const double* __restrict__ x, long N, double* __restrict__ out) {
+  __shared__ double sm[256];
+  double s = 0;
+  for (int k = threadIdx.x; k < n; k += 256)
+    for (int v = 0; v < 3; ++v) s += val[3 * k + v] * x[node[k] + v * N];
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sm[0];
+}
+
+// New densities on the device: bit 0 of *bad for a non-finite stiffness, bit 1
+// for a cell whose material status (E != 0) would change.
+__global__ void simp_E_check_kernel(int nin, const int* __restrict__ in_block, const int* __restrict__ in_zoff,
+                                    const double* __restrict__ rho, double penalty, double emin, double rho_min,
+                                    double mu0, const double* __restrict__ E, int* bad) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nin) * 64) return;
+  const int b = int(t >> 6), e = int(t & 63);
+  const int blk = in_block[b];
+  if (blk < 0) return;
+  const double d = rho[t];
+  double val = 0;
+  if (d > 0) val = penalty != 0 ? (1 - emin) * pow(fmax(rho_min, d), penalty) + emin : d;
+  const double old = E[long(blk) * 128 + (e >> 4) * 32 + ((e >> 2) & 3) * 8 + (e & 3) + in_zoff[b]];
+  if (!isfinite(val)) atomicOr(bad, 1);
+  if ((val * mu0 != 0) != (old * mu0 != 0)) atomicOr(bad, 2);
+}
+
 void Solver::dot(const double* a, const double* b, double* out_unused) {
   (void)out_unused;
   launch(dot_partial_kernel, RED_BLOCKS, RED_THREADS, 0, a, b, 3 * N0(), red.p);
@@ -1272,6 +1478,62 @@ void Solver::precondition() {
     launch(precond_out_kernel<double>, RED_BLOCKS, RED_THREADS, 0, q.p, q.p, f.p, l0.flags.p, N, red.p);
   }
   ++launch_counter;
+}
+
+// Inner solve of a large bottom level: CG on its unknowns (see InnerSolve).
+void Solver::inner_pcg(int l) {
+  Level<double>& D = *L64[l];
+  const long N = D.N, n3 = 3 * N;
+  const int rb = int(std::min<long>(RED_BLOCKS, std::max<long>(1, (n3 + RED_THREADS - 1) / RED_THREADS)));
+  auto dotp = [&](const double* a, const double* b, int what) {
+    launch(dot_partial_kernel, rb, RED_THREADS, 0, a, b, n3, red.p);
+    launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, rb, 0, ib.scal.p, what);
+    launch_counter += 2;
+  };
+  double init[16] = {0};
+  init[1] = 1e300;  // rho_old: beta = 0 in the first iteration
+  SGS_CUDA(cudaMemcpyAsync(ib.scal.p, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+  ib.x.zero(stream);
+  ib.p.zero(stream);
+  launch(inner_mask_kernel, blocks_for(N, 256), 256, 0, ib.r.p, ib.b.p, D.spokes.p, N);
+  dotp(ib.r.p, ib.r.p, 3);
+  double h[16];
+  SGS_CUDA(cudaMemcpyAsync(h, ib.scal.p, sizeof(h), cudaMemcpyDeviceToHost, stream));
+  SGS_CUDA(cudaStreamSynchronize(stream));
+  const double b2 = h[8];
+  ib.last_iterations = 0;
+  if (!(b2 > 0)) return;  // x = 0
+  const double tol2 = 1e-26 * b2;
+  double best = b2;
+  int since_best = 0;
+  for (int it = 1; it <= 300; ++it) {
+    // z = V(r) on the unknowns
+    SGS_CUDA(cudaMemcpyAsync(D.b.p, ib.r.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    inner_vcycle(l);
+    launch(inner_mask_kernel, blocks_for(N, 256), 256, 0, ib.z.p, D.u.p, D.spokes.p, N);
+    dotp(ib.r.p, ib.z.p, 0);                                     // rho, beta = rho / rho_old
+    launch(axpy_kernel, blocks_for(n3, 256), 256, 0, ib.p.p, ib.scal.p, 4, ib.p.p, ib.z.p, n3, 0);  // p = beta p + z
+    launch(rho_shift_kernel, 1, 1, 0, ib.scal.p);
+    stencil<double, SOP_MUL>(l, nullptr, D.nb, ib.p.p, nullptr, nullptr, ib.q.p, 0, 0, 0);
+    launch(inner_mask_kernel, blocks_for(N, 256), 256, 0, ib.q.p, ib.q.p, D.spokes.p, N);
+    dotp(ib.p.p, ib.q.p, 1);                                     // alpha, breakdown flag
+    launch(axpy_kernel, blocks_for(n3, 256), 256, 0, ib.x.p, ib.scal.p, 5, ib.p.p, ib.x.p, n3, 0);  // x += alpha p
+    launch(axpy_kernel, blocks_for(n3, 256), 256, 0, ib.r.p, ib.scal.p, 6, ib.q.p, ib.r.p, n3, 0);  // r -= alpha q
+    dotp(ib.r.p, ib.r.p, 3);
+    launch_counter += 6;
+    SGS_CUDA(cudaMemcpyAsync(h, ib.scal.p, sizeof(h), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    ib.last_iterations = it;
+    if (h[7] != 0 || !std::isfinite(h[8]))
+      throw CudaError("the bottom level's operator is not positive definite", SGS_ERR_BREAKDOWN);
+    if (h[8] <= tol2) break;
+    if (h[8] < 0.5 * best) {
+      best = h[8];
+      since_best = 0;
+    } else if (++since_best >= 8) {
+      break;  // round-off floor reached
+    }
+  }
 }
 
 // the FP32 copy of the residual for the mixed V-cycle
@@ -1367,9 +1629,11 @@ void Solver::solve() {
   project_null<double>(l0, f.p);
   linf(f.p, nullptr);
   stage_residual();
-  // capture one iteration as a CUDA graph
+  // capture one iteration as a CUDA graph (not with an inner bottom solve,
+  // whose iteration count is decided on the host)
   long capture_launches = 0;
-  if (!iter_graph) {
+  const bool use_graph = !inner();
+  if (use_graph && !iter_graph) {
     cudaGraph_t g;
     long before = launch_counter;
     SGS_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -1400,8 +1664,12 @@ void Solver::solve() {
       final_residual = norm;
       break;
     }
-    SGS_CUDA(cudaGraphLaunch(iter_graph, stream));
-    solve_launches += launches_per_iteration;
+    if (use_graph) {
+      SGS_CUDA(cudaGraphLaunch(iter_graph, stream));
+      solve_launches += launches_per_iteration;
+    } else {
+      record_iteration();
+    }
   }
   launch(add_kernel, blocks_for(n3, 256), 256, 0, x.p, ubk.p, n3);
   ++launch_counter;
@@ -1982,7 +2250,7 @@ static int apply_op(Solver& S, int op, int level, int arg, const double* in, con
       get_field<T>(S, out, d.r.p, N);
       return 0;
     case 6:
-      if (level != n - 1 || S.P.disable_mg) return SGS_ERR_INPUT;
+      if (level != S.nout() - 1 || S.P.disable_mg) return SGS_ERR_INPUT;
       put_field<T>(S, d.b.p, in, N);
       S.bottom_solve<T>(level);
       get_field<T>(S, out, d.u.p, N);
@@ -2356,6 +2624,99 @@ SGS_API int sgs_set_density(sgs_session* h, const double* density) {
     return e.code;
   }
   return 0;
+}
+
+// ---- device-resident calls for the PyTorch layer ---------------------------
+// The session's stream waits for the caller's stream (an event, no host wait)
+// before it reads the caller's buffers; the calls return once the session's
+// stream has finished, so the caller may use the results on any stream.
+static void wait_for_caller(Solver& S, void* caller_stream) {
+  if (!caller_stream) {
+    SGS_CUDA(cudaDeviceSynchronize());
+    return;
+  }
+  cudaEvent_t ev;
+  SGS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  SGS_CUDA(cudaEventRecord(ev, static_cast<cudaStream_t>(caller_stream)));
+  SGS_CUDA(cudaStreamWaitEvent(S.stream, ev, 0));
+  SGS_CUDA(cudaEventDestroy(ev));
+}
+
+static int device_call(sgs_session* h, void* caller_stream, const std::function<void(Solver&)>& body) {
+  if (!h || host_only(h)) return SGS_ERR_INPUT;
+  Solver& S = *h->solver;
+  try {
+    int dev = -1;
+    SGS_CUDA(cudaGetDevice(&dev));
+    if (dev != S.device) {
+      h->error = "a device-resident call needs the session's device to be current";
+      return SGS_ERR_INPUT;
+    }
+    wait_for_caller(S, caller_stream);
+    body(S);
+    SGS_CUDA(cudaGetLastError());
+    SGS_CUDA(cudaStreamSynchronize(S.stream));
+  } catch (const CudaError& e) {
+    h->error = e.what();
+    return e.code;
+  }
+  return 0;
+}
+
+SGS_API int64_t sgs_solution_size(sgs_session* h) { return h && !host_only(h) ? 3 * h->solver->N0() : 0; }
+
+SGS_API int sgs_set_density_device(sgs_session* h, const double* density_dev, void* caller_stream) {
+  if (!density_dev) return SGS_ERR_INPUT;
+  std::string msg;
+  const int rc = device_call(h, caller_stream, [&](Solver& S) {
+    const long nin = long(S.P.in_block.size());
+    if (nin == 0) return;
+    DevBuf<int> bad;
+    bad.alloc(1);
+    bad.zero(S.stream);
+    simp_E_check_kernel<<<blocks_for(nin * 64, 256), 256, 0, S.stream>>>(
+        int(nin), S.in_block.p, S.in_zoff.p, density_dev, S.P.penalty, S.P.minimum_stiffness, S.P.minimum_density,
+        S.P.mu0, S.E64.p, bad.p);
+    SGS_CUDA(cudaGetLastError());
+    int hbad = 0;
+    SGS_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, S.stream));
+    SGS_CUDA(cudaStreamSynchronize(S.stream));
+    if (hbad & 1) msg = "non-finite density";
+    else if (hbad & 2) msg = "the set of material cells changed; create a new session";
+    else S.design_refresh(density_dev);
+  });
+  if (rc) return rc;
+  if (!msg.empty()) {
+    h->error = msg;
+    return SGS_ERR_INPUT;
+  }
+  return 0;
+}
+
+SGS_API int sgs_solution_device(sgs_session* h, double* u_dev, void* caller_stream) {
+  if (!u_dev) return SGS_ERR_INPUT;
+  return device_call(h, caller_stream, [&](Solver& S) {
+    SGS_CUDA(cudaMemcpyAsync(u_dev, S.x.p, 3 * S.N0() * sizeof(double), cudaMemcpyDeviceToDevice, S.stream));
+  });
+}
+
+SGS_API int sgs_compliance_device(sgs_session* h, double* out_dev, void* caller_stream) {
+  if (!out_dev) return SGS_ERR_INPUT;
+  return device_call(h, caller_stream, [&](Solver& S) {
+    compliance_kernel<<<1, 256, 0, S.stream>>>(S.load_node.p, S.load_val.p, int(S.load_node.n), S.x.p, S.N0(), out_dev);
+  });
+}
+
+SGS_API int sgs_sensitivity_device(sgs_session* h, const double* u_dev, const double* density_dev, double factor,
+                                   const double* scale_dev, double* grad_dev, void* caller_stream) {
+  if (!density_dev || !grad_dev) return SGS_ERR_INPUT;
+  return device_call(h, caller_stream, [&](Solver& S) {
+    const long nin = long(S.P.in_block.size());
+    if (nin == 0) return;
+    sensitivity_grad_kernel<<<blocks_for(nin * 64, 256), 256, 0, S.stream>>>(
+        int(nin), S.in_block.p, S.in_zoff.p, S.L64[0]->nbr.p, u_dev ? u_dev : S.x.p, S.N0(), density_dev,
+        S.P.penalty, S.P.minimum_stiffness, factor, scale_dev, grad_dev);
+  });
 }
 
 SGS_API int sgs_level_count(sgs_session* h) { return h ? h->solver->nlev() : 0; }

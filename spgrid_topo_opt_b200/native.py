@@ -28,7 +28,8 @@ EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", 
                     "sgs_band_set_density", "sgs_band_get_density", "sgs_band_set_fat", "sgs_band_update",
                     "sgs_band_maps", "sgs_band_attach", "sgs_band_session", "sgs_band_step", "sgs_render",
                     "sgs_band_render", "sgs_band_get_flags", "sgs_band_filter_voxels", "sgs_band_kill_below",
-                    "sgs_band_threshold_density")
+                    "sgs_band_threshold_density", "sgs_solution_size", "sgs_set_density_device",
+                    "sgs_solution_device", "sgs_compliance_device", "sgs_sensitivity_device")
 
 CELL_INSIDE, CELL_FORCE, CELL_FIXED = 1, 2, 4   # SGS_CELL_* (driver TopOptFlags bits 0-2)
 
@@ -224,6 +225,16 @@ def load(build_if_missing: bool = False):
     L.sgs_render.restype = C.c_int
     L.sgs_band_render.argtypes = [P, C.POINTER(RenderParams), P, P]
     L.sgs_band_render.restype = C.c_int
+    L.sgs_solution_size.argtypes = [P]
+    L.sgs_solution_size.restype = C.c_int64
+    L.sgs_set_density_device.argtypes = [P, P, P]
+    L.sgs_set_density_device.restype = C.c_int
+    L.sgs_solution_device.argtypes = [P, P, P]
+    L.sgs_solution_device.restype = C.c_int
+    L.sgs_compliance_device.argtypes = [P, P, P]
+    L.sgs_compliance_device.restype = C.c_int
+    L.sgs_sensitivity_device.argtypes = [P, P, P, C.c_double, P, P, P]
+    L.sgs_sensitivity_device.restype = C.c_int
     _lib = L
     return L
 
@@ -438,6 +449,34 @@ class Session:
             raise ValueError("density must have one row of 64 values per input block")
         self._check(load().sgs_set_density(self.h, _ptr(rho)))
         self.inputs.density.data = rho.copy()
+
+    # ---- device-resident calls (torch tensors on the session's device)
+    @staticmethod
+    def _stream():
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def set_density_device(self, rho) -> None:
+        """New densities from a contiguous float64 CUDA tensor [nblocks, 64]."""
+        self._check(load().sgs_set_density_device(self.h, C.c_void_p(rho.data_ptr()), self._stream()))
+
+    def solution_size(self) -> int:
+        return int(load().sgs_solution_size(self.h))
+
+    def solution_device(self, out) -> None:
+        """Copy the last solution (level-0 layout) into a float64 CUDA tensor."""
+        self._check(load().sgs_solution_device(self.h, C.c_void_p(out.data_ptr()), self._stream()))
+
+    def compliance_device(self, out) -> None:
+        """out[0] = f.u of the last solve (a float64 CUDA tensor)."""
+        self._check(load().sgs_compliance_device(self.h, C.c_void_p(out.data_ptr()), self._stream()))
+
+    def sensitivity_device(self, u, rho, factor: float, scale, grad) -> None:
+        """grad = factor * scale * p rho^(p-1) (1-Emin) u_e^T K0 u_e on the device;
+        u a saved solution or None for the last solve, scale a one-element tensor or None."""
+        self._check(load().sgs_sensitivity_device(
+            self.h, None if u is None else C.c_void_p(u.data_ptr()), C.c_void_p(rho.data_ptr()), float(factor),
+            None if scale is None else C.c_void_p(scale.data_ptr()), C.c_void_p(grad.data_ptr()), self._stream()))
 
     def time_op(self, op: int, reps: int = 20) -> float:
         """Average device milliseconds of a level-0 operator (0 the FP64 PCG

@@ -20,6 +20,10 @@ CASES = {
     "config0_box32": (lambda: configs.cantilever_box(32, density=0.1, bottom_size=16), 1e-4, 1e-10, False),
     "config0_box64": (lambda: configs.cantilever_box(64, density=0.1, bottom_size=16), 1e-4, 1e-10, False),
     "shell64": (lambda: configs.sphere_shell(64, bottom_size=16), 1e-6, 1e-10, False),
+    # the driver's default mg_bottom_size 64 (spgrid_topo_opt.cpp:1022-1030): one
+    # level, the whole problem is the bottom (factored by PARDISO in the reference)
+    "cantilever16_bottom64": (lambda: configs.cantilever_box(16, density=(0.2, 1.0), bottom_size=64), 1e-10, 1e-10,
+                              True),
 }
 SAMPLES = 4096  # nodes sampled (seeded) from the displacement field where it is not stored whole
 

@@ -76,3 +76,27 @@ def test_set_density_keeps_material_pattern(model):
     with pytest.raises(native.SolverError):
         m.session.set_density(bad)
     m.session.set_density(inp.density.data)
+
+
+def test_forward_and_backward_stay_on_the_device(model):
+    """With the densities on the GPU, neither pass copies a field to the host:
+    the library's device-to-host byte count grows only by the solver's
+    per-iteration convergence scalars, far below one copy of u."""
+    import torch
+
+    inp, m = model
+    rho_host = torch.tensor(inp.density.data, dtype=torch.float64, requires_grad=True)
+    m(rho_host).backward()
+    rho = torch.tensor(inp.density.data, dtype=torch.float64, device="cuda", requires_grad=True)
+    with torch.no_grad():
+        m(rho)
+    before = m.last_stats["d2h_bytes"]
+    c = m(rho)
+    c.backward()
+    with torch.no_grad():
+        m(rho)  # its solve reports the bytes moved since the previous one, backward included
+    moved = m.last_stats["d2h_bytes"] - before
+    field_bytes = 8 * m.session.solution_size()
+    assert moved < field_bytes / 20, (moved, field_bytes)
+    assert rho.grad.is_cuda and rho.grad.shape == rho.shape
+    assert torch.allclose(rho.grad.cpu(), rho_host.grad, rtol=1e-10, atol=0)

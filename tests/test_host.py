@@ -120,3 +120,22 @@ def test_negative_and_nan_density_cells_are_empty(native_lib):
         for lev in range(ref.levels):
             assert np.array_equal(ses.blocks(lev), ref.blocks(lev)), (fill, lev)
             assert np.array_equal(ses.flags(lev), ref.flags(lev)), (fill, lev)
+
+
+def test_levels_below_a_large_bottom_leave_the_v_cycle_levels_unchanged(native_lib):
+    """A bottom above the dense limit gets further levels for its inner solve;
+    the V-cycle's own levels (mg_level of them) stay as the reference builds
+    them."""
+    prob = configs.cantilever_box(16, density=(0.2, 1.0), bottom_size=64)
+    inp = configs.to_inputs(prob)
+    assert inp.mg_level == 1
+    plain = native.Session(inp, precision=native.HOST_SETUP_ONLY)
+    inp.extra_ints["sgs_dense_bottom_max"] = 1000
+    deep = native.Session(inp, precision=native.HOST_SETUP_ONLY)
+    assert plain.levels == 1 and deep.levels > 1
+    assert np.array_equal(plain.blocks(0), deep.blocks(0))
+    assert np.array_equal(plain.flags(0), deep.flags(0))
+    ref = Oracle(configs.to_inputs(configs.cantilever_box(16, density=(0.2, 1.0), bottom_size=4)), mode=MODE_FP64)
+    for lev in range(1, deep.levels):  # the same coarsening rule as the reference's levels
+        assert np.array_equal(deep.blocks(lev), ref.blocks(lev)), lev
+        assert np.array_equal(deep.flags(lev), ref.flags(lev)), lev
