@@ -235,7 +235,11 @@ SGS_API int sgs_boundary_blocks(sgs_session* s, int level, int32_t* ordinals);
  *  2 one smoothing sweep    (arg bit0 forward, bit1 boundary band only)
  *  3 restriction level -> level+1     4 prolongation level+1 -> level (accumulate)
  *  5 stencil multiply       6 bottom solve (the V-cycle's last level, mg_level - 1)
- *  7 one V-cycle on level 0 */
+ *  7 one V-cycle on level 0
+ *  8 level-0 residual b - K u as the V-cycle computes it on its packed (u, E)
+ *    iterate: in FP32 on the tensor cores in mixed sessions (extra_ints
+ *    "sgs_tensor_cores" = 0 selects the CUDA-core kernel), FP64 otherwise;
+ *    sessions whose V-cycle has more than one level */
 SGS_API int sgs_apply(sgs_session* s, int op, int level, int arg, const double* in, const double* in2, double* out);
 
 /* Galerkin stencils of a level as [nblocks*128][243] (row node, comp v; column

@@ -27,6 +27,7 @@
 #include "kernels.cuh"
 #include "setup.hpp"
 #include "setup_kernels.cuh"
+#include "tc_kernels.cuh"
 #include "topo_kernels.cuh"
 #include "wire.hpp"
 
@@ -118,6 +119,14 @@ __global__ void inner_select_kernel(T* __restrict__ out, const double* __restric
   for (int v = 0; v < 3; ++v) out[i + v * N] = T(on ? x[i + v * N] : b[i + v * N]);
 }
 
+// The packed level-0 iterate from planar fields: (u_x, u_y, u_z, E) per node slot.
+template <typename T>
+__global__ void pack_u4_kernel(typename Pack4<T>::type* __restrict__ u4, const T* __restrict__ u, const T* __restrict__ E,
+                               long N) {
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < N) u4[i] = Pack4<T>::make(u[i], u[i + N], u[i + 2 * N], E[i]);
+}
+
 // Scratch of the allocation-free sensitivity entry point (sgs_sensitivity_static):
 // per-CTA partial sums of the objective in a static device array that every GPU
 // loading the library holds until the process exits.
@@ -132,6 +141,10 @@ class Solver {
   int precision = PREC_REFERENCE;
   int device = -1;                    // CUDA device of the session (current at set-up)
   double* static_partials = nullptr;  // device address of g_sensitivity_partials on that device
+  // the FP32 level-0 residual of the mixed V-cycle on the tensor cores (level0_tc_kernel)
+  bool tensor_cores = true;
+  int tc_grid = 0;
+  DevBuf<int> tc_err;  // set by a tensor-core kernel whose wait gave up
   cudaStream_t stream = nullptr;
   // level data (double for reference/fp64, float for the mixed V-cycle)
   std::vector<std::unique_ptr<Level<double>>> L64;
@@ -217,6 +230,15 @@ class Solver {
     // take caller-owned device buffers check that it is current again
     SGS_CUDA(cudaGetDevice(&device));
     SGS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    {
+      int sms = 0;
+      SGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+      tc_grid = 3 * sms;  // three 63 KB CTAs per SM
+      SGS_CUDA(cudaFuncSetAttribute(level0_tc_kernel<OP_RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+      SGS_CUDA(cudaFuncSetAttribute(level0_tc_kernel<OP_KU>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+      tc_err.alloc(1);
+      tc_err.zero(stream);
+    }
     // the host-side name of a __device__ array is not its device address:
     // resolve it here, once per session, with the session's device current
     {
@@ -941,6 +963,34 @@ class Solver {
 
   void inner_pcg(int l);
 
+  // a tensor-core kernel whose MMA wait gave up reports it here (after a sync)
+  void check_tensor_core_waits() {
+    int bad = 0;
+    SGS_CUDA(cudaMemcpyAsync(&bad, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    if (bad) throw CudaError("a tensor-core MMA wait timed out", SGS_ERR_CUDA);
+  }
+
+  // K u (OP_KU) or b - K u (OP_RES) on the packed level-0 iterate: the tensor-core
+  // kernel in single precision, the shared-memory CUDA-core kernel otherwise
+  template <typename T, int OP>
+  void level0_packed(const T* b, T* out) {
+    Level<T>& d = lev<T>(0);
+    if (d.nb <= 0) return;
+    if constexpr (sizeof(T) == 4) {
+      if (tensor_cores) {
+        launch(level0_tc_kernel<OP>, std::min(d.nb, tc_grid), TC_THREADS, size_t(TC_SMEM_BYTES), d.nb, d.nbrz.p,
+               reinterpret_cast<const float4*>(d.u4.p), b, out, d.N, float(P.dx), float(P.mu0 / 72.0),
+               float(P.lambda0 / 72.0), tc_err.p);
+        ++launch_counter;
+        return;
+      }
+    }
+    if (OP != OP_RES) throw CudaError("K u on the packed iterate runs on the tensor-core kernel only", SGS_ERR_INPUT);
+    launch(level0_res4_kernel<T>, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, b, out, d.N, T(P.dx));
+    ++launch_counter;
+  }
+
   // V-cycle (Run_VCycle): level-0 right-hand side b0, correction written to u0.
   template <typename T>
   void vcycle(const T* b0, T* u0) {
@@ -975,8 +1025,7 @@ class Solver {
       if (smooth) {
         if (l == 0) {
           if (packed) {
-            launch(level0_res4_kernel<T>, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, B(0), d.r.p, d.N, T(P.dx));
-            ++launch_counter;
+            level0_packed<T, OP_RES>(B(0), d.r.p);
           } else {
             level0<T, OP_RES>(U(0), B(0), d.r.p);
           }
@@ -1677,6 +1726,7 @@ void Solver::solve() {
   SGS_CUDA(cudaGetLastError());
   SGS_CUDA(cudaStreamSynchronize(stream));
   solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  check_tensor_core_waits();
   float ms = 0;
   SGS_CUDA(cudaEventElapsedTime(&ms, ev_start, ev_end));
   solve_device_seconds = ms * 1e-3;
@@ -2173,6 +2223,7 @@ static int session_from_inputs(const FEMInputs& in, int precision, sgs_session**
   }
   h->solver->P.max_iterations = 500;  // the reference hard-codes 500 (SPGrid_CPU_Solver.cpp:326)
   if (in.get_int("sgs_honor_max_iterations", 0)) h->solver->P.max_iterations = in.krylov.max_iterations;
+  h->solver->tensor_cores = in.get_int("sgs_tensor_cores", 1) != 0;
   if (precision == SGS_HOST_SETUP_ONLY) {  // inspection of the host-side hierarchy, no device work
     h->solver->precision = precision;
     *out = h.release();
@@ -2255,6 +2306,15 @@ static int apply_op(Solver& S, int op, int level, int arg, const double* in, con
       S.bottom_solve<T>(level);
       get_field<T>(S, out, d.u.p, N);
       return 0;
+    case 8:  // the V-cycle's level-0 residual on the packed iterate (tensor cores in mixed sessions)
+      if (level != 0 || !S.packed0()) return SGS_ERR_INPUT;
+      put_field<T>(S, d.u.p, in, N);
+      put_field<T>(S, d.b.p, in2, N);
+      S.launch(pack_u4_kernel<T>, blocks_for(N, 256), 256, 0, d.u4.p, d.u.p, S.Edev<T>(), N);
+      S.level0_packed<T, OP_RES>(d.b.p, d.r.p);
+      S.check_tensor_core_waits();
+      get_field<T>(S, out, d.r.p, N);
+      return 0;
     case 7: {
       if (level != 0) return SGS_ERR_INPUT;
       std::vector<double> tmp(in, in + 3 * N);
@@ -2282,7 +2342,7 @@ static double time_op(Solver& S, int op, int reps) {
       S.level0<double, OP_KUP>(S.s.p, nullptr, S.q.p);  // the PCG matvec, FP64 in every mode
     } else if (op == 1) {
       if (packed) {
-        S.launch(level0_res4_kernel<T>, d.nb, 128, 0, d.nb, d.nbrz.p, d.u4.p, d.b.p, d.r.p, d.N, T(S.P.dx));
+        S.level0_packed<T, OP_RES>(d.b.p, d.r.p);
         return;
       }
       S.level0<T, OP_RES>(d.u.p, d.b.p, d.r.p);
@@ -2290,8 +2350,9 @@ static double time_op(Solver& S, int op, int reps) {
       S.sweep<T>(0, packed ? nullptr : d.u.p, d.b.p, true, false);
     } else if (op == 3) {
       S.precondition();
-    } else if (op == 4) {
-      S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);  // K u in the V-cycle's precision
+    } else if (op == 4) {  // K u in the V-cycle's precision, on the tensor cores where the V-cycle uses them
+      if (packed && sizeof(T) == 4 && S.tensor_cores) S.level0_packed<T, OP_KU>(nullptr, d.r.p);
+      else S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);
     }
   };
   run();
@@ -2299,6 +2360,7 @@ static double time_op(Solver& S, int op, int reps) {
   for (int i = 0; i < reps; ++i) run();
   SGS_CUDA(cudaEventRecord(b, S.stream));
   SGS_CUDA(cudaEventSynchronize(b));
+  S.check_tensor_core_waits();
   float ms = 0;
   SGS_CUDA(cudaEventElapsedTime(&ms, a, b));
   cudaEventDestroy(a);

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libspgrid_gpu_solver.so")
 
 PRECISION_REFERENCE, PRECISION_FP64, PRECISION_MIXED, HOST_SETUP_ONLY = 0, 1, 2, 3
-OP_KU, OP_RESIDUAL, OP_SMOOTH, OP_RESTRICT, OP_PROLONG, OP_STENCIL, OP_BOTTOM, OP_VCYCLE = range(8)
+OP_KU, OP_RESIDUAL, OP_SMOOTH, OP_RESTRICT, OP_PROLONG, OP_STENCIL, OP_BOTTOM, OP_VCYCLE, OP_PACKED_RESIDUAL = range(9)
 
 EXPORTED_SYMBOLS = ("fem_solve", "fem_solve_free", "sgs_create", "sgs_destroy", "sgs_last_error", "sgs_solve",
                     "sgs_residual_history", "sgs_displacements", "sgs_sensitivity", "sgs_level_count",

@@ -58,6 +58,22 @@ def test_level0_matvec_and_residual(small):
     assert _rel(ses.apply(native.OP_RESIDUAL, 0, u, b), ref.apply(orc.OP_RESIDUAL, 0, u, b)) < 1e-11
 
 
+@pytest.mark.parametrize("tensor_cores", [1, 0])
+def test_packed_fp32_residual_matches_fp64_oracle(small, tensor_cores):
+    """The mixed V-cycle's level-0 residual in FP32: on the tensor cores (TF32
+    split into high and low parts, FP32 accumulation) and on the CUDA cores,
+    both within FP32 rounding (1e-5 of the field's magnitude) of the FP64
+    oracle, and within 1e-5 of each other."""
+    inp, ref, _ = small
+    i2 = fi.deserialize_inputs(fi.serialize_inputs(inp))
+    i2.extra_ints["sgs_tensor_cores"] = tensor_cores
+    with native.Session(i2, precision=native.PRECISION_MIXED) as s:
+        u, b = _field(s, 0, 21), _field(s, 0, 22)
+        got = s.apply(native.OP_PACKED_RESIDUAL, 0, u, b)
+    want = ref.apply(orc.OP_RESIDUAL, 0, u, b)
+    assert _rel(got, want) < 1e-5
+
+
 @pytest.mark.parametrize("arg", [0, 1, 2, 3])
 def test_level0_smoother(small, arg):
     _, ref, ses = small

@@ -11,7 +11,8 @@ drop-in fem_solve:
   iteration count, displacements to 1e-6 relative (L-inf, over the stored
   nodes, scaled by the field's largest displacement);
 * FP64 mode against the FP64 build: the same iteration count, the residual
-  history to 1e-8 and the displacements to 1e-9;
+  history to 1e-8 (1e-11 of the initial residual for entries at round-off) and
+  the displacements to 1e-9;
 * mixed precision (FP32 V-cycle) against the FP64 build: displacements to
   1e-8 when both solve to 1e-10, and to 1e-5 at the benchmark's 1e-6.
 """
@@ -53,7 +54,9 @@ def test_fp64_matches_fp64_reference(native_lib, name):
     out = solve(name, CASES[name][2], native.PRECISION_FP64)
     assert out.extra_ints["iterations"] == int(REF[key + "/iterations"])
     h, hr = np.asarray(out.residuals), REF[key + "/history"]
-    assert len(h) == len(hr) and np.max(np.abs(h - hr) / hr) < 1e-8
+    # entries at round-off (an exact bottom solve converges in one step) are held
+    # to 1e-11 of the initial residual instead
+    assert len(h) == len(hr) and np.all(np.abs(h - hr) <= 1e-8 * hr + 1e-11 * hr[0])
     assert rel_u(out.displacements.data, key) < 1e-9
 
 
