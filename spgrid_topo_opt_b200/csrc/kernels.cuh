@@ -764,46 +764,95 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__
 // Transfers (solver/MG/Restriction.h:52-88, solver/MG/Prolongation.h:151-193)
 // ---------------------------------------------------------------------------
 // coarse(c) = sum_{d in {-1,0,1}^3} w(d) fine(2c - (4,4,8) + d), w = prod (1/2,1,1/2);
-// Dirichlet components zeroed afterwards.
+// Dirichlet components zeroed afterwards.  One CTA per coarse block (launched
+// with nb CTAs of 128 threads, thread = node): the 9x9x17 fine nodes the block
+// reads are staged in shared memory once (the 27 fine blocks they lie in are
+// looked up once), then every node sums its 27 in the reference's order; a
+// missing fine node reads 0, which adds nothing.
 template <typename T>
-__global__ void restrict_kernel(int nb, const int* __restrict__ coords, const uint32_t* __restrict__ cflags,
-                                GridView fine, const T* __restrict__ fin, long Nf, T* __restrict__ cout, long Nc) {
+__global__ void __launch_bounds__(128) restrict_kernel(int nb, const int* __restrict__ coords,
+                                                       const uint32_t* __restrict__ cflags, GridView fine,
+                                                       const T* __restrict__ fin, long Nf, T* __restrict__ cout,
+                                                       long Nc) {
+  constexpr int RX = 9, RY = 9, RZ = 17, RN = RX * RY * RZ;
+  __shared__ T sf[3][RN];
+  __shared__ int sblk[27];
+  const int bi = blockIdx.x, e = threadIdx.x;
+  if (bi >= nb) return;
+  const int CX = coords[3 * bi], CY = coords[3 * bi + 1], CZ = coords[3 * bi + 2];
+  const int x0 = 2 * CX - 5, y0 = 2 * CY - 5, z0 = 2 * CZ - 9;  // fine region origin
+  const int bx0 = x0 >> 2, by0 = y0 >> 2, bz0 = z0 >> 3;
+  if (e < 27) {  // block indices are fixed during a solve: looked up before the wait
+    const int bx = bx0 + e / 9, by = by0 + (e / 3) % 3, bz = bz0 + e % 3;
+    const long n = fine.node(bx * 4, by * 4, bz * 8);
+    sblk[e] = n < 0 ? -1 : int(n >> 7);
+  }
   pdl_wait();
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= long(nb) * 128) return;
-  const int bi = int(t >> 7), e = int(t & 127);
-  const int x = coords[3 * bi] + (e >> 5), y = coords[3 * bi + 1] + ((e >> 3) & 3), z = coords[3 * bi + 2] + (e & 7);
-  const int fx = 2 * x - 4, fy = 2 * y - 4, fz = 2 * z - 8;
+  __syncthreads();
+  for (int h = e; h < RN; h += 128) {
+    const int fx = x0 + h / (RY * RZ), fy = y0 + (h / RZ) % RY, fz = z0 + h % RZ;
+    const int b = sblk[((fx >> 2) - bx0) * 9 + ((fy >> 2) - by0) * 3 + ((fz >> 3) - bz0)];
+    T a = 0, c = 0, d = 0;
+    if (b >= 0) {
+      const long n = long(b) * 128 + ((fx & 3) << 5) + ((fy & 3) << 3) + (fz & 7);
+      a = fin[n];
+      c = fin[n + Nf];
+      d = fin[n + 2 * Nf];
+    }
+    sf[0][h] = a;
+    sf[1][h] = c;
+    sf[2][h] = d;
+  }
+  __syncthreads();
+  const int lx = e >> 5, ly = (e >> 3) & 3, lz = e & 7;
   T v0 = 0, v1 = 0, v2 = 0;
   for (int q = 0; q < 27; ++q) {
     const int i = q / 9, j = (q / 3) % 3, k = q % 3;
-    const long n = fine.node(fx + i - 1, fy + j - 1, fz + k - 1);
-    if (n < 0) continue;
+    const int h = (2 * lx + i) * (RY * RZ) + (2 * ly + j) * RZ + (2 * lz + k);
     const T w = T((i == 1 ? 1.0 : 0.5) * (j == 1 ? 1.0 : 0.5) * (k == 1 ? 1.0 : 0.5));
-    v0 += w * fin[n];
-    v1 += w * fin[n + Nf];
-    v2 += w * fin[n + 2 * Nf];
+    v0 += w * sf[0][h];
+    v1 += w * sf[1][h];
+    v2 += w * sf[2][h];
   }
+  const long t = long(bi) * 128 + e;
   const uint32_t fl = cflags[t];
   cout[t] = (fl & DIR_X) ? T(0) : v0;
   cout[t + Nc] = (fl & DIR_Y) ? T(0) : v1;
   cout[t + 2 * Nc] = (fl & DIR_Z) ? T(0) : v2;
 }
 
+// The 3x3x5 coarse nodes that the 4x4x8 fine nodes of a fine block interpolate
+// from ((f + (4,4,8)) >> 1 + {0,1}^3), staged in shared memory by one CTA per
+// fine block (128 threads, thread = node); missing coarse nodes read 0.
+template <typename T>
+__device__ __forceinline__ void stage_coarse_patch(T (*sc)[45], int FX, int FY, int FZ, GridView coarse,
+                                                   const T* __restrict__ cin, long Nc) {
+  const int e = threadIdx.x;
+  if (e < 45) {
+    const long n = coarse.node(FX / 2 + 2 + e / 15, FY / 2 + 2 + (e / 5) % 3, FZ / 2 + 4 + e % 5);
+    sc[0][e] = n < 0 ? T(0) : cin[n];
+    sc[1][e] = n < 0 ? T(0) : cin[n + Nc];
+    sc[2][e] = n < 0 ? T(0) : cin[n + 2 * Nc];
+  }
+  __syncthreads();
+}
+
 // fine(f) += sum of trilinear weights * coarse(((f + (4,4,8)) >> 1) + {0,1}^3); then
 // Project (Dirichlet), optional float rounding, Project_Null_Space (inactive nodes),
 // as Run_VCycle does after Prolongate (solver/MG/Multigrid_Hierarchy.h:600-603).
 template <typename T>
-__global__ void prolongate_kernel(int nb, const int* __restrict__ coords, const uint32_t* __restrict__ fflags,
-                                  GridView coarse, const T* __restrict__ cin, long Nc, T* __restrict__ fu, long Nf,
-                                  int round_out) {
+__global__ void __launch_bounds__(128) prolongate_kernel(int nb, const int* __restrict__ coords,
+                                                         const uint32_t* __restrict__ fflags, GridView coarse,
+                                                         const T* __restrict__ cin, long Nc, T* __restrict__ fu,
+                                                         long Nf, int round_out) {
+  __shared__ T sc[3][45];
+  const int bi = blockIdx.x, e = threadIdx.x;
+  if (bi >= nb) return;
+  const int FX = coords[3 * bi], FY = coords[3 * bi + 1], FZ = coords[3 * bi + 2];
   pdl_wait();
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= long(nb) * 128) return;
-  const int bi = int(t >> 7), e = int(t & 127);
+  stage_coarse_patch<T>(sc, FX, FY, FZ, coarse, cin, Nc);
   const int lx = e >> 5, ly = (e >> 3) & 3, lz = e & 7;
-  const int x = coords[3 * bi] + lx, y = coords[3 * bi + 1] + ly, z = coords[3 * bi + 2] + lz;
-  const int cx = (x + 4) >> 1, cy = (y + 4) >> 1, cz = (z + 8) >> 1;
+  const long t = long(bi) * 128 + e;
   T v0 = fu[t], v1 = fu[t + Nf], v2 = fu[t + 2 * Nf];
   for (int q = 0; q < 8; ++q) {
     const int ii = q >> 2, jj = (q >> 1) & 1, kk = q & 1;
@@ -812,11 +861,10 @@ __global__ void prolongate_kernel(int nb, const int* __restrict__ coords, const 
     const double wz = (lz & 1) ? 0.5 : (kk ? 0.0 : 1.0);
     const T w = T(wx * wy * wz);
     if (!(w > T(0))) continue;
-    const long n = coarse.node(cx + ii, cy + jj, cz + kk);
-    if (n < 0) continue;
-    v0 += w * cin[n];
-    v1 += w * cin[n + Nc];
-    v2 += w * cin[n + 2 * Nc];
+    const int h = ((lx >> 1) + ii) * 15 + ((ly >> 1) + jj) * 5 + (lz >> 1) + kk;
+    v0 += w * sc[0][h];
+    v1 += w * sc[1][h];
+    v2 += w * sc[2][h];
   }
   const uint32_t fl = fflags[t];
   if (fl & DIR_X) v0 = 0;
@@ -831,16 +879,18 @@ __global__ void prolongate_kernel(int nb, const int* __restrict__ coords, const 
 
 // prolongate_kernel into the packed level-0 iterate (E in .w is kept)
 template <typename T>
-__global__ void prolongate4_kernel(int nb, const int* __restrict__ coords, const uint32_t* __restrict__ fflags,
-                                   GridView coarse, const T* __restrict__ cin, long Nc,
-                                   typename Pack4<T>::type* __restrict__ fu4) {
+__global__ void __launch_bounds__(128) prolongate4_kernel(int nb, const int* __restrict__ coords,
+                                                          const uint32_t* __restrict__ fflags, GridView coarse,
+                                                          const T* __restrict__ cin, long Nc,
+                                                          typename Pack4<T>::type* __restrict__ fu4) {
+  __shared__ T sc[3][45];
+  const int bi = blockIdx.x, e = threadIdx.x;
+  if (bi >= nb) return;
+  const int FX = coords[3 * bi], FY = coords[3 * bi + 1], FZ = coords[3 * bi + 2];
   pdl_wait();
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= long(nb) * 128) return;
-  const int bi = int(t >> 7), e = int(t & 127);
+  stage_coarse_patch<T>(sc, FX, FY, FZ, coarse, cin, Nc);
   const int lx = e >> 5, ly = (e >> 3) & 3, lz = e & 7;
-  const int x = coords[3 * bi] + lx, y = coords[3 * bi + 1] + ly, z = coords[3 * bi + 2] + lz;
-  const int cx = (x + 4) >> 1, cy = (y + 4) >> 1, cz = (z + 8) >> 1;
+  const long t = long(bi) * 128 + e;
   auto v = fu4[t];
   for (int q = 0; q < 8; ++q) {
     const int ii = q >> 2, jj = (q >> 1) & 1, kk = q & 1;
@@ -849,11 +899,10 @@ __global__ void prolongate4_kernel(int nb, const int* __restrict__ coords, const
     const double wz = (lz & 1) ? 0.5 : (kk ? 0.0 : 1.0);
     const T w = T(wx * wy * wz);
     if (!(w > T(0))) continue;
-    const long n = coarse.node(cx + ii, cy + jj, cz + kk);
-    if (n < 0) continue;
-    v.x += w * cin[n];
-    v.y += w * cin[n + Nc];
-    v.z += w * cin[n + 2 * Nc];
+    const int h = ((lx >> 1) + ii) * 15 + ((ly >> 1) + jj) * 5 + (lz >> 1) + kk;
+    v.x += w * sc[0][h];
+    v.y += w * sc[1][h];
+    v.z += w * sc[2][h];
   }
   const uint32_t fl = fflags[t];
   if (fl & DIR_X) v.x = 0;

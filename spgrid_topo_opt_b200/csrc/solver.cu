@@ -233,7 +233,7 @@ class Solver {
     {
       int sms = 0;
       SGS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-      tc_grid = 3 * sms;  // three 63 KB CTAs per SM
+      tc_grid = 5 * sms;  // five 44 KB CTAs per SM
       SGS_CUDA(cudaFuncSetAttribute(level0_tc_kernel<OP_RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
       SGS_CUDA(cudaFuncSetAttribute(level0_tc_kernel<OP_KU>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
       tc_err.alloc(1);
@@ -716,7 +716,7 @@ class Solver {
       load_node.upload(nodes, stream);
       load_val.upload(vals, stream);
     }
-    red.alloc(size_t(std::max<long>(1024, P.levels[0].nb)));  // reduction partials (one per level-0 block at most)
+    red.alloc(size_t(std::max<long>(2048, P.levels[0].nb)));  // reduction partials (one per level-0 block at most)
     scal.alloc(16);
     scal.zero(stream);
     in_block.upload(P.in_block, stream);
@@ -1049,7 +1049,7 @@ class Solver {
   void dot(const double* a, const double* b, double* out);
   void linf(const double* a, double* out);
   void axpy(double* dst, double sign, int coef_slot, const double* xv, const double* yv);
-  void precondition();
+  int precondition();  // returns the number of rho partials it wrote
   void stage_residual();
   void record_iteration();
   void solve();
@@ -1130,6 +1130,8 @@ const float* Solver::Edev<float>() { return E32.p; }
 // CG vector kernels
 // ---------------------------------------------------------------------------
 constexpr int RED_BLOCKS = 592, RED_THREADS = 256;  // 4 CTAs per SM on 148 SMs
+// the PCG's streaming kernels over node pairs (16-byte loads): 8 CTAs per SM
+constexpr int PAIR_BLOCKS = 1184;
 
 __global__ void dot_partial_kernel(const double* __restrict__ a, const double* __restrict__ b, long n,
                                    double* __restrict__ part) {
@@ -1294,6 +1296,115 @@ __global__ void cg_update_kernel(double* x, const double* __restrict__ s, double
     double t = 0;
     for (int w = 0; w < RED_THREADS / 32; ++w) t = fmax(t, sm[w]);
     part[blockIdx.x] = t;
+  }
+}
+
+// precond_out4_kernel over node pairs: two nodes per thread with 16-byte loads and
+// stores (N is a multiple of 128), the same arithmetic per node.
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS, 4) precond_out4_pair_kernel(const typename Pack4<T>::type* __restrict__ z4,
+                                                                       double* __restrict__ q,
+                                                                       const double* __restrict__ f,
+                                                                       const uint32_t* __restrict__ flags, long N,
+                                                                       double* __restrict__ part) {
+  pdl_wait();
+  __shared__ double sm[RED_THREADS / 32];
+  double s = 0;
+  const long P = N >> 1;
+  for (long p = long(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += long(gridDim.x) * blockDim.x) {
+    const uint2 fl = reinterpret_cast<const uint2*>(flags)[p];
+    const auto za = z4[2 * p], zb = z4[2 * p + 1];
+    const double zc[2][3] = {{double(za.x), double(za.y), double(za.z)}, {double(zb.x), double(zb.y), double(zb.z)}};
+    const uint32_t fls[2] = {fl.x, fl.y};
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      double2 out;
+      const double2 fv = reinterpret_cast<const double2*>(f + v * N)[p];
+      out.x = ((fls[0] & ACTIVE_NODE) && !(fls[0] & (DIR_X << v))) ? zc[0][v] : 0.0;
+      out.y = ((fls[1] & ACTIVE_NODE) && !(fls[1] & (DIR_X << v))) ? zc[1][v] : 0.0;
+      reinterpret_cast<double2*>(q + v * N)[p] = out;
+      s += out.x * fv.x;
+      s += out.y * fv.y;
+    }
+  }
+  for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t += sm[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+// cg_update_kernel over node pairs (16-byte loads and stores), the same arithmetic per node.
+__global__ void __launch_bounds__(RED_THREADS, 4) cg_update_pair_kernel(double* __restrict__ x, const double* __restrict__ s,
+                                                                    double* __restrict__ f, const double* __restrict__ q,
+                                                                    const double* __restrict__ scal,
+                                                                    const uint32_t* __restrict__ flags, long N,
+                                                                    int float_round, float* __restrict__ b32,
+                                                                    double* __restrict__ part) {
+  pdl_wait();
+  __shared__ double sm[RED_THREADS / 32];
+  const double a = scal[5], na = scal[6];
+  double m = 0;
+  const long P = N >> 1;
+  for (long p = long(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += long(gridDim.x) * blockDim.x) {
+    const uint2 fl = reinterpret_cast<const uint2*>(flags)[p];
+    const bool act[2] = {(fl.x & ACTIVE_NODE) != 0, (fl.y & ACTIVE_NODE) != 0};
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const long o = v * (N >> 1) + p;
+      const double2 xv = reinterpret_cast<const double2*>(x)[o], sv = reinterpret_cast<const double2*>(s)[o];
+      const double2 fv = reinterpret_cast<const double2*>(f)[o], qv = reinterpret_cast<const double2*>(q)[o];
+      double2 xo, fo;
+      if (float_round) {
+        xo.x = double(__fadd_rn(__fmul_rn(float(a), float(sv.x)), float(xv.x)));
+        xo.y = double(__fadd_rn(__fmul_rn(float(a), float(sv.y)), float(xv.y)));
+        fo.x = double(__fadd_rn(__fmul_rn(float(na), float(qv.x)), float(fv.x)));
+        fo.y = double(__fadd_rn(__fmul_rn(float(na), float(qv.y)), float(fv.y)));
+      } else {
+        xo.x = a * sv.x + xv.x;
+        xo.y = a * sv.y + xv.y;
+        fo.x = na * qv.x + fv.x;
+        fo.y = na * qv.y + fv.y;
+      }
+      if (!act[0]) fo.x = 0;
+      if (!act[1]) fo.y = 0;
+      reinterpret_cast<double2*>(x)[o] = xo;
+      reinterpret_cast<double2*>(f)[o] = fo;
+      if (b32) reinterpret_cast<float2*>(b32)[o] = make_float2(float(fo.x), float(fo.y));
+      m = fmax(m, fmax(fabs(fo.x), fabs(fo.y)));
+    }
+  }
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) t = fmax(t, sm[w]);
+    part[blockIdx.x] = t;
+  }
+}
+
+// axpy_kernel over pairs (n even), grid-stride
+__global__ void __launch_bounds__(RED_THREADS, 4) axpy_pair_kernel(double* dst, const double* __restrict__ scal, int slot,
+                                                               const double* xv, const double* yv, long n,
+                                                               int float_round) {
+  pdl_wait();
+  const double c = scal[slot];
+  const long P = n >> 1;
+  for (long p = long(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += long(gridDim.x) * blockDim.x) {
+    const double2 a = reinterpret_cast<const double2*>(xv)[p], b = reinterpret_cast<const double2*>(yv)[p];
+    double2 o;
+    if (float_round) {
+      o.x = double(__fadd_rn(__fmul_rn(float(c), float(a.x)), float(b.x)));
+      o.y = double(__fadd_rn(__fmul_rn(float(c), float(a.y)), float(b.y)));
+    } else {
+      o.x = c * a.x + b.x;
+      o.y = c * a.y + b.y;
+    }
+    reinterpret_cast<double2*>(dst)[p] = o;
   }
 }
 
@@ -1504,9 +1615,10 @@ void Solver::axpy(double* dst, double, int slot, const double* xv, const double*
 // partial sums of rho = q.r.  In mixed precision the V-cycle starts from the
 // FP32 copy of r in level 0's b, written by stage_residual() or by the previous
 // iteration's update.
-void Solver::precondition() {
+int Solver::precondition() {
   Level<double>& l0 = *L64[0];
   const long N = l0.N;
+  int parts = RED_BLOCKS;
   if (P.disable_mg) {
     SGS_CUDA(cudaMemcpyAsync(q.p, f.p, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     launch(precond_out_kernel<double>, RED_BLOCKS, RED_THREADS, 0, q.p, q.p, f.p, l0.flags.p, N, red.p);
@@ -1514,19 +1626,22 @@ void Solver::precondition() {
     Level<float>& m0 = *L32[0];
     if (packed0()) {
       vcycle<float>(m0.b.p, nullptr);
-      launch(precond_out4_kernel<float>, RED_BLOCKS, RED_THREADS, 0, m0.u4.p, q.p, f.p, l0.flags.p, N, red.p);
+      launch(precond_out4_pair_kernel<float>, PAIR_BLOCKS, RED_THREADS, 0, m0.u4.p, q.p, f.p, l0.flags.p, N, red.p);
+      parts = PAIR_BLOCKS;
     } else {
       vcycle<float>(m0.b.p, m0.u.p);
       launch(precond_out_kernel<float>, RED_BLOCKS, RED_THREADS, 0, m0.u.p, q.p, f.p, l0.flags.p, N, red.p);
     }
   } else if (packed0()) {
     vcycle<double>(f.p, nullptr);
-    launch(precond_out4_kernel<double>, RED_BLOCKS, RED_THREADS, 0, l0.u4.p, q.p, f.p, l0.flags.p, N, red.p);
+    launch(precond_out4_pair_kernel<double>, PAIR_BLOCKS, RED_THREADS, 0, l0.u4.p, q.p, f.p, l0.flags.p, N, red.p);
+    parts = PAIR_BLOCKS;
   } else {
     vcycle<double>(f.p, q.p);
     launch(precond_out_kernel<double>, RED_BLOCKS, RED_THREADS, 0, q.p, q.p, f.p, l0.flags.p, N, red.p);
   }
   ++launch_counter;
+  return parts;
 }
 
 // Inner solve of a large bottom level: CG on its unknowns (see InnerSolve).
@@ -1597,14 +1712,15 @@ void Solver::stage_residual() {
 // the next iteration's Project_Nullspace and norm (:32-33).
 void Solver::record_iteration() {
   Level<double>& l0 = *L64[0];
-  precondition();                                                        // q = z, rho partials
-  launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, RED_BLOCKS, 0, scal.p, 0);  // rho, beta
-  axpy(s.p, 1, 4, s.p, q.p);                                             // s = beta*s + z
+  const int parts = precondition();                                      // q = z, rho partials
+  launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, parts, 0, scal.p, 0);  // rho, beta
+  launch(axpy_pair_kernel, PAIR_BLOCKS, RED_THREADS, 0, s.p, scal.p, 4, s.p, q.p, 3 * N0(),
+         round_ref() ? 1 : 0);                                           // s = beta*s + z
   level0<double, OP_KUP>(s.p, nullptr, q.p);                             // q = K s, Project, s.q partials
   launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, l0.nb, 0, scal.p, 1);       // alpha
-  launch(cg_update_kernel, RED_BLOCKS, RED_THREADS, 0, x.p, s.p, f.p, q.p, scal.p, l0.flags.p, l0.N,
+  launch(cg_update_pair_kernel, PAIR_BLOCKS, RED_THREADS, 0, x.p, s.p, f.p, q.p, scal.p, l0.flags.p, l0.N,
          round_ref() ? 1 : 0, (mixed() && !P.disable_mg) ? L32[0]->b.p : (float*)nullptr, red.p);
-  launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, RED_BLOCKS, 1, scal.p, 4);  // |r|_inf, rho_old
+  launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, PAIR_BLOCKS, 1, scal.p, 4);  // |r|_inf, rho_old
   launch_counter += 4;
 }
 
