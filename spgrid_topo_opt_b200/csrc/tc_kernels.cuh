@@ -13,7 +13,9 @@
 // so the products keep ~22 bits: the result matches FP32 arithmetic.  The
 // thread that owns a row forms y[I] = E (mu0 D[0:24] + lambda0 D[24:48]) / 72
 // and stores it in shared memory; then every node sums the y of its 8 cells in
-// a fixed corner order, so the result does not depend on scheduling.
+// a fixed corner order, so the result does not depend on scheduling.  Shared
+// memory is the kernel's bottleneck, so its layouts avoid bank conflicts: A rows
+// go out as 16-byte chunks, y is stored column-major.
 //
 // The CTA is persistent over blocks.  While one block is computed, the halo of
 // the next one (its u/E nodes and b) is already in flight with cp.async into
@@ -46,7 +48,7 @@ constexpr int TC_CELLS = 225;                    // cells [-1,3]x[-1,3]x[-1,7]
 constexpr uint64_t TC_WAIT_NS = 1000000000ull;   // an MMA wait gives up after one second
 
 // dynamic shared memory layout (byte offsets from a 128-aligned base)
-constexpr int TC_OFF_AHI = 0;                                  // also y[128][24] after the MMA
+constexpr int TC_OFF_AHI = 0;                                  // also y[24][128] after the MMA
 constexpr int TC_OFF_ALO = TC_OFF_AHI + TC_A_BYTES;
 constexpr int TC_OFF_B = TC_OFF_ALO + TC_A_BYTES;
 constexpr int TC_OFF_HALO = TC_OFF_B + TC_B_BYTES;             // 2 x 360 float4
@@ -119,7 +121,7 @@ __global__ void __launch_bounds__(TC_THREADS) level0_tc_kernel(int nblocks, cons
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(tc_raw) + 127) & ~uintptr_t(127));
   uint8_t* sA_hi = sm + TC_OFF_AHI;
   uint8_t* sA_lo = sm + TC_OFF_ALO;
-  float* sY = reinterpret_cast<float*>(sm + TC_OFF_AHI);  // y[row][24] once the products are in
+  float* sY = reinterpret_cast<float*>(sm + TC_OFF_AHI);  // y[24][row] once the products are in
   uint8_t* sB = sm + TC_OFF_B;
   float4* halo_buf = reinterpret_cast<float4*>(sm + TC_OFF_HALO);
   float* bv_buf = reinterpret_cast<float*>(sm + TC_OFF_BV);
@@ -218,21 +220,26 @@ __global__ void __launch_bounds__(TC_THREADS) level0_tc_kernel(int nblocks, cons
     const int ex = tid >> 5, ey = (tid >> 3) & 3, ez = tid & 7;
     for (int t0 = 0; t0 < rows; t0 += TC_ROWS) {
       const int nrow = min(TC_ROWS, rows - t0);
-      // A rows of this tile: thread r builds row t0 + r
+      // A rows of this tile: thread r builds row t0 + r in registers and stores it
+      // as 16-byte chunks (8 consecutive rows of a chunk fill all 32 banks)
       if (tid < nrow) {
         const int c = row_cell[t0 + tid];
         const int cx = c / 45, cy = (c / 9) % 5, cz = c % 9;
+        float a[TC_K];
 #pragma unroll
         for (int J = 0; J < 8; ++J) {
           const float4 v = halo[(cx + (J >> 2)) * 60 + (cy + ((J >> 1) & 1)) * 10 + cz + (J & 1)];
-          const float a[3] = {v.x, v.y, v.z};
+          a[3 * J] = v.x;
+          a[3 * J + 1] = v.y;
+          a[3 * J + 2] = v.z;
+        }
 #pragma unroll
-          for (int w = 0; w < 3; ++w) {
-            const float hi = tc_hi(a[w]);
-            const int off = tc_off(tid, J * 3 + w);
-            *reinterpret_cast<float*>(sA_hi + off) = hi;
-            *reinterpret_cast<float*>(sA_lo + off) = a[w] - hi;
-          }
+        for (int q = 0; q < TC_KCHUNKS; ++q) {
+          const float4 hi = make_float4(tc_hi(a[4 * q]), tc_hi(a[4 * q + 1]), tc_hi(a[4 * q + 2]), tc_hi(a[4 * q + 3]));
+          const float4 lo = make_float4(a[4 * q] - hi.x, a[4 * q + 1] - hi.y, a[4 * q + 2] - hi.z, a[4 * q + 3] - hi.w);
+          const int off = tc_off(tid, 4 * q);
+          *reinterpret_cast<float4*>(sA_hi + off) = hi;
+          *reinterpret_cast<float4*>(sA_lo + off) = lo;
         }
       }
       // the MMA reads A through the async proxy
@@ -294,20 +301,13 @@ __global__ void __launch_bounds__(TC_THREADS) level0_tc_kernel(int nblocks, cons
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;");
       __syncthreads();  // A is no longer read: y overwrites it
+      // y stored column-major, sY[n][row]: the row owners write consecutive words
       if (tid < nrow) {
         const int c = row_cell[t0 + tid];
         const float E = halo[(c / 45) * 60 + ((c / 9) % 5) * 10 + c % 9].w;
-        float4* yr = reinterpret_cast<float4*>(sY + tid * 24);
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          float y[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int n = 4 * q + j;
-            y[j] = E * (mu72 * __uint_as_float(d[n]) + la72 * __uint_as_float(d[24 + n]));
-          }
-          yr[q] = make_float4(y[0], y[1], y[2], y[3]);
-        }
+        for (int n = 0; n < 24; ++n)
+          sY[n * TC_ROWS + tid] = E * (mu72 * __uint_as_float(d[n]) + la72 * __uint_as_float(d[24 + n]));
       }
       __syncthreads();
       // node (ex, ey, ez) takes corner I of the cell (ex, ey, ez) - I: halo cell + 1 - I
@@ -316,10 +316,10 @@ __global__ void __launch_bounds__(TC_THREADS) level0_tc_kernel(int nblocks, cons
         const int cx = ex + 1 - (I >> 2), cy = ey + 1 - ((I >> 1) & 1), cz = ez + 1 - (I & 1);
         const int r = int(cell_row[cx * 45 + cy * 9 + cz]) - t0;  // 255: no row
         if (cell_row[cx * 45 + cy * 9 + cz] != 255 && r >= 0 && r < nrow) {
-          const float* yr = sY + r * 24 + 3 * I;
+          const float* yr = sY + 3 * I * TC_ROWS + r;
           f0 += yr[0];
-          f1 += yr[1];
-          f2 += yr[2];
+          f1 += yr[TC_ROWS];
+          f2 += yr[2 * TC_ROWS];
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;");
