@@ -19,7 +19,7 @@ SOURCES = ["solver.cu", "band.cu", "render.cu", "setup.cpp", "wire.cpp"]
 # the renderer's ray arithmetic is kept free of fused multiply-adds so that it
 # rounds like its float32 restatement in the oracle
 FILE_FLAGS = {"render.cu": ["-fmad=false"]}
-HEADERS = ["common.cuh", "band.hpp", "kernels.cuh", "setup_kernels.cuh", "topo_kernels.cuh", "setup.hpp", "wire.hpp"]
+HEADERS = ["common.cuh", "band.hpp", "kernels.cuh", "setup_kernels.cuh", "tc_kernels.cuh", "topo_kernels.cuh", "setup.hpp", "wire.hpp"]
 
 
 def nvcc() -> str:
