@@ -314,6 +314,7 @@ def run_ours(args, rank, world):
     sweep_ms = mixed.time_op(2, reps=20)
     ku32_ms = mixed.time_op(4, reps=20)
     res32_ms = mixed.time_op(1, reps=20)
+    res32tc_ms = mixed.time_op(5, reps=20)
     ku64_ms = mixed.time_op(0, reps=20)
     vcyc_ms = mixed.time_op(3, reps=5)
     nodes = dof // 3
@@ -329,12 +330,19 @@ def run_ours(args, rank, world):
                 "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch_set": sweep_bytes, "sweep_ms": round(sweep_ms, 4),
                 "vcycle_ms": round(vcyc_ms, 4),
-                "ku_fp32": {"kernel": "level0_op_kernel<float, K u>", "ms": round(ku32_ms, 4),
+                "ku_fp32": {"kernel": "level0_op_kernel<float, K u> (planar fields, CUDA cores)",
+                            "ms": round(ku32_ms, 4),
                             "algorithmic_bytes": ku32_bytes, "achieved": round(gbs(ku32_bytes, ku32_ms), 1),
                             "frac": round(gbs(ku32_bytes, ku32_ms) / peak, 4)},
-                "residual_fp32": {"kernel": "level0_res4_kernel<float> (V-cycle residual)", "ms": round(res32_ms, 4),
+                "residual_fp32": {"kernel": "level0_res4_kernel<float> (the V-cycle's residual, CUDA cores)",
+                                  "ms": round(res32_ms, 4),
                                   "algorithmic_bytes": res32_bytes, "achieved": round(gbs(res32_bytes, res32_ms), 1),
                                   "frac": round(gbs(res32_bytes, res32_ms) / peak, 4)},
+                "residual_fp32_tensor_cores": {"kernel": "level0_tc_kernel<b - K u> (tcgen05 TF32 hi/lo split, "
+                                                         "FP32 result; not the default)",
+                                               "ms": round(res32tc_ms, 4), "algorithmic_bytes": res32_bytes,
+                                               "achieved": round(gbs(res32_bytes, res32tc_ms), 1),
+                                               "frac": round(gbs(res32_bytes, res32tc_ms) / peak, 4)},
                 "ku_fp64": {"kernel": "level0_op_kernel<double, PCG matvec>", "ms": round(ku64_ms, 4),
                             "algorithmic_bytes": ku64_bytes, "achieved": round(gbs(ku64_bytes, ku64_ms), 1),
                             "frac": round(gbs(ku64_bytes, ku64_ms) / peak, 4)}}

@@ -44,6 +44,9 @@ extern "C" {
  *                        V-cycle casts, the default), 1 = FP64, 2 = FP32 V-cycle
  *                        with FP64 outer PCG;
  *   "sgs_honor_max_iterations"  1 = stop at krylov.max_iterations instead of 500;
+ *   "sgs_tensor_cores"  1 = the FP32 V-cycle's level-0 residual on the tensor
+ *                        cores (tcgen05), 0 = on the CUDA cores (default, faster
+ *                        as measured);
  *   "sgs_dense_bottom_max"  largest bottom (unknowns) inverted densely (default
  *                        24576).  A larger bottom -- the reference driver's
  *                        default mg_bottom_size 64 gives 10^5-10^6 unknowns,
@@ -237,9 +240,9 @@ SGS_API int sgs_boundary_blocks(sgs_session* s, int level, int32_t* ordinals);
  *  5 stencil multiply       6 bottom solve (the V-cycle's last level, mg_level - 1)
  *  7 one V-cycle on level 0
  *  8 level-0 residual b - K u as the V-cycle computes it on its packed (u, E)
- *    iterate: in FP32 on the tensor cores in mixed sessions (extra_ints
- *    "sgs_tensor_cores" = 0 selects the CUDA-core kernel), FP64 otherwise;
- *    sessions whose V-cycle has more than one level */
+ *    iterate: in FP32 in mixed sessions (on the tensor cores with extra_ints
+ *    "sgs_tensor_cores" = 1), FP64 otherwise; sessions whose V-cycle has more
+ *    than one level */
 SGS_API int sgs_apply(sgs_session* s, int op, int level, int arg, const double* in, const double* in2, double* out);
 
 /* Galerkin stencils of a level as [nblocks*128][243] (row node, comp v; column
@@ -249,8 +252,10 @@ SGS_API int sgs_level_stencils(sgs_session* s, int level, double* out, uint32_t*
 /* Average device time (ms, CUDA events) of `reps` back-to-back runs of a level-0
  * operator on the session's resident data: 0 the PCG matvec q = K s (FP64, with
  * Project and the s.q partials), 1 residual, 2 one smoothing sweep (8 colours),
- * 3 one preconditioner application (V-cycle), 4 K u on the planar fields.  Ops
- * 1, 2 and 4 run in the V-cycle's precision (FP32 in mixed sessions). */
+ * 3 one preconditioner application (V-cycle), 4 K u on the planar fields (on
+ * the tensor cores when the session uses them), 5 the V-cycle's residual on
+ * the tensor cores (mixed sessions).  Ops 1, 2, 4 and 5 run in the V-cycle's
+ * precision (FP32 in mixed sessions). */
 SGS_API int sgs_time_op(sgs_session* s, int op, int reps, double* ms);
 
 /* Decode a blob and encode it again with this library's codec (which = 0 for

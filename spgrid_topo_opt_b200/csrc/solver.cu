@@ -141,8 +141,9 @@ class Solver {
   int precision = PREC_REFERENCE;
   int device = -1;                    // CUDA device of the session (current at set-up)
   double* static_partials = nullptr;  // device address of g_sensitivity_partials on that device
-  // the FP32 level-0 residual of the mixed V-cycle on the tensor cores (level0_tc_kernel)
-  bool tensor_cores = true;
+  // the FP32 level-0 residual of the mixed V-cycle on the tensor cores (level0_tc_kernel);
+  // off by default: measured slower than the CUDA-core kernel (shared-memory bound)
+  bool tensor_cores = false;
   int tc_grid = 0;
   DevBuf<int> tc_err;  // set by a tensor-core kernel whose wait gave up
   cudaStream_t stream = nullptr;
@@ -2339,7 +2340,7 @@ static int session_from_inputs(const FEMInputs& in, int precision, sgs_session**
   }
   h->solver->P.max_iterations = 500;  // the reference hard-codes 500 (SPGrid_CPU_Solver.cpp:326)
   if (in.get_int("sgs_honor_max_iterations", 0)) h->solver->P.max_iterations = in.krylov.max_iterations;
-  h->solver->tensor_cores = in.get_int("sgs_tensor_cores", 1) != 0;
+  h->solver->tensor_cores = in.get_int("sgs_tensor_cores", 0) != 0;
   if (precision == SGS_HOST_SETUP_ONLY) {  // inspection of the host-side hierarchy, no device work
     h->solver->precision = precision;
     *out = h.release();
@@ -2466,6 +2467,12 @@ static double time_op(Solver& S, int op, int reps) {
       S.sweep<T>(0, packed ? nullptr : d.u.p, d.b.p, true, false);
     } else if (op == 3) {
       S.precondition();
+    } else if (op == 5) {  // the V-cycle residual on the tensor cores, whatever the session uses
+      if (!(packed && sizeof(T) == 4)) throw CudaError("op 5 needs a mixed-precision session", SGS_ERR_INPUT);
+      const bool keep = S.tensor_cores;
+      S.tensor_cores = true;
+      S.level0_packed<T, OP_RES>(d.b.p, d.r.p);
+      S.tensor_cores = keep;
     } else if (op == 4) {  // K u in the V-cycle's precision, on the tensor cores where the V-cycle uses them
       if (packed && sizeof(T) == 4 && S.tensor_cores) S.level0_packed<T, OP_KU>(nullptr, d.r.p);
       else S.level0<T, OP_KU>(d.u.p, nullptr, d.r.p);
@@ -3099,7 +3106,7 @@ SGS_API void fem_solve(void* input, void* output) {
 SGS_API void fem_solve_free(void* blob) { delete[] static_cast<char*>(blob); }
 
 SGS_API int sgs_time_op(sgs_session* h, int op, int reps, double* ms) {
-  if (!h || !ms || host_only(h) || reps <= 0 || op < 0 || op > 4) return SGS_ERR_INPUT;
+  if (!h || !ms || host_only(h) || reps <= 0 || op < 0 || op > 5) return SGS_ERR_INPUT;
   try {
     *ms = h->solver->mixed() && op != 0 && op != 3 ? time_op<float>(*h->solver, op, reps)
                                                    : time_op<double>(*h->solver, op, reps);

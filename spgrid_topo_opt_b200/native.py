@@ -480,8 +480,9 @@ class Session:
 
     def time_op(self, op: int, reps: int = 20) -> float:
         """Average device milliseconds of a level-0 operator (0 the FP64 PCG
-        matvec K*s, 1 residual, 2 smoothing sweep, 3 V-cycle, 4 K*u; 1, 2 and 4
-        in the V-cycle's precision) on the resident data."""
+        matvec K*s, 1 residual, 2 smoothing sweep, 3 V-cycle, 4 K*u, 5 the
+        residual on the tensor cores; 1, 2, 4 and 5 in the V-cycle's precision)
+        on the resident data."""
         ms = C.c_double(0)
         self._check(load().sgs_time_op(self.h, op, reps, C.byref(ms)))
         return ms.value

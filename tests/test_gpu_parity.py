@@ -63,7 +63,7 @@ def test_packed_fp32_residual_matches_fp64_oracle(small, tensor_cores):
     """The mixed V-cycle's level-0 residual in FP32: on the tensor cores (TF32
     split into high and low parts, FP32 accumulation) and on the CUDA cores,
     both within FP32 rounding (1e-5 of the field's magnitude) of the FP64
-    oracle, and within 1e-5 of each other."""
+    oracle."""
     inp, ref, _ = small
     i2 = fi.deserialize_inputs(fi.serialize_inputs(inp))
     i2.extra_ints["sgs_tensor_cores"] = tensor_cores
