@@ -352,7 +352,7 @@ def run_ours(args, rank, world):
     e2e_inp = fi.deserialize_inputs(fi.serialize_inputs(inp))
     e2e_inp.extra_ints["sgs_precision"] = native.PRECISION_MIXED
     blob = fi.serialize_inputs(e2e_inp)
-    e2e_times, h2d, d2h = [], 0.0, 0.0
+    e2e_times, h2d, d2h, phases = [], 0.0, 0.0, {}
     for i in range(0 if args.no_e2e else 2 + max(1, args.steps // 2)):
         t0 = time.perf_counter()
         out = native.fem_solve_outputs(blob)
@@ -362,6 +362,10 @@ def run_ours(args, rank, world):
         if i >= 2:
             e2e_times.append(dt)
             h2d, d2h = out.extra_doubles.get("h2d_bytes", 0), out.extra_doubles.get("d2h_bytes", 0)
+            for k in ("decode_seconds", "host_setup_seconds", "device_levels_seconds", "device_operators_seconds",
+                      "device_bottom_seconds", "device_vectors_seconds", "solve_seconds", "output_seconds",
+                      "teardown_seconds"):
+                phases.setdefault(k, []).append(out.extra_doubles.get(k, 0.0))
     e2e_s = float(np.mean(e2e_times)) if e2e_times else float("nan")
 
     result = None
@@ -385,6 +389,7 @@ def run_ours(args, rank, world):
             "e2e": None if args.no_e2e else {"value": round(world * dof / e2e_s / 1e6, 3), "unit": "MDOF/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "seconds_per_step": round(e2e_s, 4),
+                    "phases_seconds": {k: round(float(np.mean(v)), 4) for k, v in phases.items()},
                     "path": "fem_solve C ABI: decode, set-up, H2D, solve, pack, D2H, encode"},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
