@@ -760,122 +760,6 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__
   out_u[gidx + 2 * N] = u2;
 }
 
-// Coarse stencils stored spoke-major for one thread per node: As[k][p] with k =
-// spoke*9 + v*3 + w (the entry order of A) and p = b*128 + colour-major slot,
-// colour c = 4(x&1) + 2(y&1) + (z&1) of the node and slot c*16 + q, q = 8(x>>1)
-// + 4(y>>1) + (z>>1), so that the 16 nodes of a colour in a block are 16
-// consecutive words of every coefficient row.
-__host__ __device__ __forceinline__ int colour_slot(int e) {
-  const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
-  return (((x & 1) << 2) | ((y & 1) << 1) | (z & 1)) * 16 + ((x >> 1) << 3) + ((y >> 1) << 2) + (z >> 1);
-}
-
-template <typename TD, typename TS>
-__global__ void stencil_to_soa_kernel(TD* __restrict__ As, const TS* __restrict__ A, long N) {
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= N * 243) return;
-  const long n = t / 243;
-  const int k = int(t % 243);
-  const long p = (n & ~127L) + colour_slot(int(n & 127));
-  As[long(k) * N + p] = TD(A[t]);
-}
-
-// stencil_op_kernel with one thread per node over the spoke-major stencils:
-// the same operations per node (spokes summed in order 0..26, missing
-// neighbours contributing nothing), coalesced coefficient rows instead of a
-// warp reduction.  GS: thread = (listed block, node of the colour).
-template <typename T, int OP>
-__global__ void __launch_bounds__(256) stencil_soa_kernel(const int* __restrict__ block_list, int nblocks,
-                                                          const int* __restrict__ nbr, const T* __restrict__ As,
-                                                          const uint32_t* __restrict__ flags, const T* u, T* out_u,
-                                                          const T* __restrict__ b, T* __restrict__ out, long N, int color,
-                                                          int boundary_only, int round_out) {
-  const int per = (OP == SOP_GS) ? 16 : 128;
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  const long blk = t / per;
-  if (blk >= nblocks) {
-    pdl_wait();
-    return;
-  }
-  const int bi = block_list ? block_list[blk] : int(blk);
-  int e, p;
-  if (OP == SOP_GS) {
-    const int q = int(t % per);
-    const int px = (color >> 2) & 1, py = (color >> 1) & 1, pz = color & 1;
-    e = (((q >> 3) * 2 + px) << 5) + ((((q >> 2) & 1) * 2 + py) << 3) + ((q & 3) * 2 + pz);
-    p = color * 16 + q;
-  } else {
-    // thread k of a block takes colour-major slot k, so coefficient rows are read contiguously
-    const int k = int(t % per);
-    const int c = k >> 4, q = k & 15;
-    e = ((((q >> 3) << 1) | (c >> 2)) << 5) + (((((q >> 2) & 1) << 1) | ((c >> 1) & 1)) << 3) + (((q & 3) << 1) | (c & 1));
-    p = k;
-  }
-  const long gidx = long(bi) * 128 + e;
-  const long sp = long(bi) * 128 + p;
-  const uint32_t fl = flags[gidx];
-  if (OP == SOP_GS) {
-    if (!(fl & ACTIVE_NODE) || (boundary_only && !(fl & BOUNDARY_NODE))) {
-      pdl_wait();
-      return;
-    }
-  }
-  const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
-  const int* nb = nbr + long(bi) * 27;
-  pdl_wait();
-  T f0 = 0, f1 = 0, f2 = 0;
-#pragma unroll 3
-  for (int q = 0; q < 27; ++q) {
-    const int xx = x + q / 9 - 1, yy = y + (q / 3) % 3 - 1, zz = z + q % 3 - 1;
-    const int bsel = (xx < 0 ? 0 : (xx > 3 ? 2 : 1)) * 9 + (yy < 0 ? 0 : (yy > 3 ? 2 : 1)) * 3 + (zz < 0 ? 0 : (zz > 7 ? 2 : 1));
-    const int nbk = __ldg(nb + bsel);
-    if (nbk < 0) continue;
-    const long n = long(nbk) * 128 + ((xx & 3) << 5) + ((yy & 3) << 3) + (zz & 7);
-    const T ux = u[n], uy = u[n + N], uz = u[n + 2 * N];
-    const T* a = As + long(q) * 9 * N + sp;
-    f0 += a[0] * ux + a[N] * uy + a[2 * N] * uz;
-    f1 += a[3 * N] * ux + a[4 * N] * uy + a[5 * N] * uz;
-    f2 += a[6 * N] * ux + a[7 * N] * uy + a[8 * N] * uz;
-  }
-  if (OP == SOP_MUL) {
-    out[gidx] = (fl & DIR_X) ? T(0) : f0;
-    out[gidx + N] = (fl & DIR_Y) ? T(0) : f1;
-    out[gidx + 2 * N] = (fl & DIR_Z) ? T(0) : f2;
-    return;
-  }
-  const T r0 = b[gidx] - f0, r1 = b[gidx + N] - f1, r2 = b[gidx + 2 * N] - f2;
-  if (OP == SOP_RES) {
-    T o0 = (fl & DIR_X) ? T(0) : r0, o1 = (fl & DIR_Y) ? T(0) : r1, o2 = (fl & DIR_Z) ? T(0) : r2;
-    if (round_out) { o0 = T(round_to_float(o0)); o1 = T(round_to_float(o1)); o2 = T(round_to_float(o2)); }
-    out[gidx] = o0;
-    out[gidx + N] = o1;
-    out[gidx + 2 * N] = o2;
-    return;
-  }
-  const T* c = As + long(13) * 9 * N + sp;
-  T d0 = c[0], d1 = c[4 * N], d2 = c[8 * N], d3 = c[N], d4 = c[2 * N], d5 = c[5 * N];
-  const bool fx = fl & DIR_X, fy = fl & DIR_Y, fz = fl & DIR_Z;
-  if (fx) { d0 = 1; d3 = 0; d4 = 0; }
-  if (fy) { d1 = 1; d3 = 0; d5 = 0; }
-  if (fz) { d2 = 1; d4 = 0; d5 = 0; }
-  const T m11 = d1 * d2 - d5 * d5, m12 = d5 * d4 - d2 * d3, m13 = d3 * d5 - d4 * d1;
-  const T m22 = d2 * d0 - d4 * d4, m23 = d4 * d3 - d0 * d5, m33 = d0 * d1 - d3 * d3;
-  const T inv = T(1) / (d0 * m11 + d3 * m12 + d4 * m13);
-  T a0 = m11 * inv, a1 = m22 * inv, a2 = m33 * inv, a3 = m12 * inv, a4 = m13 * inv, a5 = m23 * inv;
-  if (fx) { a0 = 0; a3 = 0; a4 = 0; }
-  if (fy) { a1 = 0; a3 = 0; a5 = 0; }
-  if (fz) { a2 = 0; a4 = 0; a5 = 0; }
-  T u0 = u[gidx] + (a0 * r0 + a3 * r1 + a4 * r2);
-  T u1 = u[gidx + N] + (a3 * r0 + a1 * r1 + a5 * r2);
-  T u2 = u[gidx + 2 * N] + (a4 * r0 + a5 * r1 + a2 * r2);
-  if (fx) u0 = 0;
-  if (fy) u1 = 0;
-  if (fz) u2 = 0;
-  out_u[gidx] = u0;
-  out_u[gidx + N] = u1;
-  out_u[gidx + 2 * N] = u2;
-}
-
 // ---------------------------------------------------------------------------
 // Transfers (solver/MG/Restriction.h:52-88, solver/MG/Prolongation.h:151-193)
 // ---------------------------------------------------------------------------

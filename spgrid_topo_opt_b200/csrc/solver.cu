@@ -72,8 +72,7 @@ struct Level {
   GridView grid{};
   int nbound = 0, ndir[3] = {0, 0, 0};
   DevBuf<T> u, b, r;   // [3N] each
-  DevBuf<T> A;         // [N][243] stencils, node-major (levels with Galerkin operators)
-  DevBuf<T> As;        // the same spoke-major, [243][N] in colour-major slot order (FP64 and mixed modes)
+  DevBuf<T> A;         // [243][N] stencils (levels with Galerkin operators)
   bool has_matrix = false;
   // level 0: node lists of the Gauss-Seidel passes, full sweep colours 0..7
   // then boundary sweep colours 8..15, concatenated; list k is gs_off[k]..gs_off[k+1]
@@ -535,16 +534,10 @@ class Solver {
         SGS_CUDA(cudaGetLastError());
         SGS_CUDA(cudaStreamSynchronize(stream));  // the temporaries go out of scope
       }
-      // the V-cycle's copy for one thread per node: FP32 in mixed precision, FP64 in the
-      // FP64 mode (the reference-rounding mode keeps the warp-per-node kernel)
-      if (precision == PREC_FP64) {
-        d.As.alloc(243 * size_t(d.N));
-        launch(stencil_to_soa_kernel<double, double>, blocks_for(243 * d.N, 256), 256, 0, d.As.p, d.A.p, d.N);
-      }
       if (mixed()) {
         Level<float>& m = *L32[lev];
-        m.As.alloc(243 * size_t(d.N));
-        launch(stencil_to_soa_kernel<float, double>, blocks_for(243 * d.N, 256), 256, 0, m.As.p, d.A.p, d.N);
+        m.A.alloc(243 * size_t(d.N));
+        launch(convert_kernel<float, double>, blocks_for(243 * d.N, 256), 256, 0, m.A.p, d.A.p, 243 * d.N);
         m.spokes.alloc(size_t(d.N));
         SGS_CUDA(cudaMemcpyAsync(m.spokes.p, d.spokes.p, d.N * 4, cudaMemcpyDeviceToDevice, stream));
         m.has_matrix = true;
@@ -777,12 +770,6 @@ class Solver {
     Level<T>& d = lev<T>(l);
     if (count <= 0) return;
     const int per = OP == SOP_GS ? 16 : 128;
-    if (d.As.p) {  // one thread per node on the spoke-major copy
-      launch(stencil_soa_kernel<T, OP>, blocks_for(long(count) * per, 256), 256, 0, list, count, d.nbr.p, d.As.p,
-             d.flags.p, u, uo, b, out, d.N, color, boundary, round_out);
-      ++launch_counter;
-      return;
-    }
     launch(stencil_op_kernel<T, OP>, blocks_for(long(count) * per * 32, 256), 256, 0, 
         list, count, d.coords.p, d.grid, d.A.p, d.flags.p, u, uo, b, out, d.N, color, boundary, round_out);
     ++launch_counter;
