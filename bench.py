@@ -362,7 +362,8 @@ def run_ours(args, rank, world):
         if i >= 2:
             e2e_times.append(dt)
             h2d, d2h = out.extra_doubles.get("h2d_bytes", 0), out.extra_doubles.get("d2h_bytes", 0)
-            for k in ("decode_seconds", "host_setup_seconds", "device_levels_seconds", "device_operators_seconds",
+            for k in ("decode_seconds", "host_setup_seconds", "host_level0_seconds", "host_coarsen_seconds",
+                      "host_flags_seconds", "host_rest_seconds", "device_levels_seconds", "device_operators_seconds",
                       "device_bottom_seconds", "device_vectors_seconds", "solve_seconds", "output_seconds",
                       "teardown_seconds"):
                 phases.setdefault(k, []).append(out.extra_doubles.get(k, 0.0))

@@ -7,6 +7,8 @@
 // check (:145-157).
 #include "setup.hpp"
 
+#include <chrono>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -330,6 +332,13 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   P.minimum_stiffness = emin;
   P.minimum_density = rho_min;
 
+  using hclk = std::chrono::steady_clock;
+  auto tmark = hclk::now();
+  auto phase_done = [&](int k) {
+    const auto t = hclk::now();
+    P.host_phase[k] = std::chrono::duration<double>(t - tmark).count();
+    tmark = t;
+  };
   // ---- level 0: page activation and stiffness (SPGrid_CPU_Solver.cpp:102-136)
   Builder b0;
   b0.init(in.resolution[0], in.resolution[1], in.resolution[2]);
@@ -457,6 +466,7 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
       if (in.density.data[size_t(b) * 64 + e] > 0) P.E[base + size_t(cell_slot(e))] = cell_E(size_t(b), e);
   }
 
+  phase_done(0);
   // ---- coarse levels (Multigrid_Hierarchy.h:122-195)
   const int pad[3] = {2 * BLK_X, 2 * BLK_Y, 2 * BLK_Z};
   auto coarsen = [&](const HostLevel& F) {
@@ -521,9 +531,11 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
     return std::move(bc.L);
   };
   for (int lev = 1; lev < P.mg_levels; ++lev) P.levels.push_back(coarsen(P.levels[lev - 1]));
+  phase_done(1);
   for (auto& L : P.levels) flag_nodes(L);
   for (auto& L : P.levels) flag_boundary(L);
   for (auto& L : P.levels) finish_level(L);
+  phase_done(2);
   // levels below a bottom too large for the dense inverse: the bottom is then
   // solved by CG with V-cycles over them (same coarsening rule, Galerkin
   // operators down to depth 6)
@@ -590,6 +602,7 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
     P.lift_axis.push_back(d.axis);
     P.lift_val.push_back(d.value);
   }
+  phase_done(3);
   return std::string();
 }
 

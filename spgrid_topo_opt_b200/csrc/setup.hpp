@@ -56,6 +56,10 @@ struct Problem {
   // solved by CG preconditioned with V-cycles over further levels, which then
   // follow it in `levels` (at most 7 levels in all); smaller ones are inverted.
   long dense_bottom_max = 24576;
+  // host set-up phase times (seconds): level 0 (pages, SIMP map, checks,
+  // Dirichlet cells, stiffness scales), coarsening, node flags and boundary
+  // bands, the rest (inner levels, padding check, forces, Dirichlet lift)
+  double host_phase[4] = {0, 0, 0, 0};
   int explicit_level = 2;
   int smoothing = 1, boundary_smoothing = 5;
   double tolerance = 1e-4;

@@ -459,7 +459,7 @@ class Solver {
       if (first) {
         L64.back()->gs_list.upload(gsl, stream);
         std::copy(off, off + 17, L64.back()->gs_off);
-        if (precision == PREC_FP64 && P.levels.size() > 1) alloc_packed(*L64.back(), h);
+        if (precision == PREC_FP64 && nout() > 1) alloc_packed(*L64.back(), h);
       }
       if (mixed()) {
         L32.emplace_back(new Level<float>());
@@ -471,7 +471,7 @@ class Solver {
             SGS_CUDA(cudaMemcpyAsync(g32.p, L64.back()->gs_list.p, g32.n * sizeof(int), cudaMemcpyDeviceToDevice,
                                      stream));
           std::copy(off, off + 17, L32.back()->gs_off);
-          if (P.levels.size() > 1) alloc_packed(*L32.back(), h);
+          if (nout() > 1) alloc_packed(*L32.back(), h);
         }
       }
     }
@@ -3019,6 +3019,10 @@ SGS_API void fem_solve(void* input, void* output) {
       outs.extra_doubles["final_residual"] = st.final_residual;
       outs.extra_doubles["setup_seconds"] = st.setup_seconds;
       outs.extra_doubles["host_setup_seconds"] = h->solver->host_setup_seconds;
+      outs.extra_doubles["host_level0_seconds"] = h->solver->P.host_phase[0];
+      outs.extra_doubles["host_coarsen_seconds"] = h->solver->P.host_phase[1];
+      outs.extra_doubles["host_flags_seconds"] = h->solver->P.host_phase[2];
+      outs.extra_doubles["host_rest_seconds"] = h->solver->P.host_phase[3];
       outs.extra_doubles["device_levels_seconds"] = h->solver->setup_phase[0];
       outs.extra_doubles["device_operators_seconds"] = h->solver->setup_phase[1];
       outs.extra_doubles["device_bottom_seconds"] = h->solver->setup_phase[2];
