@@ -41,7 +41,9 @@ TOL = 1e-6
 TIGHT_TOL = 1e-12  # the FP64 solution the errors are measured against
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one level-0 FP32
 # sweep (its 8 colour launches) per workload, from ncu captures of this kernel
-SWEEP_DRAM_BYTES = {"sphere_shell256": 1.125e9}
+SWEEP_DRAM_BYTES = {"sphere_shell256": 1.125e9,
+                    # captured at 512^3 (1.747 GB for 6.04 M active nodes), scaled to 24.15 M
+                    "spheres_band1024": 1.747e9 * 24.15 / 6.04}
 L2_BYTES = 126 * 1024 * 1024
 
 
