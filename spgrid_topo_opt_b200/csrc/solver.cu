@@ -8,6 +8,8 @@
 // to the zero-guess residual, output packing per input block.
 #include <cuda_runtime.h>
 
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -125,6 +127,72 @@ __global__ void pack_u4_kernel(typename Pack4<T>::type* __restrict__ u4, const T
                                long N) {
   const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < N) u4[i] = Pack4<T>::make(u[i], u[i + N], u[i + 2 * N], E[i]);
+}
+
+// Node lists of the level-0 Gauss-Seidel passes, built on the device (see
+// Solver::colour_lists).  Sub-list of a slot: 2k for the updates of list k,
+// 2k + 1 for its Dirichlet-only clears; lists 0..7 the full sweep's colours,
+// 8..15 the boundary sweep's (blocks of the boundary list only).
+__device__ __forceinline__ void colour_sub(uint32_t fl, int e, bool band_block, int& full, int& band) {
+  const int c = ((e >> 5) & 1) << 2 | ((e >> 3) & 1) << 1 | (e & 1);
+  const bool act = fl & ACTIVE_NODE, dir = fl & (DIR_X | DIR_Y | DIR_Z);
+  full = act ? 2 * c : (dir ? 2 * c + 1 : -1);
+  band = -1;
+  if (band_block) band = (act && (fl & BOUNDARY_NODE)) ? 2 * (8 + c) : (dir ? 2 * (8 + c) + 1 : -1);
+}
+
+// per block (CTA of 128 threads, thread = slot): entries of each of the 32
+// sub-lists, stored sub-list major, cnt[l * nb + b]
+__global__ void colour_count_kernel(int nb, const uint32_t* __restrict__ flags, const uint8_t* __restrict__ band_block,
+                                    int* __restrict__ cnt) {
+  __shared__ int sc[32];
+  const int b = blockIdx.x, e = threadIdx.x;
+  if (e < 32) sc[e] = 0;
+  __syncthreads();
+  int full, band;
+  colour_sub(flags[long(b) * 128 + e], e, band_block[b] != 0, full, band);
+  if (full >= 0) atomicAdd(&sc[full], 1);
+  if (band >= 0) atomicAdd(&sc[band], 1);
+  __syncthreads();
+  if (e < 32) cnt[long(e) * nb + b] = sc[e];
+}
+
+// Write every entry at its sub-list's start for the block (exclusive scan of
+// the counts) plus its rank among the block's earlier slots of the same
+// sub-list, so each sub-list ascends: blocks in order, slots in order.
+__global__ void colour_fill_kernel(int nb, const uint32_t* __restrict__ flags, const uint8_t* __restrict__ band_block,
+                                   const int* __restrict__ pos, int* __restrict__ out) {
+  __shared__ int8_t sfull[128], sband[128];
+  const int b = blockIdx.x, e = threadIdx.x;
+  const long g = long(b) * 128 + e;
+  int full, band;
+  colour_sub(flags[g], e, band_block[b] != 0, full, band);
+  sfull[e] = int8_t(full);
+  sband[e] = int8_t(band);
+  __syncthreads();
+  int rf = 0, rb = 0;
+  for (int k = 0; k < e; ++k) {
+    rf += (full >= 0) && (sfull[k] == full || sband[k] == full);
+    rb += (band >= 0) && (sfull[k] == band || sband[k] == band);
+  }
+  if (full >= 0) out[pos[long(full) * nb + b] + rf] = (full & 1) ? ~int(g) : int(g);
+  if (band >= 0) out[pos[long(band) * nb + b] + rb] = (band & 1) ? ~int(g) : int(g);
+}
+
+// block grid entries naming ghost blocks (index >= nb) become -1; neighbour
+// tables with the zero pad block (index nb) in place of missing neighbours
+__global__ void active_grid_kernel(int* __restrict__ g, long n, int nb) {
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n && g[i] >= nb) g[i] = -1;
+}
+__global__ void pad_neighbours_kernel(int* __restrict__ z, const int* __restrict__ nbr, long n, int nb) {
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) z[i] = nbr[i] < 0 ? nb : nbr[i];
+}
+
+__global__ void mark_blocks_kernel(const int* __restrict__ list, int n, uint8_t* __restrict__ mark) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) mark[list[i]] = 1;
 }
 
 // Scratch of the allocation-free sensitivity entry point (sgs_sensitivity_static):
@@ -322,11 +390,10 @@ class Solver {
     d.coords.upload(h.coords.data(), size_t(h.nb) * 3, stream);
     d.nbr.upload(h.nbr, stream);
     d.flags.upload(h.flags.data(), size_t(d.N), stream);
-    std::vector<int32_t> g(h.bgrid.size());
-    const long ng = long(g.size());
-#pragma omp parallel for schedule(static)
-    for (long i = 0; i < ng; ++i) g[size_t(i)] = (h.bgrid[size_t(i)] >= 0 && h.bgrid[size_t(i)] < h.nb) ? h.bgrid[size_t(i)] : -1;
-    d.bgrid.upload(g, stream);
+    // the block grid names active blocks only (ghost blocks become -1, on the device)
+    d.bgrid.upload(h.bgrid, stream);
+    if (d.bgrid.n)
+      active_grid_kernel<<<blocks_for(long(d.bgrid.n), 256), 256, 0, stream>>>(d.bgrid.p, long(d.bgrid.n), h.nb);
     d.grid = GridView{d.bgrid.p, h.grid[0], h.grid[1], h.grid[2]};
     d.boundary.upload(h.boundary, stream);
     d.nbound = int(h.boundary.size());
@@ -380,63 +447,52 @@ class Solver {
   // sweep) or of the boundary blocks (boundary sweep), updates the active
   // (active boundary-band) ones and clears the Dirichlet components of the
   // rest; those come last in a list, encoded as ~node.  Lists ascend, so a
-  // warp's threads work on neighbouring nodes of few blocks.
-  // Built block-parallel: each block counts its entries of the 32 sub-lists
-  // (16 lists x {update, clear}), a prefix over blocks places them, and a
-  // second pass writes them, so every sub-list stays in ascending node order.
-  static void colour_lists(const HostLevel& h, std::vector<int32_t>& out, int off[17]) {
-    std::vector<char> in_boundary(size_t(h.nb), 0);
-    for (int b : h.boundary) in_boundary[size_t(b)] = 1;
-    const int nb = h.nb;
-    // sub-list of node g (or -1): 2k for updates of list k, 2k + 1 for clears
-    auto sub = [&](long g) {
-      const uint32_t fl = h.flags[size_t(g)];
-      const int e = int(g & 127);
-      const int c = ((e >> 5) & 1) << 2 | ((e >> 3) & 1) << 1 | (e & 1);
-      const bool act = fl & ACTIVE_NODE, dir = fl & (DIR_X | DIR_Y | DIR_Z);
-      int full = act ? 2 * c : (dir ? 2 * c + 1 : -1), band = -1;
-      if (in_boundary[size_t(g >> 7)]) band = (act && (fl & BOUNDARY_NODE)) ? 2 * (8 + c) : (dir ? 2 * (8 + c) + 1 : -1);
-      return std::make_pair(full, band);
-    };
-    std::vector<int32_t> cnt(size_t(nb) * 32, 0);
-#pragma omp parallel for schedule(static)
-    for (int b = 0; b < nb; ++b)
-      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
-        const auto sl = sub(long(b) * NODES_PER_BLOCK + e);
-        if (sl.first >= 0) ++cnt[size_t(b) * 32 + size_t(sl.first)];
-        if (sl.second >= 0) ++cnt[size_t(b) * 32 + size_t(sl.second)];
-      }
-    // start of every (sub-list, block) slot: sub-lists in order, blocks within
-    long total = 0;
-    off[0] = 0;
-    for (int l = 0; l < 32; ++l) {
-      for (int b = 0; b < nb; ++b) {
-        const int32_t c = cnt[size_t(b) * 32 + size_t(l)];
-        cnt[size_t(b) * 32 + size_t(l)] = int32_t(total);
-        total += c;
-      }
-      if (l & 1) off[l / 2 + 1] = int(total);
+  // warp's threads work on neighbouring nodes of few blocks.  Built on the
+  // device from the uploaded flags: per-block counts of the 32 sub-lists (16
+  // lists x {update, clear}), an exclusive scan over (sub-list, block), and a
+  // fill that ranks each entry among its block's earlier slots.
+  void colour_lists(Level<double>& d) {
+    const int nb = d.nb;
+    if (nb == 0) {
+      std::fill(d.gs_off, d.gs_off + 17, 0);
+      return;
     }
-    out.assign(size_t(total), 0);
-#pragma omp parallel for schedule(static)
-    for (int b = 0; b < nb; ++b)
-      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
-        const long g = long(b) * NODES_PER_BLOCK + e;
-        const auto sl = sub(g);
-        for (int l : {sl.first, sl.second})
-          if (l >= 0) out[size_t(cnt[size_t(b) * 32 + size_t(l)]++)] = (l & 1) ? ~int32_t(g) : int32_t(g);
-      }
+    DevBuf<uint8_t> band_block;
+    band_block.alloc(size_t(nb));
+    band_block.zero(stream);
+    if (d.nbound > 0)
+      mark_blocks_kernel<<<blocks_for(d.nbound, 256), 256, 0, stream>>>(d.boundary.p, d.nbound, band_block.p);
+    DevBuf<int> cnt, pos;
+    const long n = 32L * nb;
+    cnt.alloc(size_t(n) + 1);
+    pos.alloc(size_t(n) + 1);
+    colour_count_kernel<<<nb, 128, 0, stream>>>(nb, d.flags.p, band_block.p, cnt.p);
+    SGS_CUDA(cudaMemsetAsync(cnt.p + n, 0, sizeof(int), stream));
+    size_t tmp_bytes = 0;
+    SGS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt.p, pos.p, int(n + 1), stream));
+    DevBuf<uint8_t> tmp;
+    tmp.alloc(tmp_bytes);
+    SGS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, cnt.p, pos.p, int(n + 1), stream));
+    // list k starts where sub-list 2k does (block 0); the end is the total
+    for (int k = 0; k < 16; ++k)
+      SGS_CUDA(cudaMemcpyAsync(&d.gs_off[k], pos.p + long(2 * k) * nb, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaMemcpyAsync(&d.gs_off[16], pos.p + n, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SGS_CUDA(cudaStreamSynchronize(stream));
+    d.gs_list.alloc(size_t(d.gs_off[16]));
+    if (d.gs_off[16] > 0)
+      colour_fill_kernel<<<nb, 128, 0, stream>>>(nb, d.flags.p, band_block.p, pos.p, d.gs_list.p);
+    SGS_CUDA(cudaGetLastError());
+    SGS_CUDA(cudaStreamSynchronize(stream));  // the temporaries go out of scope
   }
 
   // the packed level-0 iterate with its zero pad block, and the neighbour table naming it
   template <typename T>
-  void alloc_packed(Level<T>& d, const HostLevel& h) {
+  void alloc_packed(Level<T>& d) {
     d.u4.alloc(size_t(d.N) + NODES_PER_BLOCK);
     SGS_CUDA(cudaMemsetAsync(d.u4.p + d.N, 0, NODES_PER_BLOCK * sizeof(typename Pack4<T>::type), stream));
-    std::vector<int32_t> z(h.nbr);
-    for (auto& v : z)
-      if (v < 0) v = h.nb;
-    d.nbrz.upload(z, stream);
+    d.nbrz.alloc(d.nbr.n);
+    if (d.nbr.n)
+      pad_neighbours_kernel<<<blocks_for(long(d.nbr.n), 256), 256, 0, stream>>>(d.nbrz.p, d.nbr.p, long(d.nbr.n), d.nb);
   }
 
   void build_levels() {
@@ -449,17 +505,13 @@ class Solver {
 #pragma omp parallel for reduction(+ : active) schedule(static)
     for (long i = 0; i < n0; ++i) active += (fl0[i] & ACTIVE_NODE) ? 1 : 0;
     active_nodes0 = active;
-    std::vector<int32_t> gsl;
-    int off[17];
-    colour_lists(P.levels[0], gsl, off);
     for (auto& h : P.levels) {
       const bool first = &h == &P.levels[0];
       L64.emplace_back(new Level<double>());
       upload_level(*L64.back(), h);
       if (first) {
-        L64.back()->gs_list.upload(gsl, stream);
-        std::copy(off, off + 17, L64.back()->gs_off);
-        if (precision == PREC_FP64 && nout() > 1) alloc_packed(*L64.back(), h);
+        colour_lists(*L64.back());
+        if (precision == PREC_FP64 && nout() > 1) alloc_packed(*L64.back());
       }
       if (mixed()) {
         L32.emplace_back(new Level<float>());
@@ -470,8 +522,8 @@ class Solver {
           if (g32.n)
             SGS_CUDA(cudaMemcpyAsync(g32.p, L64.back()->gs_list.p, g32.n * sizeof(int), cudaMemcpyDeviceToDevice,
                                      stream));
-          std::copy(off, off + 17, L32.back()->gs_off);
-          if (nout() > 1) alloc_packed(*L32.back(), h);
+          std::copy(L64.back()->gs_off, L64.back()->gs_off + 17, L32.back()->gs_off);
+          if (nout() > 1) alloc_packed(*L32.back());
         }
       }
     }
