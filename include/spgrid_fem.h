@@ -53,6 +53,14 @@ extern "C" {
  *                        which the reference factors with PARDISO -- is solved
  *                        exactly (to round-off) by CG preconditioned with
  *                        V-cycles over further levels coarsened below it.
+ *   "sgs_device_loop"  0 = test convergence on the host after every PCG
+ *                        iteration (one graph launch per iteration) instead of
+ *                        running the whole loop as one graph whose WHILE node
+ *                        the test kernel drives (default 1; the output's
+ *                        extra_ints "device_loop" says which ran);
+ *   "sgs_loop_history"  residuals one launch of the device loop records before
+ *                        it pauses for the host to take them out (2-1024,
+ *                        default 1024; smaller values only add launches).
  * A solve that reaches the iteration cap returns success = 1 as the
  * reference's does, with extra_ints "converged" = 0. 
  * Warm starting as the reference's (SPGrid_CPU_Solver.cpp:56-73, 240-321,

@@ -48,6 +48,10 @@ inline void keep_pool_memory() {
   done[dev] = true;
 }
 
+// Host-to-device copy of pageable memory through the library's pinned staging
+// buffer (defined with it); returns when the source may be reused.
+void staged_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
@@ -75,7 +79,12 @@ struct DevBuf {
   }
   void upload(const T* h, size_t count, cudaStream_t s) {
     alloc(count);
-    if (count) SGS_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    // large arrays through the pinned staging buffer (about twice the
+    // bandwidth of a pageable copy), small ones directly
+    if (count * sizeof(T) >= (size_t(8) << 20))
+      staged_h2d(p, h, count * sizeof(T), s);
+    else if (count)
+      SGS_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
     g_h2d_bytes += count * sizeof(T);
   }
   void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }

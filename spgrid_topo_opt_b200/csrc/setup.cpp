@@ -13,7 +13,10 @@
 #include <cmath>
 #include <cstdio>
 #include <memory>
+#include <parallel/algorithm>
 #include <unordered_set>
+
+#include <omp.h>
 
 namespace sgs {
 
@@ -63,8 +66,10 @@ int HostLevel::touch(int x, int y, int z, bool with_flags) {
 
 namespace {
 
-// A level under construction: blocks are created in touch order, then the
-// active ones are renumbered into page order.
+// A level under construction.  Its blocks are numbered as the reference's
+// page order has them: the active blocks (pages) in page-key order first, then
+// the ghost blocks (touched, not pages) in the order they were created; see
+// number_blocks.  Blocks touched after numbering are ghosts and are appended.
 struct Builder {
   HostLevel L;
 
@@ -74,21 +79,6 @@ struct Builder {
     L.bgrid.assign(size_t(L.grid[0]) * L.grid[1] * L.grid[2], -1);
     L.active_page.assign(L.bgrid.size(), 0);
   }
-  int set_page(int x, int y, int z, bool with_flags = true) {
-    long c = L.cell(x, y, z);
-    if (c < 0) return -1;
-    int b = L.touch(x, y, z, with_flags);
-    L.active_page[c] = 1;
-    return b;
-  }
-  // flags of the blocks created by set_page(..., false), zeroed in parallel
-  void add_flags() {
-    const size_t have = L.flags.size(), want = L.coords.size() / 3 * NODES_PER_BLOCK;
-    L.flags.resize(want);  // uninitialised
-    uint32_t* f = L.flags.data();
-#pragma omp parallel for schedule(static)
-    for (long i = long(have); i < long(want); ++i) f[i] = 0u;
-  }
   bool test_page(int x, int y, int z) const {
     long c = L.cell(x, y, z);
     return c >= 0 && L.active_page[c];
@@ -97,40 +87,65 @@ struct Builder {
     int b = L.touch(x, y, z);
     return b < 0 ? nullptr : &L.flags[size_t(b) * NODES_PER_BLOCK + node_slot(x, y, z)];
   }
-  // Renumber: active blocks in page order first, ghosts after; returns old->new map.
-  std::vector<int32_t> finalize() {
-    const int n_all = int(L.coords.size() / 3);
-    std::vector<std::pair<uint64_t, int>> act;
-    std::vector<int> ghost;
-    for (int b = 0; b < n_all; ++b) {
-      int x = L.coords[3 * b], y = L.coords[3 * b + 1], z = L.coords[3 * b + 2];
-      if (L.active_page[L.cell(x, y, z)]) act.push_back({page_key(x >> 2, y >> 2, z >> 3), b});
-      else ghost.push_back(b);
-    }
-    std::sort(act.begin(), act.end());
-    std::vector<int32_t> order;
-    for (auto& a : act) order.push_back(a.second);
-    for (int g : ghost) order.push_back(g);
-    std::vector<int32_t> remap(n_all);
-    for (int i = 0; i < n_all; ++i) remap[order[i]] = i;
-    std::vector<int32_t> coords(L.coords.size());
-    HostBuf<uint32_t> flags(L.flags.size());  // every entry is written below
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < n_all; ++i) {
-      int o = order[i];
-      for (int v = 0; v < 3; ++v) coords[3 * i + v] = L.coords[3 * o + v];
-      std::copy(&L.flags[size_t(o) * NODES_PER_BLOCK], &L.flags[size_t(o) * NODES_PER_BLOCK] + NODES_PER_BLOCK,
-                &flags[size_t(i) * NODES_PER_BLOCK]);
-    }
-    L.coords.swap(coords);
-    L.flags.swap(flags);
-#pragma omp parallel for schedule(static)
-    for (long c = 0; c < long(L.bgrid.size()); ++c)
-      if (L.bgrid[size_t(c)] >= 0) L.bgrid[size_t(c)] = remap[size_t(L.bgrid[size_t(c)])];
-    L.nb = int(act.size());
-    return remap;
-  }
 };
+
+// The cells c of a block grid of ncell cells with key_of(c) != NONE, as (key,
+// cell) pairs sorted by key; the grid is scanned in one chunk per thread
+// (counted, then gathered) and the pairs sorted in parallel.
+constexpr uint64_t NONE = ~uint64_t(0);
+template <typename KeyOf>
+std::vector<std::pair<uint64_t, long>> sorted_cells(long ncell, const KeyOf& key_of) {
+  const int nt = std::max(1, omp_get_max_threads());
+  const long chunk = (ncell + nt - 1) / nt;
+  std::vector<long> start(size_t(nt) + 1, 0);
+#pragma omp parallel for schedule(static, 1) num_threads(nt)
+  for (int t = 0; t < nt; ++t) {
+    long n = 0;
+    for (long c = long(t) * chunk; c < std::min(ncell, long(t + 1) * chunk); ++c) n += key_of(c) != NONE;
+    start[size_t(t) + 1] = n;
+  }
+  for (int t = 0; t < nt; ++t) start[size_t(t) + 1] += start[size_t(t)];
+  std::vector<std::pair<uint64_t, long>> out(static_cast<size_t>(start[size_t(nt)]));
+#pragma omp parallel for schedule(static, 1) num_threads(nt)
+  for (int t = 0; t < nt; ++t) {
+    long k = start[size_t(t)];
+    for (long c = long(t) * chunk; c < std::min(ncell, long(t + 1) * chunk); ++c) {
+      const uint64_t key = key_of(c);
+      if (key != NONE) out[size_t(k++)] = {key, c};
+    }
+  }
+  __gnu_parallel::sort(out.begin(), out.end());
+  return out;
+}
+
+// Numbers the blocks of a level under construction: the active blocks (cells
+// `act`, in page-key order) first, the ghost blocks (`ghost`, in creation
+// order) after; coordinates set, flags zeroed.
+void number_blocks(HostLevel& L, const std::vector<std::pair<uint64_t, long>>& act,
+                   const std::vector<std::pair<uint64_t, long>>& ghost) {
+  const long na = long(act.size()), nall = na + long(ghost.size());
+  const long g12 = long(L.grid[1]) * L.grid[2];
+  L.coords.resize(3 * size_t(nall));
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < nall; ++i) {
+    const long c = i < na ? act[size_t(i)].second : ghost[size_t(i - na)].second;
+    L.bgrid[size_t(c)] = int32_t(i);
+    L.coords[3 * size_t(i)] = int(c / g12) * BLK_X;
+    L.coords[3 * size_t(i) + 1] = int((c / L.grid[2]) % L.grid[1]) * BLK_Y;
+    L.coords[3 * size_t(i) + 2] = int(c % L.grid[2]) * BLK_Z;
+  }
+  L.nb = int(na);
+  L.flags.resize(size_t(nall) * NODES_PER_BLOCK);  // uninitialised
+  uint32_t* f = L.flags.data();
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < nall * NODES_PER_BLOCK; ++i) f[i] = 0u;
+}
+
+// the page key of a block-grid cell
+uint64_t cell_key(const HostLevel& L, long c) {
+  const long g12 = long(L.grid[1]) * L.grid[2];
+  return page_key(int(c / g12), int((c / L.grid[2]) % L.grid[1]), int(c % L.grid[2]));
+}
 
 // The 27 blocks (active or ghost) around block b, -1 where there is none;
 // entry (dx+1)*9 + (dy+1)*3 + (dz+1).
@@ -343,27 +358,46 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   Builder b0;
   b0.init(in.resolution[0], in.resolution[1], in.resolution[2]);
   const size_t nin = in.density.num_blocks();
-  // Each 4x4x4 input block fills one z half of a 4x4x8 solver block.  Pages are
-  // set serially (block creation order); the per-cell work then runs per input
-  // block in parallel, which writes disjoint slots unless an input block is
-  // repeated: then the cells go in input order, the last write winning.
+  // Each 4x4x4 input block fills one z half of a 4x4x8 solver block.  The
+  // solver blocks are the distinct pages of the input blocks, numbered in page
+  // order: the pages are marked in the block grid, listed, sorted by page key
+  // and numbered, in parallel.  Blocks touched later (ghosts) follow them in
+  // creation order.  The per-cell work then
+  // runs per input block in parallel, which writes disjoint slots unless an
+  // input block is repeated: then the cells go in input order, the last write
+  // winning.
   std::vector<int32_t> in_slot(nin);
-  b0.L.coords.reserve(3 * nin);  // at most one solver page per input block
   bool repeated = false;
   {
-    std::vector<uint8_t> halves;
-    for (size_t b = 0; b < nin; ++b) {
-      int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
-      if ((x & 3) || (y & 3) || (z & 3)) return fail(4, "density block base is not a multiple of 4");
-      const int bk = b0.set_page(x, y, z, false);
-      if (bk < 0) return fail(4, "density block outside the grid");
-      in_slot[b] = bk * NODES_PER_BLOCK + node_slot(x, y, z);
-      if (halves.size() <= size_t(bk)) halves.resize(size_t(bk) + 1, 0);
-      const uint8_t h = uint8_t(1u << ((z >> 2) & 1));
-      repeated |= (halves[size_t(bk)] & h) != 0;
-      halves[size_t(bk)] |= h;
+    HostLevel& L = b0.L;
+    std::vector<long> cell_of(nin);
+    std::vector<uint8_t> bad(nin);
+#pragma omp parallel for schedule(static)
+    for (long b = 0; b < long(nin); ++b) {
+      const int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
+      const bool aligned = !((x & 3) || (y & 3) || (z & 3));
+      cell_of[size_t(b)] = aligned ? L.cell(x, y, z) : -1;
+      bad[size_t(b)] = !aligned ? 1 : (cell_of[size_t(b)] < 0 ? 2 : 0);
     }
-    b0.add_flags();
+    for (size_t b = 0; b < nin; ++b)  // the first failure in input order
+      if (bad[b]) return fail(4, bad[b] == 1 ? "density block base is not a multiple of 4" : "density block outside the grid");
+    uint8_t* page = L.active_page.data();
+#pragma omp parallel for schedule(static)
+    for (long b = 0; b < long(nin); ++b) __atomic_store_n(&page[cell_of[size_t(b)]], uint8_t(1), __ATOMIC_RELAXED);
+    const auto pages = sorted_cells(long(L.active_page.size()), [&](long c) { return page[c] ? cell_key(L, c) : NONE; });
+    number_blocks(L, pages, {});
+    const int nb = L.nb;
+    std::vector<uint8_t> halves(size_t(nb), 0);
+    int rep = 0;
+#pragma omp parallel for schedule(static) reduction(| : rep)
+    for (long b = 0; b < long(nin); ++b) {
+      const int z = in.density.base[3 * b + 2];
+      const int bk = L.bgrid[size_t(cell_of[size_t(b)])];
+      in_slot[size_t(b)] = bk * NODES_PER_BLOCK + node_slot(in.density.base[3 * b], in.density.base[3 * b + 1], z);
+      const uint8_t h = uint8_t(1u << ((z >> 2) & 1));
+      rep |= (__atomic_fetch_or(&halves[size_t(bk)], h, __ATOMIC_RELAXED) & h) ? 1 : 0;
+    }
+    repeated = rep != 0;
   }
   // the SIMP map of every input cell, once (fem_interface.h:343-353); the
   // buffer is filled in parallel without a serial zero pass
@@ -446,7 +480,6 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   }
   for (auto& d : in.dirichlet_nodes)
     if (d.axis < 0 || d.axis > 2) return fail(4, "Dirichlet axis out of range");
-  const std::vector<int32_t> remap0 = b0.finalize();
   P.levels.clear();
   P.levels.push_back(std::move(b0.L));
   // the stiffness scale of every material cell at its slot in page order (the
@@ -460,8 +493,7 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   }
 #pragma omp parallel for schedule(static) if (!repeated)
   for (long b = 0; b < long(nin); ++b) {
-    const int32_t slot = in_slot[size_t(b)];
-    const size_t base = size_t(remap0[size_t(slot / NODES_PER_BLOCK)]) * NODES_PER_BLOCK + size_t(slot % NODES_PER_BLOCK);
+    const size_t base = size_t(in_slot[size_t(b)]);
     for (int e = 0; e < 64; ++e)
       if (in.density.data[size_t(b) * 64 + e] > 0) P.E[base + size_t(cell_slot(e))] = cell_E(size_t(b), e);
   }
@@ -515,19 +547,54 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
         pt.any = true;
       }
     }
+    // The coarse blocks are the patch blocks and the reached pages.  A serial
+    // pass in fine-block order would create them in that order; the pages
+    // (active) then go in page-key order and the rest (ghosts, created only as
+    // a patch block) in creation order, i.e. in the order of the first fine
+    // block whose patch lies in them.  That numbering is made directly:
+    // pages marked and patch blocks' first fine block found (atomic minimum)
+    // in parallel, both lists sorted, and the patch flags ORed into their
+    // blocks, each fine block's patch being a disjoint 2x2x4 part of one
+    // coarse block.
+    HostLevel& C = bc.L;
+    const long ncell = long(C.bgrid.size());
+    std::vector<long> own(static_cast<size_t>(F.nb), -1);
+    std::vector<int32_t> first(static_cast<size_t>(ncell), INT32_MAX);
+    uint8_t* page = C.active_page.data();
+#pragma omp parallel for schedule(static)
     for (int b = 0; b < F.nb; ++b) {
       const Patch& pt = patch[size_t(b)];
       if (!pt.any) continue;
       const int cx0 = (F.coords[3 * b] + BLK_X) >> 1, cy0 = (F.coords[3 * b + 1] + BLK_Y) >> 1,
                 cz0 = (F.coords[3 * b + 2] + BLK_Z) >> 1;
-      if (bc.L.touch(cx0, cy0, cz0) >= 0)
-        for (int l = 0; l < 16; ++l)
-          if (pt.flags[l]) *bc.flag(cx0 + (l >> 3), cy0 + ((l >> 2) & 1), cz0 + (l & 3)) |= pt.flags[l];
+      const long c = C.cell(cx0, cy0, cz0);
+      own[size_t(b)] = c;
+      if (c >= 0) {
+        int32_t cur = __atomic_load_n(&first[size_t(c)], __ATOMIC_RELAXED);
+        while (b < cur && !__atomic_compare_exchange_n(&first[size_t(c)], &cur, int32_t(b), false, __ATOMIC_RELAXED,
+                                                       __ATOMIC_RELAXED)) {
+        }
+      }
       for (int d = 0; d < 8; ++d)
-        if (pt.pages >> d & 1)
-          bc.set_page(cx0 + ((d >> 2) & 1) * BLK_X, cy0 + ((d >> 1) & 1) * BLK_Y, cz0 + (d & 1) * BLK_Z);
+        if (pt.pages >> d & 1) {
+          const long pc = C.cell(cx0 + ((d >> 2) & 1) * BLK_X, cy0 + ((d >> 1) & 1) * BLK_Y, cz0 + (d & 1) * BLK_Z);
+          if (pc >= 0) __atomic_store_n(&page[pc], uint8_t(1), __ATOMIC_RELAXED);
+        }
     }
-    bc.finalize();
+    const auto act = sorted_cells(ncell, [&](long c) { return page[c] ? cell_key(C, c) : NONE; });
+    const auto ghost = sorted_cells(
+        ncell, [&](long c) { return !page[c] && first[size_t(c)] != INT32_MAX ? uint64_t(first[size_t(c)]) : NONE; });
+    number_blocks(C, act, ghost);
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < F.nb; ++b) {
+      if (own[size_t(b)] < 0) continue;
+      const Patch& pt = patch[size_t(b)];
+      const int cx0 = (F.coords[3 * b] + BLK_X) >> 1, cy0 = (F.coords[3 * b + 1] + BLK_Y) >> 1,
+                cz0 = (F.coords[3 * b + 2] + BLK_Z) >> 1;
+      uint32_t* f = &C.flags[size_t(C.bgrid[size_t(own[size_t(b)])]) * NODES_PER_BLOCK];
+      for (int l = 0; l < 16; ++l)
+        if (pt.flags[l]) f[node_slot(cx0 + (l >> 3), cy0 + ((l >> 2) & 1), cz0 + (l & 3))] |= pt.flags[l];
+    }
     return std::move(bc.L);
   };
   for (int lev = 1; lev < P.mg_levels; ++lev) P.levels.push_back(coarsen(P.levels[lev - 1]));

@@ -7,6 +7,7 @@
 // solver/MG/Multigrid_Hierarchy.h:569-619), L-infinity stopping rule relative
 // to the zero-guess residual, output packing per input block.
 #include <cuda_runtime.h>
+#include <sys/mman.h>
 
 #include <cub/cub.cuh>
 
@@ -19,7 +20,9 @@
 #include <functional>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -246,8 +249,19 @@ class Solver {
   std::vector<double> history;
   std::string error;
   int error_code = 0;
-  // graph of one PCG iteration
+  // graph of one PCG iteration, launched by the host per iteration (with an
+  // inner bottom solve, whose iteration count the host decides, or where
+  // conditional graph nodes are unavailable)
   cudaGraphExec_t iter_graph = nullptr;
+  // the whole PCG loop as one graph: the convergence test, then a WHILE node
+  // whose body is one iteration followed by the test (no host round trip per
+  // iteration); loop_buf holds the loop record and the residual history
+  cudaGraphExec_t loop_graph = nullptr;
+  DevBuf<double> loop_buf;
+  double* h_loop = nullptr;  // pinned mirror of loop_buf
+  bool loop_unavailable = false;
+  std::string loop_note;     // why the device loop is not used, if it is not
+  int loop_history = 1024;   // residuals one launch records (2 .. LOOP_HIST)
   long launches_per_iteration = 0;
   long launch_counter = 0;   // kernels launched (or captured) by this solver
   long solve_launches = 0;   // kernels executed by the last solve
@@ -258,7 +272,9 @@ class Solver {
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_end) cudaEventDestroy(ev_end);
     if (iter_graph) cudaGraphExecDestroy(iter_graph);
+    if (loop_graph) cudaGraphExecDestroy(loop_graph);
     if (h_scal) cudaFreeHost(h_scal);
+    if (h_loop) cudaFreeHost(h_loop);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -1101,6 +1117,12 @@ class Solver {
   // ------------------------------------------------------------------ PCG
   void dot(const double* a, const double* b, double* out);
   void linf(const double* a, double* out);
+  bool build_loop_graph();
+  void drop_graphs() {
+    if (iter_graph) SGS_CUDA(cudaGraphExecDestroy(iter_graph));
+    if (loop_graph) SGS_CUDA(cudaGraphExecDestroy(loop_graph));
+    iter_graph = loop_graph = nullptr;
+  }
   void axpy(double* dst, double sign, int coef_slot, const double* xv, const double* yv);
   int precondition();  // returns the number of rho partials it wrote
   void stage_residual();
@@ -1159,10 +1181,7 @@ class Solver {
     g_h2d_bytes += P.E.size() * sizeof(double);
     if (mixed())
       launch(convert_kernel<float, double>, blocks_for(long(P.E.size()), 256), 256, 0, E32.p, E64.p, long(P.E.size()));
-    if (iter_graph) {  // the captured iteration refers to the old operator buffers
-      SGS_CUDA(cudaGraphExecDestroy(iter_graph));
-      iter_graph = nullptr;
-    }
+    drop_graphs();  // the captured iteration refers to the old operator buffers
     build_operators();
     build_bottom();
     SGS_CUDA(cudaStreamSynchronize(stream));
@@ -1353,7 +1372,11 @@ __global__ void cg_update_kernel(double* x, const double* __restrict__ s, double
 }
 
 // precond_out4_kernel over node pairs: two nodes per thread with 16-byte loads and
-// stores (N is a multiple of 128), the same arithmetic per node.
+// stores (N is a multiple of 128), the same arithmetic per node.  The pair
+// kernels skip pairs of inactive nodes: there every PCG vector is zero for the
+// whole solve (Project_Nullspace zeroes them, K u vanishes where no active cell
+// touches a node, x starts at zero), so only the flags are read for them and
+// the sectors that hold no active node are never fetched.
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS, 4) precond_out4_pair_kernel(const typename Pack4<T>::type* __restrict__ z4,
                                                                        double* __restrict__ q,
@@ -1366,6 +1389,7 @@ __global__ void __launch_bounds__(RED_THREADS, 4) precond_out4_pair_kernel(const
   const long P = N >> 1;
   for (long p = long(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += long(gridDim.x) * blockDim.x) {
     const uint2 fl = reinterpret_cast<const uint2*>(flags)[p];
+    if (!((fl.x | fl.y) & ACTIVE_NODE)) continue;
     const auto za = z4[2 * p], zb = z4[2 * p + 1];
     const double zc[2][3] = {{double(za.x), double(za.y), double(za.z)}, {double(zb.x), double(zb.y), double(zb.z)}};
     const uint32_t fls[2] = {fl.x, fl.y};
@@ -1405,6 +1429,7 @@ __global__ void __launch_bounds__(RED_THREADS, 4) cg_update_pair_kernel(double* 
   for (long p = long(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += long(gridDim.x) * blockDim.x) {
     const uint2 fl = reinterpret_cast<const uint2*>(flags)[p];
     const bool act[2] = {(fl.x & ACTIVE_NODE) != 0, (fl.y & ACTIVE_NODE) != 0};
+    if (!(act[0] || act[1])) continue;
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
       const long o = v * (N >> 1) + p;
@@ -1440,24 +1465,32 @@ __global__ void __launch_bounds__(RED_THREADS, 4) cg_update_pair_kernel(double* 
   }
 }
 
-// axpy_kernel over pairs (n even), grid-stride
+// dst = c*x + y over node pairs of three-component fields [3][N] (16-byte loads
+// and stores), grid-stride; pairs of inactive nodes are skipped (both operands
+// are zero there)
 __global__ void __launch_bounds__(RED_THREADS, 4) axpy_pair_kernel(double* dst, const double* __restrict__ scal, int slot,
-                                                               const double* xv, const double* yv, long n,
-                                                               int float_round) {
+                                                               const double* xv, const double* yv, long N,
+                                                               int float_round, const uint32_t* __restrict__ flags) {
   pdl_wait();
   const double c = scal[slot];
-  const long P = n >> 1;
+  const long P = N >> 1;
   for (long p = long(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += long(gridDim.x) * blockDim.x) {
-    const double2 a = reinterpret_cast<const double2*>(xv)[p], b = reinterpret_cast<const double2*>(yv)[p];
-    double2 o;
-    if (float_round) {
-      o.x = double(__fadd_rn(__fmul_rn(float(c), float(a.x)), float(b.x)));
-      o.y = double(__fadd_rn(__fmul_rn(float(c), float(a.y)), float(b.y)));
-    } else {
-      o.x = c * a.x + b.x;
-      o.y = c * a.y + b.y;
+    const uint2 fl = reinterpret_cast<const uint2*>(flags)[p];
+    if (!((fl.x | fl.y) & ACTIVE_NODE)) continue;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const long o = v * P + p;
+      const double2 a = reinterpret_cast<const double2*>(xv)[o], b = reinterpret_cast<const double2*>(yv)[o];
+      double2 r;
+      if (float_round) {
+        r.x = double(__fadd_rn(__fmul_rn(float(c), float(a.x)), float(b.x)));
+        r.y = double(__fadd_rn(__fmul_rn(float(c), float(a.y)), float(b.y)));
+      } else {
+        r.x = c * a.x + b.x;
+        r.y = c * a.y + b.y;
+      }
+      reinterpret_cast<double2*>(dst)[o] = r;
     }
-    reinterpret_cast<double2*>(dst)[p] = o;
   }
 }
 
@@ -1767,14 +1800,112 @@ void Solver::record_iteration() {
   Level<double>& l0 = *L64[0];
   const int parts = precondition();                                      // q = z, rho partials
   launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, parts, 0, scal.p, 0);  // rho, beta
-  launch(axpy_pair_kernel, PAIR_BLOCKS, RED_THREADS, 0, s.p, scal.p, 4, s.p, q.p, 3 * N0(),
-         round_ref() ? 1 : 0);                                           // s = beta*s + z
+  launch(axpy_pair_kernel, PAIR_BLOCKS, RED_THREADS, 0, s.p, scal.p, 4, s.p, q.p, N0(),
+         round_ref() ? 1 : 0, l0.flags.p);                               // s = beta*s + z
   level0<double, OP_KUP>(s.p, nullptr, q.p);                             // q = K s, Project, s.q partials
   launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, l0.nb, 0, scal.p, 1);       // alpha
   launch(cg_update_pair_kernel, PAIR_BLOCKS, RED_THREADS, 0, x.p, s.p, f.p, q.p, scal.p, l0.flags.p, l0.N,
          round_ref() ? 1 : 0, (mixed() && !P.disable_mg) ? L32[0]->b.p : (float*)nullptr, red.p);
   launch(finish_reduce_kernel, 1, FIN_THREADS, 0, red.p, PAIR_BLOCKS, 1, scal.p, 4);  // |r|_inf, rho_old
   launch_counter += 4;
+}
+
+// The device-side PCG loop's record, at the head of Solver::loop_buf, followed
+// by LOOP_HIST residual norms (the history of iterations base .. limit).
+constexpr int LOOP_REC = 6, LOOP_HIST = 1024;  // in doubles
+struct PcgLoop {
+  double tol, norm;
+  int it, maxit, limit, base, stopped, breakdown;
+};
+static_assert(sizeof(PcgLoop) <= LOOP_REC * sizeof(double), "loop record size");
+
+// The convergence test of the device-side PCG loop (CONJUGATE_GRADIENT.cpp:32-40),
+// run before the first iteration and at the end of every iteration: records
+// |r|_inf of iteration `it`; stops on convergence, at the iteration cap, on a
+// breakdown (a non-positive s.q, CONJUGATE_GRADIENT.cpp:49-52) or on a
+// non-finite norm; otherwise counts the iteration and keeps the WHILE node
+// running, up to `limit`, where the host takes the history out and relaunches.
+// The loop therefore ends after at most limit - base iterations.
+__global__ void pcg_check_kernel(const double* __restrict__ scal, double* loop, cudaGraphConditionalHandle h) {
+  pdl_wait();
+  PcgLoop* st = reinterpret_cast<PcgLoop*>(loop);
+  const int it = st->it;
+  const double norm = scal[3];
+  loop[LOOP_REC + (it - st->base)] = norm;
+  const bool breakdown = scal[7] != 0;
+  const bool stop = breakdown || !isfinite(norm) || norm <= st->tol || it >= st->maxit;
+  const bool more = !stop && it < st->limit;
+  if (more) st->it = it + 1;
+  st->norm = norm;
+  st->stopped = stop;
+  st->breakdown = breakdown;
+  cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+// Builds loop_graph once per operator set: [test] -> WHILE([iteration, test]).
+// Returns false, and remembers why, where the runtime refuses conditional nodes.
+bool Solver::build_loop_graph() {
+  if (loop_graph) return true;
+  if (loop_unavailable) return false;
+  if (!loop_buf.p) loop_buf.alloc(LOOP_REC + LOOP_HIST);
+  if (!h_loop) SGS_CUDA(cudaMallocHost(&h_loop, (LOOP_REC + LOOP_HIST) * sizeof(double)));
+  cudaGraph_t g = nullptr;
+  bool capturing = false;
+  auto give_up = [&](const char* what, cudaError_t e) {
+    if (capturing) {
+      cudaGraph_t partial = nullptr;
+      cudaStreamEndCapture(stream, &partial);
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    loop_unavailable = true;
+    loop_note = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+  };
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e != cudaSuccess) return give_up("cudaGraphCreate", e);
+  cudaGraphConditionalHandle h = 0;
+  e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return give_up("cudaGraphConditionalHandleCreate", e);
+  // the test before the first iteration
+  e = cudaStreamBeginCaptureToGraph(stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return give_up("cudaStreamBeginCaptureToGraph", e);
+  capturing = true;
+  launch(pcg_check_kernel, 1, 1, 0, (const double*)scal.p, loop_buf.p, h);
+  e = cudaStreamEndCapture(stream, &g);
+  capturing = false;
+  if (e != cudaSuccess) return give_up("cudaStreamEndCapture", e);
+  size_t n = 0;
+  SGS_CUDA(cudaGraphGetNodes(g, nullptr, &n));
+  std::vector<cudaGraphNode_t> deps(n);
+  SGS_CUDA(cudaGraphGetNodes(g, deps.data(), &n));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  e = cudaGraphAddNode(&wnode, g, deps.data(), n, &cp);
+  if (e != cudaSuccess) return give_up("cudaGraphAddNode (WHILE)", e);
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return give_up("cudaStreamBeginCaptureToGraph (body)", e);
+  capturing = true;
+  const long before = launch_counter;
+  record_iteration();
+  launches_per_iteration = launch_counter - before;
+  launch(pcg_check_kernel, 1, 1, 0, (const double*)scal.p, loop_buf.p, h);
+  launch_counter += 2;  // the two tests
+  e = cudaStreamEndCapture(stream, &body);
+  capturing = false;
+  if (e != cudaSuccess) return give_up("cudaStreamEndCapture (body)", e);
+  e = cudaGraphInstantiate(&loop_graph, g, 0);
+  if (e != cudaSuccess) {
+    loop_graph = nullptr;
+    return give_up("cudaGraphInstantiate", e);
+  }
+  SGS_CUDA(cudaGraphDestroy(g));
+  return true;
 }
 
 void Solver::solve() {
@@ -1847,48 +1978,76 @@ void Solver::solve() {
   project_null<double>(l0, f.p);
   linf(f.p, nullptr);
   stage_residual();
-  // capture one iteration as a CUDA graph (not with an inner bottom solve,
-  // whose iteration count is decided on the host)
+  // The loop on the device: one graph launch runs iterations until the test
+  // stops them (or pauses at the history buffer's end).  With an inner bottom
+  // solve, whose iteration count is decided on the host, or without
+  // conditional nodes: one graph launch per iteration after a host-side test.
   long capture_launches = 0;
   const bool use_graph = !inner();
-  if (use_graph && !iter_graph) {
-    cudaGraph_t g;
-    long before = launch_counter;
-    SGS_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    record_iteration();
-    SGS_CUDA(cudaStreamEndCapture(stream, &g));
-    SGS_CUDA(cudaGraphInstantiate(&iter_graph, g, 0));
-    SGS_CUDA(cudaGraphDestroy(g));
-    launches_per_iteration = launch_counter - before;
-    capture_launches = launches_per_iteration;
-  }
-  for (int it = 0;; ++it) {
-    SGS_CUDA(cudaMemcpyAsync(h_scal, scal.p, 16 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    g_d2h_bytes += 16 * sizeof(double);
-    SGS_CUDA(cudaStreamSynchronize(stream));
-    const double norm = h_scal[3];
-    history.push_back(norm);
-    if (h_scal[7] != 0) {
-      iterations = it;
-      final_residual = norm;
-      throw CudaError("CG detected an indefinite or singular operator", SGS_ERR_BREAKDOWN);
+  int it = 0;
+  double norm = 0;
+  bool breakdown = false;
+  const int max_iterations = std::max(0, P.max_iterations);
+  const long before_build = launch_counter;
+  if (use_graph && build_loop_graph()) {
+    capture_launches = launch_counter - before_build;
+    PcgLoop* st = reinterpret_cast<PcgLoop*>(h_loop);
+    for (;;) {
+      const int hist = std::max(2, std::min(loop_history, LOOP_HIST));  // >= 2: every launch makes progress
+      *st = PcgLoop{tol, 0.0, it, max_iterations, std::min(max_iterations, it + hist - 1), it, 0, 0};
+      const int it0 = it, span = st->limit - it0 + 1;
+      SGS_CUDA(cudaMemcpyAsync(loop_buf.p, h_loop, LOOP_REC * sizeof(double), cudaMemcpyHostToDevice, stream));
+      SGS_CUDA(cudaGraphLaunch(loop_graph, stream));
+      SGS_CUDA(cudaMemcpyAsync(h_loop, loop_buf.p, (LOOP_REC + span) * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      g_d2h_bytes += (LOOP_REC + span) * sizeof(double);
+      SGS_CUDA(cudaStreamSynchronize(stream));
+      it = st->it;
+      solve_launches += 1 + long(it - it0) * (launches_per_iteration + 1);
+      // a paused launch re-tests its last iteration at the next launch
+      const int recorded = it - it0 + (st->stopped ? 1 : 0);
+      for (int k = 0; k < recorded; ++k) history.push_back(h_loop[LOOP_REC + k]);
+      if (st->stopped) {
+        norm = st->norm;
+        breakdown = st->breakdown != 0;
+        break;
+      }
     }
-    if (!std::isfinite(norm)) {
-      iterations = it;
-      throw CudaError("non-finite residual", SGS_ERR_BREAKDOWN);
-    }
-    if (norm <= tol || it == P.max_iterations) {
-      iterations = it;
-      final_residual = norm;
-      break;
-    }
-    if (use_graph) {
-      SGS_CUDA(cudaGraphLaunch(iter_graph, stream));
-      solve_launches += launches_per_iteration;
-    } else {
+  } else {
+    capture_launches = launch_counter - before_build;  // a refused loop graph's capture
+    if (use_graph && !iter_graph) {
+      cudaGraph_t g;
+      long before = launch_counter;
+      SGS_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       record_iteration();
+      SGS_CUDA(cudaStreamEndCapture(stream, &g));
+      SGS_CUDA(cudaGraphInstantiate(&iter_graph, g, 0));
+      SGS_CUDA(cudaGraphDestroy(g));
+      launches_per_iteration = launch_counter - before;
+      capture_launches += launches_per_iteration;
+    }
+    for (;; ++it) {
+      SGS_CUDA(cudaMemcpyAsync(h_scal, scal.p, 16 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      g_d2h_bytes += 16 * sizeof(double);
+      SGS_CUDA(cudaStreamSynchronize(stream));
+      norm = h_scal[3];
+      history.push_back(norm);
+      breakdown = h_scal[7] != 0;
+      if (breakdown || !std::isfinite(norm) || norm <= tol || it >= max_iterations) break;
+      if (use_graph) {
+        SGS_CUDA(cudaGraphLaunch(iter_graph, stream));
+        solve_launches += launches_per_iteration;
+      } else {
+        record_iteration();
+      }
     }
   }
+  iterations = it;
+  if (breakdown) {
+    final_residual = norm;
+    throw CudaError("CG detected an indefinite or singular operator", SGS_ERR_BREAKDOWN);
+  }
+  if (!std::isfinite(norm)) throw CudaError("non-finite residual", SGS_ERR_BREAKDOWN);
+  final_residual = norm;
   launch(add_kernel, blocks_for(n3, 256), 256, 0, x.p, ubk.p, n3);
   ++launch_counter;
   SGS_CUDA(cudaEventRecord(ev_end, stream));
@@ -1909,6 +2068,41 @@ void Solver::solve() {
 static std::mutex g_staging_mutex;
 static char* g_staging = nullptr;
 constexpr size_t STAGING_HALF = size_t(32) << 20;
+
+// Chunks of the source go into one half of the staging buffer (copied by the
+// host threads) while the other half's copy to the device runs; the call ends
+// when the last copy has left the buffer, so the next user finds it free.
+void staged_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return;
+  std::lock_guard<std::mutex> lock(g_staging_mutex);
+  if (!g_staging) SGS_CUDA(cudaMallocHost(reinterpret_cast<void**>(&g_staging), 2 * STAGING_HALF));
+  cudaEvent_t done[2];
+  SGS_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+  SGS_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+  const size_t nchunks = (bytes + STAGING_HALF - 1) / STAGING_HALF;
+  cudaError_t err = cudaSuccess;
+  for (size_t c = 0; c < nchunks && err == cudaSuccess; ++c) {
+    const size_t off = c * STAGING_HALF, n = std::min(STAGING_HALF, bytes - off);
+    char* half = g_staging + (c & 1) * STAGING_HALF;
+    if (c >= 2) err = cudaEventSynchronize(done[c & 1]);  // that half's previous copy has left
+    if (err != cudaSuccess) break;
+    const char* from = static_cast<const char*>(src) + off;
+    const long pieces = long((n + (size_t(1) << 20) - 1) >> 20);
+#pragma omp parallel for schedule(static)
+    for (long k = 0; k < pieces; ++k) {
+      const size_t a = size_t(k) << 20;
+      std::memcpy(half + a, from + a, std::min(size_t(1) << 20, n - a));
+    }
+    err = cudaMemcpyAsync(static_cast<char*>(dst) + off, half, n, cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess) err = cudaEventRecord(done[c & 1], s);
+  }
+  const cudaError_t e0 = cudaEventSynchronize(done[0]), e1 = cudaEventSynchronize(done[1]);
+  cudaEventDestroy(done[0]);
+  cudaEventDestroy(done[1]);
+  SGS_CUDA(err);
+  SGS_CUDA(e0);
+  SGS_CUDA(e1);
+}
 
 void Solver::pack_outputs(void* disp, size_t pitch) {
   const long nin = long(P.in_block.size());
@@ -2138,10 +2332,7 @@ void Solver::design_refresh(const double* rho_s) {
   SGS_CUDA(cudaGetLastError());
   if (mixed())
     launch(convert_kernel<float, double>, blocks_for(long(P.E.size()), 256), 256, 0, E32.p, E64.p, long(P.E.size()));
-  if (iter_graph) {
-    SGS_CUDA(cudaGraphExecDestroy(iter_graph));
-    iter_graph = nullptr;
-  }
+  drop_graphs();
   build_operators();
   build_bottom();
   SGS_CUDA(cudaStreamSynchronize(stream));
@@ -2393,6 +2584,9 @@ static int session_from_inputs(const FEMInputs& in, int precision, sgs_session**
   h->solver->P.max_iterations = 500;  // the reference hard-codes 500 (SPGrid_CPU_Solver.cpp:326)
   if (in.get_int("sgs_honor_max_iterations", 0)) h->solver->P.max_iterations = in.krylov.max_iterations;
   h->solver->tensor_cores = in.get_int("sgs_tensor_cores", 0) != 0;
+  h->solver->loop_unavailable = in.get_int("sgs_device_loop", 1) == 0;
+  if (h->solver->loop_unavailable) h->solver->loop_note = "sgs_device_loop = 0";
+  h->solver->loop_history = in.get_int("sgs_loop_history", 1024);
   if (precision == SGS_HOST_SETUP_ONLY) {  // inspection of the host-side hierarchy, no device work
     h->solver->precision = precision;
     *out = h.release();
@@ -3007,6 +3201,46 @@ SGS_API int sgs_level_stencils(sgs_session* h, int level, double* out, uint32_t*
 }
 
 // Drop-in entry (see include/spgrid_fem.h).
+// The output blob of a large fem_solve, allocated before the solve with its
+// pages touched by a helper thread while the GPU solves (the host only waits
+// then): the displacement records are later copied into resident memory
+// instead of faulting it in page by page.  Blobs under 64 MiB are allocated
+// when they are encoded, as before.
+class OutputBlob {
+ public:
+  explicit OutputBlob(size_t bytes) : capacity_(bytes) {
+    if (bytes < (size_t(64) << 20)) return;
+    worker_ = std::thread([this] {
+      char* p = new (std::nothrow) char[capacity_];
+      if (p) {
+        const uintptr_t lo = reinterpret_cast<uintptr_t>(p), hi = lo + capacity_, huge = uintptr_t(2) << 20;
+        const uintptr_t a = (lo + huge - 1) & ~(huge - 1);
+        if (a < hi) madvise(reinterpret_cast<void*>(a), hi - a, MADV_HUGEPAGE);  // advice only
+        const long pages = long((capacity_ + 4095) / 4096);
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < pages; ++i) p[size_t(i) * 4096] = 0;
+      }
+      buffer_ = p;
+    });
+  }
+  OutputBlob(const OutputBlob&) = delete;
+  OutputBlob& operator=(const OutputBlob&) = delete;
+  ~OutputBlob() { delete[] take(); }
+  // the buffer (nullptr if none), owned by the caller from here on
+  char* take() {
+    if (worker_.joinable()) worker_.join();
+    char* p = buffer_;
+    buffer_ = nullptr;
+    return p;
+  }
+  size_t capacity() const { return capacity_; }
+
+ private:
+  size_t capacity_;
+  char* buffer_ = nullptr;
+  std::thread worker_;
+};
+
 SGS_API void fem_solve(void* input, void* output) {
   if (!output) return;
   void** out_ptr = reinterpret_cast<void**>(output);
@@ -3047,6 +3281,10 @@ SGS_API void fem_solve(void* input, void* output) {
         h->solver->forced_reuse = in.get_int("forced_reuse", 0) != 0;
       }
       sgs_stats st{};
+      // an upper bound of the output blob: the displacement grid (payload and
+      // block bases), the residual history and 1 MiB for the rest
+      OutputBlob blob_memory(in.density.num_blocks() * (256 * sizeof(double) + 3 * sizeof(int32_t)) +
+                             size_t(std::max(0, h->solver->P.max_iterations) + 2) * sizeof(double) + (size_t(1) << 20));
       rc = sgs_solve(h, 0, 0, &st);
       if (state) {
         outs.extra_ints["warm_start_reused"] = h->solver->warm_reused ? 1 : 0;
@@ -3067,6 +3305,7 @@ SGS_API void fem_solve(void* input, void* output) {
       }
       outs.residuals = h->solver->history;
       outs.extra_ints["iterations"] = st.iterations;
+      outs.extra_ints["device_loop"] = h->solver->loop_graph ? 1 : 0;
       outs.extra_doubles["initial_residual"] = st.initial_residual;
       outs.extra_doubles["final_residual"] = st.final_residual;
       outs.extra_doubles["setup_seconds"] = st.setup_seconds;
@@ -3112,7 +3351,8 @@ SGS_API void fem_solve(void* input, void* output) {
         char* blob = nullptr;
         try {
           Solver* S = h->solver.get();
-          blob = encode_outputs(outs, nullptr, [S](uint8_t* p, size_t pitch, size_t) { S->pack_outputs(p, pitch); });
+          blob = encode_outputs(outs, nullptr, [S](uint8_t* p, size_t pitch, size_t) { S->pack_outputs(p, pitch); },
+                                blob_memory.take(), blob_memory.capacity());
         } catch (const CudaError& e) {
           outs.displacements.base.clear();
           outs.success = false;

@@ -311,9 +311,17 @@ void patch_output_double(char* blob, const FEMOutputs& o, const std::string& key
 }
 
 char* encode_outputs(const FEMOutputs& o, size_t* length, const GridFill& fill) {
+  return encode_outputs(o, length, fill, nullptr, 0);
+}
+
+char* encode_outputs(const FEMOutputs& o, size_t* length, const GridFill& fill, char* buffer, size_t capacity) {
   Writer sizer;
   write_outputs(sizer, o, &fill);
-  char* out = new char[sizer.size()];
+  char* out = buffer;
+  if (!out || capacity < sizer.size()) {
+    delete[] buffer;
+    out = new char[sizer.size()];
+  }
   try {
     Writer w(reinterpret_cast<uint8_t*>(out));
     write_outputs(w, o, &fill);

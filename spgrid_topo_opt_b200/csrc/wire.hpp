@@ -135,6 +135,10 @@ char* encode_outputs(const FEMOutputs& o, size_t* length);
 // fill(first record's payload, record pitch in bytes, record count).
 using GridFill = std::function<void(uint8_t*, size_t, size_t)>;
 char* encode_outputs(const FEMOutputs& o, size_t* length, const GridFill& fill);
+// The same into `buffer` (allocated with new char[] by the caller, ownership
+// passes to the result) when its `capacity` holds the blob, else into a new one
+// (and `buffer` is released).
+char* encode_outputs(const FEMOutputs& o, size_t* length, const GridFill& fill, char* buffer, size_t capacity);
 // Overwrite extra_doubles[key] (present in o when it was encoded) in the blob.
 void patch_output_double(char* blob, const FEMOutputs& o, const std::string& key, double value);
 // Encode inputs (used by tests and tools that drive the library from C++).
