@@ -179,8 +179,12 @@ void flag_nodes(HostLevel& L) {
       if (reach[size_t(b)] >> c & 1)
         L.touch(L.coords[3 * b] + (c >> 2) * BLK_X, L.coords[3 * b + 1] + ((c >> 1) & 1) * BLK_Y,
                 L.coords[3 * b + 2] + (c & 1) * BLK_Z);
+  // The node bits are ORed into the flags in place: other threads read only the
+  // cell bits of a word, which these writes leave as they are (relaxed atomic
+  // loads and stores, one writer per word).
   const int nall = int(L.coords.size() / 3);
-  HostBuf<uint32_t> add(size_t(nall) * NODES_PER_BLOCK);  // every entry is written below
+  uint32_t* flags = L.flags.data();
+  auto cell_bits = [&](size_t i) { return __atomic_load_n(&flags[i], __ATOMIC_RELAXED); };
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nall; ++b) {
     // the blocks at offsets -(c>>2, (c>>1)&1, c&1) that hold a node's cells; only
@@ -191,36 +195,40 @@ void flag_nodes(HostLevel& L) {
       const int nb = c ? L.block_at(bx - (c >> 2) * BLK_X, by - ((c >> 1) & 1) * BLK_Y, bz - (c & 1) * BLK_Z) : b;
       src[c] = (nb >= 0 && nb < L.nb) ? nb : -1;
     }
-    const uint32_t* own = src[0] >= 0 ? &L.flags[size_t(src[0]) * NODES_PER_BLOCK] : nullptr;
-    uint32_t* out = &add[size_t(b) * NODES_PER_BLOCK];
+    const size_t own = src[0] >= 0 ? size_t(src[0]) * NODES_PER_BLOCK : ~size_t(0);
+    const size_t out = size_t(b) * NODES_PER_BLOCK;
     for (int e = 0; e < NODES_PER_BLOCK; ++e) {
       const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
       uint32_t acc = 0;
       if (x && y && z) {  // all 8 cells in this block, at slot offsets 0, 1, 8, 9, 32, 33, 40, 41 below
-        if (own)
-          acc = own[e] | own[e - 1] | own[e - 8] | own[e - 9] | own[e - 32] | own[e - 33] | own[e - 40] | own[e - 41];
+        if (own != ~size_t(0)) {
+          const size_t o = own + size_t(e);
+          acc = cell_bits(o) | cell_bits(o - 1) | cell_bits(o - 8) | cell_bits(o - 9) | cell_bits(o - 32) |
+                cell_bits(o - 33) | cell_bits(o - 40) | cell_bits(o - 41);
+        }
       } else {
         for (int c = 0; c < 8; ++c) {
           const int cx = x - (c >> 2), cy = y - ((c >> 1) & 1), cz = z - (c & 1);
           const int nb = src[(cx < 0 ? 4 : 0) | (cy < 0 ? 2 : 0) | (cz < 0 ? 1 : 0)];
-          if (nb >= 0) acc |= L.flags[size_t(nb) * NODES_PER_BLOCK + node_slot(cx, cy, cz)];
+          if (nb >= 0) acc |= cell_bits(size_t(nb) * NODES_PER_BLOCK + node_slot(cx, cy, cz));
         }
       }
-      out[e] = (acc & CELL) >> 4;
+      const uint32_t add = (acc & CELL) >> 4;
+      if (add) __atomic_store_n(&flags[out + size_t(e)], cell_bits(out + size_t(e)) | add, __ATOMIC_RELAXED);
     }
   }
-#pragma omp parallel for schedule(static)
-  for (long i = 0; i < long(add.size()); ++i) L.flags[size_t(i)] |= add[size_t(i)];
 }
 
-void flag_boundary(HostLevel& L, int band = 3) {
+using Rings = std::vector<std::array<int, 27>>;
+
+void flag_boundary(HostLevel& L, Rings& rings, int band = 3) {
   // Flaging.h:93-147: three Jacobi-style passes growing a band of active,
   // non-Dirichlet nodes around the Dirichlet nodes.  A pass can only reach
   // blocks next to a block that already holds a Dirichlet or band node, so
   // each pass visits those blocks alone.
   const uint32_t SEED = F_DIRICHLET_NODE | F_BOUNDARY_NODE;
   const int nall = int(L.coords.size() / 3);
-  std::vector<std::array<int, 27>> rings(size_t(L.nb));
+  rings.resize(size_t(L.nb));  // every entry is written below
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < L.nb; ++b) block_ring(L, b, rings[size_t(b)].data());
   auto flag_at = [&](const int* ring, int x, int y, int z) -> uint32_t {
@@ -282,7 +290,9 @@ void flag_boundary(HostLevel& L, int band = 3) {
       }
 }
 
-void finish_level(HostLevel& L) {
+// rings: the 27 blocks around each active block (flag_boundary's), of which
+// the active ones make the neighbour table
+void finish_level(HostLevel& L, const Rings& rings) {
   // Dirichlet node lists in ascending node order: per-block counts, a prefix
   // over the blocks, then a parallel fill
   std::vector<int32_t> cnt(size_t(L.nb) * 3, 0);
@@ -308,14 +318,13 @@ void finish_level(HostLevel& L) {
       for (int v = 0; v < 3; ++v)
         if (f & (F_DIRICHLET_NODE_X << v)) L.dirichlet[v][size_t(cnt[size_t(b) * 3 + v]++)] = b * NODES_PER_BLOCK + e;
     }
-  L.nbr.assign(size_t(L.nb) * 27, -1);
+  L.nbr.resize(size_t(L.nb) * 27);
 #pragma omp parallel for schedule(static)
-  for (int b = 0; b < L.nb; ++b) {
-    const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
-    for (int d = 0; d < 27; ++d)
-      L.nbr[size_t(b) * 27 + d] = L.active_block_at(bx + (d / 9 - 1) * BLK_X, by + ((d / 3) % 3 - 1) * BLK_Y,
-                                                    bz + (d % 3 - 1) * BLK_Z);
-  }
+  for (int b = 0; b < L.nb; ++b)
+    for (int d = 0; d < 27; ++d) {
+      const int nb = rings[size_t(b)][size_t(d)];
+      L.nbr[size_t(b) * 27 + d] = nb < L.nb ? nb : -1;  // ghosts are not neighbours
+    }
 }
 
 }  // namespace
@@ -600,8 +609,11 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   for (int lev = 1; lev < P.mg_levels; ++lev) P.levels.push_back(coarsen(P.levels[lev - 1]));
   phase_done(1);
   for (auto& L : P.levels) flag_nodes(L);
-  for (auto& L : P.levels) flag_boundary(L);
-  for (auto& L : P.levels) finish_level(L);
+  {
+    std::vector<Rings> rings(P.levels.size());
+    for (size_t l = 0; l < P.levels.size(); ++l) flag_boundary(P.levels[l], rings[l]);
+    for (size_t l = 0; l < P.levels.size(); ++l) finish_level(P.levels[l], rings[l]);
+  }
   phase_done(2);
   // levels below a bottom too large for the dense inverse: the bottom is then
   // solved by CG with V-cycles over them (same coarsening rule, Galerkin
@@ -615,8 +627,9 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
     while (P.levels.size() < 7 && 3 * active_nodes(P.levels.back()) > P.dense_bottom_max) {
       HostLevel L = coarsen(P.levels.back());
       flag_nodes(L);
-      flag_boundary(L);
-      finish_level(L);
+      Rings rings;
+      flag_boundary(L, rings);
+      finish_level(L, rings);
       P.levels.push_back(std::move(L));
     }
   }

@@ -107,6 +107,58 @@ __global__ void __launch_bounds__(256) galerkin_cell_kernel(int ncells, const in
   }
 }
 
+// Cell matrices of the next coarser level from this level's: a coarse cell
+// covers 2x2x2 cells of the finer level (child d at finer cell 2c - (4,4,8) + d),
+// and the trilinear basis of its corners restricted to a child is the child's
+// basis times w_d[i][a], the weight of coarse corner a at child corner i (a
+// product of 0, 1/2, 1 per axis, exact).  So
+//     K_C[(a,v),(b,w)] = sum_d sum_ij w_d[i][a] w_d[j][b] K_d[(i,v),(j,w)],
+// which equals the sum over the finest cells of galerkin_cell_kernel up to
+// rounding, at 8 children instead of 8^depth positions per coarse cell.  One
+// CTA of 576 threads per coarse cell, one output entry per thread, children in
+// fixed order.
+__global__ void __launch_bounds__(576) galerkin_coarsen_kernel(const int* __restrict__ ccoord, GridView gf,
+                                                              const int* __restrict__ fine_cell_of_slot,
+                                                              const double* __restrict__ Cf, double* __restrict__ Cc) {
+  __shared__ double sK[8][576];
+  __shared__ double sw[8][64];  // sw[d][i * 8 + a]
+  __shared__ int child[8];
+  const int cell = blockIdx.x, t = threadIdx.x;
+  if (t < 8) {
+    const int fx = 2 * ccoord[3 * cell] - 4 + ((t >> 2) & 1), fy = 2 * ccoord[3 * cell + 1] - 4 + ((t >> 1) & 1),
+              fz = 2 * ccoord[3 * cell + 2] - 8 + (t & 1);
+    const long n = gf.node(fx, fy, fz);
+    child[t] = n >= 0 ? fine_cell_of_slot[n] : -1;
+  }
+  if (t < 512) {
+    const int d = t >> 6, i = (t >> 3) & 7, a = t & 7;
+    double w = 1;
+    for (int ax = 0; ax < 3; ++ax) {
+      const int sh = 2 - ax;
+      const double pos = 0.5 * double(((d >> sh) & 1) + ((i >> sh) & 1));  // child corner in the coarse cell
+      w *= ((a >> sh) & 1) ? pos : 1 - pos;
+    }
+    sw[d][i * 8 + a] = w;
+  }
+  __syncthreads();
+  for (int d = 0; d < 8; ++d) sK[d][t] = child[d] >= 0 ? Cf[long(child[d]) * 576 + t] : 0.0;
+  __syncthreads();
+  const int a = t / 72, b = (t / 9) & 7, m = t % 9;
+  double acc = 0;
+  for (int d = 0; d < 8; ++d) {
+    if (child[d] < 0) continue;
+    for (int i = 0; i < 8; ++i) {
+      const double wa = sw[d][i * 8 + a];
+      if (wa == 0) continue;
+      for (int j = 0; j < 8; ++j) {
+        const double wab = wa * sw[d][j * 8 + b];
+        if (wab != 0) acc = __fma_rn(wab, sK[d][(i * 8 + j) * 9 + m], acc);
+      }
+    }
+  }
+  Cc[long(cell) * 576 + t] = acc;
+}
+
 // Node stencils from the cell matrices: entry (q, v, w) sums the (corner, neighbour)
 // blocks of the incident cells in a fixed order; spoke q is active when any of
 // those blocks has a non-zero entry (Galerkin_Coarsen.h:79-93).  One CTA per node.

@@ -560,6 +560,12 @@ class Solver {
     // (its bottom is level 0, factored from the depth-0 stencil as in
     // Multigrid_Hierarchy.h:215-226); the inner-solve levels are all >= them
     const int first = (nout() == 1) ? 0 : P.explicit_level;
+    // the previous level's cell matrices: the next level's come from them
+    // (galerkin_coarsen_kernel) except in the reference-rounding mode, which
+    // sums every level from the finest cells as the reference does
+    DevBuf<double> prev_cellmat;
+    DevBuf<int32_t> prev_cell;
+    int prev_lev = -1;
     for (int lev = first; lev < n; ++lev) {
       Level<double>& d = *L64[lev];
       if (lev > 6) throw CudaError("multigrid depth above 6 is not supported", SGS_ERR_INPUT);
@@ -567,40 +573,64 @@ class Solver {
       const int side = 1 << lev;
       const long npos = long(side) * side * side;
       // active coarse cells (the only ones with finest material) and their finest origin
-      std::vector<int32_t> origin, cell_of_slot(size_t(d.N), -1);
+      std::vector<int32_t> origin, ccoord, cell_of_slot(size_t(d.N), -1);
       int ncells = 0;
       const int B[3] = {BLK_X, BLK_Y, BLK_Z};
       for (long slot = 0; slot < d.N; ++slot) {
         if (!(h.flags[slot] & F_ACTIVE_CELL)) continue;
         const int b = int(slot / NODES_PER_BLOCK), e = int(slot % NODES_PER_BLOCK);
         const int c[3] = {h.coords[3 * b] + (e >> 5), h.coords[3 * b + 1] + ((e >> 3) & 3), h.coords[3 * b + 2] + (e & 7)};
-        for (int v = 0; v < 3; ++v) origin.push_back(side * c[v] - (side - 1) * B[v]);
+        for (int v = 0; v < 3; ++v) {
+          origin.push_back(side * c[v] - (side - 1) * B[v]);
+          ccoord.push_back(c[v]);
+        }
         cell_of_slot[slot] = ncells++;
       }
+      const bool recursive = !round_ref() && prev_lev == lev - 1 && lev > 0;
       d.A.alloc(243 * size_t(d.N));
       d.A.zero(stream);
       d.spokes.alloc(size_t(d.N));
       d.spokes.zero(stream);
       d.has_matrix = true;
       if (ncells > 0) {
-        DevBuf<double> table, cellmat;
-        DevBuf<int32_t> dorigin, dcell;
-        table.alloc(size_t(npos) * 576);
-        galerkin_table_kernel<<<blocks_for(npos * 64, 128), 128, 0, stream>>>(lev, table.p);
-        dorigin.upload(origin, stream);
+        DevBuf<double> cellmat;
+        DevBuf<int32_t> dcell;
         dcell.upload(cell_of_slot, stream);
         cellmat.alloc(size_t(ncells) * 576);
-        const size_t smem = 2 * GT * 65 * sizeof(double);
-        SGS_CUDA(cudaFuncSetAttribute(galerkin_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        galerkin_cell_kernel<<<dim3(576 / GT, (ncells + GT - 1) / GT), 256, smem, stream>>>(
-            ncells, dorigin.p, lev, L64[0]->grid, E64.p, table.p, cellmat.p);
+        if (recursive) {
+          DevBuf<int32_t> dcc;
+          dcc.upload(ccoord, stream);
+          galerkin_coarsen_kernel<<<unsigned(ncells), 576, 0, stream>>>(dcc.p, L64[lev - 1]->grid, prev_cell.p,
+                                                                     prev_cellmat.p, cellmat.p);
+          SGS_CUDA(cudaGetLastError());
+          SGS_CUDA(cudaStreamSynchronize(stream));  // dcc goes out of scope
+        } else {
+          DevBuf<double> table;
+          DevBuf<int32_t> dorigin;
+          table.alloc(size_t(npos) * 576);
+          galerkin_table_kernel<<<blocks_for(npos * 64, 128), 128, 0, stream>>>(lev, table.p);
+          dorigin.upload(origin, stream);
+          const size_t smem = 2 * GT * 65 * sizeof(double);
+          SGS_CUDA(cudaFuncSetAttribute(galerkin_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+          galerkin_cell_kernel<<<dim3(576 / GT, (ncells + GT - 1) / GT), 256, smem, stream>>>(
+              ncells, dorigin.p, lev, L64[0]->grid, E64.p, table.p, cellmat.p);
+          SGS_CUDA(cudaGetLastError());
+          SGS_CUDA(cudaStreamSynchronize(stream));  // the temporaries go out of scope
+        }
         galerkin_assemble_kernel<<<unsigned(d.N), 256, 0, stream>>>(d.coords.p, d.flags.p, dcell.p, d.grid, cellmat.p, d.A.p,
                                                                    d.spokes.p, P.dx);
         SGS_CUDA(cudaGetLastError());
         delete_dirichlet_kernel<<<blocks_for(d.N, 128), 128, 0, stream>>>(d.nb, d.coords.p, d.flags.p, d.spokes.p, d.grid,
                                                                          d.A.p, d.N);
         SGS_CUDA(cudaGetLastError());
-        SGS_CUDA(cudaStreamSynchronize(stream));  // the temporaries go out of scope
+        SGS_CUDA(cudaStreamSynchronize(stream));
+        std::swap(prev_cellmat.p, cellmat.p);
+        std::swap(prev_cellmat.n, cellmat.n);
+        std::swap(prev_cell.p, dcell.p);
+        std::swap(prev_cell.n, dcell.n);
+        prev_lev = lev;
+      } else {
+        prev_lev = -1;
       }
       if (mixed()) {
         Level<float>& m = *L32[lev];

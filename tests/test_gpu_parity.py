@@ -106,6 +106,27 @@ def test_galerkin_operators(small):
             assert _rel(ses.apply(native.OP_SMOOTH, lev, u, ub, arg=arg), ref.apply(orc.OP_SMOOTH, lev, u, ub, arg=arg)) < 1e-11
 
 
+@pytest.fixture(scope="module")
+def deep(native_lib):
+    """Six levels: in the FP64 and mixed modes the operators of levels 3-5 come
+    from the cell matrices of the level above them, while the oracle sums every
+    level from the finest cells (the reference's construction)."""
+    inp = configs.to_inputs(configs.cantilever_box(48, density=(0.2, 1.0), bottom_size=2))
+    ref = orc.Oracle(inp, mode=orc.MODE_FP64)
+    ses = native.Session(inp, precision=native.PRECISION_FP64)
+    assert ses.levels == 6
+    return inp, ref, ses
+
+
+def test_galerkin_operators_of_a_deep_hierarchy(deep):
+    _, ref, ses = deep
+    for lev in range(2, ses.levels):
+        a, sa = ses.stencils(lev)
+        b, sb = ref.stencils(lev)
+        assert _rel(a, b) < 1e-11, lev
+        assert np.array_equal(sa & 0x07FFFFFF, sb & 0x07FFFFFF), lev
+
+
 def test_bottom_solve_and_vcycle(small):
     _, ref, ses = small
     top = ses.levels - 1
