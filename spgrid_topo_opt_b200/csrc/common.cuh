@@ -87,7 +87,10 @@ struct DevBuf {
       SGS_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
     g_h2d_bytes += count * sizeof(T);
   }
-  void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
+  template <typename Alloc>
+  void upload(const std::vector<T, Alloc>& v, cudaStream_t s) {
+    upload(v.data(), v.size(), s);
+  }
   void zero(cudaStream_t s) {
     if (n) SGS_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
   }

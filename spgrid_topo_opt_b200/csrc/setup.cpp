@@ -76,8 +76,16 @@ struct Builder {
   void init(int sx, int sy, int sz) {
     L.size[0] = sx; L.size[1] = sy; L.size[2] = sz;
     L.grid[0] = sx / BLK_X + 3; L.grid[1] = sy / BLK_Y + 3; L.grid[2] = sz / BLK_Z + 3;
-    L.bgrid.assign(size_t(L.grid[0]) * L.grid[1] * L.grid[2], -1);
-    L.active_page.assign(L.bgrid.size(), 0);
+    const long ncell = long(L.grid[0]) * L.grid[1] * L.grid[2];
+    L.bgrid.resize(size_t(ncell));  // uninitialised: filled below, in parallel
+    L.active_page.resize(size_t(ncell));
+    int32_t* g = L.bgrid.data();
+    uint8_t* a = L.active_page.data();
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < ncell; ++c) {
+      g[c] = -1;
+      a[c] = 0;
+    }
   }
   bool test_page(int x, int y, int z) const {
     long c = L.cell(x, y, z);
@@ -219,7 +227,7 @@ void flag_nodes(HostLevel& L) {
   }
 }
 
-using Rings = std::vector<std::array<int, 27>>;
+using Rings = HostBuf<std::array<int, 27>>;  // every entry is written by flag_boundary
 
 void flag_boundary(HostLevel& L, Rings& rings, int band = 3) {
   // Flaging.h:93-147: three Jacobi-style passes growing a band of active,
@@ -408,17 +416,38 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
     }
     repeated = rep != 0;
   }
-  // the SIMP map of every input cell, once (fem_interface.h:343-353); the
-  // buffer is filled in parallel without a serial zero pass
-  std::unique_ptr<double[]> Ein(new double[nin * 64]);
-#pragma omp parallel for schedule(static)
-  for (long c = 0; c < long(nin) * 64; ++c) {
-    const double d = in.density.data[size_t(c)];
-    Ein[size_t(c)] = d > 0 ? (penalty ? (1 - emin) * std::pow(std::max(rho_min, d), penalty) + emin : d) : 0.0;
-  }
-  auto cell_E = [&](size_t b, int e) { return Ein[b * 64 + size_t(e)]; };
+  // The SIMP map of every input cell, once (fem_interface.h:343-353).  It goes
+  // straight to the cell's slot of the level-0 stiffness scales P.E (zero where
+  // there is no material), where every input cell has a slot of its own; when
+  // input blocks repeat, the values are kept per input cell first and the last
+  // input block's win in P.E below.
   // input cell e = i*16 + j*4 + k sits at slot offset i*32 + j*8 + k from the block's slot
   auto cell_slot = [](int e) { return (e >> 4) * 32 + ((e >> 2) & 3) * 8 + (e & 3); };
+  auto simp = [&](double d) {
+    return d > 0 ? (penalty ? (1 - emin) * std::pow(std::max(rho_min, d), penalty) + emin : d) : 0.0;
+  };
+  P.E.resize(size_t(b0.L.nb) * NODES_PER_BLOCK);
+  {
+    double* E = P.E.data();
+    const long nE = long(P.E.size());
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < nE; ++i) E[i] = 0.0;
+  }
+  std::unique_ptr<double[]> Ein;
+  if (repeated) {
+    Ein.reset(new double[nin * 64]);
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < long(nin) * 64; ++c) Ein[size_t(c)] = simp(in.density.data[size_t(c)]);
+  } else {
+#pragma omp parallel for schedule(static)
+    for (long b = 0; b < long(nin); ++b) {
+      const size_t base = size_t(in_slot[size_t(b)]);
+      for (int e = 0; e < 64; ++e) P.E[base + size_t(cell_slot(e))] = simp(in.density.data[size_t(b) * 64 + e]);
+    }
+  }
+  auto cell_E = [&](size_t b, int e) {
+    return repeated ? Ein[b * 64 + size_t(e)] : P.E[size_t(in_slot[b]) + size_t(cell_slot(e))];
+  };
   // Validate_With_Density (solver/CPU_Kernels/Validate_Blocks.h:311-335): every
   // material cell needs its +1 neighbour pages; the first failure in input order is reported.
   long first_bad = -1;
@@ -491,21 +520,14 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
     if (d.axis < 0 || d.axis > 2) return fail(4, "Dirichlet axis out of range");
   P.levels.clear();
   P.levels.push_back(std::move(b0.L));
-  // the stiffness scale of every material cell at its slot in page order (the
-  // last input block wins where blocks repeat)
-  P.E.resize(size_t(P.levels[0].nb) * NODES_PER_BLOCK);
-  {
-    double* E = P.E.data();
-    const long nE = long(P.E.size());
-#pragma omp parallel for schedule(static)
-    for (long i = 0; i < nE; ++i) E[i] = 0.0;
-  }
-#pragma omp parallel for schedule(static) if (!repeated)
-  for (long b = 0; b < long(nin); ++b) {
-    const size_t base = size_t(in_slot[size_t(b)]);
-    for (int e = 0; e < 64; ++e)
-      if (in.density.data[size_t(b) * 64 + e] > 0) P.E[base + size_t(cell_slot(e))] = cell_E(size_t(b), e);
-  }
+  // repeated input blocks: the last one's material wins, as a serial pass
+  // over the input blocks leaves it
+  if (repeated)
+    for (size_t b = 0; b < nin; ++b) {
+      const size_t base = size_t(in_slot[b]);
+      for (int e = 0; e < 64; ++e)
+        if (in.density.data[b * 64 + e] > 0) P.E[base + size_t(cell_slot(e))] = Ein[b * 64 + size_t(e)];
+    }
 
   phase_done(0);
   // ---- coarse levels (Multigrid_Hierarchy.h:122-195)

@@ -29,12 +29,12 @@ uint64_t page_key(int bi, int bj, int bk);
 struct HostLevel {
   int size[3] = {0, 0, 0};            // allocator size (nodes per axis)
   int grid[3] = {0, 0, 0};            // block-grid dims
-  std::vector<int32_t> bgrid;         // block grid -> block index (active or ghost), -1 if untouched
+  HostBuf<int32_t> bgrid;             // block grid -> block index (active or ghost), -1 if untouched
   int nb = 0;                         // active blocks (first nb entries of coords/flags)
   std::vector<int32_t> coords;        // block base coordinates, [nb_all*3]
   HostBuf<uint32_t> flags;            // [nb_all*128]
-  std::vector<uint8_t> active_page;   // per block-grid cell
-  std::vector<int32_t> nbr;           // [nb*27] neighbour block (active only) or -1
+  HostBuf<uint8_t> active_page;       // per block-grid cell
+  HostBuf<int32_t> nbr;               // [nb*27] neighbour block (active only) or -1
   std::vector<int32_t> boundary;      // active blocks with a boundary-band node
   std::array<std::vector<int32_t>, 3> dirichlet;  // node indices with a Dirichlet component
 

@@ -7,6 +7,7 @@
 // order.  The structs here keep the reference's field names.
 #pragma once
 #include <cstdint>
+#include <cstdlib>
 #include <functional>
 #include <map>
 #include <memory>
@@ -14,6 +15,8 @@
 #include <string>
 #include <utility>
 #include <vector>
+
+#include <sys/mman.h>
 
 namespace sgs {
 
@@ -37,16 +40,34 @@ struct KrylovSolverParameters {
 // `width` doubles per node, in-block index i*16 + j*4 + k.
 // A host vector whose resize leaves new elements uninitialised, so that a large
 // buffer can be zeroed and filled by parallel loops (first touch spread over
-// the threads) instead of one serial value-initialisation.
+// the threads) instead of one serial value-initialisation.  Buffers of 8 MiB
+// and more are 2 MiB aligned with transparent huge pages advised, so that the
+// first touch faults a 2 MiB page at a time where the kernel allows it.
 template <typename T>
 struct UninitAlloc : std::allocator<T> {
   template <typename U>
   struct rebind {
     using other = UninitAlloc<U>;
   };
+  static constexpr size_t LARGE = size_t(8) << 20, HUGE_PAGE = size_t(2) << 20;
   UninitAlloc() = default;
   template <typename U>
   UninitAlloc(const UninitAlloc<U>&) {}
+  T* allocate(size_t n) {
+    const size_t bytes = n * sizeof(T);
+    if (bytes < LARGE) return std::allocator<T>::allocate(n);
+    const size_t rounded = (bytes + HUGE_PAGE - 1) & ~(HUGE_PAGE - 1);
+    void* p = std::aligned_alloc(HUGE_PAGE, rounded);
+    if (!p) throw std::bad_alloc();
+    madvise(p, rounded, MADV_HUGEPAGE);  // advice only; without it the buffer works the same
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, size_t n) {
+    if (n * sizeof(T) < LARGE)
+      std::allocator<T>::deallocate(p, n);
+    else
+      std::free(p);
+  }
   template <typename U>
   void construct(U* p) noexcept {
     ::new (static_cast<void*>(p)) U;
