@@ -203,25 +203,29 @@ void flag_nodes(HostLevel& L) {
       const int nb = c ? L.block_at(bx - (c >> 2) * BLK_X, by - ((c >> 1) & 1) * BLK_Y, bz - (c & 1) * BLK_Z) : b;
       src[c] = (nb >= 0 && nb < L.nb) ? nb : -1;
     }
-    const size_t own = src[0] >= 0 ? size_t(src[0]) * NODES_PER_BLOCK : ~size_t(0);
+    // the cell bits of cells x-1..3, y-1..3, z-1..7 (index +1), then ORed along
+    // z, y and x in place: entry (x+1, y+1, z+1) ends as the OR of the 8 cells
+    // of node (x, y, z)
+    uint32_t A[5][5][9];
+    for (int ax = 0; ax < 5; ++ax)
+      for (int ay = 0; ay < 5; ++ay)
+        for (int az = 0; az < 9; ++az) {
+          const int cx = ax - 1, cy = ay - 1, cz = az - 1;
+          const int nb = src[(cx < 0 ? 4 : 0) | (cy < 0 ? 2 : 0) | (cz < 0 ? 1 : 0)];
+          A[ax][ay][az] = nb >= 0 ? cell_bits(size_t(nb) * NODES_PER_BLOCK + node_slot(cx, cy, cz)) & CELL : 0u;
+        }
+    for (int ax = 0; ax < 5; ++ax)
+      for (int ay = 0; ay < 5; ++ay)
+        for (int az = 8; az > 0; --az) A[ax][ay][az] |= A[ax][ay][az - 1];
+    for (int ax = 0; ax < 5; ++ax)
+      for (int ay = 4; ay > 0; --ay)
+        for (int az = 1; az < 9; ++az) A[ax][ay][az] |= A[ax][ay - 1][az];
+    for (int ax = 4; ax > 0; --ax)
+      for (int ay = 1; ay < 5; ++ay)
+        for (int az = 1; az < 9; ++az) A[ax][ay][az] |= A[ax - 1][ay][az];
     const size_t out = size_t(b) * NODES_PER_BLOCK;
     for (int e = 0; e < NODES_PER_BLOCK; ++e) {
-      const int x = e >> 5, y = (e >> 3) & 3, z = e & 7;
-      uint32_t acc = 0;
-      if (x && y && z) {  // all 8 cells in this block, at slot offsets 0, 1, 8, 9, 32, 33, 40, 41 below
-        if (own != ~size_t(0)) {
-          const size_t o = own + size_t(e);
-          acc = cell_bits(o) | cell_bits(o - 1) | cell_bits(o - 8) | cell_bits(o - 9) | cell_bits(o - 32) |
-                cell_bits(o - 33) | cell_bits(o - 40) | cell_bits(o - 41);
-        }
-      } else {
-        for (int c = 0; c < 8; ++c) {
-          const int cx = x - (c >> 2), cy = y - ((c >> 1) & 1), cz = z - (c & 1);
-          const int nb = src[(cx < 0 ? 4 : 0) | (cy < 0 ? 2 : 0) | (cz < 0 ? 1 : 0)];
-          if (nb >= 0) acc |= cell_bits(size_t(nb) * NODES_PER_BLOCK + node_slot(cx, cy, cz));
-        }
-      }
-      const uint32_t add = (acc & CELL) >> 4;
+      const uint32_t add = A[(e >> 5) + 1][((e >> 3) & 3) + 1][(e & 7) + 1] >> 4;
       if (add) __atomic_store_n(&flags[out + size_t(e)], cell_bits(out + size_t(e)) | add, __ATOMIC_RELAXED);
     }
   }
