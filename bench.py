@@ -254,6 +254,9 @@ def run_ours(args, rank, world):
     if args.profile_iterations > 0:
         prec = {"mixed": native.PRECISION_MIXED, "fp64": native.PRECISION_FP64,
                 "reference": native.PRECISION_REFERENCE}[args.precision]
+        # the per-iteration graph (same kernels as the device-side loop, whose
+        # WHILE node the profiler is not asked to walk)
+        inp.extra_ints["sgs_device_loop"] = 0
         with native.Session(inp, precision=prec) as ses:
             ses.solve(tolerance=TOL, max_iterations=args.profile_iterations)
             torch.cuda.synchronize()
