@@ -1006,7 +1006,6 @@ class Solver {
   // decreasing.  Nodes without unknowns keep b, as with PARDISO_Solve.
   struct InnerSolve {
     DevBuf<double> b, x, r, p, z, q, scal;
-    int last_iterations = 0;
   } ib;
 
   void inner_alloc(int l) {
@@ -1148,6 +1147,8 @@ class Solver {
   void dot(const double* a, const double* b, double* out);
   void linf(const double* a, double* out);
   bool build_loop_graph();
+  cudaGraphExec_t while_graph(const std::function<void(cudaGraphConditionalHandle)>& head,
+                              const std::function<void(cudaGraphConditionalHandle)>& body, std::string* why);
   void drop_graphs() {
     if (iter_graph) SGS_CUDA(cudaGraphExecDestroy(iter_graph));
     if (loop_graph) SGS_CUDA(cudaGraphExecDestroy(loop_graph));
@@ -1781,7 +1782,6 @@ void Solver::inner_pcg(int l) {
   SGS_CUDA(cudaMemcpyAsync(h, ib.scal.p, sizeof(h), cudaMemcpyDeviceToHost, stream));
   SGS_CUDA(cudaStreamSynchronize(stream));
   const double b2 = h[8];
-  ib.last_iterations = 0;
   if (!(b2 > 0)) return;  // x = 0
   const double tol2 = 1e-26 * b2;
   double best = b2;
@@ -1803,7 +1803,6 @@ void Solver::inner_pcg(int l) {
     launch_counter += 6;
     SGS_CUDA(cudaMemcpyAsync(h, ib.scal.p, sizeof(h), cudaMemcpyDeviceToHost, stream));
     SGS_CUDA(cudaStreamSynchronize(stream));
-    ib.last_iterations = it;
     if (h[7] != 0 || !std::isfinite(h[8]))
       throw CudaError("the bottom level's operator is not positive definite", SGS_ERR_BREAKDOWN);
     if (h[8] <= tol2) break;
@@ -1872,6 +1871,69 @@ __global__ void pcg_check_kernel(const double* __restrict__ scal, double* loop, 
   cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
+// A graph [head] -> WHILE([body]) whose condition the kernels that head and
+// body launch set: head(h) and body(h) are captured from the solver stream.
+// Returns the instantiated graph, or nullptr with the reason in *why where the
+// runtime refuses a step (conditional nodes need CUDA 12.4 or later).
+cudaGraphExec_t Solver::while_graph(const std::function<void(cudaGraphConditionalHandle)>& head,
+                                    const std::function<void(cudaGraphConditionalHandle)>& body, std::string* why) {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool capturing = false;
+  auto give_up = [&](const char* what, cudaError_t e) -> cudaGraphExec_t {
+    if (capturing) {
+      cudaGraph_t partial = nullptr;
+      cudaStreamEndCapture(stream, &partial);
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    *why = std::string(what) + ": " + cudaGetErrorString(e);
+    return nullptr;
+  };
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e != cudaSuccess) return give_up("cudaGraphCreate", e);
+  cudaGraphConditionalHandle h = 0;
+  e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return give_up("cudaGraphConditionalHandleCreate", e);
+  e = cudaStreamBeginCaptureToGraph(stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return give_up("cudaStreamBeginCaptureToGraph", e);
+  capturing = true;
+  head(h);
+  e = cudaStreamEndCapture(stream, &g);
+  capturing = false;
+  if (e != cudaSuccess) return give_up("cudaStreamEndCapture", e);
+  // the WHILE node follows the head's last nodes (those without dependents)
+  size_t n = 0;
+  SGS_CUDA(cudaGraphGetNodes(g, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n), deps;
+  SGS_CUDA(cudaGraphGetNodes(g, nodes.data(), &n));
+  for (cudaGraphNode_t node : nodes) {
+    size_t out = 0;
+    SGS_CUDA(cudaGraphNodeGetDependentNodes(node, nullptr, &out));
+    if (out == 0) deps.push_back(node);
+  }
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  e = cudaGraphAddNode(&wnode, g, deps.data(), deps.size(), &cp);
+  if (e != cudaSuccess) return give_up("cudaGraphAddNode (WHILE)", e);
+  cudaGraph_t bg = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(stream, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return give_up("cudaStreamBeginCaptureToGraph (body)", e);
+  capturing = true;
+  body(h);
+  e = cudaStreamEndCapture(stream, &bg);
+  capturing = false;
+  if (e != cudaSuccess) return give_up("cudaStreamEndCapture (body)", e);
+  e = cudaGraphInstantiate(&exec, g, 0);
+  if (e != cudaSuccess) return give_up("cudaGraphInstantiate", e);
+  SGS_CUDA(cudaGraphDestroy(g));
+  return exec;
+}
+
 // Builds loop_graph once per operator set: [test] -> WHILE([iteration, test]).
 // Returns false, and remembers why, where the runtime refuses conditional nodes.
 bool Solver::build_loop_graph() {
@@ -1879,63 +1941,20 @@ bool Solver::build_loop_graph() {
   if (loop_unavailable) return false;
   if (!loop_buf.p) loop_buf.alloc(LOOP_REC + LOOP_HIST);
   if (!h_loop) SGS_CUDA(cudaMallocHost(&h_loop, (LOOP_REC + LOOP_HIST) * sizeof(double)));
-  cudaGraph_t g = nullptr;
-  bool capturing = false;
-  auto give_up = [&](const char* what, cudaError_t e) {
-    if (capturing) {
-      cudaGraph_t partial = nullptr;
-      cudaStreamEndCapture(stream, &partial);
-    }
-    if (g) cudaGraphDestroy(g);
-    cudaGetLastError();
-    loop_unavailable = true;
-    loop_note = std::string(what) + ": " + cudaGetErrorString(e);
-    return false;
-  };
-  cudaError_t e = cudaGraphCreate(&g, 0);
-  if (e != cudaSuccess) return give_up("cudaGraphCreate", e);
-  cudaGraphConditionalHandle h = 0;
-  e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
-  if (e != cudaSuccess) return give_up("cudaGraphConditionalHandleCreate", e);
-  // the test before the first iteration
-  e = cudaStreamBeginCaptureToGraph(stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return give_up("cudaStreamBeginCaptureToGraph", e);
-  capturing = true;
-  launch(pcg_check_kernel, 1, 1, 0, (const double*)scal.p, loop_buf.p, h);
-  e = cudaStreamEndCapture(stream, &g);
-  capturing = false;
-  if (e != cudaSuccess) return give_up("cudaStreamEndCapture", e);
-  size_t n = 0;
-  SGS_CUDA(cudaGraphGetNodes(g, nullptr, &n));
-  std::vector<cudaGraphNode_t> deps(n);
-  SGS_CUDA(cudaGraphGetNodes(g, deps.data(), &n));
-  cudaGraphNodeParams cp = {};
-  cp.type = cudaGraphNodeTypeConditional;
-  cp.conditional.handle = h;
-  cp.conditional.type = cudaGraphCondTypeWhile;
-  cp.conditional.size = 1;
-  cudaGraphNode_t wnode;
-  e = cudaGraphAddNode(&wnode, g, deps.data(), n, &cp);
-  if (e != cudaSuccess) return give_up("cudaGraphAddNode (WHILE)", e);
-  cudaGraph_t body = cp.conditional.phGraph_out[0];
-  e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return give_up("cudaStreamBeginCaptureToGraph (body)", e);
-  capturing = true;
-  const long before = launch_counter;
-  record_iteration();
-  launches_per_iteration = launch_counter - before;
-  launch(pcg_check_kernel, 1, 1, 0, (const double*)scal.p, loop_buf.p, h);
-  launch_counter += 2;  // the two tests
-  e = cudaStreamEndCapture(stream, &body);
-  capturing = false;
-  if (e != cudaSuccess) return give_up("cudaStreamEndCapture (body)", e);
-  e = cudaGraphInstantiate(&loop_graph, g, 0);
-  if (e != cudaSuccess) {
-    loop_graph = nullptr;
-    return give_up("cudaGraphInstantiate", e);
-  }
-  SGS_CUDA(cudaGraphDestroy(g));
-  return true;
+  loop_graph = while_graph(
+      [&](cudaGraphConditionalHandle h) {  // the test before the first iteration
+        launch(pcg_check_kernel, 1, 1, 0, (const double*)scal.p, loop_buf.p, h);
+      },
+      [&](cudaGraphConditionalHandle h) {
+        const long before = launch_counter;
+        record_iteration();
+        launches_per_iteration = launch_counter - before;
+        launch(pcg_check_kernel, 1, 1, 0, (const double*)scal.p, loop_buf.p, h);
+        launch_counter += 2;  // the two tests
+      },
+      &loop_note);
+  if (!loop_graph) loop_unavailable = true;
+  return loop_graph != nullptr;
 }
 
 void Solver::solve() {
