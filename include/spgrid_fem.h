@@ -61,6 +61,10 @@ extern "C" {
  *   "sgs_loop_history"  residuals one launch of the device loop records before
  *                        it pauses for the host to take them out (2-1024,
  *                        default 1024; smaller values only add launches).
+ *   "sgs_inner_smoothing", "sgs_inner_boundary_smoothing"  full and
+ *                        boundary-band sweeps per level and direction of the
+ *                        V-cycle inside the inner CG of a large bottom (default
+ *                        3 and 0; the bottom is solved to round-off either way).
  * A solve that reaches the iteration cap returns success = 1 as the
  * reference's does, with extra_ints "converged" = 0. 
  * Warm starting as the reference's (SPGrid_CPU_Solver.cpp:56-73, 240-321,

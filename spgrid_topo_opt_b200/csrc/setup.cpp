@@ -361,6 +361,8 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   P.dense_bottom_max = in.get_int("sgs_dense_bottom_max", 24576);
   P.smoothing = in.pre_and_post_smoothing_iter;
   P.boundary_smoothing = in.get_int("boundary_smoothing", 5);
+  P.inner_smoothing = std::max(1, in.get_int("sgs_inner_smoothing", P.inner_smoothing));
+  P.inner_boundary_smoothing = std::max(0, in.get_int("sgs_inner_boundary_smoothing", P.inner_boundary_smoothing));
   P.tolerance = in.krylov.tolerance;
   const double penalty = in.get_double("penalty", 0.0), emin = in.get_double("minimum_stiffness", 0.0),
                rho_min = in.get_double("minimum_density", 0.0);

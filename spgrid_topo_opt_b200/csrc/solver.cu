@@ -1039,9 +1039,9 @@ class Solver {
 
   void inner_sweeps(int l, bool forward) {
     Level<double>& d = *L64[l];
-    for (int t = 0; t < P.boundary_smoothing; ++t) sweep<double>(l, d.u.p, d.b.p, forward, true, false);
-    for (int t = 0; t < std::max(1, P.smoothing); ++t) sweep<double>(l, d.u.p, d.b.p, forward, false, false);
-    for (int t = 0; t < P.boundary_smoothing; ++t) sweep<double>(l, d.u.p, d.b.p, forward, true, false);
+    for (int t = 0; t < P.inner_boundary_smoothing; ++t) sweep<double>(l, d.u.p, d.b.p, forward, true, false);
+    for (int t = 0; t < std::max(1, P.inner_smoothing); ++t) sweep<double>(l, d.u.p, d.b.p, forward, false, false);
+    for (int t = 0; t < P.inner_boundary_smoothing; ++t) sweep<double>(l, d.u.p, d.b.p, forward, true, false);
   }
 
   template <typename T>
