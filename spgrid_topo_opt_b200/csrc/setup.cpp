@@ -231,41 +231,41 @@ void flag_nodes(HostLevel& L) {
   }
 }
 
-using Rings = HostBuf<std::array<int, 27>>;  // every entry is written by flag_boundary
-
-void flag_boundary(HostLevel& L, Rings& rings, int band = 3) {
+void flag_boundary(HostLevel& L, int band = 3) {
   // Flaging.h:93-147: three Jacobi-style passes growing a band of active,
   // non-Dirichlet nodes around the Dirichlet nodes.  A pass can only reach
   // blocks next to a block that already holds a Dirichlet or band node, so
-  // each pass visits those blocks alone.
+  // each pass visits those blocks alone: the neighbours of the seeded blocks
+  // (the neighbour relation is symmetric), whose 27-block rings are looked up
+  // when they first become candidates.
   const uint32_t SEED = F_DIRICHLET_NODE | F_BOUNDARY_NODE;
   const int nall = int(L.coords.size() / 3);
-  rings.resize(size_t(L.nb));  // every entry is written below
-#pragma omp parallel for schedule(static)
-  for (int b = 0; b < L.nb; ++b) block_ring(L, b, rings[size_t(b)].data());
+  HostBuf<std::array<int, 27>> rings(static_cast<size_t>(L.nb));  // entries filled on first use
+  std::vector<uint8_t> have_ring(static_cast<size_t>(L.nb), 0), banded(static_cast<size_t>(L.nb), 0);
+  std::vector<uint8_t> seeded(static_cast<size_t>(nall), 0), is_cand(static_cast<size_t>(L.nb), 0);
   auto flag_at = [&](const int* ring, int x, int y, int z) -> uint32_t {
     const int nb = ring[(x < 0 ? 0 : (x > 3 ? 2 : 1)) * 9 + (y < 0 ? 0 : (y > 3 ? 2 : 1)) * 3 + (z < 0 ? 0 : (z > 7 ? 2 : 1))];
     return nb < 0 ? 0u : L.flags[size_t(nb) * NODES_PER_BLOCK + node_slot(x, y, z)];
   };
-  std::vector<uint8_t> seeded(static_cast<size_t>(nall), 0), is_cand(static_cast<size_t>(L.nb), 0);
-  std::vector<int> cand;
-  // blocks holding a Dirichlet or band node; after the first pass only the
-  // candidates of the last pass can have gained band nodes
+  // blocks holding a Dirichlet or band node (ghost blocks included)
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nall; ++b) {
     uint8_t s = 0;
     for (int e = 0; e < NODES_PER_BLOCK && !s; ++e) s = (L.flags[size_t(b) * NODES_PER_BLOCK + e] & SEED) != 0;
     seeded[size_t(b)] = s;
   }
+  std::vector<int> seeds, cand;
+  for (int b = 0; b < nall; ++b)
+    if (seeded[size_t(b)]) seeds.push_back(b);
   for (int pass = 0; pass < band; ++pass) {
+    // candidates: the active blocks among the seeded blocks' 27 neighbours, ascending
+    std::fill(is_cand.begin(), is_cand.end(), uint8_t(0));
 #pragma omp parallel for schedule(static)
-    for (int b = 0; b < L.nb; ++b) {
-      uint8_t near = 0;
-      for (int d = 0; d < 27 && !near; ++d) {
-        const int nb = rings[size_t(b)][d];
-        near = nb >= 0 && seeded[size_t(nb)];
-      }
-      is_cand[size_t(b)] = near;
+    for (long k = 0; k < long(seeds.size()); ++k) {
+      int ring[27];
+      block_ring(L, seeds[size_t(k)], ring);
+      for (int d = 0; d < 27; ++d)
+        if (ring[d] >= 0 && ring[d] < L.nb) __atomic_store_n(&is_cand[size_t(ring[d])], uint8_t(1), __ATOMIC_RELAXED);
     }
     cand.clear();
     for (int b = 0; b < L.nb; ++b)
@@ -273,6 +273,10 @@ void flag_boundary(HostLevel& L, Rings& rings, int band = 3) {
 #pragma omp parallel for schedule(dynamic, 16)
     for (long k = 0; k < long(cand.size()); ++k) {
       const int b = cand[size_t(k)];
+      if (!have_ring[size_t(b)]) {
+        block_ring(L, b, rings[size_t(b)].data());
+        have_ring[size_t(b)] = 1;
+      }
       const int* ring = rings[size_t(b)].data();
       for (int e = 0; e < NODES_PER_BLOCK; ++e) {
         uint32_t& f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
@@ -289,22 +293,22 @@ void flag_boundary(HostLevel& L, Rings& rings, int band = 3) {
         uint32_t& f = L.flags[size_t(cand[size_t(k)]) * NODES_PER_BLOCK + e];
         if (f & F_BOUNDARY_TEMP) {
           f = (f & ~F_BOUNDARY_TEMP) | F_BOUNDARY_NODE;
-          seeded[size_t(cand[size_t(k)])] = 1;
+          banded[size_t(cand[size_t(k)])] = 1;
         }
       }
+    for (int b : cand)  // the blocks that gained band nodes seed the next pass
+      if (banded[size_t(b)] && !seeded[size_t(b)]) {
+        seeded[size_t(b)] = 1;
+        seeds.push_back(b);
+      }
   }
+  // the blocks with a boundary-band node: only candidates gain them
   L.boundary.clear();
   for (int b = 0; b < L.nb; ++b)
-    for (int e = 0; e < NODES_PER_BLOCK; ++e)
-      if (L.flags[size_t(b) * NODES_PER_BLOCK + e] & F_BOUNDARY_NODE) {
-        L.boundary.push_back(b);
-        break;
-      }
+    if (banded[size_t(b)]) L.boundary.push_back(b);
 }
 
-// rings: the 27 blocks around each active block (flag_boundary's), of which
-// the active ones make the neighbour table
-void finish_level(HostLevel& L, const Rings& rings) {
+void finish_level(HostLevel& L) {
   // Dirichlet node lists in ascending node order: per-block counts, a prefix
   // over the blocks, then a parallel fill
   std::vector<int32_t> cnt(size_t(L.nb) * 3, 0);
@@ -329,13 +333,6 @@ void finish_level(HostLevel& L, const Rings& rings) {
       const uint32_t f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
       for (int v = 0; v < 3; ++v)
         if (f & (F_DIRICHLET_NODE_X << v)) L.dirichlet[v][size_t(cnt[size_t(b) * 3 + v]++)] = b * NODES_PER_BLOCK + e;
-    }
-  L.nbr.resize(size_t(L.nb) * 27);
-#pragma omp parallel for schedule(static)
-  for (int b = 0; b < L.nb; ++b)
-    for (int d = 0; d < 27; ++d) {
-      const int nb = rings[size_t(b)][size_t(d)];
-      L.nbr[size_t(b) * 27 + d] = nb < L.nb ? nb : -1;  // ghosts are not neighbours
     }
 }
 
@@ -637,11 +634,8 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   for (int lev = 1; lev < P.mg_levels; ++lev) P.levels.push_back(coarsen(P.levels[lev - 1]));
   phase_done(1);
   for (auto& L : P.levels) flag_nodes(L);
-  {
-    std::vector<Rings> rings(P.levels.size());
-    for (size_t l = 0; l < P.levels.size(); ++l) flag_boundary(P.levels[l], rings[l]);
-    for (size_t l = 0; l < P.levels.size(); ++l) finish_level(P.levels[l], rings[l]);
-  }
+  for (auto& L : P.levels) flag_boundary(L);
+  for (auto& L : P.levels) finish_level(L);
   phase_done(2);
   // levels below a bottom too large for the dense inverse: the bottom is then
   // solved by CG with V-cycles over them (same coarsening rule, Galerkin
@@ -655,9 +649,8 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
     while (P.levels.size() < 7 && 3 * active_nodes(P.levels.back()) > P.dense_bottom_max) {
       HostLevel L = coarsen(P.levels.back());
       flag_nodes(L);
-      Rings rings;
-      flag_boundary(L, rings);
-      finish_level(L, rings);
+      flag_boundary(L);
+      finish_level(L);
       P.levels.push_back(std::move(L));
     }
   }

@@ -34,7 +34,6 @@ struct HostLevel {
   std::vector<int32_t> coords;        // block base coordinates, [nb_all*3]
   HostBuf<uint32_t> flags;            // [nb_all*128]
   HostBuf<uint8_t> active_page;       // per block-grid cell
-  HostBuf<int32_t> nbr;               // [nb*27] neighbour block (active only) or -1
   std::vector<int32_t> boundary;      // active blocks with a boundary-band node
   std::array<std::vector<int32_t>, 3> dirichlet;  // node indices with a Dirichlet component
 

@@ -182,6 +182,18 @@ __global__ void colour_fill_kernel(int nb, const uint32_t* __restrict__ flags, c
   if (band >= 0) out[pos[long(band) * nb + b] + rb] = (band & 1) ? ~int(g) : int(g);
 }
 
+// Neighbour table of a level: entry (dx+1)*9 + (dy+1)*3 + (dz+1) of block b is
+// the active block at offset (dx, dy, dz) blocks, -1 where there is none or
+// only a ghost block (the block grid names active blocks only).
+__global__ void block_neighbours_kernel(int nb, const int* __restrict__ coords, GridView g, int* __restrict__ nbr) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nb) * 27) return;
+  const int b = int(t / 27), d = int(t % 27);
+  const long n = g.node(coords[3 * b] + (d / 9 - 1) * BLK_X, coords[3 * b + 1] + ((d / 3) % 3 - 1) * BLK_Y,
+                        coords[3 * b + 2] + (d % 3 - 1) * BLK_Z);
+  nbr[t] = n < 0 ? -1 : int(n >> 7);
+}
+
 // block grid entries naming ghost blocks (index >= nb) become -1; neighbour
 // tables with the zero pad block (index nb) in place of missing neighbours
 __global__ void active_grid_kernel(int* __restrict__ g, long n, int nb) {
@@ -404,13 +416,17 @@ class Solver {
     d.nb = h.nb;
     d.N = long(h.nb) * NODES_PER_BLOCK;
     d.coords.upload(h.coords.data(), size_t(h.nb) * 3, stream);
-    d.nbr.upload(h.nbr, stream);
     d.flags.upload(h.flags.data(), size_t(d.N), stream);
     // the block grid names active blocks only (ghost blocks become -1, on the device)
     d.bgrid.upload(h.bgrid, stream);
     if (d.bgrid.n)
       active_grid_kernel<<<blocks_for(long(d.bgrid.n), 256), 256, 0, stream>>>(d.bgrid.p, long(d.bgrid.n), h.nb);
     d.grid = GridView{d.bgrid.p, h.grid[0], h.grid[1], h.grid[2]};
+    // the 27 neighbour blocks of every active block, from the block grid
+    d.nbr.alloc(size_t(h.nb) * 27);
+    if (h.nb)
+      block_neighbours_kernel<<<blocks_for(long(h.nb) * 27, 256), 256, 0, stream>>>(h.nb, d.coords.p, d.grid, d.nbr.p);
+    SGS_CUDA(cudaGetLastError());
     d.boundary.upload(h.boundary, stream);
     d.nbound = int(h.boundary.size());
     for (int v = 0; v < 3; ++v) {
