@@ -23,6 +23,7 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <map>
 #include <unordered_map>
 #include <vector>
 
@@ -218,6 +219,34 @@ static __device__ __align__(256) double g_sensitivity_partials[SGS_SENSITIVITY_S
 // ---------------------------------------------------------------------------
 // The solver: device hierarchy + PCG
 // ---------------------------------------------------------------------------
+// Scratch for the Galerkin set-up's cell matrices, per device and kept for the
+// process (grown when a larger problem needs it): two buffers of up to
+// gigabytes (the level being built and the one above it), which a fresh
+// allocation from the stream-ordered pool could take a tenth of a second to
+// map whenever the pool's free memory was fragmented.  One set-up uses it at
+// a time per device (cell_scratch_lock).
+struct CellScratch {
+  double* p[2] = {nullptr, nullptr};
+  size_t n[2] = {0, 0};
+};
+static std::mutex g_cell_scratch_mutex;
+static std::map<int, CellScratch> g_cell_scratch;
+static std::unique_lock<std::mutex> cell_scratch_lock() { return std::unique_lock<std::mutex>(g_cell_scratch_mutex); }
+// buffer `slot` of the current device's scratch, at least `count` doubles (the caller holds the lock)
+static double* cell_scratch(int slot, size_t count) {
+  int dev = 0;
+  SGS_CUDA(cudaGetDevice(&dev));
+  CellScratch& c = g_cell_scratch[dev];
+  if (c.n[slot] < count) {
+    if (c.p[slot]) SGS_CUDA(cudaFree(c.p[slot]));
+    c.p[slot] = nullptr;
+    c.n[slot] = 0;
+    SGS_CUDA(cudaMalloc(reinterpret_cast<void**>(&c.p[slot]), count * sizeof(double)));
+    c.n[slot] = count;
+  }
+  return c.p[slot];
+}
+
 class Solver {
  public:
   Problem P;
@@ -578,8 +607,12 @@ class Solver {
     const int first = (nout() == 1) ? 0 : P.explicit_level;
     // the previous level's cell matrices: the next level's come from them
     // (galerkin_coarsen_kernel) except in the reference-rounding mode, which
-    // sums every level from the finest cells as the reference does
-    DevBuf<double> prev_cellmat;
+    // sums every level from the finest cells as the reference does; both
+    // levels' matrices live in the process's cell scratch (buffers `cur` and
+    // 1 - `cur`)
+    auto scratch = cell_scratch_lock();
+    int cur = 0;
+    double* prev_cellmat = nullptr;
     DevBuf<int32_t> prev_cell;
     int prev_lev = -1;
     for (int lev = first; lev < n; ++lev) {
@@ -609,15 +642,14 @@ class Solver {
       d.spokes.zero(stream);
       d.has_matrix = true;
       if (ncells > 0) {
-        DevBuf<double> cellmat;
         DevBuf<int32_t> dcell;
         dcell.upload(cell_of_slot, stream);
-        cellmat.alloc(size_t(ncells) * 576);
+        double* cellmat = cell_scratch(cur, size_t(ncells) * 576);
         if (recursive) {
           DevBuf<int32_t> dcc;
           dcc.upload(ccoord, stream);
           galerkin_coarsen_kernel<<<unsigned(ncells), 576, 0, stream>>>(dcc.p, L64[lev - 1]->grid, prev_cell.p,
-                                                                     prev_cellmat.p, cellmat.p);
+                                                                     prev_cellmat, cellmat);
           SGS_CUDA(cudaGetLastError());
           SGS_CUDA(cudaStreamSynchronize(stream));  // dcc goes out of scope
         } else {
@@ -629,19 +661,19 @@ class Solver {
           const size_t smem = 2 * GT * 65 * sizeof(double);
           SGS_CUDA(cudaFuncSetAttribute(galerkin_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
           galerkin_cell_kernel<<<dim3(576 / GT, (ncells + GT - 1) / GT), 256, smem, stream>>>(
-              ncells, dorigin.p, lev, L64[0]->grid, E64.p, table.p, cellmat.p);
+              ncells, dorigin.p, lev, L64[0]->grid, E64.p, table.p, cellmat);
           SGS_CUDA(cudaGetLastError());
           SGS_CUDA(cudaStreamSynchronize(stream));  // the temporaries go out of scope
         }
-        galerkin_assemble_kernel<<<unsigned(d.N), 256, 0, stream>>>(d.coords.p, d.flags.p, dcell.p, d.grid, cellmat.p, d.A.p,
+        galerkin_assemble_kernel<<<unsigned(d.N), 256, 0, stream>>>(d.coords.p, d.flags.p, dcell.p, d.grid, cellmat, d.A.p,
                                                                    d.spokes.p, P.dx);
         SGS_CUDA(cudaGetLastError());
         delete_dirichlet_kernel<<<blocks_for(d.N, 128), 128, 0, stream>>>(d.nb, d.coords.p, d.flags.p, d.spokes.p, d.grid,
                                                                          d.A.p, d.N);
         SGS_CUDA(cudaGetLastError());
         SGS_CUDA(cudaStreamSynchronize(stream));
-        std::swap(prev_cellmat.p, cellmat.p);
-        std::swap(prev_cellmat.n, cellmat.n);
+        prev_cellmat = cellmat;
+        cur = 1 - cur;
         std::swap(prev_cell.p, dcell.p);
         std::swap(prev_cell.n, dcell.n);
         prev_lev = lev;
