@@ -70,10 +70,33 @@ def test_fem_solve_rejects_missing_neighbour_blocks(native_lib):
     assert not out.success and out.error_code == 5
 
 
-@pytest.mark.parametrize("problem", ["cantilever", "shell"])
+def _shuffled_repeated_cantilever():
+    """A cantilever whose input blocks come in a seeded random order, a third of
+    them twice (the later copy with scaled densities: the last one wins)."""
+    inp = configs.to_inputs(configs.cantilever_box(24, density=(0.05, 1.0), bottom_size=4))
+    n = inp.density.base.shape[0]
+    rng = np.random.default_rng(3)
+    perm = rng.permutation(n)
+    idx = np.concatenate([perm, perm[: n // 3]])
+    inp.density.base = inp.density.base[idx].copy()
+    inp.density.data = inp.density.data[idx].copy()
+    inp.density.data[n:] *= rng.uniform(0.5, 1.0, size=inp.density.data[n:].shape)
+    return inp
+
+
+@pytest.mark.parametrize("problem", ["cantilever", "shell", "band", "shuffled"])
 def test_host_hierarchy_matches_oracle(native_lib, problem):
-    prob = configs.cantilever_box(16, bottom_size=4) if problem == "cantilever" else configs.sphere_shell(24, bottom_size=4)
-    inp = configs.to_inputs(prob)
+    """Page order, ghost blocks, flags and band lists of every level, bit for bit:
+    the blocks are numbered by parallel passes that must reproduce the serial
+    construction's order, which sparse bands (many ghost blocks on every level)
+    and shuffled, repeated input blocks exercise."""
+    if problem == "band":
+        inp = configs.spheres_band_inputs(96, bottom_size=4)
+    elif problem == "shuffled":
+        inp = _shuffled_repeated_cantilever()
+    else:
+        prob = configs.cantilever_box(16, bottom_size=4) if problem == "cantilever" else configs.sphere_shell(24, bottom_size=4)
+        inp = configs.to_inputs(prob)
     ref = Oracle(inp, mode=MODE_FP64)
     ses = native.Session(inp, precision=native.HOST_SETUP_ONLY)
     assert ses.levels == ref.levels
