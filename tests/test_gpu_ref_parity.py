@@ -60,7 +60,7 @@ def test_fp64_matches_fp64_reference(native_lib, name):
     assert rel_u(out.displacements.data, key) < 1e-9
 
 
-@pytest.mark.parametrize("name", ["config0_box64", "shell64", "cantilever16"])
+@pytest.mark.parametrize("name", ["config0_box64", "shell64", "cantilever16", "spheres_band96"])
 def test_mixed_precision_matches_fp64_reference(native_lib, name):
     key = f"{name}/fp64"
     tight = solve(name, 1e-10, native.PRECISION_MIXED)
