@@ -655,8 +655,9 @@ enum { SOP_MUL = 0, SOP_RES = 1, SOP_GS = 2 };
 
 // One warp per node: lane q < 27 multiplies the 3x3 block of spoke q with the
 // neighbour's u, the warp sums the three components.  Stencils are node-major,
-// A[node*243 + q*9 + v*3 + w], so a warp reads one node's coefficients in one
-// coalesced sweep.  GS updates only colour-`color` nodes (16 per block).
+// A[node*243 + q*9 + v*3 + w]: lane q reads its nine entries, and the warp's
+// reads together cover one contiguous row (972 bytes in FP32), which L1
+// fetches once.  GS updates only colour-`color` nodes (16 per block).
 // Results on Dirichlet components are zeroed (Project).  The reference
 // projects the whole level after every colour; here only updated nodes are
 // projected, which is the same because the V-cycle keeps u zero on Dirichlet
