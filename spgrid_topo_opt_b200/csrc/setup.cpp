@@ -170,17 +170,22 @@ void flag_nodes(HostLevel& L) {
   // active block reaches are created (serially), then every node ORs the bits
   // of its 8 incident cells in active blocks (in parallel).
   const uint32_t CELL = F_ACTIVE_CELL | F_DIRICHLET_CELL;
-  std::vector<uint8_t> reach(size_t(L.nb), 0);  // bit (dx*4+dy*2+dz): a cell on that +face combination
+  // bit (dx*4+dy*2+dz) of corner_reach[e]: the corners of cell e reach the block at +(dx, dy, dz)
+  uint8_t corner_reach[NODES_PER_BLOCK];
+  for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+    const int kx = (e >> 5) == 3, ky = ((e >> 3) & 3) == 3, kz = (e & 7) == 7;
+    unsigned m = 0;
+    for (int c = 1; c < 8; ++c)
+      if ((!(c & 4) || kx) && (!(c & 2) || ky) && (!(c & 1) || kz)) m |= 1u << c;
+    corner_reach[e] = uint8_t(m);
+  }
+  std::vector<uint8_t> reach(size_t(L.nb), 0);  // per block: the OR over its cells with a CELL bit
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < L.nb; ++b) {
-    uint8_t m = 0;
-    for (int e = 0; e < NODES_PER_BLOCK; ++e) {
-      if (!(L.flags[size_t(b) * NODES_PER_BLOCK + e] & CELL)) continue;
-      const int kx = (e >> 5) == 3, ky = ((e >> 3) & 3) == 3, kz = (e & 7) == 7;
-      for (int c = 1; c < 8; ++c)
-        if ((!(c & 4) || kx) && (!(c & 2) || ky) && (!(c & 1) || kz)) m |= uint8_t(1u << c);
-    }
-    reach[size_t(b)] = m;
+    const uint32_t* f = L.flags.data() + size_t(b) * NODES_PER_BLOCK;
+    unsigned m = 0;
+    for (int e = 0; e < NODES_PER_BLOCK; ++e) m |= (f[e] & CELL) ? corner_reach[e] : 0u;
+    reach[size_t(b)] = uint8_t(m);
   }
   for (int b = 0; b < L.nb; ++b)
     for (int c = 1; c < 8; ++c)
@@ -206,14 +211,17 @@ void flag_nodes(HostLevel& L) {
     // the cell bits of cells x-1..3, y-1..3, z-1..7 (index +1), then ORed along
     // z, y and x in place: entry (x+1, y+1, z+1) ends as the OR of the 8 cells
     // of node (x, y, z)
+    // z-column (ax, ay): entry 0 from the -z block's z = 7, entries 1-8 from z = 0-7
     uint32_t A[5][5][9];
     for (int ax = 0; ax < 5; ++ax)
-      for (int ay = 0; ay < 5; ++ay)
-        for (int az = 0; az < 9; ++az) {
-          const int cx = ax - 1, cy = ay - 1, cz = az - 1;
-          const int nb = src[(cx < 0 ? 4 : 0) | (cy < 0 ? 2 : 0) | (cz < 0 ? 1 : 0)];
-          A[ax][ay][az] = nb >= 0 ? cell_bits(size_t(nb) * NODES_PER_BLOCK + node_slot(cx, cy, cz)) & CELL : 0u;
-        }
+      for (int ay = 0; ay < 5; ++ay) {
+        const int s = (ax == 0 ? 4 : 0) | (ay == 0 ? 2 : 0);
+        const size_t col = size_t(((ax + 3) & 3) * 32 + ((ay + 3) & 3) * 8);
+        const int below = src[s | 1], own = src[s];
+        A[ax][ay][0] = below >= 0 ? cell_bits(size_t(below) * NODES_PER_BLOCK + col + 7) & CELL : 0u;
+        for (int z = 0; z < 8; ++z)
+          A[ax][ay][z + 1] = own >= 0 ? cell_bits(size_t(own) * NODES_PER_BLOCK + col + size_t(z)) & CELL : 0u;
+      }
     for (int ax = 0; ax < 5; ++ax)
       for (int ay = 0; ay < 5; ++ay)
         for (int az = 8; az > 0; --az) A[ax][ay][az] |= A[ax][ay][az - 1];
@@ -310,17 +318,24 @@ void flag_boundary(HostLevel& L, int band = 3) {
 
 void finish_level(HostLevel& L) {
   // Dirichlet node lists in ascending node order: per-block counts, a prefix
-  // over the blocks, then a parallel fill
+  // over the blocks, then a parallel fill of the few blocks that hold one
   std::vector<int32_t> cnt(size_t(L.nb) * 3, 0);
+  const uint32_t DIR = F_DIRICHLET_NODE_X | (F_DIRICHLET_NODE_X << 1) | (F_DIRICHLET_NODE_X << 2);
 #pragma omp parallel for schedule(static)
+  for (int b = 0; b < L.nb; ++b) {
+    const uint32_t* f = L.flags.data() + size_t(b) * NODES_PER_BLOCK;
+    uint32_t any = 0;
+    for (int e = 0; e < NODES_PER_BLOCK; ++e) any |= f[e];
+    if (!(any & DIR)) continue;
+    for (int e = 0; e < NODES_PER_BLOCK; ++e)
+      for (int v = 0; v < 3; ++v) cnt[size_t(b) * 3 + v] += (f[e] & (F_DIRICHLET_NODE_X << v)) ? 1 : 0;
+  }
+  std::vector<int> holders;
   for (int b = 0; b < L.nb; ++b)
-    for (int e = 0; e < NODES_PER_BLOCK; ++e) {
-      const uint32_t f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
-      for (int v = 0; v < 3; ++v) cnt[size_t(b) * 3 + v] += (f & (F_DIRICHLET_NODE_X << v)) ? 1 : 0;
-    }
+    if (cnt[size_t(b) * 3] | cnt[size_t(b) * 3 + 1] | cnt[size_t(b) * 3 + 2]) holders.push_back(b);
   for (int v = 0; v < 3; ++v) {
     int32_t total = 0;
-    for (int b = 0; b < L.nb; ++b) {
+    for (int b : holders) {
       const int32_t c = cnt[size_t(b) * 3 + v];
       cnt[size_t(b) * 3 + v] = total;
       total += c;
@@ -328,12 +343,14 @@ void finish_level(HostLevel& L) {
     L.dirichlet[v].assign(size_t(total), 0);
   }
 #pragma omp parallel for schedule(static)
-  for (int b = 0; b < L.nb; ++b)
+  for (long k = 0; k < long(holders.size()); ++k) {
+    const int b = holders[size_t(k)];
     for (int e = 0; e < NODES_PER_BLOCK; ++e) {
       const uint32_t f = L.flags[size_t(b) * NODES_PER_BLOCK + e];
       for (int v = 0; v < 3; ++v)
         if (f & (F_DIRICHLET_NODE_X << v)) L.dirichlet[v][size_t(cnt[size_t(b) * 3 + v]++)] = b * NODES_PER_BLOCK + e;
     }
+  }
 }
 
 }  // namespace
@@ -387,6 +404,7 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   // input block is repeated: then the cells go in input order, the last write
   // winning.
   std::vector<int32_t> in_slot(nin);
+  std::vector<uint8_t> halves;  // per block: bit h set when an input block fills its z half h
   bool repeated = false;
   {
     HostLevel& L = b0.L;
@@ -407,7 +425,7 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
     const auto pages = sorted_cells(long(L.active_page.size()), [&](long c) { return page[c] ? cell_key(L, c) : NONE; });
     number_blocks(L, pages, {});
     const int nb = L.nb;
-    std::vector<uint8_t> halves(size_t(nb), 0);
+    halves.assign(size_t(nb), 0);
     int rep = 0;
 #pragma omp parallel for schedule(static) reduction(| : rep)
     for (long b = 0; b < long(nin); ++b) {
@@ -429,50 +447,85 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
   auto simp = [&](double d) {
     return d > 0 ? (penalty ? (1 - emin) * std::pow(std::max(rho_min, d), penalty) + emin : d) : 0.0;
   };
+  // A material cell's corners leave its page only across a +face of the page,
+  // so an input block needs at most the 7 pages beyond its +faces.  Bit n of
+  // face_need[zl][e] is set when input cell e reaches the page at offset
+  // (n>>2, (n>>1)&1, n&1); zl = 1 for an input block in the upper z half of its page.
+  uint8_t face_need[2][64];
+  for (int zl = 0; zl < 2; ++zl)
+    for (int e = 0; e < 64; ++e) {
+      const int ex = (e >> 4) == 3, ey = ((e >> 2) & 3) == 3, ez = zl && (e & 3) == 3;
+      unsigned m = 0;
+      for (int n = 1; n < 8; ++n)
+        if ((!(n & 4) || ex) && (!(n & 2) || ey) && (!(n & 1) || ez)) m |= 1u << n;
+      face_need[zl][e] = uint8_t(m);
+    }
   P.E.resize(size_t(b0.L.nb) * NODES_PER_BLOCK);
   {
+    // without repeated input blocks every z half that an input block covers is
+    // written in full below: only the other halves are cleared here
     double* E = P.E.data();
-    const long nE = long(P.E.size());
 #pragma omp parallel for schedule(static)
-    for (long i = 0; i < nE; ++i) E[i] = 0.0;
+    for (long b = 0; b < long(b0.L.nb); ++b)
+      for (int h = 0; h < 2; ++h)
+        if (repeated || !((halves[size_t(b)] >> h) & 1))
+          for (int xy = 0; xy < 16; ++xy)
+            for (int k = 0; k < 4; ++k) E[size_t(b) * NODES_PER_BLOCK + size_t(xy * 8 + 4 * h + k)] = 0.0;
   }
   std::unique_ptr<double[]> Ein;
+  std::vector<uint8_t> need(nin, 0);  // per input block: the +face pages its material cells need
   if (repeated) {
     Ein.reset(new double[nin * 64]);
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < long(nin) * 64; ++c) Ein[size_t(c)] = simp(in.density.data[size_t(c)]);
+#pragma omp parallel for schedule(static)
+    for (long b = 0; b < long(nin); ++b) {
+      const int zl = (in.density.base[3 * b + 2] & 4) != 0;
+      unsigned m = 0;
+      for (int e = 0; e < 64; ++e)
+        if (Ein[size_t(b) * 64 + size_t(e)] * P.mu0 > 0) m |= face_need[zl][e];
+      need[size_t(b)] = uint8_t(m);
+    }
   } else {
+    // one pass over the input cells: the stiffness scale, the pages the
+    // material needs, and ACTIVE_CELL where the density is positive and
+    // mu != 0 (Flaging.h:31-44), written before renumbering (a failed
+    // validation below discards the level)
+    double* E = P.E.data();
+    uint32_t* flags = b0.L.flags.data();
 #pragma omp parallel for schedule(static)
     for (long b = 0; b < long(nin); ++b) {
       const size_t base = size_t(in_slot[size_t(b)]);
-      for (int e = 0; e < 64; ++e) P.E[base + size_t(cell_slot(e))] = simp(in.density.data[size_t(b) * 64 + e]);
+      const int zl = (in.density.base[3 * b + 2] & 4) != 0;
+      unsigned m = 0;
+      for (int e = 0; e < 64; ++e) {
+        const double d = in.density.data[size_t(b) * 64 + size_t(e)];
+        const double Ev = simp(d);
+        const size_t slot = base + size_t(cell_slot(e));
+        E[slot] = Ev;
+        if (Ev * P.mu0 > 0) m |= face_need[zl][e];
+        if (d > 0 && Ev * P.mu0 != 0) flags[slot] |= F_ACTIVE_CELL;
+      }
+      need[size_t(b)] = uint8_t(m);
     }
   }
   auto cell_E = [&](size_t b, int e) {
     return repeated ? Ein[b * 64 + size_t(e)] : P.E[size_t(in_slot[b]) + size_t(cell_slot(e))];
   };
   // Validate_With_Density (solver/CPU_Kernels/Validate_Blocks.h:311-335): every
-  // material cell needs its +1 neighbour pages; the first failure in input order is reported.
+  // material cell needs its +1 neighbour pages; the first failure in input order
+  // is reported.  The pages an input block needs are tested once, and only a
+  // block that misses one is searched cell by cell.
   long first_bad = -1;
   {
     std::vector<long> bad(nin, -1);
-    // A corner leaves the block's page only across a +face of the page, so a
-    // block needs at most the 7 pages beyond its +faces: those are tested once
-    // per block, and only a block that misses one is searched cell by cell.
 #pragma omp parallel for schedule(static)
     for (long b = 0; b < long(nin); ++b) {
       const int x = in.density.base[3 * b], y = in.density.base[3 * b + 1], z = in.density.base[3 * b + 2];
-      const bool zlast = (z & 4) != 0;  // the upper 4x4x4 half of a 4x4x8 page
-      unsigned need = 0;
-      for (int e = 0; e < 64; ++e) {
-        if (!(cell_E(size_t(b), e) * P.mu0 > 0)) continue;
-        const int ex = (e >> 4) == 3, ey = ((e >> 2) & 3) == 3, ez = zlast && (e & 3) == 3;
-        for (int n = 1; n < 8; ++n)
-          if ((!(n & 4) || ex) && (!(n & 2) || ey) && (!(n & 1) || ez)) need |= 1u << n;
-      }
+      const unsigned nb_need = need[size_t(b)];
       bool ok = true;
       for (int n = 1; n < 8 && ok; ++n)
-        if (need >> n & 1) ok = b0.test_page(x + (n >> 2) * 4, y + ((n >> 1) & 1) * 4, z + (n & 1) * 4);
+        if (nb_need >> n & 1) ok = b0.test_page(x + (n >> 2) * 4, y + ((n >> 1) & 1) * 4, z + (n & 1) * 4);
       if (ok) continue;
       for (int e = 0; e < 64 && bad[size_t(b)] < 0; ++e) {
         if (!(cell_E(size_t(b), e) * P.mu0 > 0)) continue;
@@ -493,12 +546,12 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
                   in.density.base[3 * b + 1] + ((e >> 2) & 3), in.density.base[3 * b + 2] + (e & 3));
     return fail(5, msg);
   }
-  // ACTIVE_CELL where mu != 0 (Flaging.h:31-44); written before renumbering
-#pragma omp parallel for schedule(static) if (!repeated)
-  for (long b = 0; b < long(nin); ++b)
-    for (int e = 0; e < 64; ++e)
-      if (in.density.data[size_t(b) * 64 + e] > 0 && cell_E(size_t(b), e) * P.mu0 != 0)
-        b0.L.flags[size_t(in_slot[size_t(b)] + cell_slot(e))] |= F_ACTIVE_CELL;
+  // ACTIVE_CELL with repeated input blocks: serially, since copies of a block share slots
+  if (repeated)
+    for (size_t b = 0; b < nin; ++b)
+      for (int e = 0; e < 64; ++e)
+        if (in.density.data[b * 64 + size_t(e)] > 0 && cell_E(b, e) * P.mu0 != 0)
+          b0.L.flags[size_t(in_slot[b] + cell_slot(e))] |= F_ACTIVE_CELL;
   // Dirichlet node -> cell: a cell is fixed on axis v when all 8 corners are
   // listed on axis v (SPGrid_CPU_Solver.cpp:169-192)
   for (int v = 0; v < 3; ++v) {
@@ -556,30 +609,44 @@ std::string build_problem(const FEMInputs& in, Problem& P, int* error_code) {
       uint8_t pages;
       bool any;
     };
+    // Whether a cell's coarse image lies on its page's last layer depends on the
+    // cell's slot e and on the parity of the fine block's coordinates (x/4, y/4,
+    // z/8 mod 2) alone: the patch cell, the reached pages and the reached pages
+    // without n = 0 are tabulated per parity p (bit 4: x/4 odd, 2: y/4, 1: z/8),
+    // from a representative block of each parity.
+    uint8_t patch_cell[NODES_PER_BLOCK], reach_tab[8][NODES_PER_BLOCK], no_self_tab[8][NODES_PER_BLOCK];
+    for (int p = 0; p < 8; ++p)
+      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+        const int bx = (p >> 2) * BLK_X, by = ((p >> 1) & 1) * BLK_Y, bz = (p & 1) * BLK_Z;
+        const int cx = (bx + (e >> 5) + BLK_X) >> 1, cy = (by + ((e >> 3) & 3) + BLK_Y) >> 1,
+                  cz = (bz + (e & 7) + BLK_Z) >> 1;
+        const int kx = (cx & 3) == 3, ky = (cy & 3) == 3, kz = (cz & 7) == 7;
+        unsigned reach = 0;
+        for (int dx = 0; dx <= kx; ++dx)
+          for (int dy = 0; dy <= ky; ++dy)
+            for (int dz = 0; dz <= kz; ++dz) reach |= 1u << (dx * 4 + dy * 2 + dz);
+        reach_tab[p][e] = uint8_t(reach);
+        no_self_tab[p][e] = uint8_t((kx && ky && kz) ? (reach & ~1u) : reach);
+        patch_cell[e] = uint8_t(((e >> 5) >> 1) * 8 + (((e >> 3) & 3) >> 1) * 4 + ((e & 7) >> 1));
+      }
     std::vector<Patch> patch(static_cast<size_t>(F.nb));
 #pragma omp parallel for schedule(static)
     for (int b = 0; b < F.nb; ++b) {
       Patch& pt = patch[size_t(b)];
       std::fill(pt.flags, pt.flags + 16, 0u);
-      pt.pages = 0;
-      pt.any = false;
-      const int bx = F.coords[3 * b], by = F.coords[3 * b + 1], bz = F.coords[3 * b + 2];
+      const int p = (((F.coords[3 * b] / BLK_X) & 1) << 2) | (((F.coords[3 * b + 1] / BLK_Y) & 1) << 1) |
+                    ((F.coords[3 * b + 2] / BLK_Z) & 1);
+      const uint32_t* fl = F.flags.data() + size_t(b) * NODES_PER_BLOCK;
+      unsigned pages = 0, any = 0;
       for (int e = 0; e < NODES_PER_BLOCK; ++e) {
-        const uint32_t ff = F.flags[size_t(b) * NODES_PER_BLOCK + e];
-        if (!(ff & (F_ACTIVE_CELL | F_DIRICHLET_CELL))) continue;
-        const int cx = (bx + (e >> 5) + BLK_X) >> 1, cy = (by + ((e >> 3) & 3) + BLK_Y) >> 1,
-                  cz = (bz + (e & 7) + BLK_Z) >> 1;
-        const int kx = (cx & 3) == 3, ky = (cy & 3) == 3, kz = (cz & 7) == 7;
-        uint8_t reach = 0;
-        for (int dx = 0; dx <= kx; ++dx)
-          for (int dy = 0; dy <= ky; ++dy)
-            for (int dz = 0; dz <= kz; ++dz) reach |= uint8_t(1u << (dx * 4 + dy * 2 + dz));
-        const uint8_t no_self = (kx && ky && kz) ? uint8_t(reach & ~1u) : reach;
-        const int l = ((e >> 5) >> 1) * 8 + (((e >> 3) & 3) >> 1) * 4 + ((e & 7) >> 1);
-        pt.flags[l] |= ff & (F_ACTIVE_CELL | F_DIRICHLET_CELL);
-        pt.pages |= (ff & F_ACTIVE_CELL) ? reach : no_self;
-        pt.any = true;
+        const uint32_t ff = fl[e] & (F_ACTIVE_CELL | F_DIRICHLET_CELL);
+        if (!ff) continue;
+        pt.flags[patch_cell[e]] |= ff;
+        pages |= (ff & F_ACTIVE_CELL) ? reach_tab[p][e] : no_self_tab[p][e];
+        any = 1;
       }
+      pt.pages = uint8_t(pages);
+      pt.any = any != 0;
     }
     // The coarse blocks are the patch blocks and the reached pages.  A serial
     // pass in fine-block order would create them in that order; the pages

@@ -2,8 +2,67 @@
 #include "wire.hpp"
 
 #include <cstring>
+#include <mutex>
+#include <unordered_map>
 
 namespace sgs {
+
+namespace {
+constexpr size_t HUGE_PAGE = size_t(2) << 20, HOST_CACHE_BYTES = size_t(4) << 30;
+struct HostCache {
+  std::mutex mutex;
+  std::multimap<size_t, void*> free_blocks;   // size -> released block
+  std::unordered_map<void*, size_t> live;     // block handed out -> its size
+  size_t cached = 0;                          // bytes in free_blocks
+};
+// never destroyed: buffers of static objects may be released after exit begins
+HostCache& host_cache() {
+  static HostCache* c = new HostCache;
+  return *c;
+}
+}  // namespace
+
+void* host_large_alloc(size_t bytes) {
+  const size_t rounded = (bytes + HUGE_PAGE - 1) & ~(HUGE_PAGE - 1);
+  HostCache& c = host_cache();
+  std::lock_guard<std::mutex> lock(c.mutex);
+  auto it = c.free_blocks.lower_bound(rounded);
+  if (it != c.free_blocks.end() && it->first - rounded <= rounded / 4) {
+    void* p = it->second;
+    c.cached -= it->first;
+    c.live.emplace(p, it->first);
+    c.free_blocks.erase(it);
+    return p;
+  }
+  void* p = std::aligned_alloc(HUGE_PAGE, rounded);
+  if (!p) {  // give the cached blocks back and try once more
+    for (auto& fb : c.free_blocks) std::free(fb.second);
+    c.free_blocks.clear();
+    c.cached = 0;
+    p = std::aligned_alloc(HUGE_PAGE, rounded);
+    if (!p) throw std::bad_alloc();
+  }
+  madvise(p, rounded, MADV_HUGEPAGE);  // advice only; without it the buffer works the same
+  c.live.emplace(p, rounded);
+  return p;
+}
+
+void host_large_free(void* p) {
+  if (!p) return;
+  HostCache& c = host_cache();
+  std::lock_guard<std::mutex> lock(c.mutex);
+  auto it = c.live.find(p);
+  if (it == c.live.end()) return;  // not a block of this allocator
+  const size_t size = it->second;
+  c.live.erase(it);
+  if (c.cached + size <= HOST_CACHE_BYTES) {
+    c.free_blocks.emplace(size, p);
+    c.cached += size;
+  } else {
+    std::free(p);
+  }
+}
+
 namespace {
 
 // Writes a record into a caller-sized buffer; with no buffer it only counts

@@ -36,37 +36,39 @@ struct KrylovSolverParameters {
   bool print_residuals = false;
 };
 
-// BlockedGrid with 4x4x4 blocks (fem_interface.h:109-160); payload per block is
-// `width` doubles per node, in-block index i*16 + j*4 + k.
+// Host buffers of 8 MiB and more: 2 MiB aligned with transparent huge pages
+// advised (the first touch faults a 2 MiB page at a time where the kernel
+// allows it).  A released buffer goes to a process-wide cache (up to 4 GiB in
+// all), from which the next request of at least four fifths of its size takes
+// it back (the smallest such buffer): the buffers of repeated solves are then
+// neither mapped nor faulted in again.  A buffer taken from the cache holds
+// the contents it was released with.
+void* host_large_alloc(size_t bytes);
+void host_large_free(void* p);
+
 // A host vector whose resize leaves new elements uninitialised, so that a large
 // buffer can be zeroed and filled by parallel loops (first touch spread over
 // the threads) instead of one serial value-initialisation.  Buffers of 8 MiB
-// and more are 2 MiB aligned with transparent huge pages advised, so that the
-// first touch faults a 2 MiB page at a time where the kernel allows it.
+// and more come from host_large_alloc.
 template <typename T>
 struct UninitAlloc : std::allocator<T> {
   template <typename U>
   struct rebind {
     using other = UninitAlloc<U>;
   };
-  static constexpr size_t LARGE = size_t(8) << 20, HUGE_PAGE = size_t(2) << 20;
+  static constexpr size_t LARGE = size_t(8) << 20;
   UninitAlloc() = default;
   template <typename U>
   UninitAlloc(const UninitAlloc<U>&) {}
   T* allocate(size_t n) {
-    const size_t bytes = n * sizeof(T);
-    if (bytes < LARGE) return std::allocator<T>::allocate(n);
-    const size_t rounded = (bytes + HUGE_PAGE - 1) & ~(HUGE_PAGE - 1);
-    void* p = std::aligned_alloc(HUGE_PAGE, rounded);
-    if (!p) throw std::bad_alloc();
-    madvise(p, rounded, MADV_HUGEPAGE);  // advice only; without it the buffer works the same
-    return static_cast<T*>(p);
+    if (n * sizeof(T) < LARGE) return std::allocator<T>::allocate(n);
+    return static_cast<T*>(host_large_alloc(n * sizeof(T)));
   }
   void deallocate(T* p, size_t n) {
     if (n * sizeof(T) < LARGE)
       std::allocator<T>::deallocate(p, n);
     else
-      std::free(p);
+      host_large_free(p);
   }
   template <typename U>
   void construct(U* p) noexcept {
@@ -79,6 +81,9 @@ struct UninitAlloc : std::allocator<T> {
 };
 template <typename T>
 using HostBuf = std::vector<T, UninitAlloc<T>>;
+
+// BlockedGrid with 4x4x4 blocks (fem_interface.h:109-160); payload per block is
+// `width` doubles per node, in-block index i*16 + j*4 + k.
 
 struct BlockedGrid {
   int32_t resolution[3] = {0, 0, 0};

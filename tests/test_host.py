@@ -106,6 +106,37 @@ def test_host_hierarchy_matches_oracle(native_lib, problem):
         assert np.array_equal(ses.boundary_blocks(lev), ref.boundary_blocks(lev)), lev
 
 
+def test_host_hierarchy_on_recycled_buffers(native_lib):
+    """Host buffers of 8 MiB and more go back to a process-wide cache when
+    released and come out of it with their old contents.  A 256^3 band
+    (21354 level-0 blocks: its density records, stiffness scales and level-0
+    flags are above 8 MiB) is set up, then a decoy with the same blocks and
+    other densities (a tenth of the cells empty) is set up and released, and
+    the band is set up again on the decoy's buffers: every level must come out
+    as the first time."""
+    inp = configs.spheres_band_inputs(256, bottom_size=8)
+
+    def hierarchy(inputs):
+        ses = native.Session(inputs, precision=native.HOST_SETUP_ONLY)
+        try:
+            return [(ses.blocks(lev), ses.flags(lev), ses.boundary_blocks(lev)) for lev in range(ses.levels)]
+        finally:
+            ses.close()
+
+    first = hierarchy(inp)
+    decoy = fi.deserialize_inputs(fi.serialize_inputs(inp))
+    rng = np.random.default_rng(11)
+    decoy.density.data = decoy.density.data * rng.uniform(0.3, 0.9, size=decoy.density.data.shape)
+    decoy.density.data[rng.random(decoy.density.data.shape) < 0.1] = 0.0
+    decoyed = hierarchy(decoy)
+    assert any(not np.array_equal(a[1], b[1]) for a, b in zip(first, decoyed))  # the decoy's flags differ
+    again = hierarchy(inp)
+    assert len(again) == len(first)
+    for lev, (a, b) in enumerate(zip(first, again)):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), lev
+
+
 # ---- host-injected failures (the reference's abort/throw sites, SURVEY of
 # CG_SYSTEM.cpp:59-74 and CONJUGATE_GRADIENT.cpp:49-52): each one is caught on
 # the host before any device work and comes back as success = 0 with a code
