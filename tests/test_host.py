@@ -137,8 +137,8 @@ def test_host_hierarchy_on_recycled_buffers(native_lib):
             assert np.array_equal(x, y), lev
 
 
-# ---- host-injected failures (the reference's abort/throw sites, SURVEY of
-# CG_SYSTEM.cpp:59-74 and CONJUGATE_GRADIENT.cpp:49-52): each one is caught on
+# ---- host-injected failures (the reference's abort/throw sites,
+# solver/CG/CG_SYSTEM.cpp:59-74 and solver/CG/CONJUGATE_GRADIENT.cpp:49-52): each one is caught on
 # the host before any device work and comes back as success = 0 with a code
 @pytest.mark.parametrize("bad", [np.nan, np.inf])
 def test_fem_solve_rejects_non_finite_force(native_lib, bad):
