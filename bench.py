@@ -65,8 +65,11 @@ def parse():
     ap.add_argument("--profile-iterations", type=int, default=0,
                     help="profiling mode: set up, warm up, then one solve of this many PCG iterations "
                          "between cudaProfilerStart/Stop (for ncu --profile-from-start off); prints stats only")
+    ap.add_argument("--profile-setup", action="store_true",
+                    help="profiling mode: after one warm-up set-up, one more session set-up (levels, "
+                         "operators, bottom solve) between cudaProfilerStart/Stop; prints its wall time only")
     ap.add_argument("--precision", choices=["mixed", "fp64", "reference"], default="mixed",
-                    help="precision of the profiled solve")
+                    help="precision of the profiled solve or set-up")
     args = ap.parse_args()
     if args.n is None:
         args.n = 256 if args.workload == "shell" else 1024
@@ -251,9 +254,20 @@ def run_ours(args, rank, world):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     native.load(build_if_missing=(rank == 0))
     prob, inp = workload(args.n, args.bottom_size, args.workload)
+    prec = {"mixed": native.PRECISION_MIXED, "fp64": native.PRECISION_FP64,
+            "reference": native.PRECISION_REFERENCE}[args.precision]
+    if args.profile_setup:
+        with native.Session(inp, precision=prec):  # the process-wide scratch and staging are made here
+            pass
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+        t0 = time.perf_counter()
+        with native.Session(inp, precision=prec):
+            torch.cuda.synchronize()
+            setup_seconds = time.perf_counter() - t0
+            torch.cuda.cudart().cudaProfilerStop()
+        return {"profile": True, "setup_seconds": round(setup_seconds, 4)} if rank == 0 else None
     if args.profile_iterations > 0:
-        prec = {"mixed": native.PRECISION_MIXED, "fp64": native.PRECISION_FP64,
-                "reference": native.PRECISION_REFERENCE}[args.precision]
         # the per-iteration graph (same kernels as the device-side loop, whose
         # WHILE node the profiler is not asked to walk)
         inp.extra_ints["sgs_device_loop"] = 0

@@ -621,19 +621,38 @@ class Solver {
       const HostLevel& h = P.levels[lev];
       const int side = 1 << lev;
       const long npos = long(side) * side * side;
-      // active coarse cells (the only ones with finest material) and their finest origin
-      std::vector<int32_t> origin, ccoord, cell_of_slot(size_t(d.N), -1);
-      int ncells = 0;
+      // active coarse cells (the only ones with finest material) numbered in
+      // slot order, and their coordinates and finest origin: per-block counts,
+      // a prefix over the blocks, then a parallel fill
+      const int nblk = int(d.N / NODES_PER_BLOCK);
+      std::vector<int32_t> first_cell(size_t(nblk) + 1, 0);
+#pragma omp parallel for schedule(static)
+      for (int b = 0; b < nblk; ++b) {
+        int k = 0;
+        for (int e = 0; e < NODES_PER_BLOCK; ++e) k += (h.flags[size_t(b) * NODES_PER_BLOCK + e] & F_ACTIVE_CELL) ? 1 : 0;
+        first_cell[size_t(b) + 1] = k;
+      }
+      for (int b = 0; b < nblk; ++b) first_cell[size_t(b) + 1] += first_cell[size_t(b)];
+      const int ncells = first_cell[size_t(nblk)];
+      std::vector<int32_t> origin(3 * size_t(ncells)), ccoord(3 * size_t(ncells));
+      HostBuf<int32_t> cell_of_slot(size_t(d.N));
       const int B[3] = {BLK_X, BLK_Y, BLK_Z};
-      for (long slot = 0; slot < d.N; ++slot) {
-        if (!(h.flags[slot] & F_ACTIVE_CELL)) continue;
-        const int b = int(slot / NODES_PER_BLOCK), e = int(slot % NODES_PER_BLOCK);
-        const int c[3] = {h.coords[3 * b] + (e >> 5), h.coords[3 * b + 1] + ((e >> 3) & 3), h.coords[3 * b + 2] + (e & 7)};
-        for (int v = 0; v < 3; ++v) {
-          origin.push_back(side * c[v] - (side - 1) * B[v]);
-          ccoord.push_back(c[v]);
+#pragma omp parallel for schedule(static)
+      for (int b = 0; b < nblk; ++b) {
+        int k = first_cell[size_t(b)];
+        for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+          const size_t slot = size_t(b) * NODES_PER_BLOCK + size_t(e);
+          if (!(h.flags[slot] & F_ACTIVE_CELL)) {
+            cell_of_slot[slot] = -1;
+            continue;
+          }
+          const int c[3] = {h.coords[3 * b] + (e >> 5), h.coords[3 * b + 1] + ((e >> 3) & 3), h.coords[3 * b + 2] + (e & 7)};
+          for (int v = 0; v < 3; ++v) {
+            origin[3 * size_t(k) + size_t(v)] = side * c[v] - (side - 1) * B[v];
+            ccoord[3 * size_t(k) + size_t(v)] = c[v];
+          }
+          cell_of_slot[slot] = k++;
         }
-        cell_of_slot[slot] = ncells++;
       }
       const bool recursive = !round_ref() && prev_lev == lev - 1 && lev > 0;
       d.A.alloc(243 * size_t(d.N));
