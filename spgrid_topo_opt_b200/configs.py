@@ -240,7 +240,9 @@ def spheres_band_inputs(n: int = 1024, nspheres: int = 8, thickness: int = 12, s
     # node blocks: the +x/+y/+z neighbours of material blocks (zero density)
     fwd = np.array([[a, b, c] for a in (0, 1) for b in (0, 1) for c in (0, 1)], np.int64)
     allb = np.unique((mat_blocks[:, None, :] + fwd[None]).reshape(-1, 3), axis=0)
-    key = lambda b: (b[:, 0] * nb + b[:, 1]) * nb + b[:, 2]
+    # node blocks reach index nb on each axis: the key's stride is nb + 1 so that
+    # a block past the box never shares a key with a material block
+    key = lambda b: (b[:, 0] * (nb + 1) + b[:, 1]) * (nb + 1) + b[:, 2]
     mk = key(mat_blocks)
     order = np.argsort(mk)
     pos = np.searchsorted(mk[order], key(allb))

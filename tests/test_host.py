@@ -106,6 +106,20 @@ def test_host_hierarchy_matches_oracle(native_lib, problem):
         assert np.array_equal(ses.boundary_blocks(lev), ref.boundary_blocks(lev)), lev
 
 
+def test_small_band_keeps_material_inside_the_box(native_lib):
+    """At 64^3 the 12-voxel band reaches the box's faces, so the generator adds
+    node blocks one past the last block index; none may carry material (a
+    material cell there would need pages beyond the grid)."""
+    inp = configs.spheres_band_inputs(64, bottom_size=4)
+    blk = (inp.density.base - configs.PADDING) // 4
+    outside = (blk >= 64 // 4).any(axis=1)
+    assert outside.any()
+    assert not (inp.density.data.reshape(len(blk), -1)[outside] > 0).any()
+    ses = native.Session(inp, precision=native.HOST_SETUP_ONLY)
+    assert ses.levels >= 2
+    ses.close()
+
+
 def test_host_hierarchy_on_recycled_buffers(native_lib):
     """Host buffers of 8 MiB and more go back to a process-wide cache when
     released and come out of it with their old contents.  A 256^3 band
