@@ -657,14 +657,18 @@ enum { SOP_MUL = 0, SOP_RES = 1, SOP_GS = 2 };
 // neighbour's u, the warp sums the three components.  Stencils are node-major,
 // A[node*243 + q*9 + v*3 + w]: lane q reads its nine entries, and the warp's
 // reads together cover one contiguous row (972 bytes in FP32), which L1
-// fetches once.  GS updates only colour-`color` nodes (16 per block).
+// fetches once.  The neighbour's block comes from the level's 27-entry
+// neighbour table (one load that needs only the block index, issued with the
+// flags load), and the row is loaded whether or not the neighbour exists, so
+// no load waits for another; a missing neighbour's spoke is skipped.  GS
+// updates only colour-`color` nodes (16 per block).
 // Results on Dirichlet components are zeroed (Project).  The reference
 // projects the whole level after every colour; here only updated nodes are
 // projected, which is the same because the V-cycle keeps u zero on Dirichlet
 // components (cleared levels, projected transfers and updates).
 template <typename T, int OP>
 __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__ block_list, int nblocks,
-                                                         const int* __restrict__ coords, GridView g,
+                                                         const int* __restrict__ nbr,
                                                          const T* __restrict__ A, const uint32_t* __restrict__ flags,
                                                          const T* u, T* out_u, const T* __restrict__ b,
                                                          T* __restrict__ out, long N, int color, int boundary_only,
@@ -687,23 +691,26 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__
     e = int(w % per);
   }
   const long gidx = long(bi) * 128 + e;
+  // prologue: flags, neighbour table and stencil row do not change during a solve
+  // neighbour (X, Y, Z) of the node in block coordinates, -1..4 x -1..4 x -1..8
+  const int X = (e >> 5) + lane / 9 - 1, Y = ((e >> 3) & 3) + (lane / 3) % 3 - 1, Z = (e & 7) + lane % 3 - 1;
   const uint32_t fl = flags[gidx];
+  const int nbk = lane < 27 ? nbr[long(bi) * 27 + (X < 0 ? 0 : (X > 3 ? 2 : 1)) * 9 + (Y < 0 ? 0 : (Y > 3 ? 2 : 1)) * 3 +
+                                  (Z < 0 ? 0 : (Z > 7 ? 2 : 1))]
+                            : -1;
   if (OP == SOP_GS) {
     if (!(fl & ACTIVE_NODE) || (boundary_only && !(fl & BOUNDARY_NODE))) {
       pdl_wait();
       return;
     }
   }
-  // prologue: the stencil row (and the neighbour's index) does not change during a solve
-  long n = -1;
   T a[9];
   if (lane < 27) {
-    const int x = coords[3 * bi] + (e >> 5), y = coords[3 * bi + 1] + ((e >> 3) & 3), z = coords[3 * bi + 2] + (e & 7);
-    n = g.node(x + lane / 9 - 1, y + (lane / 3) % 3 - 1, z + lane % 3 - 1);
     const T* ap = A + gidx * 243 + lane * 9;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) a[k] = n >= 0 ? ap[k] : T(0);
+    for (int k = 0; k < 9; ++k) a[k] = ap[k];
   }
+  const long n = nbk < 0 ? -1 : long(nbk) * 128 + ((X & 3) << 5) + ((Y & 3) << 3) + (Z & 7);
   T d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0;
   if (OP == SOP_GS && lane == 0) {
     const T* c = A + gidx * 243 + 13 * 9;

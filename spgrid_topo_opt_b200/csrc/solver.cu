@@ -936,7 +936,7 @@ class Solver {
     if (count <= 0) return;
     const int per = OP == SOP_GS ? 16 : 128;
     launch(stencil_op_kernel<T, OP>, blocks_for(long(count) * per * 32, 256), 256, 0, 
-        list, count, d.coords.p, d.grid, d.A.p, d.flags.p, u, uo, b, out, d.N, color, boundary, round_out);
+        list, count, d.nbr.p, d.A.p, d.flags.p, u, uo, b, out, d.N, color, boundary, round_out);
     ++launch_counter;
   }
 
