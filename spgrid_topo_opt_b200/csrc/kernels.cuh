@@ -661,36 +661,28 @@ enum { SOP_MUL = 0, SOP_RES = 1, SOP_GS = 2 };
 // neighbour table (one load that needs only the block index, issued with the
 // flags load), and the row is loaded whether or not the neighbour exists, so
 // no load waits for another; a missing neighbour's spoke is skipped.  GS
-// updates only colour-`color` nodes (16 per block).
+// updates the nodes of a list: the active nodes of one colour, or the active
+// boundary-band nodes of one colour (no node has a neighbour of its own
+// colour, so the order inside a pass does not change the result).
 // Results on Dirichlet components are zeroed (Project).  The reference
 // projects the whole level after every colour; here only updated nodes are
 // projected, which is the same because the V-cycle keeps u zero on Dirichlet
 // components (cleared levels, projected transfers and updates).
 template <typename T, int OP>
-__global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__ block_list, int nblocks,
+__global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__ list, int count,
                                                          const int* __restrict__ nbr,
                                                          const T* __restrict__ A, const uint32_t* __restrict__ flags,
                                                          const T* u, T* out_u, const T* __restrict__ b,
-                                                         T* __restrict__ out, long N, int color, int boundary_only,
-                                                         int round_out) {
-  const int per = (OP == SOP_GS) ? 16 : 128;
+                                                         T* __restrict__ out, long N, int round_out) {
   const long w = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;  // one warp per node
   const int lane = threadIdx.x & 31;
-  const long blk = w / per;
-  if (blk >= nblocks) {
+  // GS: node list[w] of the `count` listed; MUL / RES: node w of the first `count` blocks
+  if (w >= (OP == SOP_GS ? long(count) : long(count) * 128)) {
     pdl_wait();
     return;
   }
-  const int bi = block_list ? block_list[blk] : int(blk);
-  int e;
-  if (OP == SOP_GS) {
-    const int q = int(w % per);  // 16 nodes of the colour: (x/2, y/2, z/2) in 2x2x4
-    const int px = (color >> 2) & 1, py = (color >> 1) & 1, pz = color & 1;
-    e = (((q >> 3) * 2 + px) << 5) + ((((q >> 2) & 1) * 2 + py) << 3) + ((q & 3) * 2 + pz);
-  } else {
-    e = int(w % per);
-  }
-  const long gidx = long(bi) * 128 + e;
+  const long gidx = OP == SOP_GS ? long(list[w]) : w;
+  const int bi = int(gidx >> 7), e = int(gidx & 127);
   // prologue: flags, neighbour table and stencil row do not change during a solve
   // neighbour (X, Y, Z) of the node in block coordinates, -1..4 x -1..4 x -1..8
   const int X = (e >> 5) + lane / 9 - 1, Y = ((e >> 3) & 3) + (lane / 3) % 3 - 1, Z = (e & 7) + lane % 3 - 1;
@@ -698,12 +690,6 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__
   const int nbk = lane < 27 ? nbr[long(bi) * 27 + (X < 0 ? 0 : (X > 3 ? 2 : 1)) * 9 + (Y < 0 ? 0 : (Y > 3 ? 2 : 1)) * 3 +
                                   (Z < 0 ? 0 : (Z > 7 ? 2 : 1))]
                             : -1;
-  if (OP == SOP_GS) {
-    if (!(fl & ACTIVE_NODE) || (boundary_only && !(fl & BOUNDARY_NODE))) {
-      pdl_wait();
-      return;
-    }
-  }
   T a[9];
   if (lane < 27) {
     const T* ap = A + gidx * 243 + lane * 9;

@@ -84,6 +84,11 @@ struct Level {
   // then boundary sweep colours 8..15, concatenated; list k is gs_off[k]..gs_off[k+1]
   DevBuf<int> gs_list;
   int gs_off[17] = {0};
+  // levels with stencils: node lists of the Gauss-Seidel passes, active nodes of
+  // colour c (list c) and active boundary-band nodes of colour c (list 8 + c),
+  // each ascending; list k is sgs_off[k]..sgs_off[k+1]
+  DevBuf<int> sgs_list;
+  int sgs_off[17] = {0};
   // level 0 of the V-cycle (mixed and FP64 modes): the iterate packed as (u, E) per
   // node, followed by one all-zero pad block (index nb) that nbrz names for missing neighbours
   DevBuf<typename Pack4<T>::type> u4;
@@ -598,6 +603,41 @@ class Solver {
   // Galerkin operators of the levels >= explicit_level (all on the GPU):
   // table of the depth, cell matrices as a GEMM over the finest cells, node
   // stencils, Dirichlet deletion (Multigrid_Hierarchy.h:215-226).
+  // The node lists of a stencil level's Gauss-Seidel passes, from the host
+  // flags: per-block counts of the 16 lists, a prefix over (list, block), and
+  // a parallel fill, so each list ascends.  A node's colour is the parity of
+  // its slot (blocks have even extents).
+  void stencil_lists(Level<double>& d, const HostLevel& h) {
+    const int nb = d.nb;
+    std::vector<int32_t> pos(16 * size_t(nb) + 1, 0);
+    auto colour = [](int e) { return ((e >> 5) & 1) * 4 + ((e >> 3) & 1) * 2 + (e & 1); };
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < nb; ++b)
+      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+        const uint32_t fl = h.flags[size_t(b) * NODES_PER_BLOCK + size_t(e)];
+        if (!(fl & F_ACTIVE_NODE)) continue;
+        const int c = colour(e);
+        ++pos[size_t(c) * nb + size_t(b) + 1];
+        if (fl & F_BOUNDARY_NODE) ++pos[size_t(8 + c) * nb + size_t(b) + 1];
+      }
+    for (size_t i = 1; i < pos.size(); ++i) pos[i] += pos[i - 1];
+    std::vector<int32_t> list(size_t(pos.back()));
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < nb; ++b) {
+      int32_t at[16];
+      for (int k = 0; k < 16; ++k) at[k] = pos[size_t(k) * nb + size_t(b)];
+      for (int e = 0; e < NODES_PER_BLOCK; ++e) {
+        const uint32_t fl = h.flags[size_t(b) * NODES_PER_BLOCK + size_t(e)];
+        if (!(fl & F_ACTIVE_NODE)) continue;
+        const int c = colour(e), node = b * NODES_PER_BLOCK + e;
+        list[size_t(at[c]++)] = node;
+        if (fl & F_BOUNDARY_NODE) list[size_t(at[8 + c]++)] = node;
+      }
+    }
+    for (int k = 0; k <= 16; ++k) d.sgs_off[k] = pos[size_t(k) * nb];
+    d.sgs_list.upload(list, stream);
+  }
+
   void build_operators() {
     if (P.disable_mg) return;
     const int n = nlev();
@@ -660,6 +700,7 @@ class Solver {
       d.spokes.alloc(size_t(d.N));
       d.spokes.zero(stream);
       d.has_matrix = true;
+      stencil_lists(d, h);
       if (ncells > 0) {
         DevBuf<int32_t> dcell;
         dcell.upload(cell_of_slot, stream);
@@ -705,6 +746,11 @@ class Solver {
         launch(convert_kernel<float, double>, blocks_for(243 * d.N, 256), 256, 0, m.A.p, d.A.p, 243 * d.N);
         m.spokes.alloc(size_t(d.N));
         SGS_CUDA(cudaMemcpyAsync(m.spokes.p, d.spokes.p, d.N * 4, cudaMemcpyDeviceToDevice, stream));
+        m.sgs_list.alloc(d.sgs_list.n);
+        if (d.sgs_list.n)
+          SGS_CUDA(cudaMemcpyAsync(m.sgs_list.p, d.sgs_list.p, d.sgs_list.n * sizeof(int), cudaMemcpyDeviceToDevice,
+                                   stream));
+        std::copy(d.sgs_off, d.sgs_off + 17, m.sgs_off);
         m.has_matrix = true;
       }
     }
@@ -929,14 +975,15 @@ class Solver {
     ++launch_counter;
   }
 
+  // SOP_GS: `list` names `count` nodes; SOP_MUL / SOP_RES: all nodes of the
+  // level's `count` blocks (list == nullptr)
   template <typename T, int OP>
-  void stencil(int l, const int* list, int count, const T* u, T* uo, const T* b, T* out, int color, int boundary,
-               int round_out) {
+  void stencil(int l, const int* list, int count, const T* u, T* uo, const T* b, T* out, int round_out) {
     Level<T>& d = lev<T>(l);
     if (count <= 0) return;
-    const int per = OP == SOP_GS ? 16 : 128;
-    launch(stencil_op_kernel<T, OP>, blocks_for(long(count) * per * 32, 256), 256, 0, 
-        list, count, d.nbr.p, d.A.p, d.flags.p, u, uo, b, out, d.N, color, boundary, round_out);
+    const long nodes = OP == SOP_GS ? long(count) : long(count) * NODES_PER_BLOCK;
+    launch(stencil_op_kernel<T, OP>, blocks_for(nodes * 32, 256), 256, 0, list, count, d.nbr.p, d.A.p, d.flags.p, u,
+           uo, b, out, d.N, round_out);
     ++launch_counter;
   }
 
@@ -944,9 +991,7 @@ class Solver {
   template <typename T>
   void sweep(int l, T* u, const T* b, bool forward, bool boundary, bool matrix_free = true) {
     Level<T>& d = lev<T>(l);
-    const int* list = boundary ? d.boundary.p : nullptr;
-    const int count = boundary ? d.nbound : d.nb;
-    if (count == 0) return;
+    if ((boundary ? d.nbound : d.nb) == 0) return;
     if (l == 0 && matrix_free) {
       for (int k = 0; k < 8; ++k) {
         const int c = (boundary ? 8 : 0) + (forward ? k : 7 - k);
@@ -982,8 +1027,10 @@ class Solver {
       return;
     }
     static const int order[2][8] = {{1, 5, 4, 6, 7, 3, 2, 0}, {0, 2, 3, 7, 6, 4, 5, 1}};
-    for (int k = 0; k < 8; ++k)
-      stencil<T, SOP_GS>(l, list, count, u, u, b, nullptr, forward ? order[0][k] : order[1][k], boundary ? 1 : 0, 0);
+    for (int k = 0; k < 8; ++k) {
+      const int li = (boundary ? 8 : 0) + (forward ? order[0][k] : order[1][k]);
+      stencil<T, SOP_GS>(l, d.sgs_list.p + d.sgs_off[li], d.sgs_off[li + 1] - d.sgs_off[li], u, u, b, nullptr, 0);
+    }
   }
 
   template <typename T>
@@ -1094,7 +1141,7 @@ class Solver {
       Level<double>& c = *L64[l + 1];
       SGS_CUDA(cudaMemsetAsync(c.u.p, 0, 3 * c.N * sizeof(double), stream));
       SGS_CUDA(cudaMemsetAsync(c.b.p, 0, 3 * c.N * sizeof(double), stream));
-      stencil<double, SOP_RES>(l, nullptr, d.nb, d.u.p, nullptr, d.b.p, d.r.p, 0, 0, 0);
+      stencil<double, SOP_RES>(l, nullptr, d.nb, d.u.p, nullptr, d.b.p, d.r.p, 0);
       restrict_to<double>(l + 1, d.r.p);
     }
     bottom_dense<double>(n - 1, false);
@@ -1196,7 +1243,7 @@ class Solver {
           }
           if (rr) round3(d, d.r.p);
         } else {
-          stencil<T, SOP_RES>(l, nullptr, d.nb, U(l), nullptr, B(l), d.r.p, 0, 0, rr ? 1 : 0);
+          stencil<T, SOP_RES>(l, nullptr, d.nb, U(l), nullptr, B(l), d.r.p, rr ? 1 : 0);
         }
         restrict_to<T>(l + 1, d.r.p);
       } else {
@@ -1861,7 +1908,7 @@ void Solver::inner_pcg(int l) {
     dotp(ib.r.p, ib.z.p, 0);                                     // rho, beta = rho / rho_old
     launch(axpy_kernel, blocks_for(n3, 256), 256, 0, ib.p.p, ib.scal.p, 4, ib.p.p, ib.z.p, n3, 0);  // p = beta p + z
     launch(rho_shift_kernel, 1, 1, 0, ib.scal.p);
-    stencil<double, SOP_MUL>(l, nullptr, D.nb, ib.p.p, nullptr, nullptr, ib.q.p, 0, 0, 0);
+    stencil<double, SOP_MUL>(l, nullptr, D.nb, ib.p.p, nullptr, nullptr, ib.q.p, 0);
     launch(inner_mask_kernel, blocks_for(N, 256), 256, 0, ib.q.p, ib.q.p, D.spokes.p, N);
     dotp(ib.p.p, ib.q.p, 1);                                     // alpha, breakdown flag
     launch(axpy_kernel, blocks_for(n3, 256), 256, 0, ib.x.p, ib.scal.p, 5, ib.p.p, ib.x.p, n3, 0);  // x += alpha p
@@ -2776,7 +2823,7 @@ static int apply_op(Solver& S, int op, int level, int arg, const double* in, con
     case 5:
       if (!d.has_matrix) return SGS_ERR_INPUT;
       put_field<T>(S, d.u.p, in, N);
-      S.stencil<T, SOP_MUL>(level, nullptr, d.nb, d.u.p, nullptr, nullptr, d.r.p, 0, 0, 0);
+      S.stencil<T, SOP_MUL>(level, nullptr, d.nb, d.u.p, nullptr, nullptr, d.r.p, 0);
       get_field<T>(S, out, d.r.p, N);
       return 0;
     case 6:
