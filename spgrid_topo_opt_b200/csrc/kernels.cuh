@@ -871,7 +871,10 @@ __global__ void __launch_bounds__(128) prolongate_kernel(int nb, const int* __re
   fu[t + 2 * Nf] = v2;
 }
 
-// prolongate_kernel into the packed level-0 iterate (E in .w is kept)
+// prolongate_kernel into the packed level-0 iterate (E in .w is kept).  Only
+// active nodes are read and written: the V-cycle starts from u = 0 and no
+// kernel before this one writes an inactive node's displacement, so those
+// slots already hold the zeros that the projection would write.
 template <typename T>
 __global__ void __launch_bounds__(128) prolongate4_kernel(int nb, const int* __restrict__ coords,
                                                           const uint32_t* __restrict__ fflags, GridView coarse,
@@ -881,10 +884,12 @@ __global__ void __launch_bounds__(128) prolongate4_kernel(int nb, const int* __r
   const int bi = blockIdx.x, e = threadIdx.x;
   if (bi >= nb) return;
   const int FX = coords[3 * bi], FY = coords[3 * bi + 1], FZ = coords[3 * bi + 2];
+  const long t = long(bi) * 128 + e;
+  const uint32_t fl = fflags[t];
   pdl_wait();
   stage_coarse_patch<T>(sc, FX, FY, FZ, coarse, cin, Nc);
+  if (!(fl & ACTIVE_NODE)) return;
   const int lx = e >> 5, ly = (e >> 3) & 3, lz = e & 7;
-  const long t = long(bi) * 128 + e;
   auto v = fu4[t];
   for (int q = 0; q < 8; ++q) {
     const int ii = q >> 2, jj = (q >> 1) & 1, kk = q & 1;
@@ -898,11 +903,9 @@ __global__ void __launch_bounds__(128) prolongate4_kernel(int nb, const int* __r
     v.y += w * sc[1][h];
     v.z += w * sc[2][h];
   }
-  const uint32_t fl = fflags[t];
   if (fl & DIR_X) v.x = 0;
   if (fl & DIR_Y) v.y = 0;
   if (fl & DIR_Z) v.z = 0;
-  if (!(fl & ACTIVE_NODE)) v.x = v.y = v.z = 0;
   fu4[t] = v;
 }
 
