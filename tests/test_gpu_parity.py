@@ -127,6 +127,19 @@ def test_galerkin_operators_of_a_deep_hierarchy(deep):
         assert np.array_equal(sa & 0x07FFFFFF, sb & 0x07FFFFFF), lev
 
 
+def test_coarse_smoothers_of_a_deep_hierarchy(deep):
+    """Full and boundary-band sweeps, both directions, on every level with
+    stencils: each colour pass runs over the level's list of the active (or
+    active band) nodes of that colour, down to levels of a few blocks."""
+    _, ref, ses = deep
+    for lev in range(2, ses.levels - 1):
+        u = _field(ses, lev, 41 + lev, dirichlet_zero=True)
+        b = _field(ses, lev, 47 + lev)
+        for arg in (0, 1, 2, 3):
+            assert _rel(ses.apply(native.OP_SMOOTH, lev, u, b, arg=arg),
+                        ref.apply(orc.OP_SMOOTH, lev, u, b, arg=arg)) < 1e-11, (lev, arg)
+
+
 def test_bottom_solve_and_vcycle(small):
     _, ref, ses = small
     top = ses.levels - 1
