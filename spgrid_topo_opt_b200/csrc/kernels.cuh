@@ -690,11 +690,17 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__
   const int nbk = lane < 27 ? nbr[long(bi) * 27 + (X < 0 ? 0 : (X > 3 ? 2 : 1)) * 9 + (Y < 0 ? 0 : (Y > 3 ? 2 : 1)) * 3 +
                                   (Z < 0 ? 0 : (Z > 7 ? 2 : 1))]
                             : -1;
+  // an inactive node's row is all +0 (the operator build writes only the rows of
+  // active nodes into zeroed storage): its zeros come from registers, and its
+  // products with the neighbours' u are formed as before
   T a[9];
-  if (lane < 27) {
+  if (lane < 27 && (OP == SOP_GS || (fl & ACTIVE_NODE))) {
     const T* ap = A + gidx * 243 + lane * 9;
 #pragma unroll
     for (int k = 0; k < 9; ++k) a[k] = ap[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = T(0);
   }
   const long n = nbk < 0 ? -1 : long(nbk) * 128 + ((X & 3) << 5) + ((Y & 3) << 3) + (Z & 7);
   T d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0;
