@@ -709,6 +709,18 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const int* __restrict__
     d0 = c[0]; d1 = c[4]; d2 = c[8]; d3 = c[1]; d4 = c[2]; d5 = c[5];
   }
   pdl_wait();
+  // lane 0 reads its right-hand side (and in GS its own u) after the warp's
+  // reduction; prefetched here, after the wait, those loads find them in L1
+  if (OP != SOP_MUL && lane == 0) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(b + gidx));
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(b + gidx + N));
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(b + gidx + 2 * N));
+    if (OP == SOP_GS) {
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(u + gidx));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(u + gidx + N));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(u + gidx + 2 * N));
+    }
+  }
   T f0 = 0, f1 = 0, f2 = 0;
   if (n >= 0) {
     const T ux = u[n], uy = u[n + N], uz = u[n + 2 * N];
