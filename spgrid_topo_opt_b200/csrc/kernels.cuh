@@ -532,6 +532,11 @@ __global__ void __launch_bounds__(128) gs0_cell4_kernel(const int* __restrict__ 
     }
     return;
   }
+  if (sizeof(T) == 4 && I == 0) {  // the right-hand side, read after the shuffles, into L1 now
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(b + g));
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(b + g + N));
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(b + g + 2 * N));
+  }
   const T s0 = Ix ? T(-1) : T(1), s1 = Iy ? T(-1) : T(1), s2 = Iz ? T(-1) : T(1);
   T gv[3] = {0, 0, 0}, Ec = 0, uc[3] = {0, 0, 0};
 #pragma unroll
